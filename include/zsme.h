@@ -1,0 +1,158 @@
+/*
+ * zsme.h -- C ABI of the B200 shallow-water-moment (SME) time step.
+ *
+ * The entry points replace the hot-path calls of the reference's
+ * MUSCLSolver driver (reference file:line cited on each declaration):
+ *   TransportStep::FormRHS          (TransportStep.hpp:325)  -> zsme_rhs
+ *   TransportStep::UpdateState      (TransportStep.hpp:196)  -> zsme_update_state
+ *   SourceStep::Solve               (SourceStep.hpp:72)      -> zsme_source
+ *   VirtualSolver::ComputeTimeStep  (VirtualSolver.hpp:285)  -> zsme_compute_dt
+ *   MUSCLSolver::Run step loop      (MUSCLSolver.hpp:140-188)-> zsme_step
+ *
+ * Conventions (mirroring PETSc's): every function returns an int status,
+ * ZSME_OK (0) on success; on failure zsme_last_error() describes it.  The
+ * caller owns host buffers; the library owns device buffers.  A handle is
+ * single-threaded and stream-ordered (one CUDA stream per handle).  States
+ * cross the boundary cell-major/interleaved ("AoS", [n_cells][n_dof_q], the
+ * layout of the reference's PETSc Vec with block size n_dof_q) in the
+ * caller's cell order; inside, the library renumbers cells along a Hilbert
+ * curve and stores every variable as its own FP64 array.
+ */
+#ifndef ZSME_H
+#define ZSME_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZSME_OK 0
+#define ZSME_ERR_ARG 1      /* invalid argument (null pointer, size, name) */
+#define ZSME_ERR_CUDA 2     /* a CUDA call failed; message has the CUDA error */
+#define ZSME_ERR_MODEL 3    /* unknown model name */
+#define ZSME_ERR_STATE 4    /* non-finite state or negative depth detected */
+#define ZSME_ERR_MESH 5     /* inconsistent mesh connectivity */
+#define ZSME_ERR_LIMIT 6    /* a compiled size limit was exceeded */
+
+/* Face boundary markers in zsme_mesh.face_bc */
+#define ZSME_FACE_INTERIOR (-1)
+#define ZSME_FACE_NO_CONDITION (-2)  /* exterior face whose tag has no BC: no flux */
+
+/*
+ * Cell-centred finite-volume mesh: the quantities the reference takes from
+ * DMPlexGetGeometryFVM and the DMPlex cone/support (TransportStep.hpp:388-410).
+ * Coordinates are always 2 doubles per point (y = 0 for 1-D meshes).
+ */
+typedef struct zsme_mesh {
+    int32_t dim;                  /* 1 or 2; must equal the model's dimension */
+    int32_t n_cells;
+    int32_t n_faces;
+    int32_t max_faces;            /* K: faces per cell (2 for 1-D, 3 triangles) */
+    const double* cell_centroid;  /* [n_cells][2] */
+    const double* cell_volume;    /* [n_cells] */
+    const int32_t* cell_faces;    /* [n_cells][K] cone order, -1 padded */
+    const int32_t* face_cells;    /* [n_faces][2] support; [1] = -1 on the boundary */
+    const double* face_centroid;  /* [n_faces][2] */
+    const double* face_normal;    /* [n_faces][2] area-weighted, support[0] -> support[1] */
+    const int32_t* face_bc;       /* [n_faces] ZSME_FACE_INTERIOR, bc index >= 0, or
+                                     ZSME_FACE_NO_CONDITION */
+} zsme_mesh;
+
+#define ZSME_LIMITER_NONE 0       /* settings.solver.limiter == "none" */
+#define ZSME_LIMITER_TVD 1        /* VacuumLimiter + TVDLimiter (Reconstruction.hpp:170-175) */
+#define ZSME_GRADIENT_GREEN_GAUSS 0 /* GreenGaussGradient (Gradient.hpp:43-191) */
+#define ZSME_GRADIENT_LSQ 1       /* LeastSquaresGradient (Gradient.hpp:196-360) */
+
+/* The solver keys of the reference's Settings (Settings.hpp:13-40) that change
+ * the step. */
+typedef struct zsme_settings {
+    double cfl;                   /* solver.cfl */
+    double t_end;                 /* solver.t_end */
+    double min_dt;                /* solver.min_dt (floor of the first dt only) */
+    int32_t reconstruction_order; /* 1: PCM + forward Euler; 2: linear + SSP-RK(s,2) */
+    int32_t limiter;              /* ZSME_LIMITER_* */
+    int32_t gradient;             /* ZSME_GRADIENT_* */
+    int32_t ssp_stages;           /* s of SSP-RK(s,2), >= 2 */
+    int32_t source;               /* 1: operator-split implicit source ("splitting") */
+    int32_t block_size;           /* CUDA block size, 0 = library default */
+    int32_t reserved[6];
+} zsme_settings;
+
+/* Health counters of the last step (failure detection without faulting). */
+typedef struct zsme_diag {
+    int64_t steps;                /* steps taken since zsme_set_state */
+    double time;                  /* simulated time */
+    double dt;                    /* dt of the next step (CFL) */
+    int32_t n_nonfinite;          /* cells with a non-finite value */
+    int32_t n_negative_depth;     /* cells with h < -1e-10 (MUSCLSolver.hpp:206) */
+    int32_t n_newton_unconverged; /* cells whose Newton hit 15 iterations */
+    int32_t reserved;
+} zsme_diag;
+
+typedef struct zsme_handle zsme_handle;
+
+/* Library version string. */
+const char* zsme_version(void);
+/* Message of the last failed call on this thread (never NULL). */
+const char* zsme_last_error(void);
+/* Number of compiled models and their names (e.g. "sme2d_l2"). */
+int zsme_num_models(void);
+const char* zsme_model_name(int i);
+/* Model constants: n_dof_q, n_dof_qaux, n_parameters, dimension. */
+int zsme_model_info(const char* model, int32_t* n_dof_q, int32_t* n_dof_qaux,
+                    int32_t* n_parameters, int32_t* dimension);
+
+/* Build a solver for `model` on `mesh` (VirtualSolver::SetupArchitecture,
+ * VirtualSolver.hpp:386-525; ModularSolver::InitializeComponents,
+ * ModularSolver.hpp:39-76; LeastSquaresGradient::Setup, Gradient.hpp:222-298).
+ * params: n_parameters doubles, or NULL for the model defaults. */
+int zsme_create(const char* model, const zsme_mesh* mesh, const zsme_settings* settings,
+                const double* params, int device, zsme_handle** out);
+int zsme_destroy(zsme_handle* h);
+
+/* Load Q (host, AoS, caller order) as the state at time t, apply the physical
+ * constraints and compute the first dt = max(ComputeTimeStep, min_dt)
+ * (MUSCLSolver.hpp:51-54,103). */
+int zsme_set_state(zsme_handle* h, const double* q_aos, double t);
+/* Copy the state / aux state out (host, AoS, caller order). */
+int zsme_get_state(zsme_handle* h, double* q_aos);
+int zsme_get_aux(zsme_handle* h, double* a_aos);
+/* Same with device pointers (zero-copy from torch), caller order. */
+int zsme_set_state_device(zsme_handle* h, const double* d_q_aos, double t);
+int zsme_get_state_device(zsme_handle* h, double* d_q_aos);
+
+/* F = dQ/dt of the transport for state X (TransportStep::FormRHS,
+ * TransportStep.hpp:325-357).  Host AoS buffers, caller order. */
+int zsme_rhs(zsme_handle* h, double t, const double* x_aos, double* f_aos);
+/* Physical constraints on the resident state (MUSCLSolver.hpp:234-254):
+ * update_variables clamp + update_aux_variables (TransportStep.hpp:196-230). */
+int zsme_update_state(zsme_handle* h);
+/* Implicit per-cell source over dt on the resident state
+ * (SourceStep::Solve, SourceStep.hpp:72-122). */
+int zsme_source(zsme_handle* h, double dt);
+/* CFL time step of the resident state (VirtualSolver.hpp:285-357). */
+int zsme_compute_dt(zsme_handle* h, double* dt);
+
+/* Advance nsteps steps of the MUSCLSolver loop (MUSCLSolver.hpp:140-188):
+ * dt clamped to land on t_end, SSP-RK(s,2) transport, constraints, implicit
+ * source, constraints, CFL dt.  Steps after t_end are no-ops.  Runs on the
+ * device without host synchronisation (one CUDA graph per step). */
+int zsme_step(zsme_handle* h, int32_t nsteps);
+/* Same, but with the dt of every step imposed by the caller (dts[nsteps]). */
+int zsme_step_dt(zsme_handle* h, int32_t nsteps, const double* dts);
+/* Wait for the handle's stream; returns ZSME_ERR_STATE if the last step left
+ * non-finite values or negative depth (counts in zsme_diag). */
+int zsme_sync(zsme_handle* h);
+int zsme_get_diag(zsme_handle* h, zsme_diag* out);
+int zsme_get_time(zsme_handle* h, double* t, double* dt);
+int zsme_set_params(zsme_handle* h, const double* params);
+/* The CUDA stream (cudaStream_t) the handle launches on. */
+void* zsme_stream(zsme_handle* h);
+/* Kernel launches issued by the last zsme_step call (per step). */
+int zsme_launches_per_step(zsme_handle* h, int32_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZSME_H */

@@ -1,0 +1,778 @@
+// ORACLE -- test infrastructure, not the product.
+//
+// A PETSc-free CPU restatement of the reference's SME time step, used only by
+// tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg as the
+// checker.  Every routine follows one reference function (cited inline):
+//
+//   FormRHS            TransportStep.hpp:325-357
+//   UpdateState        TransportStep.hpp:196-230
+//   UpdateNeighborBounds TransportStep.hpp:122-154 (SetupTopology 106-120)
+//   ComputeFluxes      TransportStep.hpp:383-565
+//   LeastSquares       Gradient.hpp:196-360 (Setup 222-298, Compute 300-359)
+//   GreenGauss         Gradient.hpp:43-191 (BC callback ModularSolver.hpp:68-71)
+//   Linear/PCM + Vacuum + TVD  Reconstruction.hpp:23-81, 143-244
+//   SourceStep         SourceStep.hpp:26-242
+//   ComputeTimeStep    VirtualSolver.hpp:285-357
+//   SSP-RK(s,2)        PETSc TSSSP "rks2" (SolverStrategies.hpp:33-35)
+//   Euler (order 1)    PETSc TSEULER (SolverStrategies.hpp:37)
+//   step loop          MUSCLSolver.hpp:140-188, EnforcePhysicalConstraints 234-254
+//
+// The face loop computes each face's contributions independently and every
+// cell then sums them in increasing face order -- the order in which the
+// reference's sequential face loop accumulates -- so the result does not
+// depend on the number of OpenMP threads.
+//
+// Parity status: the pointwise model arithmetic is pinned against the
+// reference's own shipped Model.H/Numerics.H compiled here (oracle/_ref); the
+// step composition cannot be run from the reference (PETSc is absent) and is
+// pinned only by this restatement.
+#include "model_prelude.h"
+#include "zsme.h"
+
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace sme1d_l0_malpasset {
+#include "sme1d_l0_malpasset/Model.H"
+#include "sme1d_l0_malpasset/Numerics.H"
+}
+namespace sme2d_l0 {
+#include "sme2d_l0/Model.H"
+#include "sme2d_l0/Numerics.H"
+}
+namespace sme2d_l1 {
+#include "sme2d_l1/Model.H"
+#include "sme2d_l1/Numerics.H"
+}
+namespace sme2d_l2 {
+#include "sme2d_l2/Model.H"
+#include "sme2d_l2/Numerics.H"
+}
+namespace sme2d_l4 {
+#include "sme2d_l4/Model.H"
+#include "sme2d_l4/Numerics.H"
+}
+#ifdef ORACLE_WITH_REFERENCE_MODEL
+// The reference's own generated 1-D level-0 headers (oracle/_ref build only).
+// Its field-level update_aux_variables needs a mesh handle and
+// compute_derivative (reference UserFunctions.H:46-112); the derivative aux is
+// never refreshed on this path, so inert stand-ins suffice.
+namespace ref1d {
+struct ZoomyMesh {};
+template <typename T>
+inline void compute_derivative(T*, const T*, int, int, int, const ZoomyMesh&) {}
+#include "Model.H"
+#include "Numerics.H"
+}
+#endif
+
+namespace {
+
+// Static-chunked parallel loop over [0, n) on std::thread workers.  Each
+// index is handled by exactly one worker and no loop here has cross-index
+// dependencies, so results do not depend on the thread count.
+int g_threads = 1;
+template <class Fn>
+void par_for(int n, Fn fn) {
+    int nt = std::max(1, std::min(g_threads, n / 256 + 1));
+    if (nt == 1) {
+        for (int i = 0; i < n; ++i) fn(i, 0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([=, &fn] {
+            int a = (int)((long long)n * t / nt), b = (int)((long long)n * (t + 1) / nt);
+            for (int i = a; i < b; ++i) fn(i, t);
+        });
+    for (auto& x : th) x.join();
+}
+int par_width(int n) { return std::max(1, std::min(g_threads, n / 256 + 1)); }
+
+thread_local std::string g_err;
+int fail(int code, const std::string& m) {
+    g_err = m;
+    return code;
+}
+
+struct OracleBase {
+    virtual ~OracleBase() = default;
+    virtual int nq() const = 0;
+    virtual int naux() const = 0;
+    virtual void set_state(const double* q, double t) = 0;
+    virtual void get_state(double* q) const = 0;
+    virtual void get_aux(double* a) const = 0;
+    virtual void rhs(double t, const double* x, double* f) = 0;
+    virtual void update_state() = 0;
+    virtual void source(double dt) = 0;
+    virtual double compute_dt() = 0;
+    virtual void step(int n, const double* dts) = 0;
+    virtual void get_time(double* t, double* dt) const = 0;
+    virtual void set_params(const double* p) = 0;
+    virtual int newton_unconverged() const = 0;
+    virtual void gradient(const double* x, double* g) = 0;
+};
+
+template <template <typename> class MT, template <typename> class NT>
+struct Oracle : OracleBase {
+    using T = double;
+    using M = MT<T>;
+    using N = NT<T>;
+    static constexpr int NQ = M::n_dof_q;
+    static constexpr int NA = M::n_dof_qaux;
+    static constexpr int DIM = M::dimension;
+
+    // mesh, caller order
+    int C = 0, F = 0, K = 0;
+    std::vector<double> cc, vol, fc, fn;
+    std::vector<int> cf, fcell, fbc;
+    std::vector<int> nb_off, nb_list;    // face neighbours, cone order
+    std::vector<double> lsq_w;           // DIM weights per neighbour entry
+    std::vector<int> cell_face_sorted;   // each cell's faces, increasing id
+    zsme_settings st{};
+    std::vector<double> params;
+    std::vector<double> X, A, G;
+    double time = 0.0, dt = 0.0;
+    int n_unconv = 0;
+
+    Oracle(const zsme_mesh* m, const zsme_settings* s, const double* p) {
+        C = m->n_cells; F = m->n_faces; K = m->max_faces;
+        cc.assign(m->cell_centroid, m->cell_centroid + 2 * C);
+        vol.assign(m->cell_volume, m->cell_volume + C);
+        fc.assign(m->face_centroid, m->face_centroid + 2 * F);
+        fn.assign(m->face_normal, m->face_normal + 2 * F);
+        cf.assign(m->cell_faces, m->cell_faces + K * C);
+        fcell.assign(m->face_cells, m->face_cells + 2 * F);
+        fbc.assign(m->face_bc, m->face_bc + F);
+        st = *s;
+        auto dp = M::default_parameters();
+        params.assign(dp.begin(), dp.end());
+        if (p) params.assign(p, p + M::n_parameters);
+        X.assign((size_t)C * NQ, 0.0);
+        A.assign((size_t)C * NA, 0.0);
+        G.assign((size_t)C * NQ * DIM, 0.0);
+        setup_topology();
+        setup_lsq();
+    }
+
+    int nq() const override { return NQ; }
+    int naux() const override { return NA; }
+    void set_params(const double* p) override { params.assign(p, p + M::n_parameters); }
+    int newton_unconverged() const override { return n_unconv; }
+
+    // SetupTopology (TransportStep.hpp:106-120): adjacency of a cell = the
+    // other cells of its faces in cone order.
+    void setup_topology() {
+        nb_off.assign(C + 1, 0);
+        nb_list.clear();
+        cell_face_sorted.assign((size_t)C * K, -1);
+        for (int c = 0; c < C; ++c) {
+            std::vector<int> fs;
+            for (int k = 0; k < K; ++k) {
+                int f = cf[(size_t)c * K + k];
+                if (f < 0) continue;
+                fs.push_back(f);
+                int a = fcell[2 * f], b = fcell[2 * f + 1];
+                int o = (a == c) ? b : a;
+                if (o < 0 || o == c) continue;
+                bool dup = false;
+                for (int q = nb_off[c]; q < (int)nb_list.size(); ++q) dup |= nb_list[q] == o;
+                if (!dup) nb_list.push_back(o);
+            }
+            std::sort(fs.begin(), fs.end());
+            for (size_t k = 0; k < fs.size(); ++k) cell_face_sorted[(size_t)c * K + k] = fs[k];
+            nb_off[c + 1] = (int)nb_list.size();
+        }
+    }
+
+    // LeastSquaresGradient::Setup (Gradient.hpp:222-298), order 1 basis.
+    static bool solve_spd(int n, std::vector<double>& a, std::vector<double>& b) {
+        std::vector<double> L(n * n, 0.0);
+        for (int i = 0; i < n; i++) {
+            for (int j = 0; j <= i; j++) {
+                double sum = 0;
+                for (int k = 0; k < j; k++) sum += L[i * n + k] * L[j * n + k];
+                if (i == j) {
+                    double val = a[i * n + i] - sum;
+                    if (val <= 0) return false;
+                    L[i * n + j] = std::sqrt(val);
+                } else {
+                    L[i * n + j] = (a[i * n + j] - sum) / L[j * n + j];
+                }
+            }
+        }
+        for (int i = 0; i < n; i++) {
+            double sum = 0;
+            for (int k = 0; k < i; k++) sum += L[i * n + k] * b[k];
+            b[i] = (b[i] - sum) / L[i * n + i];
+        }
+        for (int i = n - 1; i >= 0; i--) {
+            double sum = 0;
+            for (int k = i + 1; k < n; k++) sum += L[k * n + i] * b[k];
+            b[i] = (b[i] - sum) / L[i * n + i];
+        }
+        return true;
+    }
+
+    void setup_lsq() {
+        lsq_w.assign(nb_list.size() * DIM, 0.0);
+        for (int c = 0; c < C; ++c) {
+            std::vector<std::vector<double>> basis;
+            for (int q = nb_off[c]; q < nb_off[c + 1]; ++q) {
+                int n = nb_list[q];
+                std::vector<double> b;
+                for (int d = 0; d < DIM; ++d) b.push_back(cc[2 * n + d] - cc[2 * c + d]);
+                basis.push_back(b);
+            }
+            std::vector<double> ata(DIM * DIM, 0.0);
+            for (auto& b : basis)
+                for (int i = 0; i < DIM; ++i)
+                    for (int j = 0; j < DIM; ++j) ata[i * DIM + j] += b[i] * b[j];
+            for (size_t k = 0; k < basis.size(); ++k) {
+                std::vector<double> rhs = basis[k], sys = ata;
+                bool ok = solve_spd(DIM, sys, rhs);
+                for (int d = 0; d < DIM; ++d)
+                    lsq_w[(size_t)(nb_off[c] + k) * DIM + d] = ok ? rhs[d] : 0.0;
+            }
+        }
+    }
+
+    // ---------------------------------------------------------------- state
+    void constrain_cell(T* q, T* a) const {
+        if constexpr (zsme::HasUpdateVariables<M>::value) {
+            auto r = M::update_variables(q, a, params.data(), 0.0);
+            for (int i = 0; i < NQ; ++i) q[i] = r[i];
+        }
+        const T X0[3] = {0, 0, 0};
+        auto ra = M::update_aux_variables(q, a, params.data(), 0.0, X0);
+        for (int i = 0; i < NA; ++i) a[i] = ra[i];
+    }
+    // TransportStep::UpdateState (TransportStep.hpp:196-230)
+    void update_state_vec(std::vector<T>& x, std::vector<T>& a) const {
+        par_for(C, [&](int c, int) { constrain_cell(&x[(size_t)c * NQ], &a[(size_t)c * NA]); });
+    }
+
+    // ------------------------------------------------------------ gradients
+    void gradient_lsq(const std::vector<T>& x, std::vector<T>& g) const {
+par_for(C, [&](int c, int) {
+            T* gc = &g[(size_t)c * NQ * DIM];
+            for (int k = 0; k < NQ * DIM; ++k) gc[k] = 0.0;
+            const T* qc = &x[(size_t)c * NQ];
+            for (int q = nb_off[c]; q < nb_off[c + 1]; ++q) {
+                const T* qn = &x[(size_t)nb_list[q] * NQ];
+                const double* w = &lsq_w[(size_t)q * DIM];
+                for (int i = 0; i < NQ; ++i) {
+                    T du = qn[i] - qc[i];
+                    for (int d = 0; d < DIM; ++d) gc[i * DIM + d] += w[d] * du;
+                }
+            }
+        });
+    }
+    // GreenGaussGradient::Compute: face loop, boundary ghost value q_bc * N,
+    // then / volume.  Accumulated per cell in increasing face order.
+    void gradient_gg(const std::vector<T>& x, std::vector<T>& g) const {
+par_for(C, [&](int c, int) {
+            T* gc = &g[(size_t)c * NQ * DIM];
+            for (int k = 0; k < NQ * DIM; ++k) gc[k] = 0.0;
+            for (int k = 0; k < K; ++k) {
+                int f = cell_face_sorted[(size_t)c * K + k];
+                if (f < 0) break;
+                int L = fcell[2 * f], R = fcell[2 * f + 1];
+                const double* Nf = &fn[2 * f];
+                if (R >= 0) {
+                    const T* qL = &x[(size_t)L * NQ];
+                    const T* qR = &x[(size_t)R * NQ];
+                    for (int i = 0; i < NQ; ++i) {
+                        T fv = 0.5 * (qL[i] + qR[i]);
+                        for (int d = 0; d < DIM; ++d) {
+                            T v = fv * Nf[d];
+                            if (c == L) gc[i * DIM + d] += v; else gc[i * DIM + d] -= v;
+                        }
+                    }
+                } else if (fbc[f] >= 0) {
+                    T area = 0;
+                    for (int d = 0; d < DIM; ++d) area += Nf[d] * Nf[d];
+                    area = std::sqrt(area);
+                    T nh[3] = {0, 0, 0};
+                    for (int d = 0; d < DIM; ++d) nh[d] = Nf[d] / area;
+                    auto qb = M::boundary_conditions(fbc[f], &x[(size_t)c * NQ], nullptr, params.data(), nh,
+                                                     &fc[2 * f], 0.0, 0.0);
+                    for (int i = 0; i < NQ; ++i)
+                        for (int d = 0; d < DIM; ++d) gc[i * DIM + d] += qb[i] * Nf[d];
+                }
+            }
+            if (vol[c] > 1e-15)
+                for (int k = 0; k < NQ * DIM; ++k) gc[k] /= vol[c];
+        });
+    }
+
+    // --------------------------------------------------------- reconstruct
+    // LinearReconstructor::Reconstruct with VacuumLimiter + TVDLimiter, or PCM.
+    void reconstruct(const T* q, const T* g, const double* xc, const double* xf, const T* qmin,
+                     const T* qmax, T* out) const {
+        if (st.reconstruction_order < 2) {
+            for (int i = 0; i < NQ; ++i) out[i] = q[i];
+            return;
+        }
+        T dx[3];
+        for (int d = 0; d < DIM; ++d) dx[d] = xf[d] - xc[d];
+        T qfu[NQ], delta[NQ];
+        for (int i = 0; i < NQ; ++i) {
+            delta[i] = 0.0;
+            if (g)
+                for (int d = 0; d < DIM; ++d) delta[i] += g[i * DIM + d] * dx[d];
+            qfu[i] = q[i] + delta[i];
+        }
+        T fin[NQ];
+        for (int i = 0; i < NQ; ++i) fin[i] = 1.0;
+        if (st.limiter != ZSME_LIMITER_NONE) {
+            // VacuumLimiter (tol 1e-2): h = component 1
+            T tmp[NQ];
+            for (int i = 0; i < NQ; ++i) tmp[i] = 1.0;
+            if (NQ > 1 && qmin && qmin[1] < 1e-2)
+                for (int i = 0; i < NQ; ++i) tmp[i] = 0.0;
+            for (int i = 0; i < NQ; ++i) if (tmp[i] < fin[i]) fin[i] = tmp[i];
+            // TVDLimiter (face-local Barth-Jespersen ratio)
+            for (int i = 0; i < NQ; ++i) tmp[i] = 1.0;
+            if (qmin && qmax) {
+                for (int i = 0; i < NQ; ++i) {
+                    T dq = qfu[i] - q[i];
+                    if (std::abs(dq) < 1e-12) continue;
+                    T al = 1.0;
+                    if (dq > 0) {
+                        if (qmax[i] > q[i]) al = std::min((T)1.0, (qmax[i] - q[i]) / dq);
+                        else al = 0.0;
+                    } else {
+                        if (qmin[i] < q[i]) al = std::min((T)1.0, (qmin[i] - q[i]) / dq);
+                        else al = 0.0;
+                    }
+                    tmp[i] = al;
+                }
+            }
+            for (int i = 0; i < NQ; ++i) if (tmp[i] < fin[i]) fin[i] = tmp[i];
+        }
+        T alpha = 1.;
+        for (int i = 0; i < NQ; ++i) if (alpha > fin[i]) alpha = fin[i];
+        for (int i = 0; i < NQ; ++i) out[i] = q[i] + alpha * delta[i];
+    }
+
+    // ------------------------------------------------------------- FormRHS
+    void form_rhs(double t, const std::vector<T>& xg, std::vector<T>& f) {
+        std::vector<T> xl = xg, al = A;          // local copies
+        update_state_vec(xl, al);
+        const bool o2 = st.reconstruction_order >= 2;
+        std::vector<T> vmin, vmax;
+        if (o2) {
+            vmin.assign((size_t)C * NQ, 0.0);
+            vmax.assign((size_t)C * NQ, 0.0);
+par_for(C, [&](int c, int) {
+                const T* q = &xl[(size_t)c * NQ];
+                T* mn = &vmin[(size_t)c * NQ];
+                T* mx = &vmax[(size_t)c * NQ];
+                for (int i = 0; i < NQ; ++i) { mn[i] = q[i]; mx[i] = q[i]; }
+                for (int k = nb_off[c]; k < nb_off[c + 1]; ++k) {
+                    const T* qn = &xl[(size_t)nb_list[k] * NQ];
+                    for (int i = 0; i < NQ; ++i) {
+                        if (qn[i] < mn[i]) mn[i] = qn[i];
+                        if (qn[i] > mx[i]) mx[i] = qn[i];
+                    }
+                }
+            });
+            // gradient of the UNCLAMPED global state (TransportStep.hpp:339)
+            if (st.gradient == ZSME_GRADIENT_LSQ) gradient_lsq(xg, G); else gradient_gg(xg, G);
+        }
+        // per-face contributions: nc into L, nc into R, flux (all * area)
+        std::vector<T> fb((size_t)F * 3 * NQ, 0.0);
+        std::vector<char> active(F, 0);
+par_for(F, [&](int f, int) {
+            const double* Nf = &fn[2 * f];
+            double area = 0;
+            for (int d = 0; d < DIM; ++d) area += Nf[d] * Nf[d];
+            area = std::sqrt(area);
+            if (area <= 1e-15) return;
+            T nh[3] = {0, 0, 0};
+            for (int d = 0; d < DIM; ++d) nh[d] = Nf[d] / area;
+            const double* xf = &fc[2 * f];
+            int L = fcell[2 * f], R = fcell[2 * f + 1];
+            T* ncL = &fb[(size_t)f * 3 * NQ];
+            T* ncR = ncL + NQ;
+            T* fl = ncR + NQ;
+            if (R >= 0) {
+                T qLf[NQ], qRf[NQ], aLf[NA], aRf[NA];
+                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], xf,
+                            o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
+                reconstruct(&xl[(size_t)R * NQ], o2 ? &G[(size_t)R * NQ * DIM] : nullptr, &cc[2 * R], xf,
+                            o2 ? &vmin[(size_t)R * NQ] : nullptr, o2 ? &vmax[(size_t)R * NQ] : nullptr, qRf);
+                for (int i = 0; i < NA; ++i) { aLf[i] = al[(size_t)L * NA + i]; aRf[i] = al[(size_t)R * NA + i]; }
+                auto ra = M::update_aux_variables(qLf, aLf, params.data(), 0.0, xf);
+                for (int i = 0; i < NA; ++i) aLf[i] = ra[i];
+                auto rb = M::update_aux_variables(qRf, aRf, params.data(), 0.0, xf);
+                for (int i = 0; i < NA; ++i) aRf[i] = rb[i];
+                auto flux = N::numerical_flux(qLf, qRf, aLf, aRf, params.data(), nh);
+                auto nc = N::numerical_fluctuations(qLf, qRf, aLf, aRf, params.data(), nh);
+                for (int i = 0; i < NQ; ++i) {
+                    ncL[i] = nc[NQ + i] * area;
+                    ncR[i] = nc[i] * area;
+                    fl[i] = flux[i] * area;
+                }
+                active[f] = 1;
+            } else if (fbc[f] >= 0) {
+                T qLf[NQ], aLf[NA], aRf[NA];
+                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], xf,
+                            o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
+                for (int i = 0; i < NA; ++i) aLf[i] = al[(size_t)L * NA + i];
+                auto ra = M::update_aux_variables(qLf, aLf, params.data(), t, xf);
+                for (int i = 0; i < NA; ++i) aLf[i] = ra[i];
+                auto qR = M::boundary_conditions(fbc[f], qLf, aLf, params.data(), nh, xf, t, 0.0);
+                auto rb = M::update_aux_variables(qR.data, aLf, params.data(), t, xf);
+                for (int i = 0; i < NA; ++i) aRf[i] = rb[i];
+                auto flux = N::numerical_flux(qLf, qR.data, aLf, aRf, params.data(), nh);
+                auto nc = N::numerical_fluctuations(qLf, qR.data, aLf, aRf, params.data(), nh);
+                for (int i = 0; i < NQ; ++i) {
+                    ncL[i] = nc[NQ + i] * area;
+                    fl[i] = flux[i] * area;
+                }
+                active[f] = 2;
+            }
+        });
+        // per cell: accumulate in increasing face order, then / volume
+        f.assign((size_t)C * NQ, 0.0);
+par_for(C, [&](int c, int) {
+            T* fcq = &f[(size_t)c * NQ];
+            for (int k = 0; k < K; ++k) {
+                int fi = cell_face_sorted[(size_t)c * K + k];
+                if (fi < 0) break;
+                if (!active[fi]) continue;
+                const T* ncL = &fb[(size_t)fi * 3 * NQ];
+                const T* ncR = ncL + NQ;
+                const T* fl = ncR + NQ;
+                if (fcell[2 * fi] == c) {
+                    for (int i = 0; i < NQ; ++i) fcq[i] -= ncL[i];
+                    for (int i = 0; i < NQ; ++i) fcq[i] -= fl[i];
+                } else {
+                    for (int i = 0; i < NQ; ++i) fcq[i] -= ncR[i];
+                    for (int i = 0; i < NQ; ++i) fcq[i] += fl[i];
+                }
+            }
+            if (vol[c] > 1e-15)
+                for (int i = 0; i < NQ; ++i) fcq[i] /= vol[c];
+        });
+    }
+
+    // ------------------------------------------------------------- source
+    template <int n_q, int n_aux>
+    static void aux_jacobian(const T* q, const T* aux, const T* p, T* J) {
+        const T X0[3] = {0, 0, 0};
+        if constexpr (zsme::HasAuxJacobian<M>::value) {
+            auto r = M::update_aux_variables_jacobian_wrt_variables(q, aux, p);
+            for (int i = 0; i < n_aux * n_q; ++i) J[i] = r[i];
+        } else {
+            for (int i = 0; i < n_aux * n_q; ++i) J[i] = 0;
+            auto a0 = M::update_aux_variables(q, aux, p, 0.0, X0);
+            T qp[n_q];
+            for (int j = 0; j < n_q; ++j) {
+                for (int m = 0; m < n_q; ++m) qp[m] = q[m];
+                T h = (T)1e-7 * (std::abs(q[j]) + (T)1e-7);
+                qp[j] += h;
+                auto a1 = M::update_aux_variables(qp, aux, p, 0.0, X0);
+                for (int k = 0; k < n_aux; ++k) J[k * n_q + j] = (a1[k] - a0[k]) / h;
+            }
+        }
+    }
+    static bool gepp(T* a, T* b, T* x) {
+        const int n = NQ;
+        for (int k = 0; k < n; ++k) {
+            int mr = k;
+            T mv = std::abs(a[k * n + k]);
+            for (int i = k + 1; i < n; ++i)
+                if (std::abs(a[i * n + k]) > mv) { mv = std::abs(a[i * n + k]); mr = i; }
+            if (mv < 1e-14) return false;
+            if (mr != k) {
+                for (int j = k; j < n; ++j) std::swap(a[k * n + j], a[mr * n + j]);
+                std::swap(b[k], b[mr]);
+            }
+            for (int i = k + 1; i < n; ++i) {
+                T fct = a[i * n + k] / a[k * n + k];
+                for (int j = k; j < n; ++j) a[i * n + j] -= fct * a[k * n + j];
+                b[i] -= fct * b[k];
+            }
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            T sum = 0.0;
+            for (int j = i + 1; j < n; ++j) sum += a[i * n + j] * x[j];
+            x[i] = (b[i] - sum) / a[i * n + i];
+        }
+        return true;
+    }
+    // SourceStep::SolveLocalCell; returns 1 if the iteration limit was hit.
+    int solve_cell(T dtl, T* q, const T* aux_init) const {
+        const T X0[3] = {0, 0, 0};
+        T q_old[NQ], aux[NA], res[NQ], delta[NQ], J[NQ * NQ];
+        for (int i = 0; i < NQ; ++i) q_old[i] = q[i];
+        for (int i = 0; i < NA; ++i) aux[i] = aux_init[i];
+        const T* p = params.data();
+        int iter = 0;
+        for (; iter < 15; ++iter) {
+            auto ua = M::update_aux_variables(q, aux, p, 0.0, X0);
+            for (int i = 0; i < NA; ++i) aux[i] = ua[i];
+            auto S = M::source(q, aux, p, (T)0, dtl, X0);
+            T rn = 0.0;
+            for (int i = 0; i < NQ; ++i) {
+                res[i] = q[i] - q_old[i] - dtl * S[i];
+                rn += res[i] * res[i];
+            }
+            if (std::sqrt(rn) < 1e-8) break;
+            auto dSdQ = M::source_jacobian_wrt_variables(q, aux, p);
+            auto dSdA = M::source_jacobian_wrt_aux_variables(q, aux, p);
+            T dAdQ[NA * NQ];
+            aux_jacobian<NQ, NA>(q, aux, p, dAdQ);
+            for (int i = 0; i < NQ * NQ; ++i) J[i] = 0.0;
+            for (int i = 0; i < NQ; ++i) J[i * NQ + i] = 1.0;
+            for (int i = 0; i < NQ; ++i)
+                for (int j = 0; j < NQ; ++j) {
+                    T term = dSdQ[i * NQ + j];
+                    for (int k = 0; k < NA; ++k) term += dSdA[i * NA + k] * dAdQ[k * NQ + j];
+                    J[i * NQ + j] -= dtl * term;
+                }
+            for (int i = 0; i < NQ; ++i) res[i] = -res[i];
+            if (gepp(J, res, delta)) {
+                for (int i = 0; i < NQ; ++i) q[i] += delta[i];
+            } else {
+                break;
+            }
+        }
+        return iter >= 15 ? 1 : 0;
+    }
+    void source_solve(T dtl) {
+        std::vector<int> part(par_width(C), 0);
+        par_for(C, [&](int c, int t) { part[t] += solve_cell(dtl, &X[(size_t)c * NQ], &A[(size_t)c * NA]); });
+        int nu = 0;
+        for (int v : part) nu += v;
+        n_unconv = nu;
+    }
+
+    // ----------------------------------------------------- ComputeTimeStep
+    double compute_dt() override {
+        std::vector<double> part(par_width(C), std::numeric_limits<double>::max());
+        par_for(C, [&](int c, int t) {
+            double& best = part[t];
+            const T* q = &X[(size_t)c * NQ];
+            const T* a = &A[(size_t)c * NA];
+            T eig = 0.0;
+            for (int d = 0; d < DIM; ++d) {
+                T n[3] = {0, 0, 0};
+                n[d] = 1.0;
+                auto r = N::local_max_abs_eigenvalue(q, a, params.data(), n);
+                if (r[0] > eig) eig = r[0];
+            }
+            if (eig < 1e-14) return;
+            double rc = std::numeric_limits<double>::max();
+            for (int k = 0; k < K; ++k) {
+                int f = cf[(size_t)c * K + k];
+                if (f < 0) continue;
+                double d2 = 0.0;
+                for (int d = 0; d < DIM; ++d) {
+                    double dd = cc[2 * c + d] - fc[2 * f + d];
+                    d2 += dd * dd;
+                }
+                double dist = std::sqrt(d2);
+                if (dist < rc) rc = dist;
+            }
+            if (rc < std::numeric_limits<double>::max()) {
+                double ratio = rc / eig;
+                if (ratio < best) best = ratio;
+            }
+        });
+        double best = std::numeric_limits<double>::max();
+        for (double v : part) best = std::min(best, v);
+        if (!std::isfinite(best) || best >= 0.5 * std::numeric_limits<double>::max()) return M::dt_max;
+        return st.cfl * best;
+    }
+
+    // ------------------------------------------------------------ driver
+    void set_state(const double* q, double t) override {
+        X.assign(q, q + (size_t)C * NQ);
+        std::fill(A.begin(), A.end(), 0.0);
+        time = t;
+        update_state_vec(X, A);                                  // MUSCLSolver.hpp:54
+        dt = std::max(compute_dt(), st.min_dt);                  // MUSCLSolver.hpp:103
+    }
+    void get_state(double* q) const override { std::copy(X.begin(), X.end(), q); }
+    void get_aux(double* a) const override { std::copy(A.begin(), A.end(), a); }
+    void get_time(double* t, double* d) const override { *t = time; *d = dt; }
+    void rhs(double t, const double* x, double* f) override {
+        std::vector<T> xv(x, x + (size_t)C * NQ), fv;
+        form_rhs(t, xv, fv);
+        std::copy(fv.begin(), fv.end(), f);
+    }
+    void gradient(const double* x, double* g) override {
+        std::vector<T> xv(x, x + (size_t)C * NQ), gv((size_t)C * NQ * DIM);
+        if (st.gradient == ZSME_GRADIENT_LSQ) gradient_lsq(xv, gv); else gradient_gg(xv, gv);
+        std::copy(gv.begin(), gv.end(), g);
+    }
+    void update_state() override { update_state_vec(X, A); }
+    void source(double d) override { source_solve(d); }
+
+    // TSStep: SSP-RK(s,2) for order >= 2, forward Euler for order 1.
+    void ts_step(double t0, double h) {
+        std::vector<T> F;
+        const size_t n = X.size();
+        if (st.reconstruction_order < 2) {
+            form_rhs(t0, X, F);
+            for (size_t i = 0; i < n; ++i) X[i] = X[i] + h * F[i];
+            return;
+        }
+        const int s = st.ssp_stages;
+        std::vector<T> w = X;
+        for (int i = 0; i < s - 1; ++i) {
+            double stage_time = t0 + h * (i / (s - 1.));
+            form_rhs(stage_time, w, F);
+            const double a = h / (s - 1.);
+            for (size_t k = 0; k < n; ++k) w[k] = w[k] + a * F[k];
+        }
+        form_rhs(t0 + h, w, F);
+        const double al = (s - 1.) / s, be = h / s, ga = 1. / s;
+        for (size_t k = 0; k < n; ++k) X[k] = al * w[k] + be * F[k] + ga * X[k];
+    }
+    void step(int nsteps, const double* dts) override {
+        for (int it = 0; it < nsteps; ++it) {
+            if (!(time < st.t_end)) break;
+            double t0 = time;
+            double d0 = dts ? dts[it] : dt;
+            if (t0 + d0 > st.t_end) d0 = st.t_end - t0;
+            ts_step(t0, d0);
+            time = t0 + d0;
+            update_state_vec(X, A);                            // EnforcePhysicalConstraints
+            if (st.source) {
+                source_solve(d0);
+                update_state_vec(X, A);
+            }
+            update_state_vec(X, A);                            // PostStep
+            dt = compute_dt();
+        }
+    }
+};
+
+// Pointwise evaluation of one plugin function (for pinning the generated
+// headers against the reference's).  fn: 0 numerical_flux, 1
+// numerical_fluctuations, 2 local_max_abs_eigenvalue, 3 source, 4
+// source_jacobian_wrt_variables, 5 source_jacobian_wrt_aux_variables, 6
+// update_variables, 7 update_aux_variables, 8 boundary_conditions(bc 0),
+// 9 eigenvalues, 10 flux, 11 solver-side dAux/dQ (SourceStep.hpp:26-53),
+// 12 nonconservative_matrix.
+template <template <typename> class MT, template <typename> class NT>
+int pointwise(int fn, const double* qL, const double* qR, const double* aL, const double* aR,
+              const double* p, const double* n, double s, double* out) {
+    using M = MT<double>;
+    using N = NT<double>;
+    const double X0[3] = {0, 0, 0};
+    auto put = [&](const auto& r, int k) { for (int i = 0; i < k; ++i) out[i] = r[i]; return k; };
+    constexpr int nq = M::n_dof_q, na = M::n_dof_qaux, dim = M::dimension;
+    switch (fn) {
+        case 0: return put(N::numerical_flux(qL, qR, aL, aR, p, n), nq);
+        case 1: return put(N::numerical_fluctuations(qL, qR, aL, aR, p, n), 2 * nq);
+        case 2: return put(N::local_max_abs_eigenvalue(qL, aL, p, n), 1);
+        case 3: return put(M::source(qL, aL, p, 0.0, s, X0), nq);
+        case 4: return put(M::source_jacobian_wrt_variables(qL, aL, p), nq * nq);
+        case 5: return put(M::source_jacobian_wrt_aux_variables(qL, aL, p), nq * na);
+        case 6: return put(M::update_variables(qL, aL, p, s), nq);
+        case 7: return put(M::update_aux_variables(qL, aL, p, 0.0, X0), na);
+        case 8: return put(M::boundary_conditions(0, qL, aL, p, n, X0, 0.0, 0.0), nq);
+        case 9: return put(M::eigenvalues(qL, aL, p, n), nq);
+        case 10: return put(M::flux(qL, aL, p), nq * dim);
+        case 11: {
+            double J[na * nq];
+            Oracle<MT, NT>::template aux_jacobian<nq, na>(qL, aL, p, J);
+            for (int i = 0; i < na * nq; ++i) out[i] = J[i];
+            return na * nq;
+        }
+        case 12: return put(M::nonconservative_matrix(qL, aL, p), nq * nq * dim);
+    }
+    return -1;
+}
+
+struct Entry {
+    const char* name;
+    OracleBase* (*make)(const zsme_mesh*, const zsme_settings*, const double*);
+    int (*pw)(int, const double*, const double*, const double*, const double*, const double*,
+              const double*, double, double*);
+    int nq, na, np, dim;
+};
+
+template <template <typename> class MT, template <typename> class NT>
+OracleBase* make_oracle(const zsme_mesh* m, const zsme_settings* s, const double* p) {
+    return new Oracle<MT, NT>(m, s, p);
+}
+
+#define ORACLE_ENTRY(NS)                                                                   \
+    Entry{#NS, &make_oracle<NS::Model, NS::Numerics>, &pointwise<NS::Model, NS::Numerics>,   \
+          NS::Model<double>::n_dof_q,                                                      \
+          NS::Model<double>::n_dof_qaux, NS::Model<double>::n_parameters,                  \
+          NS::Model<double>::dimension}
+
+const Entry kEntries[] = {
+    ORACLE_ENTRY(sme1d_l0_malpasset), ORACLE_ENTRY(sme2d_l0), ORACLE_ENTRY(sme2d_l1),
+    ORACLE_ENTRY(sme2d_l2), ORACLE_ENTRY(sme2d_l4),
+#ifdef ORACLE_WITH_REFERENCE_MODEL
+    ORACLE_ENTRY(ref1d),
+#endif
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* oracle_last_error() { return g_err.c_str(); }
+
+// Worker threads for the parallel loops (0 = all hardware threads).
+int oracle_set_threads(int n) {
+    g_threads = n > 0 ? n : (int)std::max(1u, std::thread::hardware_concurrency());
+    return g_threads;
+}
+
+int oracle_model_info(const char* model, int* nq, int* na, int* np, int* dim) {
+    for (auto& e : kEntries)
+        if (!std::strcmp(e.name, model)) {
+            *nq = e.nq; *na = e.na; *np = e.np; *dim = e.dim;
+            return 0;
+        }
+    return fail(ZSME_ERR_MODEL, std::string("unknown model ") + model);
+}
+
+int oracle_create(const char* model, const zsme_mesh* mesh, const zsme_settings* s, const double* params,
+                  void** out) {
+    for (auto& e : kEntries)
+        if (!std::strcmp(e.name, model)) {
+            if (mesh->dim != e.dim) return fail(ZSME_ERR_ARG, "mesh dim != model dimension");
+            *out = e.make(mesh, s, params);
+            return 0;
+        }
+    return fail(ZSME_ERR_MODEL, std::string("unknown model ") + model);
+}
+int oracle_pointwise(const char* model, int fn, const double* qL, const double* qR, const double* aL,
+                     const double* aR, const double* p, const double* n, double s, double* out) {
+    for (auto& e : kEntries)
+        if (!std::strcmp(e.name, model)) return e.pw(fn, qL, qR, aL, aR, p, n, s, out);
+    return fail(-ZSME_ERR_MODEL, std::string("unknown model ") + model);
+}
+int oracle_destroy(void* h) { delete (OracleBase*)h; return 0; }
+int oracle_set_state(void* h, const double* q, double t) { ((OracleBase*)h)->set_state(q, t); return 0; }
+int oracle_get_state(void* h, double* q) { ((OracleBase*)h)->get_state(q); return 0; }
+int oracle_get_aux(void* h, double* a) { ((OracleBase*)h)->get_aux(a); return 0; }
+int oracle_rhs(void* h, double t, const double* x, double* f) { ((OracleBase*)h)->rhs(t, x, f); return 0; }
+int oracle_gradient(void* h, const double* x, double* g) { ((OracleBase*)h)->gradient(x, g); return 0; }
+int oracle_update_state(void* h) { ((OracleBase*)h)->update_state(); return 0; }
+int oracle_source(void* h, double dt) { ((OracleBase*)h)->source(dt); return 0; }
+int oracle_compute_dt(void* h, double* dt) { *dt = ((OracleBase*)h)->compute_dt(); return 0; }
+int oracle_step(void* h, int n) { ((OracleBase*)h)->step(n, nullptr); return 0; }
+int oracle_step_dt(void* h, int n, const double* dts) { ((OracleBase*)h)->step(n, dts); return 0; }
+int oracle_get_time(void* h, double* t, double* dt) { ((OracleBase*)h)->get_time(t, dt); return 0; }
+int oracle_set_params(void* h, const double* p) { ((OracleBase*)h)->set_params(p); return 0; }
+int oracle_newton_unconverged(void* h) { return ((OracleBase*)h)->newton_unconverged(); }
+
+}  // extern "C"

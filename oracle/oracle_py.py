@@ -1,0 +1,178 @@
+"""ctypes binding of the oracle (test infrastructure, the checker only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  ``Oracle`` mirrors the C ABI of the product (include/zsme.h) so
+that a parity test drives both the same way.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "liboracle_ref.so")
+
+FN = dict(numerical_flux=0, numerical_fluctuations=1, local_max_abs_eigenvalue=2, source=3,
+          source_jacobian_wrt_variables=4, source_jacobian_wrt_aux_variables=5,
+          update_variables=6, update_aux_variables=7, boundary_conditions=8, eigenvalues=9,
+          flux=10, aux_jacobian=11, nonconservative_matrix=12)
+
+
+def build(ref: bool = False):
+    """Compile the oracle (and, with ref=True, the reference-header variant)."""
+    targets = ["all"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+_libs = {}
+
+
+def load(ref: bool = False):
+    path = REF_LIB if ref else LIB
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise FileNotFoundError(path + " is not built (make -C oracle%s)" % (" ref" if ref else ""))
+    lib = ct.CDLL(path)
+    P = ct.POINTER(ct.c_double)
+    vp = ct.c_void_p
+    lib.oracle_last_error.restype = ct.c_char_p
+    lib.oracle_create.argtypes = [ct.c_char_p, vp, vp, P, ct.POINTER(vp)]
+    lib.oracle_destroy.argtypes = [vp]
+    lib.oracle_set_state.argtypes = [vp, P, ct.c_double]
+    lib.oracle_get_state.argtypes = [vp, P]
+    lib.oracle_get_aux.argtypes = [vp, P]
+    lib.oracle_rhs.argtypes = [vp, ct.c_double, P, P]
+    lib.oracle_gradient.argtypes = [vp, P, P]
+    lib.oracle_update_state.argtypes = [vp]
+    lib.oracle_source.argtypes = [vp, ct.c_double]
+    lib.oracle_compute_dt.argtypes = [vp, P]
+    lib.oracle_step.argtypes = [vp, ct.c_int]
+    lib.oracle_step_dt.argtypes = [vp, ct.c_int, P]
+    lib.oracle_get_time.argtypes = [vp, P, P]
+    lib.oracle_set_params.argtypes = [vp, P]
+    lib.oracle_newton_unconverged.argtypes = [vp]
+    lib.oracle_set_threads.argtypes = [ct.c_int]
+    lib.oracle_model_info.argtypes = [ct.c_char_p] + [ct.POINTER(ct.c_int)] * 4
+    lib.oracle_pointwise.argtypes = [ct.c_char_p, ct.c_int, P, P, P, P, P, P, ct.c_double, P]
+    _libs[path] = lib
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+def model_info(model: str, ref: bool = False):
+    lib = load(ref)
+    v = [ct.c_int() for _ in range(4)]
+    rc = lib.oracle_model_info(model.encode(), *[ct.byref(x) for x in v])
+    if rc:
+        raise ValueError(lib.oracle_last_error().decode())
+    return dict(n_dof_q=v[0].value, n_dof_qaux=v[1].value, n_parameters=v[2].value, dimension=v[3].value)
+
+
+def pointwise(model: str, fn: str, qL, aL, p, n=None, qR=None, aR=None, s=0.0, ref=False):
+    lib = load(ref)
+    f = lambda a: np.ascontiguousarray(a if a is not None else np.zeros(16), dtype=np.float64)
+    qL, aL, p = f(qL), f(aL), f(p)
+    qR = f(qR if qR is not None else qL)
+    aR = f(aR if aR is not None else aL)
+    n = f(n if n is not None else np.array([1.0, 0.0, 0.0]))
+    out = np.zeros(4096)
+    k = lib.oracle_pointwise(model.encode(), FN[fn], _p(qL), _p(qR), _p(aL), _p(aR), _p(p), _p(n),
+                             float(s), _p(out))
+    if k < 0:
+        raise ValueError(lib.oracle_last_error().decode())
+    return out[:k].copy()
+
+
+def set_threads(n: int = 0, ref: bool = False) -> int:
+    return load(ref).oracle_set_threads(n)
+
+
+class Oracle:
+    """CPU restatement of the reference step on one mesh (caller cell order)."""
+
+    def __init__(self, model: str, mesh_abi: dict, settings_struct, params=None, ref=False):
+        from zoomy_dmplex_b200 import native  # the zsme_mesh / zsme_settings layouts
+
+        self.lib = load(ref)
+        self.info = model_info(model, ref)
+        self.nq = self.info["n_dof_q"]
+        self.na = self.info["n_dof_qaux"]
+        self.C = mesh_abi["n_cells"]
+        self._mesh_keep = native.make_mesh_struct(mesh_abi)
+        self._settings = settings_struct
+        h = ct.c_void_p()
+        pp = None
+        if params is not None:
+            self._params = np.ascontiguousarray(params, dtype=np.float64)
+            pp = _p(self._params)
+        rc = self.lib.oracle_create(model.encode(), ct.addressof(self._mesh_keep[0]),
+                                    ct.addressof(self._settings), pp, ct.byref(h))
+        if rc:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.oracle_destroy(self.h)
+            self.h = None
+
+    def set_state(self, q, t=0.0):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.C, self.nq)
+        self.lib.oracle_set_state(self.h, _p(q), float(t))
+
+    def get_state(self):
+        q = np.zeros((self.C, self.nq))
+        self.lib.oracle_get_state(self.h, _p(q))
+        return q
+
+    def get_aux(self):
+        a = np.zeros((self.C, self.na))
+        self.lib.oracle_get_aux(self.h, _p(a))
+        return a
+
+    def rhs(self, x, t=0.0):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.C, self.nq)
+        f = np.zeros_like(x)
+        self.lib.oracle_rhs(self.h, float(t), _p(x), _p(f))
+        return f
+
+    def gradient(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.C, self.nq)
+        dim = self.info["dimension"]
+        g = np.zeros((self.C, self.nq * dim))
+        self.lib.oracle_gradient(self.h, _p(x), _p(g))
+        return g
+
+    def update_state(self):
+        self.lib.oracle_update_state(self.h)
+
+    def source(self, dt):
+        self.lib.oracle_source(self.h, float(dt))
+
+    def compute_dt(self):
+        d = ct.c_double()
+        self.lib.oracle_compute_dt(self.h, ct.byref(d))
+        return d.value
+
+    def step(self, n=1, dts=None):
+        if dts is None:
+            self.lib.oracle_step(self.h, int(n))
+        else:
+            d = np.ascontiguousarray(dts, dtype=np.float64)
+            self.lib.oracle_step_dt(self.h, int(d.size), _p(d))
+
+    def time(self):
+        t, d = ct.c_double(), ct.c_double()
+        self.lib.oracle_get_time(self.h, ct.byref(t), ct.byref(d))
+        return t.value, d.value
+
+    def newton_unconverged(self):
+        return self.lib.oracle_newton_unconverged(self.h)

@@ -1,0 +1,64 @@
+// Prelude that every translation unit includes before a generated model
+// plugin (Model.H / Numerics.H).
+//
+// The generated headers define SimpleArray only if ZOOMY_SIMPLE_ARRAY is not
+// yet defined (reference Model.H:5-17); their own definition is host-only.
+// Predefining a __host__ __device__ SimpleArray here is what lets the same
+// unmodified headers compile as device functions.  Heaviside is the one
+// free function the generated bodies call by bare name (reference
+// Model.H:242); sympy's convention Heaviside(0) = h0 is kept.
+#pragma once
+#include <cmath>
+#include <array>
+#include <vector>
+#include <string>
+#include <algorithm>
+#include <type_traits>
+#include <utility>
+
+#ifdef __CUDACC__
+#define ZSME_HD __host__ __device__
+#else
+#define ZSME_HD
+#endif
+
+#ifndef ZOOMY_SIMPLE_ARRAY
+#define ZOOMY_SIMPLE_ARRAY
+template <typename T, int N>
+struct SimpleArray {
+    T data[N];
+    ZSME_HD T& operator[](int i) { return data[i]; }
+    ZSME_HD const T& operator[](int i) const { return data[i]; }
+    ZSME_HD T* begin() { return data; }
+    ZSME_HD const T* begin() const { return data; }
+    ZSME_HD T* end() { return data + N; }
+    ZSME_HD const T* end() const { return data + N; }
+};
+#endif
+
+template <typename T>
+ZSME_HD inline T Heaviside(T x, double h0) {
+    return x < T(0) ? T(0) : (x > T(0) ? T(1) : T(h0));
+}
+
+namespace zsme {
+
+// Trait detection mirroring the reference's SFINAE switches.
+// update_variables(Q, Qaux, p, dt) present?  (TransportStep.hpp:22-29)
+template <class M, typename = void>
+struct HasUpdateVariables : std::false_type {};
+template <class M>
+struct HasUpdateVariables<M, std::void_t<decltype(M::update_variables(
+    std::declval<const double*>(), std::declval<const double*>(),
+    std::declval<const double*>(), std::declval<const double>()))>> : std::true_type {};
+
+// Analytic dAux/dQ with the 3-argument signature?  (SourceStep.hpp:16-20)
+// A 5-argument update_aux_variables_jacobian_wrt_variables does not match,
+// exactly as in the reference, and the finite-difference path is taken.
+template <class M, typename = void>
+struct HasAuxJacobian : std::false_type {};
+template <class M>
+struct HasAuxJacobian<M, std::void_t<decltype(M::update_aux_variables_jacobian_wrt_variables(
+    (const double*)nullptr, (const double*)nullptr, (const double*)nullptr))>> : std::true_type {};
+
+}  // namespace zsme

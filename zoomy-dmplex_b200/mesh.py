@@ -1,0 +1,255 @@
+"""Unstructured meshes and their finite-volume geometry.
+
+The reference reads a gmsh file into a PETSc DMPlex and takes its cell-centred
+finite-volume geometry from ``DMPlexGetGeometryFVM`` (reference
+``VirtualSolver.hpp:386-525``, ``TransportStep.hpp:388-410``).  This module
+builds the same quantities without PETSc:
+
+* faces are numbered in first-encounter order over the cells, each cell's faces
+  in its local edge order ``(v0,v1), (v1,v2), (v2,v0)`` -- the order DMPlex
+  interpolation produces -- so ``face_cells[f, 0]`` (the support's first cell)
+  is the lower-numbered cell;
+* face normals are area-weighted (length = face measure) and oriented from
+  ``face_cells[f, 0]`` to ``face_cells[f, 1]``; on the boundary they point out;
+* ``cell_faces`` is the cell's cone (local edge order) and ``cell_nbrs`` its
+  face-neighbour list in cone order, i.e. what ``DMPlexGetAdjacency`` returns
+  for a finite-volume field (cells sharing a face, reference
+  ``TransportStep.hpp:106-120``);
+* boundary faces carry a boundary-condition index (``face_bc``): the
+  reference maps every exterior face of an untagged mesh to the model's
+  ``"default"`` tag, index 0 (``VirtualSolver.hpp:499-511``).
+
+Meshes of the benchmark configurations are seeded jittered-grid Delaunay
+triangulations of the unit square (``jittered_square``); 1-D interval meshes
+(``interval``) and gmsh 2.2 files (``read_msh``/``write_msh``) are supported
+as well.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+FACE_INTERIOR = -1
+FACE_NO_CONDITION = -2
+
+
+@dataclasses.dataclass
+class Mesh:
+    dim: int                      # 1 or 2
+    vertices: np.ndarray          # [V, 2]
+    cells: np.ndarray             # [C, K] vertex ids (K = 2 segments, 3 triangles)
+    cell_centroid: np.ndarray     # [C, 2]
+    cell_volume: np.ndarray       # [C]
+    cell_faces: np.ndarray        # [C, K] int32, cone order
+    face_cells: np.ndarray        # [F, 2] int32, [:,1] = -1 on the boundary
+    face_centroid: np.ndarray     # [F, 2]
+    face_normal: np.ndarray       # [F, 2] area-weighted, oriented cells[0] -> cells[1]
+    face_bc: np.ndarray           # [F] int32: -1 interior, >= 0 bc index, -2 none
+    name: str = "mesh"
+
+    @property
+    def n_cells(self):
+        return int(self.cells.shape[0])
+
+    @property
+    def n_faces(self):
+        return int(self.face_cells.shape[0])
+
+    @property
+    def max_faces(self):
+        return int(self.cell_faces.shape[1])
+
+    def cell_nbrs(self):
+        """Face neighbours of each cell in cone order, -1 padded ([C, K])."""
+        f = self.cell_faces
+        fc = self.face_cells[f]                       # [C, K, 2]
+        me = np.arange(self.n_cells)[:, None]
+        other = np.where(fc[..., 0] == me, fc[..., 1], fc[..., 0])
+        other = np.where(f < 0, -1, other)
+        # compact: boundary slots move to the end, cone order kept
+        out = np.full_like(other, -1)
+        cnt = np.zeros(self.n_cells, dtype=np.int64)
+        for k in range(other.shape[1]):
+            v = other[:, k]
+            ok = v >= 0
+            out[np.nonzero(ok)[0], cnt[ok]] = v[ok]
+            cnt += ok
+        return out.astype(np.int32)
+
+    def inradius_proxy(self):
+        """r_c = min over the cell's faces of |x_c - x_f| (reference
+        ``VirtualSolver.hpp:329-340``)."""
+        f = self.cell_faces
+        d = self.face_centroid[np.maximum(f, 0)] - self.cell_centroid[:, None, :]
+        r = np.sqrt((d[..., : self.dim] ** 2).sum(-1))
+        r = np.where(f < 0, np.inf, r)
+        return r.min(axis=1)
+
+    def as_abi_arrays(self):
+        """Contiguous arrays in the layout the C ABI (``zsme_mesh``) takes."""
+        return dict(
+            dim=self.dim,
+            n_cells=self.n_cells,
+            n_faces=self.n_faces,
+            max_faces=self.max_faces,
+            cell_centroid=np.ascontiguousarray(self.cell_centroid, dtype=np.float64),
+            cell_volume=np.ascontiguousarray(self.cell_volume, dtype=np.float64),
+            cell_faces=np.ascontiguousarray(self.cell_faces, dtype=np.int32),
+            face_cells=np.ascontiguousarray(self.face_cells, dtype=np.int32),
+            face_centroid=np.ascontiguousarray(self.face_centroid, dtype=np.float64),
+            face_normal=np.ascontiguousarray(self.face_normal, dtype=np.float64),
+            face_bc=np.ascontiguousarray(self.face_bc, dtype=np.int32),
+        )
+
+
+# ---------------------------------------------------------------------------
+# construction
+# ---------------------------------------------------------------------------
+def _faces_from_cells(cells: np.ndarray, nloc: int):
+    """First-encounter face numbering (cell order, then local face order)."""
+    C = cells.shape[0]
+    if nloc == 3:
+        a = cells[:, [0, 1, 2]]
+        b = cells[:, [1, 2, 0]]
+        lo = np.minimum(a, b).reshape(-1).astype(np.int64)
+        hi = np.maximum(a, b).reshape(-1).astype(np.int64)
+        key = lo * (int(cells.max()) + 1) + hi
+    else:  # 1-D: faces are the vertices
+        key = cells.reshape(-1).astype(np.int64)
+    uniq, first, inv = np.unique(key, return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")           # face ids by first encounter
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    fid = rank[inv].reshape(C, nloc)                    # [C, nloc]
+    F = uniq.size
+    flat_c = np.repeat(np.arange(C), nloc)
+    flat_f = fid.reshape(-1)
+    # support: the encountering cells in cell order
+    srt = np.lexsort((flat_c, flat_f))
+    ff, cc = flat_f[srt], flat_c[srt]
+    face_cells = np.full((F, 2), -1, dtype=np.int64)
+    start = np.searchsorted(ff, np.arange(F))
+    face_cells[:, 0] = cc[start]
+    cnt = np.bincount(ff, minlength=F)
+    if (cnt > 2).any():
+        raise ValueError("non-manifold mesh: a face has more than two cells")
+    two = cnt == 2
+    face_cells[two, 1] = cc[start[two] + 1]
+    return fid.astype(np.int32), face_cells.astype(np.int32), first[order]
+
+
+def from_triangles(vertices: np.ndarray, tris: np.ndarray, name="mesh", boundary_bc=0) -> Mesh:
+    vertices = np.asarray(vertices, dtype=np.float64)[:, :2].copy()
+    tris = np.asarray(tris, dtype=np.int64).copy()
+    p0, p1, p2 = vertices[tris[:, 0]], vertices[tris[:, 1]], vertices[tris[:, 2]]
+    area2 = (p1[:, 0] - p0[:, 0]) * (p2[:, 1] - p0[:, 1]) - (p1[:, 1] - p0[:, 1]) * (p2[:, 0] - p0[:, 0])
+    keep = np.abs(area2) > 1e-14 * np.abs(area2).max()
+    tris = tris[keep]
+    area2 = area2[keep]
+    neg = area2 < 0                                     # orient counter-clockwise
+    tris[neg] = tris[neg][:, [0, 2, 1]]
+    p0, p1, p2 = vertices[tris[:, 0]], vertices[tris[:, 1]], vertices[tris[:, 2]]
+    centroid = (p0 + p1 + p2) / 3.0
+    volume = 0.5 * np.abs(area2)
+    cell_faces, face_cells, first = _faces_from_cells(tris, 3)
+    C = tris.shape[0]
+    loc = first % 3                                     # local edge of the first cell
+    c0 = face_cells[:, 0]
+    va = tris[c0, loc]
+    vb = tris[c0, (loc + 1) % 3]
+    xa, xb = vertices[va], vertices[vb]
+    fcent = 0.5 * (xa + xb)
+    e = xb - xa
+    normal = np.stack([e[:, 1], -e[:, 0]], axis=1)
+    out = ((fcent - centroid[c0]) * normal).sum(1) < 0
+    normal[out] *= -1.0
+    bc = np.where(face_cells[:, 1] < 0, boundary_bc, FACE_INTERIOR).astype(np.int32)
+    return Mesh(2, vertices, tris.astype(np.int32), centroid, volume, cell_faces, face_cells,
+                fcent, normal, bc, name=name)
+
+
+def jittered_square(n: int, seed: int = 0, jitter: float = 0.2, name=None) -> Mesh:
+    """Delaunay triangulation of an n x n point grid on the unit square whose
+    interior points are jittered uniformly by +-jitter*spacing (seeded); the
+    boundary points stay on the boundary so the walls are straight."""
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    s = np.linspace(0.0, 1.0, n)
+    X, Y = np.meshgrid(s, s, indexing="xy")
+    pts = np.stack([X.ravel(), Y.ravel()], axis=1)
+    h = 1.0 / (n - 1)
+    interior = (pts[:, 0] > 0) & (pts[:, 0] < 1) & (pts[:, 1] > 0) & (pts[:, 1] < 1)
+    jit = rng.uniform(-jitter * h, jitter * h, size=pts.shape)
+    pts = pts + jit * interior[:, None]
+    tri = Delaunay(pts)
+    return from_triangles(pts, tri.simplices, name=name or "square_%d_s%d" % (n, seed))
+
+
+def interval(x: np.ndarray, name="interval", bc_left=0, bc_right=0) -> Mesh:
+    """1-D mesh of segments between sorted node coordinates x."""
+    x = np.asarray(x, dtype=np.float64)
+    V = x.size
+    verts = np.stack([x, np.zeros(V)], axis=1)
+    segs = np.stack([np.arange(V - 1), np.arange(1, V)], axis=1)
+    cell_faces, face_cells, first = _faces_from_cells(segs, 2)
+    centroid = 0.5 * (verts[segs[:, 0]] + verts[segs[:, 1]])
+    volume = np.abs(x[1:] - x[:-1])
+    vid = segs.reshape(-1)[first]
+    fcent = verts[vid]
+    normal = np.zeros((face_cells.shape[0], 2))
+    c0 = face_cells[:, 0]
+    normal[:, 0] = np.where(fcent[:, 0] >= centroid[c0, 0], 1.0, -1.0)
+    bc = np.full(face_cells.shape[0], FACE_INTERIOR, dtype=np.int32)
+    bnd = face_cells[:, 1] < 0
+    bc[bnd & (fcent[:, 0] <= x.min())] = bc_left
+    bc[bnd & (fcent[:, 0] >= x.max())] = bc_right
+    return Mesh(1, verts, segs.astype(np.int32), centroid, volume, cell_faces, face_cells,
+                fcent, normal, bc, name=name)
+
+
+# ---------------------------------------------------------------------------
+# gmsh 2.2 ASCII (the format of the reference's meshes, make_bump_case.py)
+# ---------------------------------------------------------------------------
+def write_msh(path: str, mesh: Mesh):
+    V = mesh.vertices.shape[0]
+    with open(path, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % V)
+        for i, (x, y) in enumerate(mesh.vertices):
+            f.write("%d %.17g %.17g 0.0\n" % (i + 1, x, y))
+        f.write("$EndNodes\n$Elements\n%d\n" % mesh.n_cells)
+        etype = 2 if mesh.dim == 2 else 1
+        for i, c in enumerate(mesh.cells):
+            f.write("%d %d 2 1 1 %s\n" % (i + 1, etype, " ".join(str(int(v) + 1) for v in c)))
+        f.write("$EndElements\n")
+
+
+def read_msh(path: str, boundary_bc=0) -> Mesh:
+    """Read a gmsh 2.2 ASCII mesh (triangles, or segments for 1-D)."""
+    with open(path) as f:
+        lines = [ln.strip() for ln in f]
+    i = lines.index("$Nodes")
+    nv = int(lines[i + 1])
+    ids, xy = [], []
+    for ln in lines[i + 2: i + 2 + nv]:
+        t = ln.split()
+        ids.append(int(t[0]))
+        xy.append((float(t[1]), float(t[2])))
+    idmap = {v: k for k, v in enumerate(ids)}
+    xy = np.array(xy)
+    i = lines.index("$Elements")
+    ne = int(lines[i + 1])
+    tris, segs = [], []
+    for ln in lines[i + 2: i + 2 + ne]:
+        t = [int(v) for v in ln.split()]
+        et, nt = t[1], t[2]
+        nodes = [idmap[v] for v in t[3 + nt:]]
+        if et == 2:
+            tris.append(nodes)
+        elif et == 1:
+            segs.append(nodes)
+    if tris:
+        return from_triangles(xy, np.array(tris), name=path, boundary_bc=boundary_bc)
+    xs = np.unique(xy[np.array(segs).reshape(-1), 0])
+    return interval(xs, name=path, bc_left=boundary_bc, bc_right=boundary_bc)

@@ -1,0 +1,718 @@
+#pragma once
+// Generated by models/gen_sme.py (sme2d_l2: dim=2 level=2). Do not edit by hand.
+// Plugin interface of the reference's generated headers: Model<T> / Numerics<T>
+// with static PORTABLE_FN members taking raw pointers and returning SimpleArray.
+#include <cmath>
+#include <array>
+
+#ifndef ZOOMY_SIMPLE_ARRAY
+#define ZOOMY_SIMPLE_ARRAY
+template <typename T, int N>
+struct SimpleArray {
+    T data[N];
+    T& operator[](int i) { return data[i]; }
+    const T& operator[](int i) const { return data[i]; }
+    T* begin() { return data; }
+    const T* begin() const { return data; }
+    T* end() { return data + N; }
+    const T* end() const { return data + N; }
+};
+#endif
+
+#include <vector>
+#include <string>
+#include <algorithm>
+
+#ifdef __CUDACC__
+#define PORTABLE_FN __host__ __device__
+#else
+#define PORTABLE_FN
+#endif
+
+template <typename T>
+struct Model {
+    static constexpr int n_dof_q    = 8;
+    static constexpr int n_dof_qaux = 1;
+    static constexpr int n_parameters = 6;
+    static constexpr int dimension  = 2;
+    static constexpr double dt_max = 5.0;
+    static constexpr int n_dof_gradQ = 0;
+    static constexpr bool has_diffusion = false;
+    static constexpr bool has_free_surface = true;
+    static constexpr int idx_b = 0;
+    static constexpr int idx_h = 1;
+    static constexpr int n_boundary_tags = 1;
+    static const std::vector<std::string> get_boundary_tags() { return { "default" }; }
+    static const std::vector<std::string> parameter_names() { return { "g", "nu", "lambda", "n_manning", "e_x", "e_y" }; }
+    static const std::vector<T> default_parameters() { return { 9.81, 0.0, 0.1, 0.0, 0.0, 0.0 }; }
+    PORTABLE_FN static inline SimpleArray<T, 8> flux_x(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    T t0 = ((Q[3]*Q[3])/3.0);
+    T t1 = (Q[4]*Q[4]);
+    T t2 = (2.0/5.0)*Q[4];
+    T t3 = 2.0*Qaux[0];
+    T t4 = Q[3]*Q[6];
+    T t5 = Q[4]*Q[7];
+    SimpleArray<T, 8> res;
+    res[0] = 0.0;
+    res[1] = Q[2];
+    res[2] = Qaux[0]*(t0 + (Q[2]*Q[2]) + (t1/5.0));
+    res[3] = Q[3]*t3*(Q[2] + t2);
+    res[4] = t3*(t0 + (t1/7.0) + Q[2]*Q[4]);
+    res[5] = Qaux[0]*((t4/3.0) + (t5/5.0) + Q[2]*Q[5]);
+    res[6] = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[6]*t2 + (2.0/5.0)*Q[3]*Q[7]);
+    res[7] = Qaux[0]*((2.0/3.0)*t4 + (2.0/7.0)*t5 + Q[2]*Q[7] + Q[4]*Q[5]);
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> flux_y(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    T t0 = Q[3]*Q[6];
+    T t1 = Q[4]*Q[7];
+    T t2 = (2.0/5.0)*Q[7];
+    T t3 = ((Q[6]*Q[6])/3.0);
+    T t4 = (Q[7]*Q[7]);
+    T t5 = 2.0*Qaux[0];
+    SimpleArray<T, 8> res;
+    res[0] = 0.0;
+    res[1] = Q[5];
+    res[2] = Qaux[0]*((t0/3.0) + (t1/5.0) + Q[2]*Q[5]);
+    res[3] = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[3]*t2 + (2.0/5.0)*Q[4]*Q[6]);
+    res[4] = Qaux[0]*((2.0/3.0)*t0 + (2.0/7.0)*t1 + Q[2]*Q[7] + Q[4]*Q[5]);
+    res[5] = Qaux[0]*(t3 + (Q[5]*Q[5]) + (t4/5.0));
+    res[6] = Q[6]*t5*(Q[5] + t2);
+    res[7] = t5*(t3 + (t4/7.0) + Q[5]*Q[7]);
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 64> nonconservative_matrix_x(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    T t0 = Q[3]*Qaux[0];
+    T t1 = Q[6]*Qaux[0];
+    SimpleArray<T, 64> res;
+    res[0] = 0.0;
+    res[1] = 0.0;
+    res[2] = 0.0;
+    res[3] = 0.0;
+    res[4] = 0.0;
+    res[5] = 0.0;
+    res[6] = 0.0;
+    res[7] = 0.0;
+    res[8] = 0.0;
+    res[9] = 0.0;
+    res[10] = 0.0;
+    res[11] = 0.0;
+    res[12] = 0.0;
+    res[13] = 0.0;
+    res[14] = 0.0;
+    res[15] = 0.0;
+    res[16] = Q[1]*p[0];
+    res[17] = 0.0;
+    res[18] = 0.0;
+    res[19] = 0.0;
+    res[20] = 0.0;
+    res[21] = 0.0;
+    res[22] = 0.0;
+    res[23] = 0.0;
+    res[24] = 0.0;
+    res[25] = 0.0;
+    res[26] = 0.0;
+    res[27] = Qaux[0]*((-Q[2]) + (Q[4]/5.0));
+    res[28] = (-(t0/5.0));
+    res[29] = 0.0;
+    res[30] = 0.0;
+    res[31] = 0.0;
+    res[32] = 0.0;
+    res[33] = 0.0;
+    res[34] = 0.0;
+    res[35] = (-t0);
+    res[36] = (-Qaux[0]*(Q[2] + (Q[4]/7.0)));
+    res[37] = 0.0;
+    res[38] = 0.0;
+    res[39] = 0.0;
+    res[40] = 0.0;
+    res[41] = 0.0;
+    res[42] = 0.0;
+    res[43] = 0.0;
+    res[44] = 0.0;
+    res[45] = 0.0;
+    res[46] = 0.0;
+    res[47] = 0.0;
+    res[48] = 0.0;
+    res[49] = 0.0;
+    res[50] = 0.0;
+    res[51] = Qaux[0]*((-Q[5]) + (Q[7]/5.0));
+    res[52] = (-(t1/5.0));
+    res[53] = 0.0;
+    res[54] = 0.0;
+    res[55] = 0.0;
+    res[56] = 0.0;
+    res[57] = 0.0;
+    res[58] = 0.0;
+    res[59] = (-t1);
+    res[60] = (-Qaux[0]*(Q[5] + (Q[7]/7.0)));
+    res[61] = 0.0;
+    res[62] = 0.0;
+    res[63] = 0.0;
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 64> nonconservative_matrix_y(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    T t0 = Q[3]*Qaux[0];
+    T t1 = Q[6]*Qaux[0];
+    SimpleArray<T, 64> res;
+    res[0] = 0.0;
+    res[1] = 0.0;
+    res[2] = 0.0;
+    res[3] = 0.0;
+    res[4] = 0.0;
+    res[5] = 0.0;
+    res[6] = 0.0;
+    res[7] = 0.0;
+    res[8] = 0.0;
+    res[9] = 0.0;
+    res[10] = 0.0;
+    res[11] = 0.0;
+    res[12] = 0.0;
+    res[13] = 0.0;
+    res[14] = 0.0;
+    res[15] = 0.0;
+    res[16] = 0.0;
+    res[17] = 0.0;
+    res[18] = 0.0;
+    res[19] = 0.0;
+    res[20] = 0.0;
+    res[21] = 0.0;
+    res[22] = 0.0;
+    res[23] = 0.0;
+    res[24] = 0.0;
+    res[25] = 0.0;
+    res[26] = 0.0;
+    res[27] = 0.0;
+    res[28] = 0.0;
+    res[29] = 0.0;
+    res[30] = Qaux[0]*((-Q[2]) + (Q[4]/5.0));
+    res[31] = (-(t0/5.0));
+    res[32] = 0.0;
+    res[33] = 0.0;
+    res[34] = 0.0;
+    res[35] = 0.0;
+    res[36] = 0.0;
+    res[37] = 0.0;
+    res[38] = (-t0);
+    res[39] = (-Qaux[0]*(Q[2] + (Q[4]/7.0)));
+    res[40] = Q[1]*p[0];
+    res[41] = 0.0;
+    res[42] = 0.0;
+    res[43] = 0.0;
+    res[44] = 0.0;
+    res[45] = 0.0;
+    res[46] = 0.0;
+    res[47] = 0.0;
+    res[48] = 0.0;
+    res[49] = 0.0;
+    res[50] = 0.0;
+    res[51] = 0.0;
+    res[52] = 0.0;
+    res[53] = 0.0;
+    res[54] = Qaux[0]*((-Q[5]) + (Q[7]/5.0));
+    res[55] = (-(t1/5.0));
+    res[56] = 0.0;
+    res[57] = 0.0;
+    res[58] = 0.0;
+    res[59] = 0.0;
+    res[60] = 0.0;
+    res[61] = 0.0;
+    res[62] = (-t1);
+    res[63] = (-Qaux[0]*(Q[5] + (Q[7]/7.0)));
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> eigenvalues(
+        const T* Q,
+        const T* Qaux,
+        const T* p,
+        const T* n)
+    {
+    T t0 = std::max((T)1e-14, Q[1]);
+    T t1 = (1.0/(t0));
+    T t2 = std::sqrt((((Q[3]*n[0] + Q[6]*n[1])*(Q[3]*n[0] + Q[6]*n[1])) + (3.0/5.0)*((Q[4]*n[0] + Q[7]*n[1])*(Q[4]*n[0] + Q[7]*n[1])) + (p[0]*std::max((T)0.0, (Q[1]*Q[1]*Q[1]*Q[1]*Q[1]))/(t0*t0))));
+    T t3 = (Q[2]*n[0] + Q[5]*n[1]);
+    T t4 = t1*t3;
+    SimpleArray<T, 8> res;
+    res[0] = 0.0;
+    res[1] = t1*(t3 - t2);
+    res[2] = t1*(t2 + t3);
+    res[3] = t4;
+    res[4] = t4;
+    res[5] = t4;
+    res[6] = t4;
+    res[7] = t4;
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> source(
+        const T* Q,
+        const T* Qaux,
+        const T* p,
+        const T time,
+        const T dt,
+        const T* X)
+    {
+    T t0 = (1.0/(p[2]));
+    T t1 = t0*(Q[2] + Q[3] + Q[4]);
+    T t2 = Qaux[0]*p[1];
+    T t3 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((Qaux[0]*Qaux[0])*((Q[2]*Q[2]) + (Q[5]*Q[5])));
+    T t4 = 4.0*Qaux[0];
+    T t5 = 3.0*t2;
+    T t6 = 12.0*Qaux[0];
+    T t7 = 5.0*t2;
+    T t8 = t0*(Q[5] + Q[6] + Q[7]);
+    SimpleArray<T, 8> res;
+    res[0] = 0.0;
+    res[1] = 0.0;
+    res[2] = ((-Q[2]*t3) - t1*t2 + Q[1]*p[0]*p[4]);
+    res[3] = (-t5*(t1 + Q[3]*t4));
+    res[4] = (-t7*(t1 + Q[4]*t6));
+    res[5] = ((-Q[5]*t3) - t2*t8 + Q[1]*p[0]*p[5]);
+    res[6] = (-t5*(t8 + Q[6]*t4));
+    res[7] = (-t7*(t8 + Q[7]*t6));
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 16> flux(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    T t0 = ((Q[3]*Q[3])/3.0);
+    T t1 = (Q[4]*Q[4]);
+    T t2 = (2.0/5.0)*Q[4];
+    T t3 = 2.0*Qaux[0];
+    T t4 = Q[3]*Q[6];
+    T t5 = Q[4]*Q[7];
+    T t6 = Qaux[0]*((t4/3.0) + (t5/5.0) + Q[2]*Q[5]);
+    T t7 = (2.0/5.0)*Q[7];
+    T t8 = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[3]*t7 + Q[6]*t2);
+    T t9 = Qaux[0]*((2.0/3.0)*t4 + (2.0/7.0)*t5 + Q[2]*Q[7] + Q[4]*Q[5]);
+    T t10 = ((Q[6]*Q[6])/3.0);
+    T t11 = (Q[7]*Q[7]);
+    SimpleArray<T, 16> res;
+    res[0] = 0.0;
+    res[1] = Q[2];
+    res[2] = Qaux[0]*(t0 + (Q[2]*Q[2]) + (t1/5.0));
+    res[3] = Q[3]*t3*(Q[2] + t2);
+    res[4] = t3*(t0 + (t1/7.0) + Q[2]*Q[4]);
+    res[5] = t6;
+    res[6] = t8;
+    res[7] = t9;
+    res[8] = 0.0;
+    res[9] = Q[5];
+    res[10] = t6;
+    res[11] = t8;
+    res[12] = t9;
+    res[13] = Qaux[0]*(t10 + (Q[5]*Q[5]) + (t11/5.0));
+    res[14] = Q[6]*t3*(Q[5] + t7);
+    res[15] = t3*(t10 + (t11/7.0) + Q[5]*Q[7]);
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 128> nonconservative_matrix(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    T t0 = Q[1]*p[0];
+    T t1 = Qaux[0]*((-Q[2]) + (Q[4]/5.0));
+    T t2 = Q[3]*Qaux[0];
+    T t3 = (-(t2/5.0));
+    T t4 = (-t2);
+    T t5 = (-Qaux[0]*(Q[2] + (Q[4]/7.0)));
+    T t6 = Qaux[0]*((-Q[5]) + (Q[7]/5.0));
+    T t7 = Q[6]*Qaux[0];
+    T t8 = (-(t7/5.0));
+    T t9 = (-t7);
+    T t10 = (-Qaux[0]*(Q[5] + (Q[7]/7.0)));
+    SimpleArray<T, 128> res;
+    res[0] = 0.0;
+    res[1] = 0.0;
+    res[2] = 0.0;
+    res[3] = 0.0;
+    res[4] = 0.0;
+    res[5] = 0.0;
+    res[6] = 0.0;
+    res[7] = 0.0;
+    res[8] = 0.0;
+    res[9] = 0.0;
+    res[10] = 0.0;
+    res[11] = 0.0;
+    res[12] = 0.0;
+    res[13] = 0.0;
+    res[14] = 0.0;
+    res[15] = 0.0;
+    res[16] = t0;
+    res[17] = 0.0;
+    res[18] = 0.0;
+    res[19] = 0.0;
+    res[20] = 0.0;
+    res[21] = 0.0;
+    res[22] = 0.0;
+    res[23] = 0.0;
+    res[24] = 0.0;
+    res[25] = 0.0;
+    res[26] = 0.0;
+    res[27] = t1;
+    res[28] = t3;
+    res[29] = 0.0;
+    res[30] = 0.0;
+    res[31] = 0.0;
+    res[32] = 0.0;
+    res[33] = 0.0;
+    res[34] = 0.0;
+    res[35] = t4;
+    res[36] = t5;
+    res[37] = 0.0;
+    res[38] = 0.0;
+    res[39] = 0.0;
+    res[40] = 0.0;
+    res[41] = 0.0;
+    res[42] = 0.0;
+    res[43] = 0.0;
+    res[44] = 0.0;
+    res[45] = 0.0;
+    res[46] = 0.0;
+    res[47] = 0.0;
+    res[48] = 0.0;
+    res[49] = 0.0;
+    res[50] = 0.0;
+    res[51] = t6;
+    res[52] = t8;
+    res[53] = 0.0;
+    res[54] = 0.0;
+    res[55] = 0.0;
+    res[56] = 0.0;
+    res[57] = 0.0;
+    res[58] = 0.0;
+    res[59] = t9;
+    res[60] = t10;
+    res[61] = 0.0;
+    res[62] = 0.0;
+    res[63] = 0.0;
+    res[64] = 0.0;
+    res[65] = 0.0;
+    res[66] = 0.0;
+    res[67] = 0.0;
+    res[68] = 0.0;
+    res[69] = 0.0;
+    res[70] = 0.0;
+    res[71] = 0.0;
+    res[72] = 0.0;
+    res[73] = 0.0;
+    res[74] = 0.0;
+    res[75] = 0.0;
+    res[76] = 0.0;
+    res[77] = 0.0;
+    res[78] = 0.0;
+    res[79] = 0.0;
+    res[80] = 0.0;
+    res[81] = 0.0;
+    res[82] = 0.0;
+    res[83] = 0.0;
+    res[84] = 0.0;
+    res[85] = 0.0;
+    res[86] = 0.0;
+    res[87] = 0.0;
+    res[88] = 0.0;
+    res[89] = 0.0;
+    res[90] = 0.0;
+    res[91] = 0.0;
+    res[92] = 0.0;
+    res[93] = 0.0;
+    res[94] = t1;
+    res[95] = t3;
+    res[96] = 0.0;
+    res[97] = 0.0;
+    res[98] = 0.0;
+    res[99] = 0.0;
+    res[100] = 0.0;
+    res[101] = 0.0;
+    res[102] = t4;
+    res[103] = t5;
+    res[104] = t0;
+    res[105] = 0.0;
+    res[106] = 0.0;
+    res[107] = 0.0;
+    res[108] = 0.0;
+    res[109] = 0.0;
+    res[110] = 0.0;
+    res[111] = 0.0;
+    res[112] = 0.0;
+    res[113] = 0.0;
+    res[114] = 0.0;
+    res[115] = 0.0;
+    res[116] = 0.0;
+    res[117] = 0.0;
+    res[118] = t6;
+    res[119] = t8;
+    res[120] = 0.0;
+    res[121] = 0.0;
+    res[122] = 0.0;
+    res[123] = 0.0;
+    res[124] = 0.0;
+    res[125] = 0.0;
+    res[126] = t9;
+    res[127] = t10;
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 64> source_jacobian_wrt_variables(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    T t0 = (1.0/(p[2]));
+    T t1 = t0*(Q[2] + Q[3] + Q[4]);
+    T t2 = (Qaux[0]*Qaux[0]);
+    T t3 = p[1]*t2;
+    T t4 = (Q[2]*Q[2]);
+    T t5 = (Q[5]*Q[5]);
+    T t6 = (t4 + t5);
+    T t7 = std::sqrt(t2*t6);
+    T t8 = p[0]*(p[3]*p[3]);
+    T t9 = t7*t8;
+    T t10 = (4.0/3.0)*t9*std::pow(Qaux[0], (7.0/3.0));
+    T t11 = (t8/(t7));
+    T t12 = t11*t6*std::pow(Qaux[0], (13.0/3.0));
+    T t13 = t11*std::pow(Qaux[0], (10.0/3.0));
+    T t14 = Qaux[0]*p[1];
+    T t15 = t0*t14;
+    T t16 = (t15 + t9*std::pow(Qaux[0], (4.0/3.0)));
+    T t17 = (-t15);
+    T t18 = (-Q[2]*Q[5]*t13);
+    T t19 = 8.0*Qaux[0];
+    T t20 = 3.0*t3;
+    T t21 = (-3.0*t15);
+    T t22 = (-3.0*t14*(t0 + 4.0*Qaux[0]));
+    T t23 = 24.0*Qaux[0];
+    T t24 = 5.0*t3;
+    T t25 = (-5.0*t15);
+    T t26 = (-5.0*t14*(t0 + 12.0*Qaux[0]));
+    T t27 = t0*(Q[5] + Q[6] + Q[7]);
+    SimpleArray<T, 64> res;
+    res[0] = 0.0;
+    res[1] = 0.0;
+    res[2] = 0.0;
+    res[3] = 0.0;
+    res[4] = 0.0;
+    res[5] = 0.0;
+    res[6] = 0.0;
+    res[7] = 0.0;
+    res[8] = 0.0;
+    res[9] = 0.0;
+    res[10] = 0.0;
+    res[11] = 0.0;
+    res[12] = 0.0;
+    res[13] = 0.0;
+    res[14] = 0.0;
+    res[15] = 0.0;
+    res[16] = 0.0;
+    res[17] = (Q[2]*t10 + Q[2]*t12 + p[0]*p[4] + t1*t3);
+    res[18] = ((-t16) - t13*t4);
+    res[19] = t17;
+    res[20] = t17;
+    res[21] = t18;
+    res[22] = 0.0;
+    res[23] = 0.0;
+    res[24] = 0.0;
+    res[25] = t20*(t1 + Q[3]*t19);
+    res[26] = t21;
+    res[27] = t22;
+    res[28] = t21;
+    res[29] = 0.0;
+    res[30] = 0.0;
+    res[31] = 0.0;
+    res[32] = 0.0;
+    res[33] = t24*(t1 + Q[4]*t23);
+    res[34] = t25;
+    res[35] = t25;
+    res[36] = t26;
+    res[37] = 0.0;
+    res[38] = 0.0;
+    res[39] = 0.0;
+    res[40] = 0.0;
+    res[41] = (Q[5]*t10 + Q[5]*t12 + p[0]*p[5] + t27*t3);
+    res[42] = t18;
+    res[43] = 0.0;
+    res[44] = 0.0;
+    res[45] = ((-t16) - t13*t5);
+    res[46] = t17;
+    res[47] = t17;
+    res[48] = 0.0;
+    res[49] = t20*(t27 + Q[6]*t19);
+    res[50] = 0.0;
+    res[51] = 0.0;
+    res[52] = 0.0;
+    res[53] = t21;
+    res[54] = t22;
+    res[55] = t21;
+    res[56] = 0.0;
+    res[57] = t24*(t27 + Q[7]*t23);
+    res[58] = 0.0;
+    res[59] = 0.0;
+    res[60] = 0.0;
+    res[61] = t25;
+    res[62] = t25;
+    res[63] = t26;
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> source_jacobian_wrt_aux_variables(
+        const T* Q,
+        const T* Qaux,
+        const T* p)
+    {
+    SimpleArray<T, 8> res;
+    res[0] = 0.0;
+    res[1] = 0.0;
+    res[2] = 0.0;
+    res[3] = 0.0;
+    res[4] = 0.0;
+    res[5] = 0.0;
+    res[6] = 0.0;
+    res[7] = 0.0;
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> update_variables(
+        const T* Q,
+        const T* Qaux,
+        const T* p,
+        const T dt)
+    {
+    T t0 = 30.0*std::max((T)0.0, ((-1.0/100.0) + Q[1]));
+    T t1 = (-t0);
+    SimpleArray<T, 8> res;
+    res[0] = Q[0];
+    res[1] = Q[1];
+    res[2] = std::max(t1, std::min(Q[2], t0));
+    res[3] = std::max(t1, std::min(Q[3], t0));
+    res[4] = std::max(t1, std::min(Q[4], t0));
+    res[5] = std::max(t1, std::min(Q[5], t0));
+    res[6] = std::max(t1, std::min(Q[6], t0));
+    res[7] = std::max(t1, std::min(Q[7], t0));
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 1> update_aux_variables(
+        const T* Q,
+        const T* Qaux,
+        const T* p,
+        const T time,
+        const T* X)
+    {
+    SimpleArray<T, 1> res;
+    res[0] = (std::sqrt(2.0)*std::max((T)0.0, Q[1])/std::sqrt(((Q[1]*Q[1]*Q[1]*Q[1]) + (std::max((T)1e-08, Q[1])*std::max((T)1e-08, Q[1])*std::max((T)1e-08, Q[1])*std::max((T)1e-08, Q[1])))));
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> update_aux_variables_jacobian_wrt_variables(
+        const T* Q,
+        const T* Qaux,
+        const T* p,
+        const T time,
+        const T* X)
+    {
+    T t0 = std::max((T)1e-08, Q[1]);
+    T t1 = ((Q[1]*Q[1]*Q[1]*Q[1]) + (t0*t0*t0*t0));
+    SimpleArray<T, 8> res;
+    res[0] = 0.0;
+    res[1] = (std::sqrt(2.0)*((-(2.0*((Q[1]*Q[1]*Q[1]) + (t0*t0*t0)*Heaviside(((-1e-08) + Q[1]), (1.0/2.0)))*std::max((T)0.0, Q[1])/(t1))) + Heaviside(Q[1], (1.0/2.0)))/std::sqrt(t1));
+    res[2] = 0.0;
+    res[3] = 0.0;
+    res[4] = 0.0;
+    res[5] = 0.0;
+    res[6] = 0.0;
+    res[7] = 0.0;
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> initial_condition(
+        const T* X,
+        const T* p)
+    {
+    SimpleArray<T, 8> res;
+    res[0] = 1.0;
+    res[1] = 0.0;
+    res[2] = 0.0;
+    res[3] = 0.0;
+    res[4] = 0.0;
+    res[5] = 0.0;
+    res[6] = 0.0;
+    res[7] = 0.0;
+    return res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 8> boundary_conditions(
+        const int bc_idx,
+        const T* Q,
+        const T* Qaux,
+        const T* p,
+        const T* n,
+        const T* X,
+        const T time,
+        const T dX)
+    {
+    if (bc_idx == 0) {
+        T t0 = (Q[2]*n[0] + Q[5]*n[1]);
+        T t1 = 2.0*n[0];
+        T t2 = (Q[3]*n[0] + Q[6]*n[1]);
+        T t3 = (Q[4]*n[0] + Q[7]*n[1]);
+        T t4 = 2.0*n[1];
+        SimpleArray<T, 8> res;
+        res[0] = Q[0];
+        res[1] = Q[1];
+        res[2] = (Q[2] - t0*t1);
+        res[3] = (Q[3] - t1*t2);
+        res[4] = (Q[4] - t1*t3);
+        res[5] = (Q[5] - t0*t4);
+        res[6] = (Q[6] - t2*t4);
+        res[7] = (Q[7] - t3*t4);
+        return res;
+    }
+    SimpleArray<T, 8> default_res = {0};
+    return default_res;
+    }
+
+    PORTABLE_FN static inline SimpleArray<T, 1> aux_boundary_conditions(
+        const int bc_idx,
+        const T* Q,
+        const T* Qaux,
+        const T* p,
+        const T* n,
+        const T* X,
+        const T time,
+        const T dX)
+    {
+    if (bc_idx == 0) {
+        SimpleArray<T, 1> res;
+        res[0] = Qaux[0];
+        return res;
+    }
+    SimpleArray<T, 1> default_res = {0};
+    return default_res;
+    }
+
+};

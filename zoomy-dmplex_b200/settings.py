@@ -1,0 +1,100 @@
+"""The solver subset of the reference's JSON settings.
+
+Mirrors ``Settings::from_json`` (reference ``Settings.hpp:73-138``) for the
+keys that change the SME step, with the same defaults, plus the model
+parameter overrides by name (``VirtualSolver.hpp:199-217``).  Two keys are
+additions of this implementation: ``solver.gradient`` (``"least_squares"``,
+the default, or ``"green_gauss"``, the gradient the reference's MUSCL path
+installs, ``ModularSolver.hpp:62-67``) and ``solver.block_size``.
+
+How the reference interprets the strings, and so how they map here:
+* ``limiter``: only ``"none"`` changes anything; every other value (including
+  the default ``"venkatakrishnan"``) installs Vacuum + TVD limiting through
+  the backward-compatible ``LinearReconstructor`` constructor
+  (``MUSCLSolver.hpp:43``, ``Reconstruction.hpp:170-175``);
+* ``time_integration``: ``"splitting"`` (explicit transport + implicit source)
+  is the only strategy of this path; ``"imex"``/``"implicit"`` are rejected;
+* ``positivity``: ``"none"`` only (``"zhang_shu"``/``"mood"`` are rejected).
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+from typing import Dict, Optional
+
+from . import native
+
+
+@dataclasses.dataclass
+class SolverSettings:
+    t_end: float = 1.0
+    cfl: float = 0.5
+    reconstruction_order: int = 1
+    min_dt: float = 1.0e-12
+    limiter: str = "venkatakrishnan"
+    time_integration: str = "splitting"
+    positivity: str = "none"
+    wet_dry_eps: float = 1.0e-2
+    ssp_stages: int = 5
+    gradient: str = "least_squares"
+    block_size: int = 0
+
+    def to_struct(self) -> native.ZsmeSettings:
+        if self.time_integration != "splitting":
+            raise ValueError("time_integration %r is not on this path (only 'splitting')"
+                             % self.time_integration)
+        if self.positivity != "none":
+            raise ValueError("positivity %r is not supported (only 'none')" % self.positivity)
+        if self.gradient not in ("least_squares", "green_gauss"):
+            raise ValueError("gradient must be 'least_squares' or 'green_gauss'")
+        if self.reconstruction_order >= 2 and self.ssp_stages < 2:
+            raise ValueError("ssp_stages must be >= 2")
+        s = native.ZsmeSettings()
+        s.cfl, s.t_end, s.min_dt = self.cfl, self.t_end, self.min_dt
+        s.reconstruction_order = int(self.reconstruction_order)
+        s.limiter = native.ZSME_LIMITER_NONE if self.limiter == "none" else native.ZSME_LIMITER_TVD
+        s.gradient = (native.ZSME_GRADIENT_LSQ if self.gradient == "least_squares"
+                      else native.ZSME_GRADIENT_GREEN_GAUSS)
+        s.ssp_stages = int(self.ssp_stages)
+        s.source = 1
+        s.block_size = int(self.block_size)
+        return s
+
+
+@dataclasses.dataclass
+class Settings:
+    name: str = "Simulation"
+    solver: SolverSettings = dataclasses.field(default_factory=SolverSettings)
+    parameters: Dict[str, float] = dataclasses.field(default_factory=dict)
+
+    @staticmethod
+    def from_dict(j: dict) -> "Settings":
+        s = Settings(name=j.get("name", "Simulation"))
+        js = j.get("solver", {})
+        d = SolverSettings()
+        for f in dataclasses.fields(SolverSettings):
+            if f.name in js:
+                setattr(d, f.name, type(getattr(d, f.name))(js[f.name]))
+        s.solver = d
+        for k, v in j.get("model", {}).get("parameters", {}).items():
+            if isinstance(v, (int, float)):
+                s.parameters[k] = float(v)
+        return s
+
+    @staticmethod
+    def from_json(path: str) -> "Settings":
+        with open(path) as f:
+            return Settings.from_dict(json.load(f))
+
+
+def resolve_parameters(names, defaults, overrides: Optional[Dict[str, float]]):
+    """Model parameter vector with overrides by name; unknown names are
+    reported and ignored, as the reference does."""
+    p = [float(v) for v in defaults]
+    unknown = []
+    for k, v in (overrides or {}).items():
+        if k in names:
+            p[names.index(k)] = float(v)
+        else:
+            unknown.append(k)
+    return p, unknown
