@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Benchmark of the SME time step (cell-steps/s and fraction of the HBM
+roofline).
+
+Workload (default): SME level 4 (12 FP64 state slots) on the Hilbert-
+renumbered Delaunay mesh of a 1400x1400 jittered grid (3.91M triangles),
+16-Gaussian bathymetry, Navier-slip source; order 2 (least squares + Vacuum/
+TVD limiting), SSP-RK2, CFL 0.45.  A "step" is one full time step (two SSP
+stages, constraints, implicit source, CFL dt).  Inputs (375 MB of state +
+1.1 GB of face states) exceed the 126 MB L2, so no flush is needed between
+steps.
+
+Launch: ``python bench.py [--gpus N --steps K --warmup W]``; for N > 1 one
+rank per GPU under torchrun, each rank advancing its own replica (the single
+mesh is not partitioned: replicas, weak scaling).  ``--impl reference`` times
+the CPU restatement of the reference step (the oracle) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SME cell-steps/s & % HBM roofline"
+UNIT = "cell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--side", type=int, default=1400, help="jittered grid side of the mesh")
+    ap.add_argument("--cpu-side", type=int, default=300, help="grid side of the bounded CPU sample")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ roofline
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(kind, C, F, nq, na, K, stages):
+    """Compulsory HBM bytes of one launch of each kernel when every array it
+    touches is read or written exactly once (neighbour re-reads are free)."""
+    d = 2
+    if kind == "prep":
+        return C * (8 * nq + 8 * na + 4 * K + 4 * K + 8 * d * K + 8 * d * K + 8 * K * nq)
+    if kind == "flux":
+        state_passes = (2 * (stages - 1) + 3) / stages      # FIRST/MID: in+out, FINAL: in+base+out
+        return (C * (8 * K * nq + 12 * K + 4 + 8 * na + 8 + 8 * nq * state_passes)
+                + F * (8 * d + 8 + 8 * d))
+    if kind == "finalize":
+        return C * (16 * nq + 16 * na + 8)
+    return 0.0
+
+
+def step_bytes_survey(nq):
+    """Per cell-step bytes of a fully fused SSP-RK2 step (5 m_e + 2 state
+    arrays + 304 B of geometry, m_e = evolving variables)."""
+    me = nq - 1
+    return 8 * (5 * me + 2) + 304
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for ln in self.lines:
+            v = [x.strip() for x in ln.split(",")]
+            if len(v) >= 9:
+                rows.append(v)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ cases
+def params_of(case):
+    from zoomy_dmplex_b200 import models
+
+    names, vals = models.parameter_table(case.model)
+    for k, v in case.params.items():
+        vals[names.index(k)] = v
+    return np.array(vals)
+
+
+def cpu_sample(side, steps, warm=1):
+    """The oracle (CPU restatement of the reference step) on a bounded
+    sample of the workload: same model and physics on a side x side mesh."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as O
+    from zoomy_dmplex_b200 import cases
+
+    c = cases.roofline_l4(side)
+    nt = O.set_threads(0)
+    o = O.Oracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), params_of(c))
+    o.set_state(c.q0)
+    o.step(warm)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    return c.mesh.n_cells * steps / dt, nt, c.mesh.n_cells, dt
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        # warmup + K timed oracle steps on the bounded sample
+        v, nt, C, dt = cpu_sample(a.cpu_side, max(1, a.steps), warm=max(1, a.warmup))
+        line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / max(1, a.steps),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": "sme2d_l4 jittered-Delaunay %dx%d (%d cells) order 2 LSQ+TVD SSP-RK2"
+                           % (a.cpu_side, a.cpu_side, C), "parallelism": "host threads"},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
+                                 "sample": "%d steps of the CPU restatement on a %dx%d-grid mesh (%d cells)"
+                                           % (a.steps, a.cpu_side, a.cpu_side, C)},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+
+    from zoomy_dmplex_b200 import cases, native
+    from zoomy_dmplex_b200.solver import Solver
+
+    case = cases.roofline_l4(a.side)
+    C, F = case.mesh.n_cells, case.mesh.n_faces
+    g = Solver(case.model, case.mesh, case.settings, params_of(case), device=dev)
+    g.set_state(case.q0)
+    nq, na = g.nq, g.naux
+    stream = torch.cuda.ExternalStream(g.stream, device=dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    # warm-up (graph path, then the profiled path once)
+    g.step(a.warmup)
+    g.set_profiling(True)
+    g.step(1)
+    g.sync()
+    g.set_profiling(True)           # reset counters
+
+    clk = ClockSampler(dev)
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.step(a.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    diag = g.sync(check=True)
+    prof = g.read_profile()
+    g.set_profiling(False)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = C * a.steps * world / (ms_max / 1e3)
+
+    # roofline of the dominant kernel (algorithmic bytes / live average duration)
+    hbm, peak_src = peaks()
+    dom = max((k for k in prof if prof[k][1] > 0), key=lambda k: prof[k][0])
+    dom_ms = prof[dom][0] / prof[dom][1]
+    alg = algorithmic_bytes(dom, C, F, nq, na, case.mesh.max_faces, case.settings.ssp_stages)
+    achieved = alg / (dom_ms / 1e3) / 1e9
+    traffic = load_traffic().get("%s/%s" % (case.model, dom))
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg,
+                "traffic": (traffic["dram_bytes_per_cell"] * C) if traffic else None,
+                "kernel_ms": dom_ms}
+    step_ms = ms_max / a.steps
+    sb = step_bytes_survey(nq)
+    roofline_step = {"bytes_per_cell_step": sb, "achieved": sb * C / (step_ms / 1e3) / 1e9, "peak": hbm,
+                     "unit": "GB/s", "frac": sb * C / (step_ms / 1e3) / 1e9 / hbm}
+    kernel_share = {k: {"ms_per_launch": v[0] / v[1], "launches": v[1], "share": v[0] / max(1e-30, sum(
+        x[0] for x in prof.values()))} for k, v in prof.items() if v[1]}
+
+    # end to end through the public API: pinned host state in, one step, state out
+    ne = a.e2e_steps or a.steps
+    q_host = torch.from_numpy(np.ascontiguousarray(case.q0)).pin_memory()
+    out_host = torch.empty_like(q_host).pin_memory()
+    lib = native.load()
+    import ctypes as ct
+
+    qp = ct.cast(q_host.data_ptr(), ct.POINTER(ct.c_double))
+    op = ct.cast(out_host.data_ptr(), ct.POINTER(ct.c_double))
+    native.check(lib.zsme_set_state(g.h, qp, 0.0))
+    g.step(1)
+    native.check(lib.zsme_get_state(g.h, op))
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(ne):
+        native.check(lib.zsme_set_state(g.h, qp, 0.0))
+        native.check(lib.zsme_step(g.h, 1))
+        native.check(lib.zsme_get_state(g.h, op))
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t2 = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = C * ne * world / (float(t2.item()) / 1e3)
+    nbytes = C * nq * 8
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "sme2d_l4 SME level 4, jittered-Delaunay %dx%d grid (%d cells, %d faces), "
+                                   "Hilbert-renumbered, order 2 LSQ + Vacuum/TVD, SSP-RK2, CFL 0.45, "
+                                   "Navier-slip Newton source" % (a.side, a.side, C, F),
+                       "model": case.model, "cells": C, "faces": F, "n_dof_q": nq,
+                       "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
+                       "l2_flush": "not needed: state %.0f MB + face states %.0f MB > 126 MB L2"
+                                   % (C * nq * 8 / 1e6, C * nq * 3 * 8 / 1e6),
+                       "timing": "CUDA events on the solver stream around K steps; per-kernel events inside"},
+            "roofline": roofline, "roofline_step": roofline_step, "kernels": kernel_share,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                    "steps": ne, "api": "zsme_set_state(pinned host) + zsme_step(1) + zsme_get_state(pinned host)"},
+            "gpu_launches": a.steps * g.launches_per_step(),
+            "diag": {"nonfinite": diag.n_nonfinite, "negative_depth": diag.n_negative_depth,
+                     "newton_unconverged": diag.n_newton_unconverged},
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        v, nt, Cs, dts = cpu_sample(a.cpu_side, a.cpu_steps)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
+                                "sample": "%d steps of the CPU restatement (oracle) of the same model on a "
+                                          "%dx%d-grid mesh (%d cells), %.1f s" % (a.cpu_steps, a.cpu_side,
+                                                                                 a.cpu_side, Cs, dts)}
+    if rank == 0:
+        print(json.dumps(line))
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

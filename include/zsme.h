@@ -149,8 +149,21 @@ int zsme_get_time(zsme_handle* h, double* t, double* dt);
 int zsme_set_params(zsme_handle* h, const double* params);
 /* The CUDA stream (cudaStream_t) the handle launches on. */
 void* zsme_stream(zsme_handle* h);
-/* Kernel launches issued by the last zsme_step call (per step). */
+/* Kernel launches of one zsme_step step. */
 int zsme_launches_per_step(zsme_handle* h, int32_t* n);
+
+/* Per-kernel CUDA-event timing.  While enabled, zsme_step launches without
+ * the CUDA graph, brackets every kernel with events on the handle's stream
+ * and, at the end of each call, accumulates the durations per kind. */
+#define ZSME_KERNEL_BEGIN 0     /* begin_step: dt clamp to t_end */
+#define ZSME_KERNEL_PREP 1      /* clamp + bounds + gradient + face states */
+#define ZSME_KERNEL_FLUX 2      /* face fluxes + stage update */
+#define ZSME_KERNEL_FINALIZE 3  /* constraints + source + CFL partials */
+#define ZSME_KERNEL_END 4       /* dt reduction + time advance */
+#define ZSME_KERNEL_KINDS 5
+int zsme_set_profiling(zsme_handle* h, int enable);
+/* ms[ZSME_KERNEL_KINDS]: summed milliseconds; n[...]: launches. */
+int zsme_read_profile(zsme_handle* h, double* ms, int64_t* n);
 
 #ifdef __cplusplus
 }

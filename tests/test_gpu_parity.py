@@ -1,0 +1,211 @@
+"""GPU step (libzsme.so, through the C ABI) against the CPU oracle.
+
+Bar: per-step relative L2 and relative max error of h and of every moment
+<= 1e-12 (TOL).  The kernels are compiled without FMA contraction, so for
+models whose plugins use only + - * / sqrt the two sides round identically
+and the results are expected to be bit-identical; Manning friction calls
+cbrt, whose last bit may differ between CUDA and glibc.
+"""
+import numpy as np
+import pytest
+
+import oracle_py as O
+from zoomy_dmplex_b200 import cases, mesh as M, models
+from zoomy_dmplex_b200.solver import Solver
+
+TOL = 1e-12
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _threads():
+    O.set_threads(0)
+
+
+def params(model, d):
+    names, vals = models.parameter_table(model)
+    for k, v in d.items():
+        vals[names.index(k)] = v
+    return np.array(vals)
+
+
+def pair(case, **kw):
+    s = cases.default_settings(**kw)
+    p = params(case.model, case.params)
+    g = Solver(case.model, case.mesh, s, p)
+    o = O.Oracle(case.model, case.mesh.as_abi_arrays(), s.to_struct(), p)
+    g.set_state(case.q0)
+    o.set_state(case.q0)
+    return g, o
+
+
+def errs(a, b):
+    """per-variable relative L2 and relative max error of a vs reference b."""
+    out = []
+    for i in range(b.shape[1]):
+        nb = np.linalg.norm(b[:, i])
+        mb = np.abs(b[:, i]).max()
+        e = a[:, i] - b[:, i]
+        out.append((np.linalg.norm(e) / nb if nb > 0 else np.linalg.norm(e),
+                    np.abs(e).max() / mb if mb > 0 else np.abs(e).max()))
+    return np.array(out)
+
+
+def assert_close(a, b, tol=TOL, what=""):
+    e = errs(a, b)
+    assert np.all(np.isfinite(a)), what
+    assert e.max() <= tol, "%s: per-variable (relL2, relmax) = %s" % (what, e)
+
+
+def case_1d():
+    m = M.interval(np.linspace(-1.5, 1.5, 301))
+    x = m.cell_centroid[:, 0]
+    b = 0.2 * np.exp(-x ** 2 / 0.05)
+    h = 1.0 - b + 0.1 * np.exp(-(x + 0.5) ** 2 / 0.01)
+    q = np.stack([b, h, 0.3 * h], axis=1)
+    return cases.Case("1d", "sme1d_l0_malpasset", m, q, cases.default_settings(),
+                      dict(g=9.81, rho=1.0, nu=1.0, lambda_s=0.2, e_x=0.01), 50)
+
+
+def small_cases():
+    return {
+        "l0": cases.plain_l0(40),
+        "l1": cases.adjoint_l1(40),
+        "l2": cases.level2(40),
+        "l4": cases.roofline_l4(40),
+        "1d": case_1d(),
+    }
+
+
+CASES = small_cases()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("order,grad", [(1, "least_squares"), (2, "least_squares"), (2, "green_gauss")])
+def test_rhs_one_step_map(name, order, grad):
+    c = CASES[name]
+    g, o = pair(c, reconstruction_order=order, gradient=grad)
+    rng = np.random.default_rng(5)
+    x = c.q0.copy()
+    x[:, 2:] += 0.05 * rng.standard_normal(x[:, 2:].shape) * x[:, 1:2]
+    fg, fo = g.rhs(x), o.rhs(x)
+    assert_close(fg, fo, what="rhs %s o%d %s" % (name, order, grad))
+
+
+@pytest.mark.parametrize("name", ["l2", "l4", "1d"])
+def test_rhs_bitwise_without_cbrt(name):
+    """No FMA contraction + IEEE sqrt/div: identical rounding."""
+    c = CASES[name]
+    g, o = pair(c)
+    x = c.q0.copy()
+    x[:, 2] += 0.01
+    assert np.array_equal(g.rhs(x), o.rhs(x))
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_constraints_source_dt(name):
+    c = CASES[name]
+    g, o = pair(c)
+    assert_close(g.get_state(), o.get_state(), what="set_state constraints")
+    assert_close(g.get_aux(), o.get_aux(), what="aux")
+    dg, do = g.compute_dt(), o.compute_dt()
+    assert abs(dg - do) <= TOL * do
+    g.source(5e-3)
+    o.source(5e-3)
+    assert_close(g.get_state(), o.get_state(), what="source")
+    g.update_state()
+    o.update_state()
+    assert_close(g.get_state(), o.get_state(), what="update_state")
+
+
+@pytest.mark.parametrize("name,steps", [("l0", 200), ("l1", 60), ("l2", 60), ("l4", 30), ("1d", 100)])
+def test_trajectory_per_step(name, steps):
+    """Free-running oracle; the GPU takes the oracle's dt each step; every
+    step is compared."""
+    c = CASES[name]
+    g, o = pair(c)
+    worst = 0.0
+    for k in range(steps):
+        _, dt = o.time()
+        o.step(1)
+        g.step(1, dts=[dt])
+        qg, qo = g.get_state(), o.get_state()
+        e = errs(qg, qo).max()
+        worst = max(worst, e)
+        assert e <= TOL, "step %d: %g" % (k, e)
+        assert qg[:, 1].min() >= 0.0
+    d = g.sync()
+    assert d.n_nonfinite == 0 and d.n_negative_depth == 0
+
+
+@pytest.mark.parametrize("name", ["l0", "l2"])
+def test_free_running_dt_and_state(name):
+    """Both sides choose their own CFL dt (device-side reduction, CUDA graph)."""
+    c = CASES[name]
+    g, o = pair(c)
+    n = 50
+    g.step(n)
+    o.step(n)
+    tg, dtg = g.time()
+    to, dto = o.time()
+    assert abs(tg - to) <= TOL * to and abs(dtg - dto) <= TOL * dto
+    assert_close(g.get_state(), o.get_state(), what="free run")
+
+
+def test_t_end_landing():
+    c = CASES["l0"]
+    s = cases.default_settings(t_end=0.0123)
+    p = params(c.model, c.params)
+    g = Solver(c.model, c.mesh, s, p)
+    o = O.Oracle(c.model, c.mesh.as_abi_arrays(), s.to_struct(), p)
+    g.set_state(c.q0)
+    o.set_state(c.q0)
+    g.step(500)           # steps past t_end are no-ops
+    o.step(500)
+    assert g.time()[0] == pytest.approx(0.0123, abs=1e-15)
+    assert_close(g.get_state(), o.get_state(), what="t_end")
+
+
+def test_deterministic_bitwise():
+    c = CASES["l4"]
+    outs = []
+    for _ in range(2):
+        g, _o = pair(c)
+        g.step(10)
+        outs.append(g.get_state())
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_lake_at_rest_first_order_gpu():
+    c = cases.plain_l0(40)
+    c.q0[:, 1] = 1.0 - c.q0[:, 0]
+    g, _ = pair(c, reconstruction_order=1)
+    g.step(50)
+    q = g.get_state()
+    assert np.abs(q[:, 0] + q[:, 1] - 1.0).max() < 1e-14
+    assert np.abs(q[:, 2:]).max() < 1e-14
+
+
+def test_config0_full_run():
+    """Configuration 0 as specified: 60x60 jittered grid, 200 steps."""
+    c = cases.plain_l0(60)
+    g, o = pair(c)
+    g.step(200)
+    o.step(200)
+    assert_close(g.get_state(), o.get_state(), what="config 0, 200 steps")
+    q = g.get_state()
+    assert q[:, 1].min() >= 0
+    vol = c.mesh.cell_volume
+    assert abs((q[:, 1] * vol).sum() - (c.q0[:, 1] * vol).sum()) < 1e-13
+
+
+def test_device_pointer_state_roundtrip():
+    torch = pytest.importorskip("torch")
+    c = CASES["l2"]
+    g, _ = pair(c)
+    t = torch.tensor(c.q0, dtype=torch.float64, device="cuda")
+    g.set_state_device(t.data_ptr())
+    out = torch.empty_like(t)
+    g.get_state_device(out.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), g.get_state())

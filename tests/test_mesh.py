@@ -1,0 +1,68 @@
+import numpy as np
+
+from zoomy_dmplex_b200 import mesh as M
+
+
+def _closure(m):
+    C = m.n_cells
+    s = np.zeros((C, 2))
+    for k in range(m.max_faces):
+        f = m.cell_faces[:, k]
+        sign = np.where(m.face_cells[f, 0] == np.arange(C), 1.0, -1.0)
+        s += sign[:, None] * m.face_normal[f]
+    return np.abs(s).max()
+
+
+def test_jittered_square_geometry():
+    m = M.jittered_square(30, seed=3)
+    assert m.n_cells == 2 * 29 * 29
+    assert abs(m.cell_volume.sum() - 1.0) < 1e-12
+    assert (m.cell_volume > 0).all()
+    assert _closure(m) < 1e-14                      # closed cells
+    # normals point from support[0] to support[1] / outwards
+    d = m.face_centroid - m.cell_centroid[m.face_cells[:, 0]]
+    assert ((d * m.face_normal).sum(1) > 0).all()
+    # Euler: F = C + V - 1 for a disc-like triangulation
+    assert m.n_faces == m.n_cells + m.vertices.shape[0] - 1
+    bnd = m.face_cells[:, 1] < 0
+    assert (m.face_bc[bnd] == 0).all() and (m.face_bc[~bnd] == -1).all()
+    assert abs(np.linalg.norm(m.face_normal[bnd], axis=1).sum() - 4.0) < 1e-12
+
+
+def test_face_numbering_first_encounter():
+    m = M.jittered_square(12, seed=0)
+    # support[0] is the first cell that lists the face
+    first = np.full(m.n_faces, -1)
+    for c in range(m.n_cells):
+        for f in m.cell_faces[c]:
+            if first[f] < 0:
+                first[f] = c
+    assert (first == m.face_cells[:, 0]).all()
+    # faces are numbered in first-encounter order
+    order = [f for c in range(m.n_cells) for f in m.cell_faces[c]]
+    seen = []
+    for f in order:
+        if f not in seen:
+            seen.append(f)
+    assert seen == list(range(m.n_faces))
+
+
+def test_neighbours_cone_order():
+    m = M.jittered_square(10, seed=1)
+    nb = m.cell_nbrs()
+    for c in range(m.n_cells):
+        want = [int(m.face_cells[f, 1] if m.face_cells[f, 0] == c else m.face_cells[f, 0])
+                for f in m.cell_faces[c]]
+        want = [v for v in want if v >= 0]
+        assert list(nb[c][: len(want)]) == want
+
+
+def test_interval_and_msh_roundtrip(tmp_path):
+    m = M.interval(np.linspace(0, 1, 11))
+    assert m.n_cells == 10 and m.n_faces == 11 and m.dim == 1
+    assert np.allclose(np.abs(m.face_normal[:, 0]), 1.0)
+    m2 = M.jittered_square(8, seed=2)
+    p = tmp_path / "m.msh"
+    M.write_msh(str(p), m2)
+    m3 = M.read_msh(str(p))
+    assert m3.n_cells == m2.n_cells and np.allclose(m3.cell_volume.sum(), 1.0)

@@ -1,0 +1,133 @@
+"""The benchmark cases: seeded synthetic meshes, initial conditions and
+settings of the five configurations (SME level 0 plain, level 2, level 4 at
+roofline size, the level-2 ensemble and the level-1 adjoint case).
+
+The reference projects its initial condition onto cell centroids
+(``VirtualSolver.hpp:258-281``); here the initial state is evaluated at the
+centroids in numpy.  State layout: ``[b, h, hu_0..hu_L, hv_0..hv_L]``.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import mesh as meshmod
+from .settings import SolverSettings
+
+
+def _gauss(x, y, cx, cy, w2):
+    return np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / w2)
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    model: str
+    mesh: meshmod.Mesh
+    q0: np.ndarray
+    settings: SolverSettings
+    params: Dict[str, float]
+    steps: int
+
+
+def _state(level, h, b, hu=None, hv=None):
+    C = h.size
+    nm = level + 1
+    q = np.zeros((C, 2 + 2 * nm))
+    q[:, 0] = b
+    q[:, 1] = h
+    if hu is not None:
+        for k, v in enumerate(hu):
+            q[:, 2 + k] = v
+    if hv is not None:
+        for k, v in enumerate(hv):
+            q[:, 2 + nm + k] = v
+    return q
+
+
+def default_settings(**kw) -> SolverSettings:
+    s = SolverSettings(t_end=1e9, cfl=0.45, reconstruction_order=2, limiter="tvd", ssp_stages=2,
+                       gradient="least_squares")
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def plain_l0(n: int = 60, seed: int = 0, steps: int = 200) -> Case:
+    """SME level 0 (shallow water), hump over a Gaussian bump, Manning n=0.03."""
+    m = meshmod.jittered_square(n, seed=seed)
+    x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
+    b = 0.2 * _gauss(x, y, 0.5, 0.5, 0.01)
+    h = 1.0 - b + 0.05 * _gauss(x, y, 0.3, 0.3, 0.005)
+    q = _state(0, h, b)
+    return Case("plain_l0_%d" % n, "sme2d_l0", m, q, default_settings(),
+                dict(g=9.81, n_manning=0.03, nu=0.0), steps)
+
+
+def level2(n: int = 240, seed: int = 1, steps: int = 500) -> Case:
+    """SME level 2: same bathymetry and hump, u = 0.5, alpha_1 = 0.1,
+    Navier slip lambda = 0.1, nu = 1e-3."""
+    m = meshmod.jittered_square(n, seed=seed)
+    x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
+    b = 0.2 * _gauss(x, y, 0.5, 0.5, 0.01)
+    h = 1.0 - b + 0.05 * _gauss(x, y, 0.3, 0.3, 0.005)
+    q = _state(2, h, b, hu=[0.5 * h, 0.1 * h, 0 * h], hv=[0 * h] * 3)
+    return Case("level2_%d" % n, "sme2d_l2", m, q, default_settings(),
+                dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), steps)
+
+
+def roofline_l4(n: int = 1400, seed: int = 2, steps: int = 100, m: Optional[meshmod.Mesh] = None) -> Case:
+    """SME level 4 at roofline size: bathymetry = 16 seeded Gaussians
+    (amplitude U[0.02,0.1], width U[0.02,0.08], centre U[0,1]^2),
+    h = 1 - b + U(+-0.01), alpha_1 ~ U[0, 0.05], other moments 0."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.02, 0.1, 16)
+    wid = rng.uniform(0.02, 0.08, 16)
+    cen = rng.uniform(0.0, 1.0, (16, 2))
+    if m is None:
+        m = meshmod.jittered_square(n, seed=seed)
+    x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
+    b = np.zeros_like(x)
+    for a, w, c in zip(amp, wid, cen):
+        b += a * _gauss(x, y, c[0], c[1], w * w)
+    h = 1.0 - b + rng.uniform(-0.01, 0.01, x.size)
+    a1 = rng.uniform(0.0, 0.05, x.size)
+    q = _state(4, h, b, hu=[0 * h, a1 * h] + [0 * h] * 3, hv=[0 * h] * 5)
+    return Case("roofline_l4_%d" % n, "sme2d_l4", m, q, default_settings(),
+                dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), steps)
+
+
+def ensemble_member(i: int, seed: int = 3, side_range=(40, 400)) -> Case:
+    """Instance i of the level-2 ensemble: grid side log-uniform in
+    [40, 400], 1-4 Gaussian bumps (amplitude U[0.05,0.2], width
+    U[0.005,0.03]), one hump (amplitude U[0.01,0.1])."""
+    rng = np.random.default_rng([seed, i])
+    side = int(round(np.exp(rng.uniform(np.log(side_range[0]), np.log(side_range[1])))))
+    m = meshmod.jittered_square(side, seed=int(rng.integers(1 << 30)))
+    x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
+    b = np.zeros_like(x)
+    for _ in range(int(rng.integers(1, 5))):
+        a, w2 = rng.uniform(0.05, 0.2), rng.uniform(0.005, 0.03)
+        c = rng.uniform(0.2, 0.8, 2)
+        b += a * _gauss(x, y, c[0], c[1], w2)
+    c = rng.uniform(0.2, 0.8, 2)
+    h = 1.0 - b + rng.uniform(0.01, 0.1) * _gauss(x, y, c[0], c[1], 0.005)
+    q = _state(2, h, b, hu=[0 * h] * 3, hv=[0 * h] * 3)
+    return Case("ensemble_%d" % i, "sme2d_l2", m, q, default_settings(),
+                dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), 200)
+
+
+def adjoint_l1(n: int = 200, seed: int = 4, steps: int = 400, target: bool = False) -> Case:
+    """SME level 1 adjoint case: b = 0.2 bump; the target run perturbs b by
+    +0.02 exp(-((x-0.6)^2+(y-0.4)^2)/0.01); Manning n = 0.03."""
+    m = meshmod.jittered_square(n, seed=seed)
+    x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
+    b = 0.2 * _gauss(x, y, 0.5, 0.5, 0.01)
+    if target:
+        b = b + 0.02 * _gauss(x, y, 0.6, 0.4, 0.01)
+    h = 1.0 - b + 0.05 * _gauss(x, y, 0.3, 0.3, 0.005)
+    q = _state(1, h, b, hu=[0 * h] * 2, hv=[0 * h] * 2)
+    return Case("adjoint_l1_%d" % n, "sme2d_l1", m, q, default_settings(),
+                dict(g=9.81, n_manning=0.03, nu=0.0), steps)

@@ -1,0 +1,202 @@
+// C ABI of the library (include/zsme.h): model registry, argument checks,
+// error reporting.  Each entry point forwards to the model's Solver.
+#include <cstring>
+#include <string>
+
+#include "prepared_mesh.h"
+#include "zsme.h"
+
+#define ZSME_MODELS(X) X(sme1d_l0_malpasset) X(sme2d_l0) X(sme2d_l1) X(sme2d_l2) X(sme2d_l4)
+
+#define ZSME_DECLARE(NS) zsme::SolverBase* zsme_make_##NS(); void zsme_info_##NS(int* v);
+ZSME_MODELS(ZSME_DECLARE)
+
+namespace zsme {
+
+namespace {
+thread_local std::string g_err = "";
+
+struct ModelEntry {
+    const char* name;
+    SolverBase* (*make)();
+    void (*info)(int*);
+};
+#define ZSME_ENTRY(NS) ModelEntry{#NS, &zsme_make_##NS, &zsme_info_##NS},
+const ModelEntry kModels[] = {ZSME_MODELS(ZSME_ENTRY)};
+const int kNumModels = sizeof(kModels) / sizeof(kModels[0]);
+
+const ModelEntry* find_model(const char* name) {
+    if (!name) return nullptr;
+    for (const auto& e : kModels)
+        if (!std::strcmp(e.name, name)) return &e;
+    return nullptr;
+}
+}  // namespace
+
+int set_error(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+}  // namespace zsme
+
+struct zsme_handle {
+    zsme::SolverBase* s;
+};
+
+using zsme::set_error;
+
+#define CHECK_H(h)                                                          \
+    do {                                                                    \
+        if (!(h) || !(h)->s) return set_error(ZSME_ERR_ARG, "null handle"); \
+    } while (0)
+
+extern "C" {
+
+const char* zsme_version(void) { return "zsme 0.1 (sm_100a, FP64)"; }
+const char* zsme_last_error(void) { return zsme::g_err.c_str(); }
+int zsme_num_models(void) { return zsme::kNumModels; }
+const char* zsme_model_name(int i) { return (i >= 0 && i < zsme::kNumModels) ? zsme::kModels[i].name : nullptr; }
+
+int zsme_model_info(const char* model, int32_t* nq, int32_t* na, int32_t* np, int32_t* dim) {
+    const auto* e = zsme::find_model(model);
+    if (!e) return set_error(ZSME_ERR_MODEL, std::string("unknown model: ") + (model ? model : "(null)"));
+    int v[4];
+    e->info(v);
+    if (nq) *nq = v[0];
+    if (na) *na = v[1];
+    if (np) *np = v[2];
+    if (dim) *dim = v[3];
+    return ZSME_OK;
+}
+
+int zsme_create(const char* model, const zsme_mesh* mesh, const zsme_settings* settings, const double* params,
+                int device, zsme_handle** out) {
+    if (!out || !mesh || !settings) return set_error(ZSME_ERR_ARG, "null argument");
+    *out = nullptr;
+    const auto* e = zsme::find_model(model);
+    if (!e) return set_error(ZSME_ERR_MODEL, std::string("unknown model: ") + (model ? model : "(null)"));
+    if (settings->reconstruction_order < 1 || settings->reconstruction_order > 2)
+        return set_error(ZSME_ERR_ARG, "reconstruction_order must be 1 or 2");
+    if (!(settings->cfl > 0)) return set_error(ZSME_ERR_ARG, "cfl must be > 0");
+    zsme::PreparedMesh pm;
+    int rc = zsme::prepare_mesh(*mesh, pm);
+    if (rc) return rc;
+    zsme::SolverBase* s = e->make();
+    rc = s->init(std::move(pm), *settings, params, device);
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    *out = new zsme_handle{s};
+    return ZSME_OK;
+}
+
+int zsme_destroy(zsme_handle* h) {
+    if (!h) return ZSME_OK;
+    delete h->s;
+    delete h;
+    return ZSME_OK;
+}
+
+int zsme_set_state(zsme_handle* h, const double* q, double t) {
+    CHECK_H(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null state");
+    return h->s->set_state(q, t, false);
+}
+int zsme_set_state_device(zsme_handle* h, const double* q, double t) {
+    CHECK_H(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null state");
+    return h->s->set_state(q, t, true);
+}
+int zsme_get_state(zsme_handle* h, double* q) {
+    CHECK_H(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->get_state(q, false);
+}
+int zsme_get_state_device(zsme_handle* h, double* q) {
+    CHECK_H(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->get_state(q, true);
+}
+int zsme_get_aux(zsme_handle* h, double* a) {
+    CHECK_H(h);
+    if (!a) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->get_aux(a);
+}
+int zsme_rhs(zsme_handle* h, double t, const double* x, double* f) {
+    CHECK_H(h);
+    if (!x || !f) return set_error(ZSME_ERR_ARG, "null buffer");
+    return h->s->rhs(t, x, f);
+}
+int zsme_update_state(zsme_handle* h) {
+    CHECK_H(h);
+    return h->s->update_state();
+}
+int zsme_source(zsme_handle* h, double dt) {
+    CHECK_H(h);
+    return h->s->source(dt);
+}
+int zsme_compute_dt(zsme_handle* h, double* dt) {
+    CHECK_H(h);
+    if (!dt) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->compute_dt(dt);
+}
+int zsme_step(zsme_handle* h, int32_t n) {
+    CHECK_H(h);
+    if (n < 0) return set_error(ZSME_ERR_ARG, "negative step count");
+    return h->s->step(n, nullptr);
+}
+int zsme_step_dt(zsme_handle* h, int32_t n, const double* dts) {
+    CHECK_H(h);
+    if (n < 0 || (n > 0 && !dts)) return set_error(ZSME_ERR_ARG, "bad dts");
+    for (int i = 0; i < n; ++i)
+        if (!(dts[i] >= 0)) return set_error(ZSME_ERR_ARG, "dts must be >= 0");
+    return h->s->step(n, dts);
+}
+int zsme_get_diag(zsme_handle* h, zsme_diag* d) {
+    CHECK_H(h);
+    if (!d) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->sync(d);
+}
+int zsme_sync(zsme_handle* h) {
+    CHECK_H(h);
+    zsme_diag d;
+    int rc = h->s->sync(&d);
+    if (rc) return rc;
+    if (d.n_nonfinite > 0 || d.n_negative_depth > 0)
+        return set_error(ZSME_ERR_STATE, "state check: " + std::to_string(d.n_nonfinite) + " non-finite, " +
+                                             std::to_string(d.n_negative_depth) + " negative-depth cell updates");
+    return ZSME_OK;
+}
+int zsme_get_time(zsme_handle* h, double* t, double* dt) {
+    CHECK_H(h);
+    zsme_diag d;
+    int rc = h->s->sync(&d);
+    if (rc) return rc;
+    if (t) *t = d.time;
+    if (dt) *dt = d.dt;
+    return ZSME_OK;
+}
+int zsme_set_params(zsme_handle* h, const double* p) {
+    CHECK_H(h);
+    if (!p) return set_error(ZSME_ERR_ARG, "null params");
+    return h->s->set_params(p);
+}
+void* zsme_stream(zsme_handle* h) { return (h && h->s) ? h->s->stream() : nullptr; }
+int zsme_launches_per_step(zsme_handle* h, int32_t* n) {
+    CHECK_H(h);
+    if (n) *n = h->s->launches_per_step();
+    return ZSME_OK;
+}
+
+int zsme_set_profiling(zsme_handle* h, int enable) {
+    CHECK_H(h);
+    return h->s->set_profiling(enable);
+}
+int zsme_read_profile(zsme_handle* h, double* ms, int64_t* n) {
+    CHECK_H(h);
+    return h->s->read_profile(ms, n);
+}
+
+}  // extern "C"

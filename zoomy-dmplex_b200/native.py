@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(PKG, "libzsme.so")
 
 ZSME_LIMITER_NONE, ZSME_LIMITER_TVD = 0, 1
 ZSME_GRADIENT_GREEN_GAUSS, ZSME_GRADIENT_LSQ = 0, 1
+KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step")
 
 
 class ZsmeMesh(ct.Structure):
@@ -98,6 +99,8 @@ def load():
     lib.zsme_stream.argtypes = [vp]
     lib.zsme_stream.restype = vp
     lib.zsme_launches_per_step.argtypes = [vp, ct.POINTER(ct.c_int32)]
+    lib.zsme_set_profiling.argtypes = [vp, ct.c_int]
+    lib.zsme_read_profile.argtypes = [vp, P, ct.POINTER(ct.c_int64)]
     _lib = lib
     return lib
 

@@ -1,0 +1,173 @@
+"""Host driver over the C ABI, shaped like the reference's MUSCLSolver.
+
+``Solver`` owns one ``zsme_handle``: the mesh and the model live on the GPU
+from construction on; ``set_state`` loads an initial condition (caller cell
+order, ``[n_cells, n_dof_q]``), ``step`` advances whole time steps on the
+device (one CUDA graph per step, no host synchronisation), ``run`` mirrors
+``MUSCLSolver::Run``'s ``while (time < t_end)`` loop (reference
+``MUSCLSolver.hpp:140-188``).  The individual hot-path calls are exposed
+too: ``rhs`` (``TransportStep::FormRHS``), ``update_state``
+(``TransportStep::UpdateState``), ``source`` (``SourceStep::Solve``) and
+``compute_dt`` (``VirtualSolver::ComputeTimeStep``).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from typing import Dict, Optional, Union
+
+import numpy as np
+
+from . import native
+from .mesh import Mesh
+from .settings import Settings, SolverSettings, resolve_parameters
+
+
+def _p(a):
+    return a.ctypes.data_as(ct.POINTER(ct.c_double))
+
+
+class Solver:
+    def __init__(self, model: str, mesh: Mesh, settings: Union[Settings, SolverSettings, None] = None,
+                 params: Union[None, Dict[str, float], np.ndarray, list] = None, device: int = 0):
+        self.lib = native.load()
+        self.model = model
+        self.info = native.model_info(model)
+        self.nq = self.info["n_dof_q"]
+        self.naux = self.info["n_dof_qaux"]
+        if isinstance(settings, Settings):
+            overrides = dict(settings.parameters)
+            solver_settings = settings.solver
+        else:
+            overrides = {}
+            solver_settings = settings or SolverSettings()
+        self.settings = solver_settings
+        self.params = self._resolve_params(params, overrides)
+        self.mesh = mesh
+        self.C = mesh.n_cells
+        self._mesh_keep = native.make_mesh_struct(mesh.as_abi_arrays())
+        self._st = solver_settings.to_struct()
+        h = ct.c_void_p()
+        native.check(self.lib.zsme_create(model.encode(), ct.addressof(self._mesh_keep[0]),
+                                          ct.addressof(self._st), _p(self.params), int(device), ct.byref(h)))
+        self.h = h
+
+    def _resolve_params(self, params, overrides):
+        from . import models as _m
+        names, defaults = _m.parameter_table(self.model)
+        if params is None or isinstance(params, dict):
+            merged = dict(overrides)
+            merged.update(params or {})
+            vals, unknown = resolve_parameters(names, defaults, merged)
+            if unknown:
+                raise KeyError("parameters not defined by model %s: %s" % (self.model, unknown))
+            return np.ascontiguousarray(vals, dtype=np.float64)
+        a = np.ascontiguousarray(params, dtype=np.float64)
+        if a.size != len(names):
+            raise ValueError("expected %d parameters" % len(names))
+        return a
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.zsme_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ state
+    def set_state(self, q: np.ndarray, t: float = 0.0):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.C, self.nq)
+        native.check(self.lib.zsme_set_state(self.h, _p(q), float(t)))
+
+    def set_state_device(self, q_dev_ptr: int, t: float = 0.0):
+        native.check(self.lib.zsme_set_state_device(self.h, ct.c_void_p(q_dev_ptr), float(t)))
+
+    def get_state(self) -> np.ndarray:
+        q = np.empty((self.C, self.nq))
+        native.check(self.lib.zsme_get_state(self.h, _p(q)))
+        return q
+
+    def get_state_device(self, q_dev_ptr: int):
+        native.check(self.lib.zsme_get_state_device(self.h, ct.c_void_p(q_dev_ptr)))
+
+    def get_aux(self) -> np.ndarray:
+        a = np.empty((self.C, self.naux))
+        native.check(self.lib.zsme_get_aux(self.h, _p(a)))
+        return a
+
+    def set_params(self, params):
+        self.params = np.ascontiguousarray(params, dtype=np.float64)
+        native.check(self.lib.zsme_set_params(self.h, _p(self.params)))
+
+    # ------------------------------------------------------- hot-path calls
+    def rhs(self, x: np.ndarray, t: float = 0.0) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.C, self.nq)
+        f = np.empty_like(x)
+        native.check(self.lib.zsme_rhs(self.h, float(t), _p(x), _p(f)))
+        return f
+
+    def update_state(self):
+        native.check(self.lib.zsme_update_state(self.h))
+
+    def source(self, dt: float):
+        native.check(self.lib.zsme_source(self.h, float(dt)))
+
+    def compute_dt(self) -> float:
+        d = ct.c_double()
+        native.check(self.lib.zsme_compute_dt(self.h, ct.byref(d)))
+        return d.value
+
+    def step(self, n: int = 1, dts: Optional[np.ndarray] = None):
+        if dts is None:
+            native.check(self.lib.zsme_step(self.h, int(n)))
+        else:
+            d = np.ascontiguousarray(dts, dtype=np.float64)
+            native.check(self.lib.zsme_step_dt(self.h, int(d.size), _p(d)))
+
+    def sync(self, check: bool = True) -> native.ZsmeDiag:
+        d = native.ZsmeDiag()
+        native.check(self.lib.zsme_get_diag(self.h, ct.byref(d)))
+        if check:
+            native.check(self.lib.zsme_sync(self.h))
+        return d
+
+    def time(self):
+        t, d = ct.c_double(), ct.c_double()
+        native.check(self.lib.zsme_get_time(self.h, ct.byref(t), ct.byref(d)))
+        return t.value, d.value
+
+    def run(self, max_steps: int = 1 << 30, chunk: int = 50):
+        """MUSCLSolver::Run's loop: step until t >= t_end (checked every
+        `chunk` steps; steps past t_end are no-ops on the device)."""
+        done = 0
+        while done < max_steps:
+            n = min(chunk, max_steps - done)
+            self.step(n)
+            done += n
+            t, _ = self.time()
+            if t >= self.settings.t_end:
+                break
+        return self.sync()
+
+    @property
+    def stream(self) -> int:
+        return self.lib.zsme_stream(self.h) or 0
+
+    def set_profiling(self, on: bool = True):
+        native.check(self.lib.zsme_set_profiling(self.h, int(bool(on))))
+
+    def read_profile(self):
+        """{kernel kind: (summed ms, launches)} since set_profiling(True)."""
+        k = len(native.KERNEL_KINDS)
+        ms = np.zeros(k)
+        n = (ct.c_int64 * k)()
+        native.check(self.lib.zsme_read_profile(self.h, _p(ms), n))
+        return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(native.KERNEL_KINDS)}
+
+    def launches_per_step(self) -> int:
+        n = ct.c_int32()
+        native.check(self.lib.zsme_launches_per_step(self.h, ct.byref(n)))
+        return n.value
