@@ -417,7 +417,9 @@ def source_terms(S, Q, hinv, p):
     ex, ey = p[S.pidx("e_x")], p[S.pidx("e_y")]
     e = [ex, ey]
     L = S.L
-    speed = sp.sqrt(sum((mom[d][0] * hinv) ** 2 for d in range(S.dim)))
+    # |u| regularised by 1e-24 (m/s)^2 so that the Jacobian term u^2/|u| is
+    # finite at rest (0 * NaN would poison the Newton matrix even for n = 0)
+    speed = sp.sqrt(sum((mom[d][0] * hinv) ** 2 for d in range(S.dim)) + sp.Float(1e-24))
     for d in range(S.dim):
         ub = sum(mom[d][k] for k in range(S.nmom)) * hinv  # bottom velocity
         for i in range(S.nmom):

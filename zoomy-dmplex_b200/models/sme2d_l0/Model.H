@@ -147,12 +147,13 @@ struct Model {
         const T* X)
     {
     T t0 = (Qaux[0]*p[1]/(p[2]));
-    T t1 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((Qaux[0]*Qaux[0])*((Q[2]*Q[2]) + (Q[3]*Q[3])));
+    T t1 = (Qaux[0]*Qaux[0]);
+    T t2 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((1e-24 + t1*(Q[2]*Q[2]) + t1*(Q[3]*Q[3])));
     SimpleArray<T, 4> res;
     res[0] = 0.0;
     res[1] = 0.0;
-    res[2] = ((-Q[2]*t0) - Q[2]*t1 + Q[1]*p[0]*p[4]);
-    res[3] = ((-Q[3]*t0) - Q[3]*t1 + Q[1]*p[0]*p[5]);
+    res[2] = ((-Q[2]*t0) - Q[2]*t2 + Q[1]*p[0]*p[4]);
+    res[3] = ((-Q[3]*t0) - Q[3]*t2 + Q[1]*p[0]*p[5]);
     return res;
     }
 
@@ -226,16 +227,15 @@ struct Model {
     T t2 = t0*t1;
     T t3 = (Q[2]*Q[2]);
     T t4 = (Q[3]*Q[3]);
-    T t5 = (t3 + t4);
-    T t6 = std::sqrt(t0*t5);
-    T t7 = p[0]*(p[3]*p[3]);
-    T t8 = t6*t7;
-    T t9 = (4.0/3.0)*t8*std::pow(Qaux[0], (7.0/3.0));
-    T t10 = (t7/(t6));
-    T t11 = t10*t5*std::pow(Qaux[0], (13.0/3.0));
-    T t12 = t10*std::pow(Qaux[0], (10.0/3.0));
-    T t13 = (Qaux[0]*t1 + t8*std::pow(Qaux[0], (4.0/3.0)));
-    T t14 = (-Q[2]*Q[3]*t12);
+    T t5 = std::sqrt((1e-24 + t0*t3 + t0*t4));
+    T t6 = p[0]*(p[3]*p[3]);
+    T t7 = t5*t6;
+    T t8 = (4.0/3.0)*t7*std::pow(Qaux[0], (7.0/3.0));
+    T t9 = (t6/(t5));
+    T t10 = t9*std::pow(Qaux[0], (13.0/3.0))*(t3 + t4);
+    T t11 = t9*std::pow(Qaux[0], (10.0/3.0));
+    T t12 = (Qaux[0]*t1 + t7*std::pow(Qaux[0], (4.0/3.0)));
+    T t13 = (-Q[2]*Q[3]*t11);
     SimpleArray<T, 16> res;
     res[0] = 0.0;
     res[1] = 0.0;
@@ -246,13 +246,13 @@ struct Model {
     res[6] = 0.0;
     res[7] = 0.0;
     res[8] = 0.0;
-    res[9] = (Q[2]*t11 + Q[2]*t2 + Q[2]*t9 + p[0]*p[4]);
-    res[10] = ((-t13) - t12*t3);
-    res[11] = t14;
+    res[9] = (Q[2]*t10 + Q[2]*t2 + Q[2]*t8 + p[0]*p[4]);
+    res[10] = ((-t12) - t11*t3);
+    res[11] = t13;
     res[12] = 0.0;
-    res[13] = (Q[3]*t11 + Q[3]*t2 + Q[3]*t9 + p[0]*p[5]);
-    res[14] = t14;
-    res[15] = ((-t13) - t12*t4);
+    res[13] = (Q[3]*t10 + Q[3]*t2 + Q[3]*t8 + p[0]*p[5]);
+    res[14] = t13;
+    res[15] = ((-t12) - t11*t4);
     return res;
     }
 

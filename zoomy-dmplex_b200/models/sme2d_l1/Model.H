@@ -197,17 +197,18 @@ struct Model {
     T t0 = (1.0/(p[2]));
     T t1 = t0*(Q[2] + Q[3]);
     T t2 = Qaux[0]*p[1];
-    T t3 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((Qaux[0]*Qaux[0])*((Q[2]*Q[2]) + (Q[4]*Q[4])));
-    T t4 = 4.0*Qaux[0];
-    T t5 = 3.0*t2;
-    T t6 = t0*(Q[4] + Q[5]);
+    T t3 = (Qaux[0]*Qaux[0]);
+    T t4 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((1e-24 + t3*(Q[2]*Q[2]) + t3*(Q[4]*Q[4])));
+    T t5 = 4.0*Qaux[0];
+    T t6 = 3.0*t2;
+    T t7 = t0*(Q[4] + Q[5]);
     SimpleArray<T, 6> res;
     res[0] = 0.0;
     res[1] = 0.0;
-    res[2] = ((-Q[2]*t3) - t1*t2 + Q[1]*p[0]*p[4]);
-    res[3] = (-t5*(t1 + Q[3]*t4));
-    res[4] = ((-Q[4]*t3) - t2*t6 + Q[1]*p[0]*p[5]);
-    res[5] = (-t5*(t6 + Q[5]*t4));
+    res[2] = ((-Q[2]*t4) - t1*t2 + Q[1]*p[0]*p[4]);
+    res[3] = (-t6*(t1 + Q[3]*t5));
+    res[4] = ((-Q[4]*t4) - t2*t7 + Q[1]*p[0]*p[5]);
+    res[5] = (-t6*(t7 + Q[5]*t5));
     return res;
     }
 
@@ -330,24 +331,23 @@ struct Model {
     T t3 = p[1]*t2;
     T t4 = (Q[2]*Q[2]);
     T t5 = (Q[4]*Q[4]);
-    T t6 = (t4 + t5);
-    T t7 = std::sqrt(t2*t6);
-    T t8 = p[0]*(p[3]*p[3]);
-    T t9 = t7*t8;
-    T t10 = (4.0/3.0)*t9*std::pow(Qaux[0], (7.0/3.0));
-    T t11 = (t8/(t7));
-    T t12 = t11*t6*std::pow(Qaux[0], (13.0/3.0));
-    T t13 = t11*std::pow(Qaux[0], (10.0/3.0));
-    T t14 = Qaux[0]*p[1];
-    T t15 = t0*t14;
-    T t16 = (t15 + t9*std::pow(Qaux[0], (4.0/3.0)));
-    T t17 = (-t15);
-    T t18 = (-Q[2]*Q[4]*t13);
-    T t19 = 8.0*Qaux[0];
-    T t20 = 3.0*t3;
-    T t21 = (-3.0*t15);
-    T t22 = (-3.0*t14*(t0 + 4.0*Qaux[0]));
-    T t23 = t0*(Q[4] + Q[5]);
+    T t6 = std::sqrt((1e-24 + t2*t4 + t2*t5));
+    T t7 = p[0]*(p[3]*p[3]);
+    T t8 = t6*t7;
+    T t9 = (4.0/3.0)*t8*std::pow(Qaux[0], (7.0/3.0));
+    T t10 = (t7/(t6));
+    T t11 = t10*std::pow(Qaux[0], (13.0/3.0))*(t4 + t5);
+    T t12 = t10*std::pow(Qaux[0], (10.0/3.0));
+    T t13 = Qaux[0]*p[1];
+    T t14 = t0*t13;
+    T t15 = (t14 + t8*std::pow(Qaux[0], (4.0/3.0)));
+    T t16 = (-t14);
+    T t17 = (-Q[2]*Q[4]*t12);
+    T t18 = 8.0*Qaux[0];
+    T t19 = 3.0*t3;
+    T t20 = (-3.0*t14);
+    T t21 = (-3.0*t13*(t0 + 4.0*Qaux[0]));
+    T t22 = t0*(Q[4] + Q[5]);
     SimpleArray<T, 36> res;
     res[0] = 0.0;
     res[1] = 0.0;
@@ -362,29 +362,29 @@ struct Model {
     res[10] = 0.0;
     res[11] = 0.0;
     res[12] = 0.0;
-    res[13] = (Q[2]*t10 + Q[2]*t12 + p[0]*p[4] + t1*t3);
-    res[14] = ((-t16) - t13*t4);
-    res[15] = t17;
-    res[16] = t18;
+    res[13] = (Q[2]*t11 + Q[2]*t9 + p[0]*p[4] + t1*t3);
+    res[14] = ((-t15) - t12*t4);
+    res[15] = t16;
+    res[16] = t17;
     res[17] = 0.0;
     res[18] = 0.0;
-    res[19] = t20*(t1 + Q[3]*t19);
-    res[20] = t21;
-    res[21] = t22;
+    res[19] = t19*(t1 + Q[3]*t18);
+    res[20] = t20;
+    res[21] = t21;
     res[22] = 0.0;
     res[23] = 0.0;
     res[24] = 0.0;
-    res[25] = (Q[4]*t10 + Q[4]*t12 + p[0]*p[5] + t23*t3);
-    res[26] = t18;
+    res[25] = (Q[4]*t11 + Q[4]*t9 + p[0]*p[5] + t22*t3);
+    res[26] = t17;
     res[27] = 0.0;
-    res[28] = ((-t16) - t13*t5);
-    res[29] = t17;
+    res[28] = ((-t15) - t12*t5);
+    res[29] = t16;
     res[30] = 0.0;
-    res[31] = t20*(t23 + Q[5]*t19);
+    res[31] = t19*(t22 + Q[5]*t18);
     res[32] = 0.0;
     res[33] = 0.0;
-    res[34] = t21;
-    res[35] = t22;
+    res[34] = t20;
+    res[35] = t21;
     return res;
     }
 

@@ -275,21 +275,22 @@ struct Model {
     T t0 = (1.0/(p[2]));
     T t1 = t0*(Q[2] + Q[3] + Q[4]);
     T t2 = Qaux[0]*p[1];
-    T t3 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((Qaux[0]*Qaux[0])*((Q[2]*Q[2]) + (Q[5]*Q[5])));
-    T t4 = 4.0*Qaux[0];
-    T t5 = 3.0*t2;
-    T t6 = 12.0*Qaux[0];
-    T t7 = 5.0*t2;
-    T t8 = t0*(Q[5] + Q[6] + Q[7]);
+    T t3 = (Qaux[0]*Qaux[0]);
+    T t4 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((1e-24 + t3*(Q[2]*Q[2]) + t3*(Q[5]*Q[5])));
+    T t5 = 4.0*Qaux[0];
+    T t6 = 3.0*t2;
+    T t7 = 12.0*Qaux[0];
+    T t8 = 5.0*t2;
+    T t9 = t0*(Q[5] + Q[6] + Q[7]);
     SimpleArray<T, 8> res;
     res[0] = 0.0;
     res[1] = 0.0;
-    res[2] = ((-Q[2]*t3) - t1*t2 + Q[1]*p[0]*p[4]);
-    res[3] = (-t5*(t1 + Q[3]*t4));
-    res[4] = (-t7*(t1 + Q[4]*t6));
-    res[5] = ((-Q[5]*t3) - t2*t8 + Q[1]*p[0]*p[5]);
-    res[6] = (-t5*(t8 + Q[6]*t4));
-    res[7] = (-t7*(t8 + Q[7]*t6));
+    res[2] = ((-Q[2]*t4) - t1*t2 + Q[1]*p[0]*p[4]);
+    res[3] = (-t6*(t1 + Q[3]*t5));
+    res[4] = (-t8*(t1 + Q[4]*t7));
+    res[5] = ((-Q[5]*t4) - t2*t9 + Q[1]*p[0]*p[5]);
+    res[6] = (-t6*(t9 + Q[6]*t5));
+    res[7] = (-t8*(t9 + Q[7]*t7));
     return res;
     }
 
@@ -489,28 +490,27 @@ struct Model {
     T t3 = p[1]*t2;
     T t4 = (Q[2]*Q[2]);
     T t5 = (Q[5]*Q[5]);
-    T t6 = (t4 + t5);
-    T t7 = std::sqrt(t2*t6);
-    T t8 = p[0]*(p[3]*p[3]);
-    T t9 = t7*t8;
-    T t10 = (4.0/3.0)*t9*std::pow(Qaux[0], (7.0/3.0));
-    T t11 = (t8/(t7));
-    T t12 = t11*t6*std::pow(Qaux[0], (13.0/3.0));
-    T t13 = t11*std::pow(Qaux[0], (10.0/3.0));
-    T t14 = Qaux[0]*p[1];
-    T t15 = t0*t14;
-    T t16 = (t15 + t9*std::pow(Qaux[0], (4.0/3.0)));
-    T t17 = (-t15);
-    T t18 = (-Q[2]*Q[5]*t13);
-    T t19 = 8.0*Qaux[0];
-    T t20 = 3.0*t3;
-    T t21 = (-3.0*t15);
-    T t22 = (-3.0*t14*(t0 + 4.0*Qaux[0]));
-    T t23 = 24.0*Qaux[0];
-    T t24 = 5.0*t3;
-    T t25 = (-5.0*t15);
-    T t26 = (-5.0*t14*(t0 + 12.0*Qaux[0]));
-    T t27 = t0*(Q[5] + Q[6] + Q[7]);
+    T t6 = std::sqrt((1e-24 + t2*t4 + t2*t5));
+    T t7 = p[0]*(p[3]*p[3]);
+    T t8 = t6*t7;
+    T t9 = (4.0/3.0)*t8*std::pow(Qaux[0], (7.0/3.0));
+    T t10 = (t7/(t6));
+    T t11 = t10*std::pow(Qaux[0], (13.0/3.0))*(t4 + t5);
+    T t12 = t10*std::pow(Qaux[0], (10.0/3.0));
+    T t13 = Qaux[0]*p[1];
+    T t14 = t0*t13;
+    T t15 = (t14 + t8*std::pow(Qaux[0], (4.0/3.0)));
+    T t16 = (-t14);
+    T t17 = (-Q[2]*Q[5]*t12);
+    T t18 = 8.0*Qaux[0];
+    T t19 = 3.0*t3;
+    T t20 = (-3.0*t14);
+    T t21 = (-3.0*t13*(t0 + 4.0*Qaux[0]));
+    T t22 = 24.0*Qaux[0];
+    T t23 = 5.0*t3;
+    T t24 = (-5.0*t14);
+    T t25 = (-5.0*t13*(t0 + 12.0*Qaux[0]));
+    T t26 = t0*(Q[5] + Q[6] + Q[7]);
     SimpleArray<T, 64> res;
     res[0] = 0.0;
     res[1] = 0.0;
@@ -529,53 +529,53 @@ struct Model {
     res[14] = 0.0;
     res[15] = 0.0;
     res[16] = 0.0;
-    res[17] = (Q[2]*t10 + Q[2]*t12 + p[0]*p[4] + t1*t3);
-    res[18] = ((-t16) - t13*t4);
-    res[19] = t17;
-    res[20] = t17;
-    res[21] = t18;
+    res[17] = (Q[2]*t11 + Q[2]*t9 + p[0]*p[4] + t1*t3);
+    res[18] = ((-t15) - t12*t4);
+    res[19] = t16;
+    res[20] = t16;
+    res[21] = t17;
     res[22] = 0.0;
     res[23] = 0.0;
     res[24] = 0.0;
-    res[25] = t20*(t1 + Q[3]*t19);
-    res[26] = t21;
-    res[27] = t22;
-    res[28] = t21;
+    res[25] = t19*(t1 + Q[3]*t18);
+    res[26] = t20;
+    res[27] = t21;
+    res[28] = t20;
     res[29] = 0.0;
     res[30] = 0.0;
     res[31] = 0.0;
     res[32] = 0.0;
-    res[33] = t24*(t1 + Q[4]*t23);
-    res[34] = t25;
-    res[35] = t25;
-    res[36] = t26;
+    res[33] = t23*(t1 + Q[4]*t22);
+    res[34] = t24;
+    res[35] = t24;
+    res[36] = t25;
     res[37] = 0.0;
     res[38] = 0.0;
     res[39] = 0.0;
     res[40] = 0.0;
-    res[41] = (Q[5]*t10 + Q[5]*t12 + p[0]*p[5] + t27*t3);
-    res[42] = t18;
+    res[41] = (Q[5]*t11 + Q[5]*t9 + p[0]*p[5] + t26*t3);
+    res[42] = t17;
     res[43] = 0.0;
     res[44] = 0.0;
-    res[45] = ((-t16) - t13*t5);
-    res[46] = t17;
-    res[47] = t17;
+    res[45] = ((-t15) - t12*t5);
+    res[46] = t16;
+    res[47] = t16;
     res[48] = 0.0;
-    res[49] = t20*(t27 + Q[6]*t19);
+    res[49] = t19*(t26 + Q[6]*t18);
     res[50] = 0.0;
     res[51] = 0.0;
     res[52] = 0.0;
-    res[53] = t21;
-    res[54] = t22;
-    res[55] = t21;
+    res[53] = t20;
+    res[54] = t21;
+    res[55] = t20;
     res[56] = 0.0;
-    res[57] = t24*(t27 + Q[7]*t23);
+    res[57] = t23*(t26 + Q[7]*t22);
     res[58] = 0.0;
     res[59] = 0.0;
     res[60] = 0.0;
-    res[61] = t25;
-    res[62] = t25;
-    res[63] = t26;
+    res[61] = t24;
+    res[62] = t24;
+    res[63] = t25;
     return res;
     }
 

@@ -509,33 +509,34 @@ struct Model {
     T t0 = (1.0/(p[2]));
     T t1 = t0*(Q[2] + Q[3] + Q[4] + Q[5] + Q[6]);
     T t2 = Qaux[0]*p[1];
-    T t3 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((Qaux[0]*Qaux[0])*((Q[2]*Q[2]) + (Q[7]*Q[7])));
-    T t4 = 4.0*Qaux[0];
-    T t5 = (t1 + Q[3]*t4);
-    T t6 = 3.0*t2;
-    T t7 = 12.0*Qaux[0];
-    T t8 = (t1 + Q[4]*t7);
-    T t9 = 5.0*t2;
-    T t10 = 24.0*Qaux[0];
-    T t11 = 7.0*t2;
-    T t12 = 40.0*Qaux[0];
-    T t13 = 9.0*t2;
-    T t14 = t0*(Q[10] + Q[11] + Q[7] + Q[8] + Q[9]);
-    T t15 = (t14 + Q[8]*t4);
-    T t16 = (t14 + Q[9]*t7);
+    T t3 = (Qaux[0]*Qaux[0]);
+    T t4 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((1e-24 + t3*(Q[2]*Q[2]) + t3*(Q[7]*Q[7])));
+    T t5 = 4.0*Qaux[0];
+    T t6 = (t1 + Q[3]*t5);
+    T t7 = 3.0*t2;
+    T t8 = 12.0*Qaux[0];
+    T t9 = (t1 + Q[4]*t8);
+    T t10 = 5.0*t2;
+    T t11 = 24.0*Qaux[0];
+    T t12 = 7.0*t2;
+    T t13 = 40.0*Qaux[0];
+    T t14 = 9.0*t2;
+    T t15 = t0*(Q[10] + Q[11] + Q[7] + Q[8] + Q[9]);
+    T t16 = (t15 + Q[8]*t5);
+    T t17 = (t15 + Q[9]*t8);
     SimpleArray<T, 12> res;
     res[0] = 0.0;
     res[1] = 0.0;
-    res[2] = ((-Q[2]*t3) - t1*t2 + Q[1]*p[0]*p[4]);
-    res[3] = (-t6*(t5 + Q[5]*t4));
-    res[4] = (-t9*(t8 + Q[6]*t7));
-    res[5] = (-t11*(t5 + Q[5]*t10));
-    res[6] = (-t13*(t8 + Q[6]*t12));
-    res[7] = ((-Q[7]*t3) - t14*t2 + Q[1]*p[0]*p[5]);
-    res[8] = (-t6*(t15 + Q[10]*t4));
-    res[9] = (-t9*(t16 + Q[11]*t7));
-    res[10] = (-t11*(t15 + Q[10]*t10));
-    res[11] = (-t13*(t16 + Q[11]*t12));
+    res[2] = ((-Q[2]*t4) - t1*t2 + Q[1]*p[0]*p[4]);
+    res[3] = (-t7*(t6 + Q[5]*t5));
+    res[4] = (-t10*(t9 + Q[6]*t8));
+    res[5] = (-t12*(t6 + Q[5]*t11));
+    res[6] = (-t14*(t9 + Q[6]*t13));
+    res[7] = ((-Q[7]*t4) - t15*t2 + Q[1]*p[0]*p[5]);
+    res[8] = (-t7*(t16 + Q[10]*t5));
+    res[9] = (-t10*(t17 + Q[11]*t8));
+    res[10] = (-t12*(t16 + Q[10]*t11));
+    res[11] = (-t14*(t17 + Q[11]*t13));
     return res;
     }
 
@@ -967,44 +968,43 @@ struct Model {
     T t3 = p[1]*t2;
     T t4 = (Q[2]*Q[2]);
     T t5 = (Q[7]*Q[7]);
-    T t6 = (t4 + t5);
-    T t7 = std::sqrt(t2*t6);
-    T t8 = p[0]*(p[3]*p[3]);
-    T t9 = t7*t8;
-    T t10 = (4.0/3.0)*t9*std::pow(Qaux[0], (7.0/3.0));
-    T t11 = (t8/(t7));
-    T t12 = t11*t6*std::pow(Qaux[0], (13.0/3.0));
-    T t13 = t11*std::pow(Qaux[0], (10.0/3.0));
-    T t14 = Qaux[0]*p[1];
-    T t15 = t0*t14;
-    T t16 = (t15 + t9*std::pow(Qaux[0], (4.0/3.0)));
-    T t17 = (-t15);
-    T t18 = (-Q[2]*Q[7]*t13);
-    T t19 = 8.0*Qaux[0];
-    T t20 = (t1 + Q[3]*t19);
-    T t21 = 3.0*t3;
-    T t22 = (-3.0*t15);
-    T t23 = t14*(t0 + 4.0*Qaux[0]);
-    T t24 = (-3.0*t23);
-    T t25 = 24.0*Qaux[0];
-    T t26 = (t1 + Q[4]*t25);
-    T t27 = 5.0*t3;
-    T t28 = (-5.0*t15);
-    T t29 = t14*(t0 + 12.0*Qaux[0]);
-    T t30 = (-5.0*t29);
-    T t31 = 48.0*Qaux[0];
-    T t32 = 7.0*t3;
-    T t33 = (-7.0*t15);
-    T t34 = (-7.0*t23);
-    T t35 = (-7.0*t14*(t0 + t25));
-    T t36 = 80.0*Qaux[0];
-    T t37 = 9.0*t3;
-    T t38 = (-9.0*t15);
-    T t39 = (-9.0*t29);
-    T t40 = (-9.0*t14*(t0 + 40.0*Qaux[0]));
-    T t41 = t0*(Q[10] + Q[11] + Q[7] + Q[8] + Q[9]);
-    T t42 = (t41 + Q[8]*t19);
-    T t43 = (t41 + Q[9]*t25);
+    T t6 = std::sqrt((1e-24 + t2*t4 + t2*t5));
+    T t7 = p[0]*(p[3]*p[3]);
+    T t8 = t6*t7;
+    T t9 = (4.0/3.0)*t8*std::pow(Qaux[0], (7.0/3.0));
+    T t10 = (t7/(t6));
+    T t11 = t10*std::pow(Qaux[0], (13.0/3.0))*(t4 + t5);
+    T t12 = t10*std::pow(Qaux[0], (10.0/3.0));
+    T t13 = Qaux[0]*p[1];
+    T t14 = t0*t13;
+    T t15 = (t14 + t8*std::pow(Qaux[0], (4.0/3.0)));
+    T t16 = (-t14);
+    T t17 = (-Q[2]*Q[7]*t12);
+    T t18 = 8.0*Qaux[0];
+    T t19 = (t1 + Q[3]*t18);
+    T t20 = 3.0*t3;
+    T t21 = (-3.0*t14);
+    T t22 = t13*(t0 + 4.0*Qaux[0]);
+    T t23 = (-3.0*t22);
+    T t24 = 24.0*Qaux[0];
+    T t25 = (t1 + Q[4]*t24);
+    T t26 = 5.0*t3;
+    T t27 = (-5.0*t14);
+    T t28 = t13*(t0 + 12.0*Qaux[0]);
+    T t29 = (-5.0*t28);
+    T t30 = 48.0*Qaux[0];
+    T t31 = 7.0*t3;
+    T t32 = (-7.0*t14);
+    T t33 = (-7.0*t22);
+    T t34 = (-7.0*t13*(t0 + t24));
+    T t35 = 80.0*Qaux[0];
+    T t36 = 9.0*t3;
+    T t37 = (-9.0*t14);
+    T t38 = (-9.0*t28);
+    T t39 = (-9.0*t13*(t0 + 40.0*Qaux[0]));
+    T t40 = t0*(Q[10] + Q[11] + Q[7] + Q[8] + Q[9]);
+    T t41 = (t40 + Q[8]*t18);
+    T t42 = (t40 + Q[9]*t24);
     SimpleArray<T, 144> res;
     res[0] = 0.0;
     res[1] = 0.0;
@@ -1031,125 +1031,125 @@ struct Model {
     res[22] = 0.0;
     res[23] = 0.0;
     res[24] = 0.0;
-    res[25] = (Q[2]*t10 + Q[2]*t12 + p[0]*p[4] + t1*t3);
-    res[26] = ((-t16) - t13*t4);
-    res[27] = t17;
-    res[28] = t17;
-    res[29] = t17;
-    res[30] = t17;
-    res[31] = t18;
+    res[25] = (Q[2]*t11 + Q[2]*t9 + p[0]*p[4] + t1*t3);
+    res[26] = ((-t15) - t12*t4);
+    res[27] = t16;
+    res[28] = t16;
+    res[29] = t16;
+    res[30] = t16;
+    res[31] = t17;
     res[32] = 0.0;
     res[33] = 0.0;
     res[34] = 0.0;
     res[35] = 0.0;
     res[36] = 0.0;
-    res[37] = t21*(t20 + Q[5]*t19);
-    res[38] = t22;
-    res[39] = t24;
-    res[40] = t22;
-    res[41] = t24;
-    res[42] = t22;
+    res[37] = t20*(t19 + Q[5]*t18);
+    res[38] = t21;
+    res[39] = t23;
+    res[40] = t21;
+    res[41] = t23;
+    res[42] = t21;
     res[43] = 0.0;
     res[44] = 0.0;
     res[45] = 0.0;
     res[46] = 0.0;
     res[47] = 0.0;
     res[48] = 0.0;
-    res[49] = t27*(t26 + Q[6]*t25);
-    res[50] = t28;
-    res[51] = t28;
-    res[52] = t30;
-    res[53] = t28;
-    res[54] = t30;
+    res[49] = t26*(t25 + Q[6]*t24);
+    res[50] = t27;
+    res[51] = t27;
+    res[52] = t29;
+    res[53] = t27;
+    res[54] = t29;
     res[55] = 0.0;
     res[56] = 0.0;
     res[57] = 0.0;
     res[58] = 0.0;
     res[59] = 0.0;
     res[60] = 0.0;
-    res[61] = t32*(t20 + Q[5]*t31);
-    res[62] = t33;
-    res[63] = t34;
-    res[64] = t33;
-    res[65] = t35;
-    res[66] = t33;
+    res[61] = t31*(t19 + Q[5]*t30);
+    res[62] = t32;
+    res[63] = t33;
+    res[64] = t32;
+    res[65] = t34;
+    res[66] = t32;
     res[67] = 0.0;
     res[68] = 0.0;
     res[69] = 0.0;
     res[70] = 0.0;
     res[71] = 0.0;
     res[72] = 0.0;
-    res[73] = t37*(t26 + Q[6]*t36);
-    res[74] = t38;
-    res[75] = t38;
-    res[76] = t39;
-    res[77] = t38;
-    res[78] = t40;
+    res[73] = t36*(t25 + Q[6]*t35);
+    res[74] = t37;
+    res[75] = t37;
+    res[76] = t38;
+    res[77] = t37;
+    res[78] = t39;
     res[79] = 0.0;
     res[80] = 0.0;
     res[81] = 0.0;
     res[82] = 0.0;
     res[83] = 0.0;
     res[84] = 0.0;
-    res[85] = (Q[7]*t10 + Q[7]*t12 + p[0]*p[5] + t3*t41);
-    res[86] = t18;
+    res[85] = (Q[7]*t11 + Q[7]*t9 + p[0]*p[5] + t3*t40);
+    res[86] = t17;
     res[87] = 0.0;
     res[88] = 0.0;
     res[89] = 0.0;
     res[90] = 0.0;
-    res[91] = ((-t16) - t13*t5);
-    res[92] = t17;
-    res[93] = t17;
-    res[94] = t17;
-    res[95] = t17;
+    res[91] = ((-t15) - t12*t5);
+    res[92] = t16;
+    res[93] = t16;
+    res[94] = t16;
+    res[95] = t16;
     res[96] = 0.0;
-    res[97] = t21*(t42 + Q[10]*t19);
+    res[97] = t20*(t41 + Q[10]*t18);
     res[98] = 0.0;
     res[99] = 0.0;
     res[100] = 0.0;
     res[101] = 0.0;
     res[102] = 0.0;
-    res[103] = t22;
-    res[104] = t24;
-    res[105] = t22;
-    res[106] = t24;
-    res[107] = t22;
+    res[103] = t21;
+    res[104] = t23;
+    res[105] = t21;
+    res[106] = t23;
+    res[107] = t21;
     res[108] = 0.0;
-    res[109] = t27*(t43 + Q[11]*t25);
+    res[109] = t26*(t42 + Q[11]*t24);
     res[110] = 0.0;
     res[111] = 0.0;
     res[112] = 0.0;
     res[113] = 0.0;
     res[114] = 0.0;
-    res[115] = t28;
-    res[116] = t28;
-    res[117] = t30;
-    res[118] = t28;
-    res[119] = t30;
+    res[115] = t27;
+    res[116] = t27;
+    res[117] = t29;
+    res[118] = t27;
+    res[119] = t29;
     res[120] = 0.0;
-    res[121] = t32*(t42 + Q[10]*t31);
+    res[121] = t31*(t41 + Q[10]*t30);
     res[122] = 0.0;
     res[123] = 0.0;
     res[124] = 0.0;
     res[125] = 0.0;
     res[126] = 0.0;
-    res[127] = t33;
-    res[128] = t34;
-    res[129] = t33;
-    res[130] = t35;
-    res[131] = t33;
+    res[127] = t32;
+    res[128] = t33;
+    res[129] = t32;
+    res[130] = t34;
+    res[131] = t32;
     res[132] = 0.0;
-    res[133] = t37*(t43 + Q[11]*t36);
+    res[133] = t36*(t42 + Q[11]*t35);
     res[134] = 0.0;
     res[135] = 0.0;
     res[136] = 0.0;
     res[137] = 0.0;
     res[138] = 0.0;
-    res[139] = t38;
-    res[140] = t38;
-    res[141] = t39;
-    res[142] = t38;
-    res[143] = t40;
+    res[139] = t37;
+    res[140] = t37;
+    res[141] = t38;
+    res[142] = t37;
+    res[143] = t39;
     return res;
     }
 
