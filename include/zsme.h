@@ -165,6 +165,27 @@ int zsme_set_profiling(zsme_handle* h, int enable);
 /* ms[ZSME_KERNEL_KINDS]: summed milliseconds; n[...]: launches. */
 int zsme_read_profile(zsme_handle* h, double* ms, int64_t* n);
 
+/* CFL time step of a caller-owned state with no device allocation.
+ * No counterpart in the reference, which has no GPU path.  It serves callers
+ * that cannot allocate device memory at the moment they need a step (a host
+ * code that reserves its device memory up front and forbids allocation
+ * afterwards, or one running under a fixed memory budget): instead of
+ * cudaMalloc it uses a 512 KB scratch array compiled into the library, which
+ * every GPU that loads the library holds until the process exits.
+ * All pointers are device pointers, cells in any order (the same in all
+ * arrays): d_q_aos [n_cells][n_dof_q], d_aux_aos [n_cells][n_dof_qaux],
+ * d_rc [n_cells] (min over the cell's faces of |x_c - x_f|), d_params
+ * [n_parameters]; dt (cfl * min r_c/lambda_c, or the model's dt_max) is
+ * written to *d_dt in stream order on `stream` (a cudaStream_t; NULL = the
+ * default stream).  n_cells > ZSME_NOALLOC_MAX_CELLS returns ZSME_ERR_LIMIT.
+ * The first call on a device looks the scratch address up and must come
+ * before any stream capture on that device.  All calls share the scratch:
+ * calls that overlap on the GPU race. */
+#define ZSME_NOALLOC_MAX_CELLS (1 << 24)
+int zsme_compute_dt_noalloc(const char* model, int32_t n_cells, const double* d_q_aos,
+                            const double* d_aux_aos, const double* d_rc, const double* d_params,
+                            double cfl, double* d_dt, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

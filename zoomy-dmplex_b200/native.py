@@ -101,6 +101,7 @@ def load():
     lib.zsme_launches_per_step.argtypes = [vp, ct.POINTER(ct.c_int32)]
     lib.zsme_set_profiling.argtypes = [vp, ct.c_int]
     lib.zsme_read_profile.argtypes = [vp, P, ct.POINTER(ct.c_int64)]
+    lib.zsme_compute_dt_noalloc.argtypes = [ct.c_char_p, ct.c_int32, vp, vp, vp, vp, ct.c_double, vp, vp]
     _lib = lib
     return lib
 
