@@ -157,13 +157,34 @@ int zsme_launches_per_step(zsme_handle* h, int32_t* n);
  * and, at the end of each call, accumulates the durations per kind. */
 #define ZSME_KERNEL_BEGIN 0     /* begin_step: dt clamp to t_end */
 #define ZSME_KERNEL_PREP 1      /* clamp + bounds + gradient + face states */
-#define ZSME_KERNEL_FLUX 2      /* face fluxes + stage update */
+#define ZSME_KERNEL_FLUX 2      /* face fluxes, each face once */
 #define ZSME_KERNEL_FINALIZE 3  /* constraints + source + CFL partials */
 #define ZSME_KERNEL_END 4       /* dt reduction + time advance */
-#define ZSME_KERNEL_KINDS 5
+#define ZSME_KERNEL_GATHER 5    /* per-cell sum of face contributions + stage update */
+#define ZSME_KERNEL_KINDS 6
 int zsme_set_profiling(zsme_handle* h, int enable);
 /* ms[ZSME_KERNEL_KINDS]: summed milliseconds; n[...]: launches. */
 int zsme_read_profile(zsme_handle* h, double* ms, int64_t* n);
+
+/* Ensembles.  No counterpart in the reference, which advances one mesh per
+ * run (MUSCLSolver::Run, MUSCLSolver.hpp:22-194); here n independent
+ * instances (own mesh, parameters, time and CFL dt) share one handle and
+ * every kernel launch of zsme_step advances all of them.  meshes[n];
+ * params: n * n_parameters doubles or NULL.  zsme_step / zsme_update_state /
+ * zsme_source act on all instances; states move per instance. */
+int zsme_batch_create(const char* model, int32_t n, const zsme_mesh* meshes, const zsme_settings* settings,
+                      const double* params, int device, zsme_handle** out);
+int zsme_batch_size(zsme_handle* h, int32_t* n);
+int zsme_batch_set_state(zsme_handle* h, int32_t i, const double* q_aos, double t);
+int zsme_batch_get_state(zsme_handle* h, int32_t i, double* q_aos);
+int zsme_batch_get_time(zsme_handle* h, int32_t i, double* t, double* dt);
+
+/* Launch configuration, 6 ints: threads per block {prep, face, gather,
+ * finalize} (multiples of 32, <= 128) and the register caps {prep, face}
+ * as resident blocks per SM (1 = uncapped .. 4): the knobs of the
+ * autotuner (zoomy-dmplex_b200/autotune.py). */
+int zsme_set_launch(zsme_handle* h, const int32_t* blocks);
+int zsme_get_launch(zsme_handle* h, int32_t* blocks);
 
 /* CFL time step of a caller-owned state with no device allocation.
  * No counterpart in the reference, which has no GPU path.  It serves callers

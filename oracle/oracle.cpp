@@ -27,6 +27,7 @@
 // step composition cannot be run from the reference (PETSc is absent) and is
 // pinned only by this restatement.
 #include "model_prelude.h"
+#include "dual.h"
 #include "zsme.h"
 
 #include <cstdio>
@@ -116,11 +117,17 @@ struct OracleBase {
     virtual void set_params(const double* p) = 0;
     virtual int newton_unconverged() const = 0;
     virtual void gradient(const double* x, double* g) = 0;
+    // tangent-linear (dual-number) instances only: seed / read directions
+    virtual void set_tangent(const double*, const double*) {}
+    virtual void get_tangent(double*) const {}
 };
 
-template <template <typename> class MT, template <typename> class NT>
+// S: the scalar of state and parameters -- double, or Dual<1> for the
+// tangent-linear run (derivative along one seeded direction, the branches
+// decided by the values exactly as in the double run).
+template <template <typename> class MT, template <typename> class NT, class Scalar = double>
 struct Oracle : OracleBase {
-    using T = double;
+    using T = Scalar;
     using M = MT<T>;
     using N = NT<T>;
     static constexpr int NQ = M::n_dof_q;
@@ -135,8 +142,8 @@ struct Oracle : OracleBase {
     std::vector<double> lsq_w;           // DIM weights per neighbour entry
     std::vector<int> cell_face_sorted;   // each cell's faces, increasing id
     zsme_settings st{};
-    std::vector<double> params;
-    std::vector<double> X, A, G;
+    std::vector<T> params;
+    std::vector<T> X, A, G;
     double time = 0.0, dt = 0.0;
     int n_unconv = 0;
 
@@ -300,8 +307,9 @@ par_for(C, [&](int c, int) {
                     area = std::sqrt(area);
                     T nh[3] = {0, 0, 0};
                     for (int d = 0; d < DIM; ++d) nh[d] = Nf[d] / area;
-                    auto qb = M::boundary_conditions(fbc[f], &x[(size_t)c * NQ], nullptr, params.data(), nh,
-                                                     &fc[2 * f], 0.0, 0.0);
+                    const T xf[3] = {fc[2 * f], fc[2 * f + 1], 0.0};
+                    auto qb = M::boundary_conditions(fbc[f], &x[(size_t)c * NQ], nullptr, params.data(), nh, xf,
+                                                     0.0, 0.0);
                     for (int i = 0; i < NQ; ++i)
                         for (int d = 0; d < DIM; ++d) gc[i * DIM + d] += qb[i] * Nf[d];
                 }
@@ -397,16 +405,16 @@ par_for(F, [&](int f, int) {
             if (area <= 1e-15) return;
             T nh[3] = {0, 0, 0};
             for (int d = 0; d < DIM; ++d) nh[d] = Nf[d] / area;
-            const double* xf = &fc[2 * f];
+            const T xf[3] = {fc[2 * f], fc[2 * f + 1], 0.0};
             int L = fcell[2 * f], R = fcell[2 * f + 1];
             T* ncL = &fb[(size_t)f * 3 * NQ];
             T* ncR = ncL + NQ;
             T* fl = ncR + NQ;
             if (R >= 0) {
                 T qLf[NQ], qRf[NQ], aLf[NA], aRf[NA];
-                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], xf,
+                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
                             o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
-                reconstruct(&xl[(size_t)R * NQ], o2 ? &G[(size_t)R * NQ * DIM] : nullptr, &cc[2 * R], xf,
+                reconstruct(&xl[(size_t)R * NQ], o2 ? &G[(size_t)R * NQ * DIM] : nullptr, &cc[2 * R], &fc[2 * f],
                             o2 ? &vmin[(size_t)R * NQ] : nullptr, o2 ? &vmax[(size_t)R * NQ] : nullptr, qRf);
                 for (int i = 0; i < NA; ++i) { aLf[i] = al[(size_t)L * NA + i]; aRf[i] = al[(size_t)R * NA + i]; }
                 auto ra = M::update_aux_variables(qLf, aLf, params.data(), 0.0, xf);
@@ -423,7 +431,7 @@ par_for(F, [&](int f, int) {
                 active[f] = 1;
             } else if (fbc[f] >= 0) {
                 T qLf[NQ], aLf[NA], aRf[NA];
-                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], xf,
+                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
                             o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
                 for (int i = 0; i < NA; ++i) aLf[i] = al[(size_t)L * NA + i];
                 auto ra = M::update_aux_variables(qLf, aLf, params.data(), t, xf);
@@ -584,7 +592,7 @@ par_for(C, [&](int c, int) {
                 if (dist < rc) rc = dist;
             }
             if (rc < std::numeric_limits<double>::max()) {
-                double ratio = rc / eig;
+                double ratio = rc / zsme::value(eig);
                 if (ratio < best) best = ratio;
             }
         });
@@ -602,18 +610,33 @@ par_for(C, [&](int c, int) {
         update_state_vec(X, A);                                  // MUSCLSolver.hpp:54
         dt = std::max(compute_dt(), st.min_dt);                  // MUSCLSolver.hpp:103
     }
-    void get_state(double* q) const override { std::copy(X.begin(), X.end(), q); }
-    void get_aux(double* a) const override { std::copy(A.begin(), A.end(), a); }
+    static void values(const std::vector<T>& v, double* out) {
+        for (size_t i = 0; i < v.size(); ++i) out[i] = zsme::value(v[i]);
+    }
+    void get_state(double* q) const override { values(X, q); }
+    void get_aux(double* a) const override { values(A, a); }
     void get_time(double* t, double* d) const override { *t = time; *d = dt; }
     void rhs(double t, const double* x, double* f) override {
         std::vector<T> xv(x, x + (size_t)C * NQ), fv;
         form_rhs(t, xv, fv);
-        std::copy(fv.begin(), fv.end(), f);
+        values(fv, f);
     }
     void gradient(const double* x, double* g) override {
         std::vector<T> xv(x, x + (size_t)C * NQ), gv((size_t)C * NQ * DIM);
         if (st.gradient == ZSME_GRADIENT_LSQ) gradient_lsq(xv, gv); else gradient_gg(xv, gv);
-        std::copy(gv.begin(), gv.end(), g);
+        values(gv, g);
+    }
+    // Seed the tangent direction of the (constrained) state and of the
+    // parameters; read the state's tangent.  Dual<1> instances only.
+    void set_tangent(const double* dq, const double* dp) override {
+        if constexpr (!std::is_same<T, double>::value) {
+            for (size_t i = 0; i < X.size(); ++i) X[i].d[0] = dq ? dq[i] : 0.0;
+            for (size_t k = 0; k < params.size(); ++k) params[k].d[0] = dp ? dp[k] : 0.0;
+        }
+    }
+    void get_tangent(double* dq) const override {
+        if constexpr (!std::is_same<T, double>::value)
+            for (size_t i = 0; i < X.size(); ++i) dq[i] = X[i].d[0];
     }
     void update_state() override { update_state_vec(X, A); }
     void source(double d) override { source_solve(d); }
@@ -702,18 +725,23 @@ struct Entry {
     int (*pw)(int, const double*, const double*, const double*, const double*, const double*,
               const double*, double, double*);
     int nq, na, np, dim;
+    OracleBase* (*make_tlm)(const zsme_mesh*, const zsme_settings*, const double*);
 };
 
 template <template <typename> class MT, template <typename> class NT>
 OracleBase* make_oracle(const zsme_mesh* m, const zsme_settings* s, const double* p) {
     return new Oracle<MT, NT>(m, s, p);
 }
+template <template <typename> class MT, template <typename> class NT>
+OracleBase* make_tlm(const zsme_mesh* m, const zsme_settings* s, const double* p) {
+    return new Oracle<MT, NT, zsme::Dual<1>>(m, s, p);
+}
 
 #define ORACLE_ENTRY(NS)                                                                   \
     Entry{#NS, &make_oracle<NS::Model, NS::Numerics>, &pointwise<NS::Model, NS::Numerics>,   \
           NS::Model<double>::n_dof_q,                                                      \
           NS::Model<double>::n_dof_qaux, NS::Model<double>::n_parameters,                  \
-          NS::Model<double>::dimension}
+          NS::Model<double>::dimension, &make_tlm<NS::Model, NS::Numerics>}
 
 const Entry kEntries[] = {
     ORACLE_ENTRY(sme1d_l0_malpasset), ORACLE_ENTRY(sme2d_l0), ORACLE_ENTRY(sme2d_l1),
@@ -760,6 +788,19 @@ int oracle_pointwise(const char* model, int fn, const double* qL, const double* 
         if (!std::strcmp(e.name, model)) return e.pw(fn, qL, qR, aL, aR, p, n, s, out);
     return fail(-ZSME_ERR_MODEL, std::string("unknown model ") + model);
 }
+// Tangent-linear instance: the same restatement on Dual<1> numbers.
+int oracle_create_tlm(const char* model, const zsme_mesh* mesh, const zsme_settings* s, const double* params,
+                      void** out) {
+    for (auto& e : kEntries)
+        if (!std::strcmp(e.name, model)) {
+            if (mesh->dim != e.dim) return fail(ZSME_ERR_ARG, "mesh dim != model dimension");
+            *out = e.make_tlm(mesh, s, params);
+            return 0;
+        }
+    return fail(ZSME_ERR_MODEL, std::string("unknown model ") + model);
+}
+int oracle_set_tangent(void* h, const double* dq, const double* dp) { ((OracleBase*)h)->set_tangent(dq, dp); return 0; }
+int oracle_get_tangent(void* h, double* dq) { ((OracleBase*)h)->get_tangent(dq); return 0; }
 int oracle_destroy(void* h) { delete (OracleBase*)h; return 0; }
 int oracle_set_state(void* h, const double* q, double t) { ((OracleBase*)h)->set_state(q, t); return 0; }
 int oracle_get_state(void* h, double* q) { ((OracleBase*)h)->get_state(q); return 0; }

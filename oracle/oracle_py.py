@@ -176,3 +176,43 @@ class Oracle:
 
     def newton_unconverged(self):
         return self.lib.oracle_newton_unconverged(self.h)
+
+
+class TangentOracle(Oracle):
+    """The oracle on Dual<1> numbers: one tangent-linear direction (state and
+    parameters) carried through the step (the branches are decided by the
+    values, as in the plain run)."""
+
+    def __init__(self, model: str, mesh_abi: dict, settings_struct, params=None, ref=False):
+        from zoomy_dmplex_b200 import native
+
+        self.lib = load(ref)
+        self.lib.oracle_create_tlm.argtypes = [ct.c_char_p, ct.c_void_p, ct.c_void_p, ct.POINTER(ct.c_double),
+                                               ct.POINTER(ct.c_void_p)]
+        self.lib.oracle_set_tangent.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
+        self.lib.oracle_get_tangent.argtypes = [ct.c_void_p, ct.POINTER(ct.c_double)]
+        self.info = model_info(model, ref)
+        self.nq = self.info["n_dof_q"]
+        self.na = self.info["n_dof_qaux"]
+        self.C = mesh_abi["n_cells"]
+        self._mesh_keep = native.make_mesh_struct(mesh_abi)
+        self._settings = settings_struct
+        h = ct.c_void_p()
+        self._params = np.ascontiguousarray(params, dtype=np.float64) if params is not None else None
+        pp = _p(self._params) if params is not None else None
+        rc = self.lib.oracle_create_tlm(model.encode(), ct.addressof(self._mesh_keep[0]),
+                                        ct.addressof(self._settings), pp, ct.byref(h))
+        if rc:
+            raise RuntimeError(self.lib.oracle_last_error().decode())
+        self.h = h
+
+    def set_tangent(self, dq=None, dp=None):
+        dq = np.zeros((self.C, self.nq)) if dq is None else np.ascontiguousarray(dq, dtype=np.float64)
+        dp = np.zeros(self.info["n_parameters"]) if dp is None else np.ascontiguousarray(dp, dtype=np.float64)
+        self._dq, self._dp = dq, dp
+        self.lib.oracle_set_tangent(self.h, _p(dq), _p(dp))
+
+    def get_tangent(self):
+        out = np.zeros((self.C, self.nq))
+        self.lib.oracle_get_tangent(self.h, _p(out))
+        return out

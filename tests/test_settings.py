@@ -16,7 +16,9 @@ def test_from_json_defaults_and_mapping(tmp_path):
     st = s.solver.to_struct()
     # any limiter other than "none" installs vacuum + TVD (Reconstruction.hpp:170-175)
     assert st.limiter == native.ZSME_LIMITER_TVD
-    assert st.gradient == native.ZSME_GRADIENT_LSQ
+    # Green-Gauss is what the reference's MUSCL path installs (ModularSolver.hpp:62-67)
+    assert st.gradient == native.ZSME_GRADIENT_GREEN_GAUSS
+    assert SolverSettings(gradient="least_squares").to_struct().gradient == native.ZSME_GRADIENT_LSQ
     assert s.parameters == {"g": 9.8, "n_manning": 0.03}
     assert SolverSettings(limiter="none").to_struct().limiter == native.ZSME_LIMITER_NONE
     assert SolverSettings().ssp_stages == 5          # reference default

@@ -48,8 +48,16 @@ def _state(level, h, b, hu=None, hv=None):
 
 
 def default_settings(**kw) -> SolverSettings:
+    """Order 2 with Vacuum + TVD (Barth-Jespersen ratio) limiting, two-stage
+    SSP-RK2, CFL 0.45, and the Green-Gauss gradient the reference's MUSCL path
+    installs (``ModularSolver.hpp:62-67``).  The least-squares gradient
+    (``gradient="least_squares"``) is never installed by that path; restated
+    as written, its one-sided wall stencil lets wall cells grow without bound
+    under inflow (flat bed, h = 1, u = 0.5 into reflective walls: |u| > 20 and
+    h < 0 within 40 steps on an 80x80 grid, and the level-2 case below within
+    100 steps), while Green-Gauss keeps the same runs bounded."""
     s = SolverSettings(t_end=1e9, cfl=0.45, reconstruction_order=2, limiter="tvd", ssp_stages=2,
-                       gradient="least_squares")
+                       gradient="green_gauss")
     for k, v in kw.items():
         setattr(s, k, v)
     return s
@@ -120,14 +128,44 @@ def ensemble_member(i: int, seed: int = 3, side_range=(40, 400)) -> Case:
 
 
 def adjoint_l1(n: int = 200, seed: int = 4, steps: int = 400, target: bool = False) -> Case:
-    """SME level 1 adjoint case: b = 0.2 bump; the target run perturbs b by
-    +0.02 exp(-((x-0.6)^2+(y-0.4)^2)/0.01); Manning n = 0.03."""
+    """SME level 1 adjoint case, Manning n = 0.03; the target run perturbs b by
+    +0.02 exp(-((x-0.6)^2+(y-0.4)^2)/0.01).
+
+    The state is chosen so that the discrete step is differentiable where it
+    starts: b = 0.2 bump + a bowl 0.1 |x - (0.4, 0.55)|^2, so that no
+    component is flat to round-off (a TVD ratio with |dq| just above the
+    reference's 1e-12 cut-off has an arbitrarily large slope); every velocity
+    and moment is non-zero (|u| at u = 0 is a kink of the Rusanov speed), with
+    the flow tapered towards the reflective walls."""
     m = meshmod.jittered_square(n, seed=seed)
     x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
-    b = 0.2 * _gauss(x, y, 0.5, 0.5, 0.01)
+    b = 0.2 * _gauss(x, y, 0.5, 0.5, 0.01) + 0.1 * ((x - 0.4) ** 2 + (y - 0.55) ** 2)
     if target:
         b = b + 0.02 * _gauss(x, y, 0.6, 0.4, 0.01)
-    h = 1.0 - b + 0.05 * _gauss(x, y, 0.3, 0.3, 0.005)
-    q = _state(1, h, b, hu=[0 * h] * 2, hv=[0 * h] * 2)
+    h = 1.0 - b + 0.05 * _gauss(x, y, 0.3, 0.3, 0.005) + 0.02 * x
+    w = (np.sin(np.pi * x) * np.sin(np.pi * y)) ** 2
+    u0 = w * (0.3 + 0.05 * np.sin(2 * np.pi * y)) + 0.02
+    v0 = w * (0.15 + 0.05 * np.cos(2 * np.pi * x)) + 0.01
+    q = _state(1, h, b, hu=[h * u0, h * 0.05 * w * (1 + 0.3 * x)],
+               hv=[h * v0, -h * 0.03 * w * (1 + 0.2 * y)])
     return Case("adjoint_l1_%d" % n, "sme2d_l1", m, q, default_settings(),
                 dict(g=9.81, n_manning=0.03, nu=0.0), steps)
+
+
+def _member(args):
+    i, seed, lo, hi = args
+    return ensemble_member(i, seed=seed, side_range=(lo, hi))
+
+
+def ensemble(n: int = 512, seed: int = 3, side_range=(40, 400), processes: int = 0):
+    """The n instances of the level-2 ensemble, built in parallel worker
+    processes (spawned, so it is safe after CUDA has been initialised)."""
+    import multiprocessing as mp
+    import os
+
+    args = [(i, seed, side_range[0], side_range[1]) for i in range(n)]
+    procs = processes or min(n, os.cpu_count() or 1)
+    if procs <= 1 or n < 4:
+        return [_member(a) for a in args]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(_member, args, chunksize=1)

@@ -1,0 +1,166 @@
+// Face fluxes, each face evaluated once, and the per-cell gather.
+//
+// face_kernel  one thread per face: reads the two reconstructed face states
+//              (face-indexed, coalesced), evaluates Numerics::numerical_flux
+//              and ::numerical_fluctuations (or the boundary ghost state) and
+//              stores nc_into_left*area, nc_into_right*area, flux*area
+//              (TransportStep.hpp:420-552).
+// gather_kernel one thread per cell: sums its faces' contributions in
+//              increasing original face order -- for each face first the
+//              fluctuation, then the flux, exactly the sequence of the
+//              reference's face loop (TransportStep.hpp:464-466, 529-531) --
+//              divides by the volume (555-560) and applies the SSP-RK(s,2)
+//              stage combination of PETSc's TSSSP "rks2" in the same pass.
+#pragma once
+
+namespace zsme {
+
+// faces [f0, f0 + fcount)
+// MINB: resident blocks per SM the register allocation must allow (1 = no cap)
+template <class M, class N, int MINB>
+__global__ void __launch_bounds__(128, MINB) face_kernel(MeshDev m, int f0, int fcount, const double* __restrict__ fs,
+                                                   const double* __restrict__ aux,
+                                                   const double* __restrict__ params, double t_host,
+                                                   const double* t_dev, double stage_frac,
+                                                   const double* __restrict__ dt_step, double* __restrict__ fb,
+                                                   const int* __restrict__ active) {
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
+    const int F = m.F, C = m.C;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= fcount) return;
+    const int f = f0 + r;
+    const int I = face_instance(m, f);
+    if (active && !active[I]) return;
+    const double* p = params + (size_t)I * m.np;
+    const int R = m.face_R[f];
+    const int bc = m.face_bc[f];
+    if (R < 0 && bc < 0) return;  // exterior face without a condition: no flux
+    const int L = m.face_L[f];
+    // stage time t0 + dt * i/(s-1) (only time-dependent BCs / aux see it)
+    const double t = t_dev ? (t_dev[I] + stage_frac * (dt_step ? dt_step[I] : 0.0)) : t_host;
+    const double area = m.farea[f];
+    const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
+    const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
+    double qL[NQ], aLc[NA];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) qL[i] = fs[(size_t)i * F + f];
+#pragma unroll
+    for (int i = 0; i < NA; ++i) aLc[i] = aux[(size_t)i * C + L];
+    double aL[NA], aR[NA];
+    if (R >= 0) {
+        double qR[NQ], aRc[NA];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) qR[i] = fs[((size_t)NQ + i) * F + f];
+#pragma unroll
+        for (int i = 0; i < NA; ++i) aRc[i] = aux[(size_t)i * C + R];
+        {
+            auto ra = M::update_aux_variables(qL, aLc, p, 0.0, xf);
+            auto rb = M::update_aux_variables(qR, aRc, p, 0.0, xf);
+#pragma unroll
+            for (int i = 0; i < NA; ++i) { aL[i] = ra[i]; aR[i] = rb[i]; }
+        }
+        const auto flux = N::numerical_flux(qL, qR, aL, aR, p, nh);
+        const auto nc = N::numerical_fluctuations(qL, qR, aL, aR, p, nh);
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) {
+            fb[(size_t)i * F + f] = nc[NQ + i] * area;
+            fb[((size_t)NQ + i) * F + f] = nc[i] * area;
+            fb[((size_t)2 * NQ + i) * F + f] = flux[i] * area;
+        }
+    } else {
+        {
+            auto ra = M::update_aux_variables(qL, aLc, p, t, xf);
+#pragma unroll
+            for (int i = 0; i < NA; ++i) aL[i] = ra[i];
+        }
+        const auto qR = M::boundary_conditions(bc, qL, aL, p, nh, xf, t, 0.0);
+        {
+            auto rb = M::update_aux_variables(qR.data, aL, p, t, xf);
+#pragma unroll
+            for (int i = 0; i < NA; ++i) aR[i] = rb[i];
+        }
+        const auto flux = N::numerical_flux(qL, qR.data, aL, aR, p, nh);
+        const auto nc = N::numerical_fluctuations(qL, qR.data, aL, aR, p, nh);
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) {
+            fb[(size_t)i * F + f] = nc[NQ + i] * area;
+            fb[((size_t)2 * NQ + i) * F + f] = flux[i] * area;
+        }
+    }
+}
+
+// cells [c0, c0 + cn)
+template <class M>
+__global__ void __launch_bounds__(128) gather_kernel(MeshDev m, Opts o, int c0, int cn,
+                                                     const double* __restrict__ fb, int mode, const double* x_in,
+                                                     double* x_out, double* base, const double* __restrict__ dt_step,
+                                                     const int* __restrict__ active) {
+    constexpr int NQ = M::n_dof_q;
+    const int C = m.C, F = m.F;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    const int I = cell_instance(m, c);
+    if (active && !active[I]) return;
+    double acc[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) acc[i] = 0.0;
+    const int ord = m.order[c];
+    for (int j = 0; j < m.K; ++j) {
+        const int k = (ord >> (2 * j)) & 3;
+        const int f = m.slot_face[k * C + c];
+        if (f < 0) continue;
+        const int meta = m.slot_meta[k * C + c];
+        if (m.slot_nbr[k * C + c] < 0 && meta_bc(meta) < 0) continue;
+        if (meta_isL(meta)) {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[(size_t)i * F + f];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)2 * NQ + i) * F + f];
+        } else {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)NQ + i) * F + f];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] += fb[((size_t)2 * NQ + i) * F + f];
+        }
+    }
+    const double v = m.vol[c];
+    if (v > 1e-15) {
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) acc[i] /= v;
+    }
+    const double h = dt_step ? dt_step[I] : 0.0;
+    const int s = o.stages;
+    switch (mode) {
+        case MODE_RHS:
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) x_out[(size_t)i * C + c] = acc[i];
+            break;
+        case MODE_FIRST:    // w = x + dt/(s-1) F
+        case MODE_MID: {    // w += dt/(s-1) F (in place)
+            const double a = h / (s - 1.);
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) x_out[(size_t)i * C + c] = x_in[(size_t)i * C + c] + a * acc[i];
+            break;
+        }
+        case MODE_FINAL: {  // X = (s-1)/s w + dt/s F + 1/s X
+            const double al = (s - 1.) / s, be = h / s, ga = 1. / s;
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                const size_t id = (size_t)i * C + c;
+                base[id] = al * x_in[id] + be * acc[i] + ga * base[id];
+            }
+            break;
+        }
+        case MODE_EULER: {  // X = X + dt F
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                const size_t id = (size_t)i * C + c;
+                base[id] = base[id] + h * acc[i];
+            }
+            break;
+        }
+    }
+}
+
+}  // namespace zsme

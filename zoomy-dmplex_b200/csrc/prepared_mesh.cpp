@@ -144,8 +144,14 @@ int prepare_mesh(const zsme_mesh& m, PreparedMesh& out) {
     p.fnr.assign(2 * (size_t)F, 0.0);
     p.fc.assign(2 * (size_t)F, 0.0);
     p.farea.assign(F, 0.0);
+    p.face_L.assign(F, -1);
+    p.face_R.assign(F, -1);
+    p.face_bc.assign(F, ZSME_FACE_INTERIOR);
     for (int i = 0; i < F; ++i) {
         const int f = fo[i];
+        p.face_L[i] = p.new_of_old[m.face_cells[2 * f]];
+        p.face_R[i] = m.face_cells[2 * f + 1] >= 0 ? p.new_of_old[m.face_cells[2 * f + 1]] : -1;
+        p.face_bc[i] = m.face_cells[2 * f + 1] >= 0 ? ZSME_FACE_INTERIOR : m.face_bc[f];
         double area = 0;
         for (int d = 0; d < D; ++d) area += m.face_normal[2 * f + d] * m.face_normal[2 * f + d];
         area = std::sqrt(area);
@@ -227,6 +233,93 @@ int prepare_mesh(const zsme_mesh& m, PreparedMesh& out) {
         for (int j = 0; j < K; ++j) code |= ks[j] << (2 * j);
         p.order[c] = code;
     }
+    p.n_inst = 1;
+    p.inst_cell_off = {0, C};
+    p.inst_face_off = {0, F};
+    return ZSME_OK;
+}
+
+int concat_meshes(std::vector<PreparedMesh>& parts, PreparedMesh& out) {
+    if (parts.empty()) return set_error(ZSME_ERR_ARG, "no instances");
+    const int K = parts[0].K, D = parts[0].dim;
+    long long Ct = 0, Ft = 0;
+    for (auto& p : parts) {
+        if (p.K != K || p.dim != D) return set_error(ZSME_ERR_MESH, "instances differ in dimension or max_faces");
+        Ct += p.C;
+        Ft += p.F;
+    }
+    if (Ct > 0x7fffffffLL || Ft > 0x7fffffffLL) return set_error(ZSME_ERR_LIMIT, "ensemble exceeds 2^31 cells/faces");
+    const int C = (int)Ct, F = (int)Ft, n = (int)parts.size();
+    PreparedMesh& o = out;
+    o = PreparedMesh();
+    o.dim = D;
+    o.K = K;
+    o.C = C;
+    o.F = F;
+    o.n_inst = n;
+    o.old_of_new.resize(C);
+    o.slot_nbr.resize((size_t)K * C);
+    o.slot_meta.resize((size_t)K * C);
+    o.slot_face.resize((size_t)K * C);
+    o.slot_dx.resize((size_t)2 * K * C);
+    o.slot_w.resize((size_t)2 * K * C);
+    o.vol.resize(C);
+    o.rc.resize(C);
+    o.order.resize(C);
+    o.fn.resize(2 * (size_t)F);
+    o.fc.resize(2 * (size_t)F);
+    o.fnr.resize(2 * (size_t)F);
+    o.farea.resize(F);
+    o.face_L.resize(F);
+    o.face_R.resize(F);
+    o.face_bc.resize(F);
+    o.cell_inst.resize(C);
+    o.face_inst.resize(F);
+    o.inst_cell_off.assign(n + 1, 0);
+    o.inst_face_off.assign(n + 1, 0);
+    int coff = 0, foff = 0;
+    for (int i = 0; i < n; ++i) {
+        PreparedMesh& p = parts[i];
+        o.inst_cell_off[i] = coff;
+        o.inst_face_off[i] = foff;
+        for (int c = 0; c < p.C; ++c) {
+            const int g = coff + c;
+            o.old_of_new[g] = p.old_of_new[c];
+            o.vol[g] = p.vol[c];
+            o.rc[g] = p.rc[c];
+            o.order[g] = p.order[c];
+            o.cell_inst[g] = i;
+            for (int k = 0; k < K; ++k) {
+                const size_t s = (size_t)k * p.C + c, t = (size_t)k * C + g;
+                const int nb = p.slot_nbr[s], fa = p.slot_face[s];
+                o.slot_nbr[t] = nb >= 0 ? nb + coff : nb;
+                o.slot_face[t] = fa >= 0 ? fa + foff : fa;
+                o.slot_meta[t] = p.slot_meta[s];
+                for (int d = 0; d < 2; ++d) {
+                    o.slot_dx[((size_t)k * 2 + d) * C + g] = p.slot_dx[((size_t)k * 2 + d) * p.C + c];
+                    o.slot_w[((size_t)k * 2 + d) * C + g] = p.slot_w[((size_t)k * 2 + d) * p.C + c];
+                }
+            }
+        }
+        for (int f = 0; f < p.F; ++f) {
+            const int g = foff + f;
+            o.farea[g] = p.farea[f];
+            o.face_L[g] = p.face_L[f] + coff;
+            o.face_R[g] = p.face_R[f] >= 0 ? p.face_R[f] + coff : -1;
+            o.face_bc[g] = p.face_bc[f];
+            o.face_inst[g] = i;
+            for (int d = 0; d < 2; ++d) {
+                o.fn[(size_t)d * F + g] = p.fn[(size_t)d * p.F + f];
+                o.fc[(size_t)d * F + g] = p.fc[(size_t)d * p.F + f];
+                o.fnr[(size_t)d * F + g] = p.fnr[(size_t)d * p.F + f];
+            }
+        }
+        coff += p.C;
+        foff += p.F;
+        p = PreparedMesh();  // release the part
+    }
+    o.inst_cell_off[n] = coff;
+    o.inst_face_off[n] = foff;
     return ZSME_OK;
 }
 

@@ -11,21 +11,35 @@ namespace zsme {
 
 // Mesh in the device layout: cells renumbered along a Hilbert curve, faces
 // renumbered by their first cell, per-cell "slots" in the caller's cone order.
+// Several independent instances (an ensemble) are concatenated cell- and
+// face-wise; old_of_new then holds instance-local caller ids.
 struct PreparedMesh {
     int dim = 2, C = 0, F = 0, K = 0;
-    std::vector<int> old_of_new;           // [C] caller cell id of device cell c
-    std::vector<int> new_of_old;           // [C]
+    std::vector<int> old_of_new;           // [C] caller cell id of device cell c (within its instance)
+    std::vector<int> new_of_old;           // [C] (single instance only)
     std::vector<int> slot_nbr, slot_meta, slot_face;  // [K][C]
     std::vector<double> slot_dx, slot_w;   // [K][2][C]
     std::vector<double> vol, rc;           // [C]
     std::vector<int> order;                // [C]
     std::vector<double> fn, farea, fc, fnr;  // [2][F], [F], [2][F], [2][F]
     std::vector<int> face_old_of_new;      // [F]
+    std::vector<int> face_L, face_R, face_bc;  // [F] support (new cell ids) and marker
+    int n_inst = 1;
+    std::vector<int> inst_cell_off, inst_face_off;  // [n_inst + 1]
+    std::vector<int> cell_inst, face_inst;          // [C], [F] (n_inst > 1 only)
+};
+
+// Block sizes of the kernels (the autotuner's knobs).
+struct LaunchConfig {
+    int prep, face, gather, finalize;  // threads per block
+    int prep_occ = 1, face_occ = 1;    // register cap: blocks per SM (1, 2, 3 or 4)
 };
 
 // Builds the layout (validates the connectivity; computes the least-squares
 // weights as LeastSquaresGradient::Setup does, Gradient.hpp:222-298).
 int prepare_mesh(const zsme_mesh& m, PreparedMesh& out);
+// Concatenates prepared instances (same dim and K) into one layout.
+int concat_meshes(std::vector<PreparedMesh>& parts, PreparedMesh& out);
 
 int set_error(int code, const std::string& msg);
 
@@ -34,21 +48,24 @@ class SolverBase {
     virtual ~SolverBase() = default;
     virtual int n_dof_q() const = 0;
     virtual int n_dof_qaux() const = 0;
+    virtual int n_instances() const = 0;
     virtual int init(PreparedMesh&& pm, const zsme_settings& st, const double* params, int device) = 0;
     virtual int set_params(const double* params) = 0;
-    virtual int set_state(const double* q, double t, bool device) = 0;
-    virtual int get_state(double* q, bool device) = 0;
-    virtual int get_aux(double* a) = 0;
+    virtual int set_state(int inst, const double* q, double t, bool device) = 0;
+    virtual int get_state(int inst, double* q, bool device) = 0;
+    virtual int get_aux(int inst, double* a) = 0;
     virtual int rhs(double t, const double* x, double* f) = 0;
     virtual int update_state() = 0;
     virtual int source(double dt) = 0;
-    virtual int compute_dt(double* dt) = 0;
+    virtual int compute_dt(int inst, double* dt) = 0;
     virtual int step(int nsteps, const double* dts) = 0;
-    virtual int sync(zsme_diag* d) = 0;
+    virtual int sync(int inst, zsme_diag* d) = 0;
     virtual void* stream() = 0;
     virtual int launches_per_step() const = 0;
     virtual int set_profiling(int on) = 0;
     virtual int read_profile(double* ms, int64_t* n) = 0;
+    virtual int set_launch(const LaunchConfig& lc) = 0;
+    virtual LaunchConfig launch() const = 0;
 };
 
 }  // namespace zsme

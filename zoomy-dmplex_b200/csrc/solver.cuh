@@ -1,6 +1,8 @@
 // Host side of one model's solver: device buffers, the CUDA stream, the
 // captured CUDA graph of one time step, and the calls behind the C ABI.
-// Included once per model translation unit after the model plugin.
+// A solver advances one or several independent instances (an ensemble of
+// meshes, concatenated cell- and face-wise); every kernel launch covers all
+// instances.  Included once per model translation unit after the plugin.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -13,6 +15,8 @@
 #include "model_prelude.h"
 #include "prepared_mesh.h"
 #include "step_kernels.cuh"
+#include "face_kernels.cuh"
+#include "source_kernels.cuh"
 #include "zsme.h"
 
 namespace zsme {
@@ -45,6 +49,8 @@ struct DevBuf {
     }
 };
 
+static inline int blocks_for(long long n, int b) { return (int)((n + b - 1) / b); }
+
 template <template <typename> class MT, template <typename> class NT>
 class Solver final : public SolverBase {
     using M = MT<double>;
@@ -53,18 +59,22 @@ class Solver final : public SolverBase {
 
     PreparedMesh pm_;
     zsme_settings st_{};
-    int device_ = 0, block_ = 128, grid_ = 0;
+    int device_ = 0, n_inst_ = 1;
+    LaunchConfig lc_{};
     cudaStream_t stream_ = nullptr;
     cudaGraphExec_t graph_ = nullptr;
     // mesh
-    DevBuf<int> slot_nbr_, slot_meta_, slot_face_, order_, old_of_new_;
+    DevBuf<int> slot_nbr_, slot_meta_, slot_face_, order_, old_of_new_, face_L_, face_R_, face_bc_;
+    DevBuf<int> cell_inst_, face_inst_;
     DevBuf<double> slot_dx_, slot_w_, vol_, rc_, fn_, farea_, fc_, fnr_;
     // state
-    DevBuf<double> x_, w_, aux_, fs_, tmp_a_, tmp_b_, params_, scal_, partial_, dts_;
-    DevBuf<int> iscal_;
+    DevBuf<double> x_, w_, aux_, fs_, fb_, tmp_a_, tmp_b_, params_, dts_;
+    // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
+    DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
+    DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..3] diag
+    DevBuf<unsigned long long> ratio_;
     MeshDev md_{};
     Opts opts_{};
-    int64_t steps_ = 0;
     // per-kernel CUDA-event timing (zsme_set_profiling)
     bool profiling_ = false;
     std::vector<cudaEvent_t> ev_pool_;
@@ -80,7 +90,11 @@ class Solver final : public SolverBase {
         if (stream_) cudaStreamDestroy(stream_);
     }
 
-    // Event pair around one launch when profiling (outside graph capture).
+    int n_dof_q() const override { return NQ; }
+    int n_dof_qaux() const override { return NA; }
+    int n_instances() const override { return n_inst_; }
+
+    // ------------------------------------------------------- profiling
     void mark(int kind, bool start) {
         if (!profiling_) return;
         if (start) {
@@ -123,22 +137,36 @@ class Solver final : public SolverBase {
         return ZSME_OK;
     }
 
-    int n_dof_q() const override { return NQ; }
-    int n_dof_qaux() const override { return NA; }
+    // ------------------------------------------------------- set-up
+    int set_launch(const LaunchConfig& lc) override {
+        for (int b : {lc.prep, lc.face, lc.gather, lc.finalize})
+            if (b < 32 || b > 128 || b % 32) return set_error(ZSME_ERR_ARG, "block sizes must be 32, 64, 96 or 128");
+        for (int o : {lc.prep_occ, lc.face_occ})
+            if (o < 1 || o > 4) return set_error(ZSME_ERR_ARG, "occupancy caps must be 1..4 blocks per SM");
+        lc_ = lc;
+        if (graph_) {
+            cudaGraphExecDestroy(graph_);
+            graph_ = nullptr;
+        }
+        return ZSME_OK;
+    }
+    LaunchConfig launch() const override { return lc_; }
 
     int init(PreparedMesh&& pm, const zsme_settings& st, const double* params, int device) override {
         pm_ = std::move(pm);
         st_ = st;
         device_ = device;
+        n_inst_ = pm_.n_inst;
         if (pm_.dim != DIM) return set_error(ZSME_ERR_ARG, "mesh dimension does not match the model");
         if (st_.reconstruction_order >= 2 && st_.ssp_stages < 2)
             return set_error(ZSME_ERR_ARG, "ssp_stages must be >= 2");
-        block_ = st_.block_size > 0 ? st_.block_size : 128;
-        if (block_ % 32 || block_ > 128) return set_error(ZSME_ERR_ARG, "block_size must be a multiple of 32, <= 128");
         ZSME_CUDA(cudaSetDevice(device_));
         ZSME_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-        const int C = pm_.C;
-        grid_ = (C + block_ - 1) / block_;
+        LaunchConfig lc{128, 128, 128, 128};
+        if (st_.block_size > 0) lc.prep = lc.face = lc.gather = st_.block_size;
+        int rc = set_launch(lc);
+        if (rc) return rc;
+        const int C = pm_.C, F = pm_.F;
         ZSME_CUDA(slot_nbr_.upload(pm_.slot_nbr, stream_));
         ZSME_CUDA(slot_meta_.upload(pm_.slot_meta, stream_));
         ZSME_CUDA(slot_face_.upload(pm_.slot_face, stream_));
@@ -152,149 +180,209 @@ class Solver final : public SolverBase {
         ZSME_CUDA(farea_.upload(pm_.farea, stream_));
         ZSME_CUDA(fc_.upload(pm_.fc, stream_));
         ZSME_CUDA(fnr_.upload(pm_.fnr, stream_));
+        ZSME_CUDA(face_L_.upload(pm_.face_L, stream_));
+        ZSME_CUDA(face_R_.upload(pm_.face_R, stream_));
+        ZSME_CUDA(face_bc_.upload(pm_.face_bc, stream_));
+        if (n_inst_ > 1) {
+            ZSME_CUDA(cell_inst_.upload(pm_.cell_inst, stream_));
+            ZSME_CUDA(face_inst_.upload(pm_.face_inst, stream_));
+        }
         md_ = MeshDev{C, pm_.K, slot_nbr_.p, slot_meta_.p, slot_face_.p, slot_dx_.p, slot_w_.p, vol_.p,
-                      rc_.p, order_.p, fn_.p, farea_.p, fc_.p, fnr_.p, pm_.F};
+                      rc_.p, order_.p, fn_.p, farea_.p, fc_.p, fnr_.p, F, face_L_.p, face_R_.p,
+                      face_bc_.p, cell_inst_.p, face_inst_.p, NP};
         opts_ = Opts{st_.reconstruction_order, st_.limiter, st_.gradient, st_.ssp_stages, st_.source};
         ZSME_CUDA(x_.alloc((size_t)NQ * C));
         ZSME_CUDA(w_.alloc((size_t)NQ * C));
         ZSME_CUDA(aux_.alloc((size_t)NA * C));
-        ZSME_CUDA(fs_.alloc((size_t)pm_.K * NQ * C));
+        ZSME_CUDA(fs_.alloc((size_t)2 * NQ * F));
+        ZSME_CUDA(fb_.alloc((size_t)3 * NQ * F));
+        // staging for state (NQ per cell) and aux (NA per cell) conversions
         ZSME_CUDA(tmp_a_.alloc((size_t)std::max(NQ, NA) * C));
         ZSME_CUDA(tmp_b_.alloc((size_t)std::max(NQ, NA) * C));
         ZSME_CUDA(cudaMemsetAsync(x_.p, 0, x_.n * sizeof(double), stream_));
         ZSME_CUDA(cudaMemsetAsync(aux_.p, 0, aux_.n * sizeof(double), stream_));
-        // scalars: t, dt_cfl, dt_step, dt_src ; ints: active, step_idx, diag[3]
-        ZSME_CUDA(scal_.alloc(4));
+        for (auto* b : {&t_, &dt_cfl_, &dt_step_, &dt_aux_}) {
+            ZSME_CUDA(b->alloc(n_inst_));
+            ZSME_CUDA(cudaMemsetAsync(b->p, 0, n_inst_ * sizeof(double), stream_));
+        }
+        ZSME_CUDA(active_.alloc(n_inst_));
+        ZSME_CUDA(cudaMemsetAsync(active_.p, 0, n_inst_ * sizeof(int), stream_));
         ZSME_CUDA(iscal_.alloc(8));
-        ZSME_CUDA(cudaMemsetAsync(scal_.p, 0, 4 * sizeof(double), stream_));
         ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, 8 * sizeof(int), stream_));
-        ZSME_CUDA(partial_.alloc(grid_));
-        std::vector<double> pv(NP);
+        ZSME_CUDA(ratio_.alloc(n_inst_));
+        std::vector<unsigned long long> none(n_inst_, ZSME_RATIO_NONE);
+        ZSME_CUDA(cudaMemcpyAsync(ratio_.p, none.data(), n_inst_ * sizeof(unsigned long long),
+                                  cudaMemcpyHostToDevice, stream_));
+        std::vector<double> pv((size_t)NP * n_inst_);
         auto dp = M::default_parameters();
-        for (int i = 0; i < NP; ++i) pv[i] = params ? params[i] : dp[i];
+        for (int i = 0; i < n_inst_; ++i)
+            for (int k = 0; k < NP; ++k) pv[(size_t)i * NP + k] = params ? params[(size_t)i * NP + k] : dp[k];
         ZSME_CUDA(params_.upload(pv, stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
         return ZSME_OK;
     }
 
     StepDev step_dev(const double* dts) {
-        return StepDev{scal_.p + 0, scal_.p + 1, scal_.p + 2, iscal_.p + 0, dts, iscal_.p + 1,
-                       st_.t_end, st_.cfl, M::dt_max, partial_.p, grid_, iscal_.p + 2};
+        return StepDev{t_.p, dt_cfl_.p, dt_step_.p, active_.p, ratio_.p, dts, iscal_.p + 0, n_inst_,
+                       st_.t_end, st_.cfl, M::dt_max, iscal_.p + 1};
     }
 
     int set_params(const double* params) override {
-        ZSME_CUDA(cudaMemcpyAsync(params_.p, params, NP * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        ZSME_CUDA(cudaMemcpyAsync(params_.p, params, (size_t)NP * n_inst_ * sizeof(double), cudaMemcpyHostToDevice,
+                                  stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
+        return ZSME_OK;
+    }
+
+    int check_inst(int i) const {
+        if (i < 0 || i >= n_inst_) return set_error(ZSME_ERR_ARG, "instance index out of range");
         return ZSME_OK;
     }
 
     // ---------------------------------------------------------- state I/O
-    int set_state(const double* q, double t, bool device) override {
-        const int C = pm_.C;
+    int set_state(int inst, const double* q, double t, bool device) override {
+        int rc = check_inst(inst);
+        if (rc) return rc;
+        const int c0 = pm_.inst_cell_off[inst], cn = pm_.inst_cell_off[inst + 1] - c0;
         const double* src = q;
         if (!device) {
-            ZSME_CUDA(cudaMemcpyAsync(tmp_a_.p, q, (size_t)NQ * C * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(tmp_a_.p, q, (size_t)NQ * cn * sizeof(double), cudaMemcpyHostToDevice, stream_));
             src = tmp_a_.p;
         }
-        aos_to_soa_kernel<<<grid_, block_, 0, stream_>>>(src, x_.p, old_of_new_.p, C, NQ);
+        aos_to_soa_kernel<<<blocks_for(cn, 128), 128, 0, stream_>>>(src, x_.p, old_of_new_.p, c0, cn, pm_.C, NQ);
         ZSME_CUDA(cudaGetLastError());
-        ZSME_CUDA(cudaMemsetAsync(aux_.p, 0, aux_.n * sizeof(double), stream_));
-        ZSME_CUDA(cudaMemcpyAsync(scal_.p, &t, sizeof(double), cudaMemcpyHostToDevice, stream_));
-        ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, 8 * sizeof(int), stream_));
-        steps_ = 0;
+        for (int k = 0; k < NA; ++k)
+            ZSME_CUDA(cudaMemsetAsync(aux_.p + (size_t)k * pm_.C + c0, 0, cn * sizeof(double), stream_));
+        ZSME_CUDA(cudaMemcpyAsync(t_.p + inst, &t, sizeof(double), cudaMemcpyHostToDevice, stream_));
+        ZSME_CUDA(cudaMemsetAsync(active_.p + inst, 0, sizeof(int), stream_));
+        if (inst == 0) ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, 8 * sizeof(int), stream_));
         // constraints, then dt_start = max(ComputeTimeStep, min_dt)
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
-        finalize_kernel<M, N><<<grid_, block_, 0, stream_>>>(md_, x_.p, aux_.p, params_.p, sd, nullptr,
-                                                             FIN_POST | FIN_WRITE | FIN_DT);
+        finalize_kernel<M, N><<<blocks_for(cn, lc_.finalize), lc_.finalize, 0, stream_>>>(
+            md_, c0, cn, x_.p, aux_.p, params_.p, sd, nullptr, FIN_POST | FIN_WRITE | FIN_DT);
         ZSME_CUDA(cudaGetLastError());
-        end_step_kernel<<<1, 256, 0, stream_>>>(sd, 0, st_.min_dt);
+        end_step_kernel<<<1, 32, 0, stream_>>>(step_dev(nullptr), inst, 1, 0, st_.min_dt, nullptr);
         ZSME_CUDA(cudaGetLastError());
         ZSME_CUDA(cudaStreamSynchronize(stream_));
         return ZSME_OK;
     }
 
-    int get_soa(const double* soa, int nv, double* out, bool device) {
-        const int C = pm_.C;
+    int get_soa(int inst, const double* soa, int nv, double* out, bool device) {
+        const int c0 = pm_.inst_cell_off[inst], cn = pm_.inst_cell_off[inst + 1] - c0;
         double* dst = device ? out : tmp_b_.p;
-        soa_to_aos_kernel<<<grid_, block_, 0, stream_>>>(soa, dst, old_of_new_.p, C, nv);
+        soa_to_aos_kernel<<<blocks_for(cn, 128), 128, 0, stream_>>>(soa, dst, old_of_new_.p, c0, cn, pm_.C, nv);
         ZSME_CUDA(cudaGetLastError());
         if (!device)
-            ZSME_CUDA(cudaMemcpyAsync(out, tmp_b_.p, (size_t)nv * C * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(out, tmp_b_.p, (size_t)nv * cn * sizeof(double), cudaMemcpyDeviceToHost, stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
         return ZSME_OK;
     }
-    int get_state(double* q, bool device) override { return get_soa(x_.p, NQ, q, device); }
-    int get_aux(double* a) override { return get_soa(aux_.p, NA, a, false); }
+    int get_state(int inst, double* q, bool device) override {
+        int rc = check_inst(inst);
+        return rc ? rc : get_soa(inst, x_.p, NQ, q, device);
+    }
+    int get_aux(int inst, double* a) override {
+        int rc = check_inst(inst);
+        return rc ? rc : get_soa(inst, aux_.p, NA, a, false);
+    }
 
     // ---------------------------------------------------------- pieces
     void launch_prep(const double* w, const int* active) {
         mark(ZSME_KERNEL_PREP, true);
-        prep_kernel<M><<<grid_, block_, 0, stream_>>>(md_, opts_, w, aux_.p, params_.p, fs_.p, active);
+        const int gb = blocks_for(pm_.C, lc_.prep);
+        switch (lc_.prep_occ) {
+#define ZSME_PREP(OCC)                                                                                          \
+    case OCC:                                                                                                   \
+        prep_kernel<M, OCC><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, aux_.p, params_.p, fs_.p,     \
+                                                          active);                                              \
+        break;
+            ZSME_PREP(2) ZSME_PREP(3) ZSME_PREP(4)
+            default: ZSME_PREP(1)
+#undef ZSME_PREP
+        }
         mark(ZSME_KERNEL_PREP, false);
     }
     void launch_flux(int mode, double t_host, const double* t_dev, double frac, const double* x_in, double* x_out,
                      double* base, const double* dt, const int* active) {
         mark(ZSME_KERNEL_FLUX, true);
-        flux_kernel<M, N><<<grid_, block_, 0, stream_>>>(md_, opts_, fs_.p, aux_.p, params_.p, mode, t_host, t_dev,
-                                                         frac, x_in, x_out, base, dt, active);
+        const int gf = blocks_for(pm_.F, lc_.face);
+        switch (lc_.face_occ) {
+#define ZSME_FACE(OCC)                                                                                          \
+    case OCC:                                                                                                   \
+        face_kernel<M, N, OCC><<<gf, lc_.face, 0, stream_>>>(md_, 0, pm_.F, fs_.p, aux_.p, params_.p, t_host,    \
+                                                             t_dev, frac, dt, fb_.p, active);                   \
+        break;
+            ZSME_FACE(2) ZSME_FACE(3) ZSME_FACE(4)
+            default: ZSME_FACE(1)
+#undef ZSME_FACE
+        }
         mark(ZSME_KERNEL_FLUX, false);
+        mark(ZSME_KERNEL_GATHER, true);
+        gather_kernel<M><<<blocks_for(pm_.C, lc_.gather), lc_.gather, 0, stream_>>>(md_, opts_, 0, pm_.C, fb_.p,
+                                                                                   mode, x_in, x_out, base, dt,
+                                                                                   active);
+        mark(ZSME_KERNEL_GATHER, false);
+    }
+    void launch_finalize(const StepDev& sd, const double* dt_src, int flags) {
+        mark(ZSME_KERNEL_FINALIZE, true);
+        finalize_kernel<M, N><<<blocks_for(pm_.C, lc_.finalize), lc_.finalize, 0, stream_>>>(
+            md_, 0, pm_.C, x_.p, aux_.p, params_.p, sd, dt_src, flags);
+        mark(ZSME_KERNEL_FINALIZE, false);
     }
 
     int rhs(double t, const double* x_aos, double* f_aos) override {
+        if (n_inst_ != 1) return set_error(ZSME_ERR_ARG, "zsme_rhs needs a single-instance handle");
         const int C = pm_.C;
         ZSME_CUDA(cudaMemcpyAsync(tmp_b_.p, x_aos, (size_t)NQ * C * sizeof(double), cudaMemcpyHostToDevice, stream_));
-        aos_to_soa_kernel<<<grid_, block_, 0, stream_>>>(tmp_b_.p, w_.p, old_of_new_.p, C, NQ);
+        aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(tmp_b_.p, w_.p, old_of_new_.p, 0, C, C, NQ);
         launch_prep(w_.p, nullptr);
         launch_flux(MODE_RHS, t, nullptr, 0.0, nullptr, tmp_a_.p, nullptr, nullptr, nullptr);
         ZSME_CUDA(cudaGetLastError());
-        return get_soa(tmp_a_.p, NQ, f_aos, false);
+        return get_soa(0, tmp_a_.p, NQ, f_aos, false);
     }
 
     int update_state() override {
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
-        finalize_kernel<M, N><<<grid_, block_, 0, stream_>>>(md_, x_.p, aux_.p, params_.p, sd, nullptr,
-                                                             FIN_PRE | FIN_WRITE);
+        launch_finalize(sd, nullptr, FIN_PRE | FIN_WRITE);
         ZSME_CUDA(cudaGetLastError());
         ZSME_CUDA(cudaStreamSynchronize(stream_));
         return ZSME_OK;
     }
 
     int source(double dt) override {
-        ZSME_CUDA(cudaMemcpyAsync(scal_.p + 3, &dt, sizeof(double), cudaMemcpyHostToDevice, stream_));
+        std::vector<double> d(n_inst_, dt);
+        ZSME_CUDA(cudaMemcpyAsync(dt_aux_.p, d.data(), n_inst_ * sizeof(double), cudaMemcpyHostToDevice, stream_));
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
-        finalize_kernel<M, N><<<grid_, block_, 0, stream_>>>(md_, x_.p, aux_.p, params_.p, sd, scal_.p + 3,
-                                                             FIN_SOURCE | FIN_WRITE);
+        launch_finalize(sd, dt_aux_.p, FIN_SOURCE | FIN_WRITE);
         ZSME_CUDA(cudaGetLastError());
         ZSME_CUDA(cudaStreamSynchronize(stream_));
         return ZSME_OK;
     }
 
-    int compute_dt(double* dt) override {
+    int compute_dt(int inst, double* dt) override {
+        int rc = check_inst(inst);
+        if (rc) return rc;
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
-        // a scratch CFL slot so that the resident dt is left alone
-        double* keep = sd.dt_cfl;
-        sd.dt_cfl = scal_.p + 3;
-        finalize_kernel<M, N><<<grid_, block_, 0, stream_>>>(md_, x_.p, aux_.p, params_.p, sd, nullptr, FIN_DT);
-        end_step_kernel<<<1, 256, 0, stream_>>>(sd, 0, -DBL_MAX);
+        launch_finalize(sd, nullptr, FIN_DT);
+        end_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_, 2, 0.0, dt_aux_.p);
         ZSME_CUDA(cudaGetLastError());
-        ZSME_CUDA(cudaMemcpyAsync(dt, sd.dt_cfl, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ZSME_CUDA(cudaMemcpyAsync(dt, dt_aux_.p + inst, sizeof(double), cudaMemcpyDeviceToHost, stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
-        (void)keep;
         return ZSME_OK;
     }
 
-    // One time step (MUSCLSolver.hpp:140-188) as a launch sequence.
+    // One time step of every instance (MUSCLSolver.hpp:140-188).
     void enqueue_step(const double* dts) {
         StepDev sd = step_dev(dts);
         const double* t = sd.t;
         const double* dt = sd.dt_step;
         const int* act = sd.active;
         mark(ZSME_KERNEL_BEGIN, true);
-        begin_step_kernel<<<1, 1, 0, stream_>>>(sd);
+        begin_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_);
         mark(ZSME_KERNEL_BEGIN, false);
         if (st_.reconstruction_order < 2) {
             launch_prep(x_.p, act);
@@ -311,27 +399,26 @@ class Solver final : public SolverBase {
             launch_flux(MODE_FINAL, 0.0, t, 1.0, w_.p, nullptr, x_.p, dt, act);
         }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
-        mark(ZSME_KERNEL_FINALIZE, true);
-        finalize_kernel<M, N><<<grid_, block_, 0, stream_>>>(md_, x_.p, aux_.p, params_.p, sd, sd.dt_step, flags);
-        mark(ZSME_KERNEL_FINALIZE, false);
+        launch_finalize(sd, sd.dt_step, flags);
         mark(ZSME_KERNEL_END, true);
-        end_step_kernel<<<1, 256, 0, stream_>>>(sd, 1, 0.0);
+        end_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_, 1, 0.0, nullptr);
         mark(ZSME_KERNEL_END, false);
     }
     int launches_per_step() const override {
-        return 3 + (st_.reconstruction_order < 2 ? 2 : 2 * st_.ssp_stages);
+        return 3 + (st_.reconstruction_order < 2 ? 3 : 3 * st_.ssp_stages);
     }
 
     int step(int nsteps, const double* dts_host) override {
         if (nsteps <= 0) return ZSME_OK;
-        ZSME_CUDA(cudaMemsetAsync(iscal_.p + 2, 0, 3 * sizeof(int), stream_));
+        if (dts_host && n_inst_ != 1) return set_error(ZSME_ERR_ARG, "imposed dts need a single-instance handle");
+        ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 3 * sizeof(int), stream_));
         if (dts_host || profiling_) {
             // imposed dts or per-kernel timing: plain launches (the step index
             // lives on the device)
             if (dts_host) {
                 ZSME_CUDA(dts_.alloc((size_t)nsteps));
                 ZSME_CUDA(cudaMemcpyAsync(dts_.p, dts_host, nsteps * sizeof(double), cudaMemcpyHostToDevice, stream_));
-                ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, sizeof(int), stream_));
+                ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));
             }
             for (int i = 0; i < nsteps; ++i) enqueue_step(dts_host ? dts_.p : nullptr);
             ZSME_CUDA(cudaGetLastError());
@@ -348,23 +435,25 @@ class Solver final : public SolverBase {
             }
             for (int i = 0; i < nsteps; ++i) ZSME_CUDA(cudaGraphLaunch(graph_, stream_));
         }
-        steps_ += nsteps;
         return ZSME_OK;
     }
 
-    int sync(zsme_diag* d) override {
+    int sync(int inst, zsme_diag* d) override {
+        int rc = check_inst(inst);
+        if (rc) return rc;
         ZSME_CUDA(cudaStreamSynchronize(stream_));
-        double sc[3];
+        double tt = 0, dd = 0;
         int is[8];
-        ZSME_CUDA(cudaMemcpy(sc, scal_.p, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+        ZSME_CUDA(cudaMemcpy(&tt, t_.p + inst, sizeof(double), cudaMemcpyDeviceToHost));
+        ZSME_CUDA(cudaMemcpy(&dd, dt_cfl_.p + inst, sizeof(double), cudaMemcpyDeviceToHost));
         ZSME_CUDA(cudaMemcpy(is, iscal_.p, 8 * sizeof(int), cudaMemcpyDeviceToHost));
         if (d) {
-            d->steps = is[1];
-            d->time = sc[0];
-            d->dt = sc[1];
-            d->n_nonfinite = is[2];
-            d->n_negative_depth = is[3];
-            d->n_newton_unconverged = is[4];
+            d->steps = is[0];
+            d->time = tt;
+            d->dt = dd;
+            d->n_nonfinite = is[1];
+            d->n_negative_depth = is[2];
+            d->n_newton_unconverged = is[3];
             d->reserved = 0;
         }
         return ZSME_OK;

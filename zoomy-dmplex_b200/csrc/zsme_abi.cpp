@@ -50,6 +50,13 @@ using zsme::set_error;
     do {                                                                    \
         if (!(h) || !(h)->s) return set_error(ZSME_ERR_ARG, "null handle"); \
     } while (0)
+// calls that address "the" state need a single-instance handle
+#define CHECK_SINGLE(h)                                                                              \
+    do {                                                                                             \
+        CHECK_H(h);                                                                                  \
+        if ((h)->s->n_instances() != 1)                                                              \
+            return set_error(ZSME_ERR_ARG, "batch handle: use the zsme_batch_* state functions");   \
+    } while (0)
 
 extern "C" {
 
@@ -100,29 +107,29 @@ int zsme_destroy(zsme_handle* h) {
 }
 
 int zsme_set_state(zsme_handle* h, const double* q, double t) {
-    CHECK_H(h);
+    CHECK_SINGLE(h);
     if (!q) return set_error(ZSME_ERR_ARG, "null state");
-    return h->s->set_state(q, t, false);
+    return h->s->set_state(0, q, t, false);
 }
 int zsme_set_state_device(zsme_handle* h, const double* q, double t) {
-    CHECK_H(h);
+    CHECK_SINGLE(h);
     if (!q) return set_error(ZSME_ERR_ARG, "null state");
-    return h->s->set_state(q, t, true);
+    return h->s->set_state(0, q, t, true);
 }
 int zsme_get_state(zsme_handle* h, double* q) {
-    CHECK_H(h);
+    CHECK_SINGLE(h);
     if (!q) return set_error(ZSME_ERR_ARG, "null output");
-    return h->s->get_state(q, false);
+    return h->s->get_state(0, q, false);
 }
 int zsme_get_state_device(zsme_handle* h, double* q) {
-    CHECK_H(h);
+    CHECK_SINGLE(h);
     if (!q) return set_error(ZSME_ERR_ARG, "null output");
-    return h->s->get_state(q, true);
+    return h->s->get_state(0, q, true);
 }
 int zsme_get_aux(zsme_handle* h, double* a) {
-    CHECK_H(h);
+    CHECK_SINGLE(h);
     if (!a) return set_error(ZSME_ERR_ARG, "null output");
-    return h->s->get_aux(a);
+    return h->s->get_aux(0, a);
 }
 int zsme_rhs(zsme_handle* h, double t, const double* x, double* f) {
     CHECK_H(h);
@@ -140,7 +147,7 @@ int zsme_source(zsme_handle* h, double dt) {
 int zsme_compute_dt(zsme_handle* h, double* dt) {
     CHECK_H(h);
     if (!dt) return set_error(ZSME_ERR_ARG, "null output");
-    return h->s->compute_dt(dt);
+    return h->s->compute_dt(0, dt);
 }
 int zsme_step(zsme_handle* h, int32_t n) {
     CHECK_H(h);
@@ -157,12 +164,12 @@ int zsme_step_dt(zsme_handle* h, int32_t n, const double* dts) {
 int zsme_get_diag(zsme_handle* h, zsme_diag* d) {
     CHECK_H(h);
     if (!d) return set_error(ZSME_ERR_ARG, "null output");
-    return h->s->sync(d);
+    return h->s->sync(0, d);
 }
 int zsme_sync(zsme_handle* h) {
     CHECK_H(h);
     zsme_diag d;
-    int rc = h->s->sync(&d);
+    int rc = h->s->sync(0, &d);
     if (rc) return rc;
     if (d.n_nonfinite > 0 || d.n_negative_depth > 0)
         return set_error(ZSME_ERR_STATE, "state check: " + std::to_string(d.n_nonfinite) + " non-finite, " +
@@ -172,7 +179,7 @@ int zsme_sync(zsme_handle* h) {
 int zsme_get_time(zsme_handle* h, double* t, double* dt) {
     CHECK_H(h);
     zsme_diag d;
-    int rc = h->s->sync(&d);
+    int rc = h->s->sync(0, &d);
     if (rc) return rc;
     if (t) *t = d.time;
     if (dt) *dt = d.dt;
@@ -197,6 +204,74 @@ int zsme_set_profiling(zsme_handle* h, int enable) {
 int zsme_read_profile(zsme_handle* h, double* ms, int64_t* n) {
     CHECK_H(h);
     return h->s->read_profile(ms, n);
+}
+
+int zsme_batch_create(const char* model, int32_t n, const zsme_mesh* meshes, const zsme_settings* settings,
+                      const double* params, int device, zsme_handle** out) {
+    if (!out || !meshes || !settings || n <= 0) return set_error(ZSME_ERR_ARG, "null argument or empty batch");
+    *out = nullptr;
+    const auto* e = zsme::find_model(model);
+    if (!e) return set_error(ZSME_ERR_MODEL, std::string("unknown model: ") + (model ? model : "(null)"));
+    if (settings->reconstruction_order < 1 || settings->reconstruction_order > 2)
+        return set_error(ZSME_ERR_ARG, "reconstruction_order must be 1 or 2");
+    if (!(settings->cfl > 0)) return set_error(ZSME_ERR_ARG, "cfl must be > 0");
+    std::vector<zsme::PreparedMesh> parts(n);
+    for (int i = 0; i < n; ++i) {
+        int rc = zsme::prepare_mesh(meshes[i], parts[i]);
+        if (rc) return set_error(rc, "instance " + std::to_string(i) + ": " + zsme_last_error());
+    }
+    zsme::PreparedMesh pm;
+    int rc = zsme::concat_meshes(parts, pm);
+    if (rc) return rc;
+    zsme::SolverBase* s = e->make();
+    rc = s->init(std::move(pm), *settings, params, device);
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    *out = new zsme_handle{s};
+    return ZSME_OK;
+}
+int zsme_batch_size(zsme_handle* h, int32_t* n) {
+    CHECK_H(h);
+    if (n) *n = h->s->n_instances();
+    return ZSME_OK;
+}
+int zsme_batch_set_state(zsme_handle* h, int32_t i, const double* q, double t) {
+    CHECK_H(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null state");
+    return h->s->set_state(i, q, t, false);
+}
+int zsme_batch_get_state(zsme_handle* h, int32_t i, double* q) {
+    CHECK_H(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->get_state(i, q, false);
+}
+int zsme_batch_get_time(zsme_handle* h, int32_t i, double* t, double* dt) {
+    CHECK_H(h);
+    zsme_diag d;
+    int rc = h->s->sync(i, &d);
+    if (rc) return rc;
+    if (t) *t = d.time;
+    if (dt) *dt = d.dt;
+    return ZSME_OK;
+}
+int zsme_set_launch(zsme_handle* h, const int32_t* blocks) {
+    CHECK_H(h);
+    if (!blocks) return set_error(ZSME_ERR_ARG, "null block sizes");
+    return h->s->set_launch(zsme::LaunchConfig{blocks[0], blocks[1], blocks[2], blocks[3], blocks[4], blocks[5]});
+}
+int zsme_get_launch(zsme_handle* h, int32_t* blocks) {
+    CHECK_H(h);
+    if (!blocks) return set_error(ZSME_ERR_ARG, "null output");
+    const zsme::LaunchConfig lc = h->s->launch();
+    blocks[0] = lc.prep;
+    blocks[1] = lc.face;
+    blocks[2] = lc.gather;
+    blocks[3] = lc.finalize;
+    blocks[4] = lc.prep_occ;
+    blocks[5] = lc.face_occ;
+    return ZSME_OK;
 }
 
 }  // extern "C"

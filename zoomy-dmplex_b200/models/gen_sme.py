@@ -118,8 +118,10 @@ class Printer:
             for a in e.args:
                 if isinstance(a, sp.Pow) and a.exp.is_Number and a.exp < 0:
                     den.append(sp.Pow(a.base, -a.exp, evaluate=False))
-                elif a.is_Rational and not a.is_Integer and a.p == 1:
-                    den.append(sp.Integer(a.q))
+                elif a.is_Rational and not a.is_Integer:
+                    # rational coefficient -> multiplication by its double
+                    # (an IEEE division by a constant costs a full sequence)
+                    num.insert(0, sp.Float(float(a), 17))
                 else:
                     num.append(a)
             ns = "*".join(self.p(a) for a in num) if num else "1.0"

@@ -51,8 +51,8 @@ struct Numerics {
     T t7 = 2.0*std::sqrt(2.0);
     SimpleArray<T, 3> res;
     res[0] = 0.0;
-    res[1] = (n[0]*((Q_minus[2]*t3/(t0)) + (Q_plus[2]*t6/(t4)))/2.0);
-    res[2] = (n[0]*((t3*t3)*(p[0] + (t3*t7*(Q_minus[2]*Q_minus[2])/((t0*t0)*std::sqrt(((t3*t3*t3*t3) + (std::max((T)1e-12, t2)*std::max((T)1e-12, t2)*std::max((T)1e-12, t2)*std::max((T)1e-12, t2))))))) + (t6*t6)*(p[0] + (t6*t7*(Q_plus[2]*Q_plus[2])/((t4*t4)*std::sqrt(((t6*t6*t6*t6) + (std::max((T)1e-12, t5)*std::max((T)1e-12, t5)*std::max((T)1e-12, t5)*std::max((T)1e-12, t5))))))))/4.0);
+    res[1] = 0.5*n[0]*((Q_minus[2]*t3/(t0)) + (Q_plus[2]*t6/(t4)));
+    res[2] = 0.25*n[0]*((t3*t3)*(p[0] + (t3*t7*(Q_minus[2]*Q_minus[2])/((t0*t0)*std::sqrt(((t3*t3*t3*t3) + (std::max((T)1e-12, t2)*std::max((T)1e-12, t2)*std::max((T)1e-12, t2)*std::max((T)1e-12, t2))))))) + (t6*t6)*(p[0] + (t6*t7*(Q_plus[2]*Q_plus[2])/((t4*t4)*std::sqrt(((t6*t6*t6*t6) + (std::max((T)1e-12, t5)*std::max((T)1e-12, t5)*std::max((T)1e-12, t5)*std::max((T)1e-12, t5))))))));
     return res;
     }
 
@@ -79,16 +79,16 @@ struct Numerics {
     T t12 = n[0]*t11;
     T t13 = t10*t8*(t4*t4*std::sqrt(t4));
     T t14 = std::max(t10*std::fabs((t12 + t13)), std::max(t5*std::fabs((t7 + t9)), std::max(t10*std::fabs((t12 - t13)), t5*std::fabs((t7 - t9)))));
-    T t15 = (t14*(t2 - t4)/2.0);
+    T t15 = 0.5*t14*(t2 - t4);
     T t16 = n[0]*p[0];
     T t17 = t14*(t6 - t11);
     SimpleArray<T, 6> res;
     res[0] = 0.0;
     res[1] = (-t15);
-    res[2] = ((-(t17/2.0)) - (t16*((Q_plus[1]*Q_plus[1]) - (t4*t4))/2.0));
+    res[2] = ((-0.5*t17) - 0.5*t16*((Q_plus[1]*Q_plus[1]) - (t4*t4)));
     res[3] = 0.0;
     res[4] = t15;
-    res[5] = ((t17/2.0) + (t16*((Q_minus[1]*Q_minus[1]) - (t2*t2))/2.0));
+    res[5] = (0.5*t17 + 0.5*t16*((Q_minus[1]*Q_minus[1]) - (t2*t2)));
     return res;
     }
 

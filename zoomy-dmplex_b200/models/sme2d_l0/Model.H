@@ -230,7 +230,7 @@ struct Model {
     T t5 = std::sqrt((1e-24 + t0*t3 + t0*t4));
     T t6 = p[0]*(p[3]*p[3]);
     T t7 = t5*t6;
-    T t8 = (4.0/3.0)*t7*std::pow(Qaux[0], (7.0/3.0));
+    T t8 = 1.3333333333333333*t7*std::pow(Qaux[0], (7.0/3.0));
     T t9 = (t6/(t5));
     T t10 = t9*std::pow(Qaux[0], (13.0/3.0))*(t3 + t4);
     T t11 = t9*std::pow(Qaux[0], (10.0/3.0));

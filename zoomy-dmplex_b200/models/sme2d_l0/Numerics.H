@@ -62,15 +62,15 @@ struct Numerics {
     T t18 = (t3*t3);
     T t19 = 2.0*t13;
     T t20 = t14*t19*t3;
-    T t21 = (n[0]/2.0);
+    T t21 = 0.5*n[0];
     T t22 = (t9*t9);
     T t23 = t16*t19*t9;
-    T t24 = (n[1]/2.0);
+    T t24 = 0.5*n[1];
     SimpleArray<T, 4> res;
     res[0] = 0.0;
-    res[1] = ((t10*t11/2.0) + (t10*t12/2.0) + (t4*t5/2.0) + (t4*t6/2.0));
-    res[2] = ((Q_minus[2]*t15*t6/2.0) + (Q_plus[2]*t12*t17/2.0) + (t18*t21*(p[0] + t20*(Q_minus[2]*Q_minus[2]))/2.0) + (t21*t22*(p[0] + t23*(Q_plus[2]*Q_plus[2]))/2.0));
-    res[3] = ((Q_minus[3]*t15*t5/2.0) + (Q_plus[3]*t11*t17/2.0) + (t18*t24*(p[0] + t20*(Q_minus[3]*Q_minus[3]))/2.0) + (t22*t24*(p[0] + t23*(Q_plus[3]*Q_plus[3]))/2.0));
+    res[1] = (0.5*t10*t11 + 0.5*t10*t12 + 0.5*t4*t5 + 0.5*t4*t6);
+    res[2] = (0.5*Q_minus[2]*t15*t6 + 0.5*Q_plus[2]*t12*t17 + 0.5*t18*t21*(p[0] + t20*(Q_minus[2]*Q_minus[2])) + 0.5*t21*t22*(p[0] + t23*(Q_plus[2]*Q_plus[2])));
+    res[3] = (0.5*Q_minus[3]*t15*t5 + 0.5*Q_plus[3]*t11*t17 + 0.5*t18*t24*(p[0] + t20*(Q_minus[3]*Q_minus[3])) + 0.5*t22*t24*(p[0] + t23*(Q_plus[3]*Q_plus[3])));
     return res;
     }
 
@@ -97,7 +97,7 @@ struct Numerics {
     T t12 = t11*(Q_plus[2]*n[0] + Q_plus[3]*n[1]);
     T t13 = t10*t8*(t4*t4*std::sqrt(t4));
     T t14 = std::max(t10*std::fabs((t12 + t13)), std::max(t5*std::fabs((t7 + t9)), std::max(t10*std::fabs((t12 - t13)), t5*std::fabs((t7 - t9)))));
-    T t15 = (t14*(t2 - t4)/2.0);
+    T t15 = 0.5*t14*(t2 - t4);
     T t16 = p[0]*((Q_plus[1]*Q_plus[1]) - (t4*t4));
     T t17 = t14*(Q_minus[2]*t6 - Q_plus[2]*t11);
     T t18 = t14*(Q_minus[3]*t6 - Q_plus[3]*t11);
@@ -105,12 +105,12 @@ struct Numerics {
     SimpleArray<T, 8> res;
     res[0] = 0.0;
     res[1] = (-t15);
-    res[2] = ((-(t17/2.0)) - (n[0]*t16/2.0));
-    res[3] = ((-(t18/2.0)) - (n[1]*t16/2.0));
+    res[2] = ((-0.5*t17) - 0.5*n[0]*t16);
+    res[3] = ((-0.5*t18) - 0.5*n[1]*t16);
     res[4] = 0.0;
     res[5] = t15;
-    res[6] = ((t17/2.0) + (n[0]*t19/2.0));
-    res[7] = ((t18/2.0) + (n[1]*t19/2.0));
+    res[6] = (0.5*t17 + 0.5*n[0]*t19);
+    res[7] = (0.5*t18 + 0.5*n[1]*t19);
     return res;
     }
 

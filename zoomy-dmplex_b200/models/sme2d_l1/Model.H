@@ -53,9 +53,9 @@ struct Model {
     SimpleArray<T, 6> res;
     res[0] = 0.0;
     res[1] = Q[2];
-    res[2] = Qaux[0]*((Q[2]*Q[2]) + ((Q[3]*Q[3])/3.0));
+    res[2] = Qaux[0]*((Q[2]*Q[2]) + 0.3333333333333333*(Q[3]*Q[3]));
     res[3] = 2.0*Q[2]*Q[3]*Qaux[0];
-    res[4] = Qaux[0]*(Q[2]*Q[4] + (Q[3]*Q[5]/3.0));
+    res[4] = Qaux[0]*(Q[2]*Q[4] + 0.3333333333333333*Q[3]*Q[5]);
     res[5] = Qaux[0]*(Q[2]*Q[5] + Q[3]*Q[4]);
     return res;
     }
@@ -68,9 +68,9 @@ struct Model {
     SimpleArray<T, 6> res;
     res[0] = 0.0;
     res[1] = Q[4];
-    res[2] = Qaux[0]*(Q[2]*Q[4] + (Q[3]*Q[5]/3.0));
+    res[2] = Qaux[0]*(Q[2]*Q[4] + 0.3333333333333333*Q[3]*Q[5]);
     res[3] = Qaux[0]*(Q[2]*Q[5] + Q[3]*Q[4]);
-    res[4] = Qaux[0]*((Q[4]*Q[4]) + ((Q[5]*Q[5])/3.0));
+    res[4] = Qaux[0]*((Q[4]*Q[4]) + 0.3333333333333333*(Q[5]*Q[5]));
     res[5] = 2.0*Q[4]*Q[5]*Qaux[0];
     return res;
     }
@@ -218,12 +218,12 @@ struct Model {
         const T* p)
     {
     T t0 = 2.0*Qaux[0];
-    T t1 = Qaux[0]*(Q[2]*Q[4] + (Q[3]*Q[5]/3.0));
+    T t1 = Qaux[0]*(Q[2]*Q[4] + 0.3333333333333333*Q[3]*Q[5]);
     T t2 = Qaux[0]*(Q[2]*Q[5] + Q[3]*Q[4]);
     SimpleArray<T, 12> res;
     res[0] = 0.0;
     res[1] = Q[2];
-    res[2] = Qaux[0]*((Q[2]*Q[2]) + ((Q[3]*Q[3])/3.0));
+    res[2] = Qaux[0]*((Q[2]*Q[2]) + 0.3333333333333333*(Q[3]*Q[3]));
     res[3] = Q[2]*Q[3]*t0;
     res[4] = t1;
     res[5] = t2;
@@ -231,7 +231,7 @@ struct Model {
     res[7] = Q[4];
     res[8] = t1;
     res[9] = t2;
-    res[10] = Qaux[0]*((Q[4]*Q[4]) + ((Q[5]*Q[5])/3.0));
+    res[10] = Qaux[0]*((Q[4]*Q[4]) + 0.3333333333333333*(Q[5]*Q[5]));
     res[11] = Q[4]*Q[5]*t0;
     return res;
     }
@@ -334,7 +334,7 @@ struct Model {
     T t6 = std::sqrt((1e-24 + t2*t4 + t2*t5));
     T t7 = p[0]*(p[3]*p[3]);
     T t8 = t6*t7;
-    T t9 = (4.0/3.0)*t8*std::pow(Qaux[0], (7.0/3.0));
+    T t9 = 1.3333333333333333*t8*std::pow(Qaux[0], (7.0/3.0));
     T t10 = (t7/(t6));
     T t11 = t10*std::pow(Qaux[0], (13.0/3.0))*(t4 + t5);
     T t12 = t10*std::pow(Qaux[0], (10.0/3.0));

@@ -73,17 +73,17 @@ struct Numerics {
     T t29 = t19*t9;
     T t30 = t25*t29;
     T t31 = t14*t29;
-    T t32 = (n[1]/2.0);
+    T t32 = 0.5*n[1];
     T t33 = t17*(Q_minus[2]*Q_minus[5] + Q_minus[3]*Q_minus[4]);
     T t34 = t20*(Q_plus[2]*Q_plus[5] + Q_plus[3]*Q_plus[4]);
     T t35 = n[0]*t14;
-    T t36 = (n[0]/2.0);
+    T t36 = 0.5*n[0];
     SimpleArray<T, 6> res;
     res[0] = 0.0;
-    res[1] = ((t10*t11/2.0) + (t10*t12/2.0) + (t4*t5/2.0) + (t4*t6/2.0));
-    res[2] = ((t15*t18/12.0) + (t15*t21/12.0) + (n[0]*t22*(t23 + t26*(Q_minus[2]*Q_minus[2]) + t27*(Q_minus[3]*Q_minus[3]))/12.0) + (n[0]*t28*(t23 + t30*(Q_plus[2]*Q_plus[2]) + t31*(Q_plus[3]*Q_plus[3]))/12.0));
+    res[1] = (0.5*t10*t11 + 0.5*t10*t12 + 0.5*t4*t5 + 0.5*t4*t6);
+    res[2] = (0.08333333333333333*t15*t18 + 0.08333333333333333*t15*t21 + 0.08333333333333333*n[0]*t22*(t23 + t26*(Q_minus[2]*Q_minus[2]) + t27*(Q_minus[3]*Q_minus[3])) + 0.08333333333333333*n[0]*t28*(t23 + t30*(Q_plus[2]*Q_plus[2]) + t31*(Q_plus[3]*Q_plus[3])));
     res[3] = t13*(t32*t33 + t32*t34 + Q_minus[3]*t17*t5 + Q_plus[3]*t11*t20);
-    res[4] = ((t18*t35/12.0) + (t21*t35/12.0) + (n[1]*t22*(t23 + t26*(Q_minus[4]*Q_minus[4]) + t27*(Q_minus[5]*Q_minus[5]))/12.0) + (n[1]*t28*(t23 + t30*(Q_plus[4]*Q_plus[4]) + t31*(Q_plus[5]*Q_plus[5]))/12.0));
+    res[4] = (0.08333333333333333*t18*t35 + 0.08333333333333333*t21*t35 + 0.08333333333333333*n[1]*t22*(t23 + t26*(Q_minus[4]*Q_minus[4]) + t27*(Q_minus[5]*Q_minus[5])) + 0.08333333333333333*n[1]*t28*(t23 + t30*(Q_plus[4]*Q_plus[4]) + t31*(Q_plus[5]*Q_plus[5])));
     res[5] = t13*(t33*t36 + t34*t36 + Q_minus[5]*t17*t6 + Q_plus[5]*t12*t20);
     return res;
     }
@@ -114,7 +114,7 @@ struct Numerics {
     T t15 = std::sqrt(((((Q_plus[3]*n[0] + Q_plus[5]*n[1])*(Q_plus[3]*n[0] + Q_plus[5]*n[1]))/(t11*t11)) + (p[0]*(t4*t4*t4)/(t14*t14))));
     T t16 = (t4/(t14));
     T t17 = std::max(t10*std::fabs((t7 + t9)), std::max(t16*std::fabs((t13 + t15)), std::max(t10*std::fabs((t7 - t9)), t16*std::fabs((t13 - t15)))));
-    T t18 = (t17*(t2 - t4)/2.0);
+    T t18 = 0.5*t17*(t2 - t4);
     T t19 = p[0]*((Q_plus[1]*Q_plus[1]) - (t4*t4));
     T t20 = t2*t6;
     T t21 = Q_minus[2]*t20;
@@ -125,7 +125,7 @@ struct Numerics {
     T t26 = 4.0*t17;
     T t27 = t25*t26;
     T t28 = (t2 + t4);
-    T t29 = (t28*std::sqrt(2.0)/std::sqrt(((std::max((T)1e-12, (t28/2.0))*std::max((T)1e-12, (t28/2.0))*std::max((T)1e-12, (t28/2.0))*std::max((T)1e-12, (t28/2.0))) + ((t28*t28*t28*t28)/16.0))));
+    T t29 = (t28*std::sqrt(2.0)/std::sqrt(((std::max((T)1e-12, 0.5*t28)*std::max((T)1e-12, 0.5*t28)*std::max((T)1e-12, 0.5*t28)*std::max((T)1e-12, 0.5*t28)) + 0.0625*(t28*t28*t28*t28))));
     T t30 = t29*(t21 + t23);
     T t31 = n[0]*t25;
     T t32 = (Q_minus[5]*t20 - Q_plus[5]*t22);
@@ -141,16 +141,16 @@ struct Numerics {
     SimpleArray<T, 12> res;
     res[0] = 0.0;
     res[1] = (-t18);
-    res[2] = ((-(t24/2.0)) - (n[0]*t19/2.0));
-    res[3] = ((-(t27/8.0)) + (t34/8.0));
-    res[4] = ((-(t37/2.0)) - (n[1]*t19/2.0));
-    res[5] = ((-(t38/8.0)) + (t40/8.0));
+    res[2] = ((-0.5*t24) - 0.5*n[0]*t19);
+    res[3] = ((-0.125*t27) + 0.125*t34);
+    res[4] = ((-0.5*t37) - 0.5*n[1]*t19);
+    res[5] = ((-0.125*t38) + 0.125*t40);
     res[6] = 0.0;
     res[7] = t18;
-    res[8] = ((t24/2.0) + (n[0]*t41/2.0));
-    res[9] = ((t27/8.0) + (t34/8.0));
-    res[10] = ((t37/2.0) + (n[1]*t41/2.0));
-    res[11] = ((t38/8.0) + (t40/8.0));
+    res[8] = (0.5*t24 + 0.5*n[0]*t41);
+    res[9] = (0.125*t27 + 0.125*t34);
+    res[10] = (0.5*t37 + 0.5*n[1]*t41);
+    res[11] = (0.125*t38 + 0.125*t40);
     return res;
     }
 

@@ -50,21 +50,21 @@ struct Model {
         const T* Qaux,
         const T* p)
     {
-    T t0 = ((Q[3]*Q[3])/3.0);
+    T t0 = 0.3333333333333333*(Q[3]*Q[3]);
     T t1 = (Q[4]*Q[4]);
-    T t2 = (2.0/5.0)*Q[4];
+    T t2 = 0.4*Q[4];
     T t3 = 2.0*Qaux[0];
     T t4 = Q[3]*Q[6];
     T t5 = Q[4]*Q[7];
     SimpleArray<T, 8> res;
     res[0] = 0.0;
     res[1] = Q[2];
-    res[2] = Qaux[0]*(t0 + (Q[2]*Q[2]) + (t1/5.0));
+    res[2] = Qaux[0]*(t0 + (Q[2]*Q[2]) + 0.2*t1);
     res[3] = Q[3]*t3*(Q[2] + t2);
-    res[4] = t3*(t0 + (t1/7.0) + Q[2]*Q[4]);
-    res[5] = Qaux[0]*((t4/3.0) + (t5/5.0) + Q[2]*Q[5]);
-    res[6] = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[6]*t2 + (2.0/5.0)*Q[3]*Q[7]);
-    res[7] = Qaux[0]*((2.0/3.0)*t4 + (2.0/7.0)*t5 + Q[2]*Q[7] + Q[4]*Q[5]);
+    res[4] = t3*(t0 + 0.14285714285714285*t1 + Q[2]*Q[4]);
+    res[5] = Qaux[0]*(0.3333333333333333*t4 + 0.2*t5 + Q[2]*Q[5]);
+    res[6] = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[6]*t2 + 0.4*Q[3]*Q[7]);
+    res[7] = Qaux[0]*(0.6666666666666666*t4 + 0.2857142857142857*t5 + Q[2]*Q[7] + Q[4]*Q[5]);
     return res;
     }
 
@@ -75,19 +75,19 @@ struct Model {
     {
     T t0 = Q[3]*Q[6];
     T t1 = Q[4]*Q[7];
-    T t2 = (2.0/5.0)*Q[7];
-    T t3 = ((Q[6]*Q[6])/3.0);
+    T t2 = 0.4*Q[7];
+    T t3 = 0.3333333333333333*(Q[6]*Q[6]);
     T t4 = (Q[7]*Q[7]);
     T t5 = 2.0*Qaux[0];
     SimpleArray<T, 8> res;
     res[0] = 0.0;
     res[1] = Q[5];
-    res[2] = Qaux[0]*((t0/3.0) + (t1/5.0) + Q[2]*Q[5]);
-    res[3] = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[3]*t2 + (2.0/5.0)*Q[4]*Q[6]);
-    res[4] = Qaux[0]*((2.0/3.0)*t0 + (2.0/7.0)*t1 + Q[2]*Q[7] + Q[4]*Q[5]);
-    res[5] = Qaux[0]*(t3 + (Q[5]*Q[5]) + (t4/5.0));
+    res[2] = Qaux[0]*(0.3333333333333333*t0 + 0.2*t1 + Q[2]*Q[5]);
+    res[3] = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[3]*t2 + 0.4*Q[4]*Q[6]);
+    res[4] = Qaux[0]*(0.6666666666666666*t0 + 0.2857142857142857*t1 + Q[2]*Q[7] + Q[4]*Q[5]);
+    res[5] = Qaux[0]*(t3 + (Q[5]*Q[5]) + 0.2*t4);
     res[6] = Q[6]*t5*(Q[5] + t2);
-    res[7] = t5*(t3 + (t4/7.0) + Q[5]*Q[7]);
+    res[7] = t5*(t3 + 0.14285714285714285*t4 + Q[5]*Q[7]);
     return res;
     }
 
@@ -126,8 +126,8 @@ struct Model {
     res[24] = 0.0;
     res[25] = 0.0;
     res[26] = 0.0;
-    res[27] = Qaux[0]*((-Q[2]) + (Q[4]/5.0));
-    res[28] = (-(t0/5.0));
+    res[27] = Qaux[0]*((-Q[2]) + 0.2*Q[4]);
+    res[28] = (-0.2*t0);
     res[29] = 0.0;
     res[30] = 0.0;
     res[31] = 0.0;
@@ -135,7 +135,7 @@ struct Model {
     res[33] = 0.0;
     res[34] = 0.0;
     res[35] = (-t0);
-    res[36] = (-Qaux[0]*(Q[2] + (Q[4]/7.0)));
+    res[36] = (-Qaux[0]*(Q[2] + 0.14285714285714285*Q[4]));
     res[37] = 0.0;
     res[38] = 0.0;
     res[39] = 0.0;
@@ -150,8 +150,8 @@ struct Model {
     res[48] = 0.0;
     res[49] = 0.0;
     res[50] = 0.0;
-    res[51] = Qaux[0]*((-Q[5]) + (Q[7]/5.0));
-    res[52] = (-(t1/5.0));
+    res[51] = Qaux[0]*((-Q[5]) + 0.2*Q[7]);
+    res[52] = (-0.2*t1);
     res[53] = 0.0;
     res[54] = 0.0;
     res[55] = 0.0;
@@ -159,7 +159,7 @@ struct Model {
     res[57] = 0.0;
     res[58] = 0.0;
     res[59] = (-t1);
-    res[60] = (-Qaux[0]*(Q[5] + (Q[7]/7.0)));
+    res[60] = (-Qaux[0]*(Q[5] + 0.14285714285714285*Q[7]));
     res[61] = 0.0;
     res[62] = 0.0;
     res[63] = 0.0;
@@ -204,8 +204,8 @@ struct Model {
     res[27] = 0.0;
     res[28] = 0.0;
     res[29] = 0.0;
-    res[30] = Qaux[0]*((-Q[2]) + (Q[4]/5.0));
-    res[31] = (-(t0/5.0));
+    res[30] = Qaux[0]*((-Q[2]) + 0.2*Q[4]);
+    res[31] = (-0.2*t0);
     res[32] = 0.0;
     res[33] = 0.0;
     res[34] = 0.0;
@@ -213,7 +213,7 @@ struct Model {
     res[36] = 0.0;
     res[37] = 0.0;
     res[38] = (-t0);
-    res[39] = (-Qaux[0]*(Q[2] + (Q[4]/7.0)));
+    res[39] = (-Qaux[0]*(Q[2] + 0.14285714285714285*Q[4]));
     res[40] = Q[1]*p[0];
     res[41] = 0.0;
     res[42] = 0.0;
@@ -228,8 +228,8 @@ struct Model {
     res[51] = 0.0;
     res[52] = 0.0;
     res[53] = 0.0;
-    res[54] = Qaux[0]*((-Q[5]) + (Q[7]/5.0));
-    res[55] = (-(t1/5.0));
+    res[54] = Qaux[0]*((-Q[5]) + 0.2*Q[7]);
+    res[55] = (-0.2*t1);
     res[56] = 0.0;
     res[57] = 0.0;
     res[58] = 0.0;
@@ -237,7 +237,7 @@ struct Model {
     res[60] = 0.0;
     res[61] = 0.0;
     res[62] = (-t1);
-    res[63] = (-Qaux[0]*(Q[5] + (Q[7]/7.0)));
+    res[63] = (-Qaux[0]*(Q[5] + 0.14285714285714285*Q[7]));
     return res;
     }
 
@@ -249,7 +249,7 @@ struct Model {
     {
     T t0 = std::max((T)1e-14, Q[1]);
     T t1 = (1.0/(t0));
-    T t2 = std::sqrt((((Q[3]*n[0] + Q[6]*n[1])*(Q[3]*n[0] + Q[6]*n[1])) + (3.0/5.0)*((Q[4]*n[0] + Q[7]*n[1])*(Q[4]*n[0] + Q[7]*n[1])) + (p[0]*std::max((T)0.0, (Q[1]*Q[1]*Q[1]*Q[1]*Q[1]))/(t0*t0))));
+    T t2 = std::sqrt((((Q[3]*n[0] + Q[6]*n[1])*(Q[3]*n[0] + Q[6]*n[1])) + 0.6*((Q[4]*n[0] + Q[7]*n[1])*(Q[4]*n[0] + Q[7]*n[1])) + (p[0]*std::max((T)0.0, (Q[1]*Q[1]*Q[1]*Q[1]*Q[1]))/(t0*t0))));
     T t3 = (Q[2]*n[0] + Q[5]*n[1]);
     T t4 = t1*t3;
     SimpleArray<T, 8> res;
@@ -299,24 +299,24 @@ struct Model {
         const T* Qaux,
         const T* p)
     {
-    T t0 = ((Q[3]*Q[3])/3.0);
+    T t0 = 0.3333333333333333*(Q[3]*Q[3]);
     T t1 = (Q[4]*Q[4]);
-    T t2 = (2.0/5.0)*Q[4];
+    T t2 = 0.4*Q[4];
     T t3 = 2.0*Qaux[0];
     T t4 = Q[3]*Q[6];
     T t5 = Q[4]*Q[7];
-    T t6 = Qaux[0]*((t4/3.0) + (t5/5.0) + Q[2]*Q[5]);
-    T t7 = (2.0/5.0)*Q[7];
+    T t6 = Qaux[0]*(0.3333333333333333*t4 + 0.2*t5 + Q[2]*Q[5]);
+    T t7 = 0.4*Q[7];
     T t8 = Qaux[0]*(Q[2]*Q[6] + Q[3]*Q[5] + Q[3]*t7 + Q[6]*t2);
-    T t9 = Qaux[0]*((2.0/3.0)*t4 + (2.0/7.0)*t5 + Q[2]*Q[7] + Q[4]*Q[5]);
-    T t10 = ((Q[6]*Q[6])/3.0);
+    T t9 = Qaux[0]*(0.6666666666666666*t4 + 0.2857142857142857*t5 + Q[2]*Q[7] + Q[4]*Q[5]);
+    T t10 = 0.3333333333333333*(Q[6]*Q[6]);
     T t11 = (Q[7]*Q[7]);
     SimpleArray<T, 16> res;
     res[0] = 0.0;
     res[1] = Q[2];
-    res[2] = Qaux[0]*(t0 + (Q[2]*Q[2]) + (t1/5.0));
+    res[2] = Qaux[0]*(t0 + (Q[2]*Q[2]) + 0.2*t1);
     res[3] = Q[3]*t3*(Q[2] + t2);
-    res[4] = t3*(t0 + (t1/7.0) + Q[2]*Q[4]);
+    res[4] = t3*(t0 + 0.14285714285714285*t1 + Q[2]*Q[4]);
     res[5] = t6;
     res[6] = t8;
     res[7] = t9;
@@ -325,9 +325,9 @@ struct Model {
     res[10] = t6;
     res[11] = t8;
     res[12] = t9;
-    res[13] = Qaux[0]*(t10 + (Q[5]*Q[5]) + (t11/5.0));
+    res[13] = Qaux[0]*(t10 + (Q[5]*Q[5]) + 0.2*t11);
     res[14] = Q[6]*t3*(Q[5] + t7);
-    res[15] = t3*(t10 + (t11/7.0) + Q[5]*Q[7]);
+    res[15] = t3*(t10 + 0.14285714285714285*t11 + Q[5]*Q[7]);
     return res;
     }
 
@@ -337,16 +337,16 @@ struct Model {
         const T* p)
     {
     T t0 = Q[1]*p[0];
-    T t1 = Qaux[0]*((-Q[2]) + (Q[4]/5.0));
+    T t1 = Qaux[0]*((-Q[2]) + 0.2*Q[4]);
     T t2 = Q[3]*Qaux[0];
-    T t3 = (-(t2/5.0));
+    T t3 = (-0.2*t2);
     T t4 = (-t2);
-    T t5 = (-Qaux[0]*(Q[2] + (Q[4]/7.0)));
-    T t6 = Qaux[0]*((-Q[5]) + (Q[7]/5.0));
+    T t5 = (-Qaux[0]*(Q[2] + 0.14285714285714285*Q[4]));
+    T t6 = Qaux[0]*((-Q[5]) + 0.2*Q[7]);
     T t7 = Q[6]*Qaux[0];
-    T t8 = (-(t7/5.0));
+    T t8 = (-0.2*t7);
     T t9 = (-t7);
-    T t10 = (-Qaux[0]*(Q[5] + (Q[7]/7.0)));
+    T t10 = (-Qaux[0]*(Q[5] + 0.14285714285714285*Q[7]));
     SimpleArray<T, 128> res;
     res[0] = 0.0;
     res[1] = 0.0;
@@ -493,7 +493,7 @@ struct Model {
     T t6 = std::sqrt((1e-24 + t2*t4 + t2*t5));
     T t7 = p[0]*(p[3]*p[3]);
     T t8 = t6*t7;
-    T t9 = (4.0/3.0)*t8*std::pow(Qaux[0], (7.0/3.0));
+    T t9 = 1.3333333333333333*t8*std::pow(Qaux[0], (7.0/3.0));
     T t10 = (t7/(t6));
     T t11 = t10*std::pow(Qaux[0], (13.0/3.0))*(t4 + t5);
     T t12 = t10*std::pow(Qaux[0], (10.0/3.0));

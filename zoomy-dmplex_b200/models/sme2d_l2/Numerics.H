@@ -97,25 +97,25 @@ struct Numerics {
     T t53 = 5.0*Q_plus[5];
     T t54 = 2.0*Q_plus[7];
     T t55 = (Q_plus[3]*t53 + Q_plus[3]*t54 + Q_plus[6]*t46 + Q_plus[6]*t47);
-    T t56 = (t13/10.0);
+    T t56 = 0.1*t13;
     T t57 = 21.0*Q_minus[2];
     T t58 = 21.0*Q_plus[2];
     T t59 = 21.0*Q_minus[5];
     T t60 = (6.0*t15 + 14.0*t14 + Q_minus[4]*t59 + Q_minus[7]*t57);
     T t61 = 21.0*Q_plus[5];
     T t62 = (6.0*t22 + 14.0*t21 + Q_plus[4]*t61 + Q_plus[7]*t58);
-    T t63 = (t13/42.0);
+    T t63 = 0.023809523809523808*t13;
     T t64 = (Q_minus[6]*Q_minus[6]);
     T t65 = (Q_minus[7]*Q_minus[7]);
     T t66 = (Q_plus[6]*Q_plus[6]);
     T t67 = (Q_plus[7]*Q_plus[7]);
     SimpleArray<T, 8> res;
     res[0] = 0.0;
-    res[1] = ((Q_minus[2]*n[0]*t4/2.0) + (Q_minus[5]*n[1]*t4/2.0) + (Q_plus[2]*n[0]*t8/2.0) + (Q_plus[5]*n[1]*t8/2.0));
-    res[2] = ((t12*t16/60.0) + (t20*t23/60.0) + (n[0]*t24*(t25 + t28*(Q_minus[2]*Q_minus[2]) + t29*t30 + t31*t33)/60.0) + (n[0]*t34*(t25 + t37*(Q_plus[2]*Q_plus[2]) + t38*t39 + t40*t41)/60.0));
+    res[1] = (0.5*Q_minus[2]*n[0]*t4 + 0.5*Q_minus[5]*n[1]*t4 + 0.5*Q_plus[2]*n[0]*t8 + 0.5*Q_plus[5]*n[1]*t8);
+    res[2] = (0.016666666666666666*t12*t16 + 0.016666666666666666*t20*t23 + 0.016666666666666666*n[0]*t24*(t25 + t28*(Q_minus[2]*Q_minus[2]) + t29*t30 + t31*t33) + 0.016666666666666666*n[0]*t34*(t25 + t37*(Q_plus[2]*Q_plus[2]) + t38*t39 + t40*t41));
     res[3] = t56*(t11*t52 + t19*t55 + Q_minus[3]*t45*(t42 + t43) + Q_plus[3]*t49*(t46 + t47));
     res[4] = t63*(t11*t60 + t19*t62 + t45*(3.0*t31 + 7.0*t29 + Q_minus[4]*t57) + t49*(3.0*t40 + 7.0*t38 + Q_plus[4]*t58));
-    res[5] = ((t16*t45/60.0) + (t23*t49/60.0) + (n[1]*t24*(t25 + t28*(Q_minus[5]*Q_minus[5]) + t30*t64 + t33*t65)/60.0) + (n[1]*t34*(t25 + t37*(Q_plus[5]*Q_plus[5]) + t39*t66 + t41*t67)/60.0));
+    res[5] = (0.016666666666666666*t16*t45 + 0.016666666666666666*t23*t49 + 0.016666666666666666*n[1]*t24*(t25 + t28*(Q_minus[5]*Q_minus[5]) + t30*t64 + t33*t65) + 0.016666666666666666*n[1]*t34*(t25 + t37*(Q_plus[5]*Q_plus[5]) + t39*t66 + t41*t67));
     res[6] = t56*(t44*t52 + t48*t55 + Q_minus[6]*t12*(t50 + t51) + Q_plus[6]*t20*(t53 + t54));
     res[7] = t63*(t12*(3.0*t65 + 7.0*t64 + Q_minus[7]*t59) + t20*(3.0*t67 + 7.0*t66 + Q_plus[7]*t61) + t44*t60 + t48*t62);
     return res;
@@ -139,17 +139,17 @@ struct Numerics {
     T t7 = t6*(Q_minus[2]*n[0] + Q_minus[5]*n[1]);
     T t8 = (1.0/(t5*t5));
     T t9 = std::max((T)1e-14, t1);
-    T t10 = std::sqrt((t8*((Q_minus[3]*n[0] + Q_minus[6]*n[1])*(Q_minus[3]*n[0] + Q_minus[6]*n[1])) + (3.0/5.0)*t8*((Q_minus[4]*n[0] + Q_minus[7]*n[1])*(Q_minus[4]*n[0] + Q_minus[7]*n[1])) + (p[0]*(t2*t2*t2)/(t9*t9))));
+    T t10 = std::sqrt((t8*((Q_minus[3]*n[0] + Q_minus[6]*n[1])*(Q_minus[3]*n[0] + Q_minus[6]*n[1])) + 0.6*t8*((Q_minus[4]*n[0] + Q_minus[7]*n[1])*(Q_minus[4]*n[0] + Q_minus[7]*n[1])) + (p[0]*(t2*t2*t2)/(t9*t9))));
     T t11 = (t2/(t9));
     T t12 = std::max((T)1e-14, Q_plus[1]);
     T t13 = (1.0/(t12));
     T t14 = t13*(Q_plus[2]*n[0] + Q_plus[5]*n[1]);
     T t15 = (1.0/(t12*t12));
     T t16 = std::max((T)1e-14, t3);
-    T t17 = std::sqrt((t15*((Q_plus[3]*n[0] + Q_plus[6]*n[1])*(Q_plus[3]*n[0] + Q_plus[6]*n[1])) + (3.0/5.0)*t15*((Q_plus[4]*n[0] + Q_plus[7]*n[1])*(Q_plus[4]*n[0] + Q_plus[7]*n[1])) + (p[0]*(t4*t4*t4)/(t16*t16))));
+    T t17 = std::sqrt((t15*((Q_plus[3]*n[0] + Q_plus[6]*n[1])*(Q_plus[3]*n[0] + Q_plus[6]*n[1])) + 0.6*t15*((Q_plus[4]*n[0] + Q_plus[7]*n[1])*(Q_plus[4]*n[0] + Q_plus[7]*n[1])) + (p[0]*(t4*t4*t4)/(t16*t16))));
     T t18 = (t4/(t16));
     T t19 = std::max(t11*std::fabs((t10 + t7)), std::max(t18*std::fabs((t14 + t17)), std::max(t11*std::fabs((t10 - t7)), t18*std::fabs((t14 - t17)))));
-    T t20 = (t19*(t2 - t4)/2.0);
+    T t20 = 0.5*t19*(t2 - t4);
     T t21 = p[0]*((Q_plus[1]*Q_plus[1]) - (t4*t4));
     T t22 = t2*t6;
     T t23 = Q_minus[2]*t22;
@@ -167,7 +167,7 @@ struct Numerics {
     T t35 = (-t34);
     T t36 = (t33 + t35);
     T t37 = (t2 + t4);
-    T t38 = (t37*std::sqrt(2.0)/std::sqrt(((std::max((T)1e-12, (t37/2.0))*std::max((T)1e-12, (t37/2.0))*std::max((T)1e-12, (t37/2.0))*std::max((T)1e-12, (t37/2.0))) + ((t37*t37*t37*t37)/16.0))));
+    T t38 = (t37*std::sqrt(2.0)/std::sqrt(((std::max((T)1e-12, 0.5*t37)*std::max((T)1e-12, 0.5*t37)*std::max((T)1e-12, 0.5*t37)*std::max((T)1e-12, 0.5*t37)) + 0.0625*(t37*t37*t37*t37))));
     T t39 = n[0]*t38;
     T t40 = t36*t39;
     T t41 = (t35 - t33 + 5.0*t23 + 5.0*t25);
@@ -203,20 +203,20 @@ struct Numerics {
     SimpleArray<T, 16> res;
     res[0] = 0.0;
     res[1] = (-t20);
-    res[2] = ((-(t26/2.0)) - (n[0]*t21/2.0));
-    res[3] = ((-(t31/40.0)) + (t53/40.0));
-    res[4] = ((-(t55/56.0)) + (t58/56.0));
-    res[5] = ((-(t61/2.0)) - (n[1]*t21/2.0));
-    res[6] = ((-(t62/40.0)) + (t65/40.0));
-    res[7] = ((-(t66/56.0)) + (t69/56.0));
+    res[2] = ((-0.5*t26) - 0.5*n[0]*t21);
+    res[3] = ((-0.025*t31) + 0.025*t53);
+    res[4] = ((-0.017857142857142856*t55) + 0.017857142857142856*t58);
+    res[5] = ((-0.5*t61) - 0.5*n[1]*t21);
+    res[6] = ((-0.025*t62) + 0.025*t65);
+    res[7] = ((-0.017857142857142856*t66) + 0.017857142857142856*t69);
     res[8] = 0.0;
     res[9] = t20;
-    res[10] = ((t26/2.0) + (n[0]*t70/2.0));
-    res[11] = ((t31/40.0) + (t53/40.0));
-    res[12] = ((t55/56.0) + (t58/56.0));
-    res[13] = ((t61/2.0) + (n[1]*t70/2.0));
-    res[14] = ((t62/40.0) + (t65/40.0));
-    res[15] = ((t66/56.0) + (t69/56.0));
+    res[10] = (0.5*t26 + 0.5*n[0]*t70);
+    res[11] = (0.025*t31 + 0.025*t53);
+    res[12] = (0.017857142857142856*t55 + 0.017857142857142856*t58);
+    res[13] = (0.5*t61 + 0.5*n[1]*t70);
+    res[14] = (0.025*t62 + 0.025*t65);
+    res[15] = (0.017857142857142856*t66 + 0.017857142857142856*t69);
     return res;
     }
 
@@ -228,7 +228,7 @@ struct Numerics {
     {
     T t0 = std::max((T)1e-14, Q[1]);
     T t1 = (1.0/(t0));
-    T t2 = std::sqrt((((Q[3]*n[0] + Q[6]*n[1])*(Q[3]*n[0] + Q[6]*n[1])) + (3.0/5.0)*((Q[4]*n[0] + Q[7]*n[1])*(Q[4]*n[0] + Q[7]*n[1])) + (p[0]*std::max((T)0.0, (Q[1]*Q[1]*Q[1]*Q[1]*Q[1]))/(t0*t0))));
+    T t2 = std::sqrt((((Q[3]*n[0] + Q[6]*n[1])*(Q[3]*n[0] + Q[6]*n[1])) + 0.6*((Q[4]*n[0] + Q[7]*n[1])*(Q[4]*n[0] + Q[7]*n[1])) + (p[0]*std::max((T)0.0, (Q[1]*Q[1]*Q[1]*Q[1]*Q[1]))/(t0*t0))));
     T t3 = (Q[2]*n[0] + Q[5]*n[1]);
     SimpleArray<T, 1> res;
     res[0] = std::max(t1*std::fabs((t2 + t3)), t1*std::fabs((t2 - t3)));

@@ -115,7 +115,7 @@ struct Numerics {
     T t71 = Q_plus[4]*Q_plus[8];
     T t72 = Q_plus[5]*Q_plus[9];
     T t73 = (20.0*t70 + 27.0*t72 + 42.0*t71 + Q_plus[10]*t62 + Q_plus[10]*t63 + Q_plus[2]*t25 + Q_plus[7]*t60 + Q_plus[9]*t61);
-    T t74 = (t13/210.0);
+    T t74 = 0.004761904761904762*t13;
     T t75 = 693.0*Q_minus[2];
     T t76 = 297.0*Q_minus[3];
     T t77 = 198.0*Q_minus[4];
@@ -130,7 +130,7 @@ struct Numerics {
     T t86 = Q_plus[5]*Q_plus[8];
     T t87 = Q_plus[6]*Q_plus[9];
     T t88 = (100.0*t24 + 132.0*t23 + 198.0*t26 + 198.0*t87 + 297.0*t86 + Q_plus[10]*t79 + Q_plus[11]*t80 + Q_plus[4]*t85 + Q_plus[9]*t78 + 462.0*Q_plus[3]*Q_plus[8]);
-    T t89 = (t13/1386.0);
+    T t89 = 0.0007215007215007215*t13;
     T t90 = 495.0*Q_minus[2];
     T t91 = 220.0*Q_minus[3];
     T t92 = 132.0*Q_minus[4];
@@ -145,7 +145,7 @@ struct Numerics {
     T t101 = 495.0*Q_plus[7];
     T t102 = 220.0*Q_plus[8];
     T t103 = (90.0*t70 + 132.0*t72 + 297.0*t71 + Q_plus[10]*t94 + Q_plus[10]*t96 + Q_plus[10]*t97 + Q_plus[11]*t95 + Q_plus[5]*t101 + Q_plus[6]*t102 + Q_plus[9]*t79);
-    T t104 = (t13/990.0);
+    T t104 = 0.00101010101010101*t13;
     T t105 = 5005.0*Q_minus[2];
     T t106 = 2860.0*Q_minus[3];
     T t107 = 1300.0*Q_minus[4];
@@ -156,7 +156,7 @@ struct Numerics {
     T t112 = (810.0*t15 + 1170.0*t14 + 1300.0*t83 + 2574.0*t17 + 2860.0*t82 + Q_minus[10]*t106 + Q_minus[11]*t105 + Q_minus[11]*t107 + Q_minus[6]*t111);
     T t113 = 5005.0*Q_plus[7];
     T t114 = (810.0*t24 + 1170.0*t23 + 1300.0*t87 + 2574.0*t26 + 2860.0*t86 + Q_plus[10]*t109 + Q_plus[11]*t108 + Q_plus[11]*t110 + Q_plus[6]*t113);
-    T t115 = (t13/10010.0);
+    T t115 = 9.99000999000999e-05*t13;
     T t116 = (Q_minus[10]*Q_minus[10]);
     T t117 = (Q_minus[11]*Q_minus[11]);
     T t118 = (Q_minus[8]*Q_minus[8]);
@@ -177,13 +177,13 @@ struct Numerics {
     T t133 = Q_plus[11]*Q_plus[9];
     SimpleArray<T, 12> res;
     res[0] = 0.0;
-    res[1] = ((Q_minus[2]*n[0]*t4/2.0) + (Q_minus[7]*n[1]*t4/2.0) + (Q_plus[2]*n[0]*t8/2.0) + (Q_plus[7]*n[1]*t8/2.0));
-    res[2] = ((t12*t18/1260.0) + (t22*t27/1260.0) + (n[0]*t28*(t29 + t32*(Q_minus[2]*Q_minus[2]) + t33*t34 + t35*t36 + t37*t38 + t39*t41)/1260.0) + (n[0]*t42*(t29 + t45*(Q_plus[2]*Q_plus[2]) + t46*t47 + t48*t49 + t50*t51 + t52*t53)/1260.0));
+    res[1] = (0.5*Q_minus[2]*n[0]*t4 + 0.5*Q_minus[7]*n[1]*t4 + 0.5*Q_plus[2]*n[0]*t8 + 0.5*Q_plus[7]*n[1]*t8);
+    res[2] = (0.0007936507936507937*t12*t18 + 0.0007936507936507937*t22*t27 + 0.0007936507936507937*n[0]*t28*(t29 + t32*(Q_minus[2]*Q_minus[2]) + t33*t34 + t35*t36 + t37*t38 + t39*t41) + 0.0007936507936507937*n[0]*t42*(t29 + t45*(Q_plus[2]*Q_plus[2]) + t46*t47 + t48*t49 + t50*t51 + t52*t53));
     res[3] = t74*(t11*t69 + t21*t73 + t59*(Q_minus[2]*t54 + Q_minus[4]*t55 + Q_minus[5]*t56 + Q_minus[5]*t57) + t65*(Q_plus[2]*t60 + Q_plus[4]*t61 + Q_plus[5]*t62 + Q_plus[5]*t63));
     res[4] = t89*(t11*t84 + t21*t88 + t59*(50.0*t39 + 66.0*t37 + 99.0*t35 + 231.0*t33 + Q_minus[4]*t75 + Q_minus[5]*t76 + Q_minus[6]*t77) + t65*(50.0*t52 + 66.0*t50 + 99.0*t48 + 231.0*t46 + Q_plus[4]*t78 + Q_plus[5]*t79 + Q_plus[6]*t80));
     res[5] = t104*(t100*t11 + t103*t21 + t59*(Q_minus[4]*t76 + Q_minus[5]*t90 + Q_minus[5]*t92 + Q_minus[5]*t93 + Q_minus[6]*t91) + t65*(Q_plus[4]*t79 + Q_plus[5]*t94 + Q_plus[5]*t96 + Q_plus[5]*t97 + Q_plus[6]*t95));
     res[6] = t115*(t11*t112 + t114*t21 + t59*(405.0*t39 + 585.0*t37 + 1287.0*t35 + Q_minus[5]*t106 + Q_minus[6]*t105 + Q_minus[6]*t107) + t65*(405.0*t52 + 585.0*t50 + 1287.0*t48 + Q_plus[5]*t109 + Q_plus[6]*t108 + Q_plus[6]*t110));
-    res[7] = ((t18*t59/1260.0) + (t27*t65/1260.0) + (n[1]*t28*(t29 + t116*t38 + t117*t41 + t118*t34 + t119*t36 + t32*(Q_minus[7]*Q_minus[7]))/1260.0) + (n[1]*t42*(t29 + t120*t51 + t121*t53 + t122*t47 + t123*t49 + t45*(Q_plus[7]*Q_plus[7]))/1260.0));
+    res[7] = (0.0007936507936507937*t18*t59 + 0.0007936507936507937*t27*t65 + 0.0007936507936507937*n[1]*t28*(t29 + t116*t38 + t117*t41 + t118*t34 + t119*t36 + t32*(Q_minus[7]*Q_minus[7])) + 0.0007936507936507937*n[1]*t42*(t29 + t120*t51 + t121*t53 + t122*t47 + t123*t49 + t45*(Q_plus[7]*Q_plus[7])));
     res[8] = t74*(t12*(20.0*t124 + 27.0*t125 + 42.0*t126 + Q_minus[7]*t16) + t22*(20.0*t127 + 27.0*t128 + 42.0*t129 + Q_plus[7]*t25) + t58*t69 + t64*t73);
     res[9] = t89*(t12*(50.0*t117 + 66.0*t116 + 99.0*t119 + 198.0*t131 + 231.0*t118 + 297.0*t130 + Q_minus[9]*t81) + t22*(50.0*t121 + 66.0*t120 + 99.0*t123 + 198.0*t133 + 231.0*t122 + 297.0*t132 + Q_plus[9]*t85) + t58*t84 + t64*t88);
     res[10] = t104*(t100*t58 + t103*t64 + t12*(90.0*t124 + 132.0*t125 + 297.0*t126 + Q_minus[10]*t98 + Q_minus[11]*t99) + t22*(90.0*t127 + 132.0*t128 + 297.0*t129 + Q_plus[10]*t101 + Q_plus[11]*t102));
@@ -209,17 +209,17 @@ struct Numerics {
     T t7 = t6*(Q_minus[2]*n[0] + Q_minus[7]*n[1]);
     T t8 = (1.0/(t5*t5));
     T t9 = std::max((T)1e-14, t1);
-    T t10 = std::sqrt((t8*((Q_minus[3]*n[0] + Q_minus[8]*n[1])*(Q_minus[3]*n[0] + Q_minus[8]*n[1])) + (t8*((Q_minus[11]*n[1] + Q_minus[6]*n[0])*(Q_minus[11]*n[1] + Q_minus[6]*n[0]))/3.0) + (3.0/5.0)*t8*((Q_minus[4]*n[0] + Q_minus[9]*n[1])*(Q_minus[4]*n[0] + Q_minus[9]*n[1])) + (3.0/7.0)*t8*((Q_minus[10]*n[1] + Q_minus[5]*n[0])*(Q_minus[10]*n[1] + Q_minus[5]*n[0])) + (p[0]*(t2*t2*t2)/(t9*t9))));
+    T t10 = std::sqrt((t8*((Q_minus[3]*n[0] + Q_minus[8]*n[1])*(Q_minus[3]*n[0] + Q_minus[8]*n[1])) + 0.3333333333333333*t8*((Q_minus[11]*n[1] + Q_minus[6]*n[0])*(Q_minus[11]*n[1] + Q_minus[6]*n[0])) + 0.6*t8*((Q_minus[4]*n[0] + Q_minus[9]*n[1])*(Q_minus[4]*n[0] + Q_minus[9]*n[1])) + 0.42857142857142855*t8*((Q_minus[10]*n[1] + Q_minus[5]*n[0])*(Q_minus[10]*n[1] + Q_minus[5]*n[0])) + (p[0]*(t2*t2*t2)/(t9*t9))));
     T t11 = (t2/(t9));
     T t12 = std::max((T)1e-14, Q_plus[1]);
     T t13 = (1.0/(t12));
     T t14 = t13*(Q_plus[2]*n[0] + Q_plus[7]*n[1]);
     T t15 = (1.0/(t12*t12));
     T t16 = std::max((T)1e-14, t3);
-    T t17 = std::sqrt((t15*((Q_plus[3]*n[0] + Q_plus[8]*n[1])*(Q_plus[3]*n[0] + Q_plus[8]*n[1])) + (t15*((Q_plus[11]*n[1] + Q_plus[6]*n[0])*(Q_plus[11]*n[1] + Q_plus[6]*n[0]))/3.0) + (3.0/5.0)*t15*((Q_plus[4]*n[0] + Q_plus[9]*n[1])*(Q_plus[4]*n[0] + Q_plus[9]*n[1])) + (3.0/7.0)*t15*((Q_plus[10]*n[1] + Q_plus[5]*n[0])*(Q_plus[10]*n[1] + Q_plus[5]*n[0])) + (p[0]*(t4*t4*t4)/(t16*t16))));
+    T t17 = std::sqrt((t15*((Q_plus[3]*n[0] + Q_plus[8]*n[1])*(Q_plus[3]*n[0] + Q_plus[8]*n[1])) + 0.3333333333333333*t15*((Q_plus[11]*n[1] + Q_plus[6]*n[0])*(Q_plus[11]*n[1] + Q_plus[6]*n[0])) + 0.6*t15*((Q_plus[4]*n[0] + Q_plus[9]*n[1])*(Q_plus[4]*n[0] + Q_plus[9]*n[1])) + 0.42857142857142855*t15*((Q_plus[10]*n[1] + Q_plus[5]*n[0])*(Q_plus[10]*n[1] + Q_plus[5]*n[0])) + (p[0]*(t4*t4*t4)/(t16*t16))));
     T t18 = (t4/(t16));
     T t19 = std::max(t11*std::fabs((t10 + t7)), std::max(t18*std::fabs((t14 + t17)), std::max(t11*std::fabs((t10 - t7)), t18*std::fabs((t14 - t17)))));
-    T t20 = (t19*(t2 - t4)/2.0);
+    T t20 = 0.5*t19*(t2 - t4);
     T t21 = p[0]*((Q_plus[1]*Q_plus[1]) - (t4*t4));
     T t22 = t2*t6;
     T t23 = Q_minus[2]*t22;
@@ -239,7 +239,7 @@ struct Numerics {
     T t37 = 5.0*t36;
     T t38 = std::sqrt(2.0);
     T t39 = (t2 + t4);
-    T t40 = (1.0/std::sqrt(((std::max((T)1e-12, (t39/2.0))*std::max((T)1e-12, (t39/2.0))*std::max((T)1e-12, (t39/2.0))*std::max((T)1e-12, (t39/2.0))) + ((t39*t39*t39*t39)/16.0))));
+    T t40 = (1.0/std::sqrt(((std::max((T)1e-12, 0.5*t39)*std::max((T)1e-12, 0.5*t39)*std::max((T)1e-12, 0.5*t39)*std::max((T)1e-12, 0.5*t39)) + 0.0625*(t39*t39*t39*t39))));
     T t41 = t38*t39*t40;
     T t42 = t41*((-t34) - t37 + 9.0*t32 + 9.0*t35);
     T t43 = Q_minus[5]*t22;
@@ -352,28 +352,28 @@ struct Numerics {
     SimpleArray<T, 24> res;
     res[0] = 0.0;
     res[1] = (-t20);
-    res[2] = ((-(t26/2.0)) - (n[0]*t21/2.0));
-    res[3] = ((-(t31/840.0)) + (t80/840.0));
-    res[4] = ((-(t82/1848.0)) + (t91/1848.0));
-    res[5] = ((-(t93/1320.0)) + (t101/1320.0));
-    res[6] = ((-(t103/8008.0)) + (t110/8008.0));
-    res[7] = ((-(t113/2.0)) - (n[1]*t21/2.0));
-    res[8] = ((-(t117/840.0)) - (t118/840.0) - (t123/840.0) - (t124/840.0) - (t125/840.0) + (n[0]*t119*t29*t38*t39*t40/40.0) + (n[1]*t119*t38*t39*t40*t78/40.0) + (n[0]*t114*t38*t39*t40*t65/168.0) + (n[1]*t114*t38*t39*t40*t72/168.0));
-    res[9] = ((-(t126/1848.0)) + (t133/1848.0));
-    res[10] = ((-(t134/1320.0)) + (t140/1320.0));
-    res[11] = ((-(t141/8008.0)) + (t146/8008.0));
+    res[2] = ((-0.5*t26) - 0.5*n[0]*t21);
+    res[3] = ((-0.0011904761904761906*t31) + 0.0011904761904761906*t80);
+    res[4] = ((-0.0005411255411255411*t82) + 0.0005411255411255411*t91);
+    res[5] = ((-0.0007575757575757576*t93) + 0.0007575757575757576*t101);
+    res[6] = ((-0.00012487512487512488*t103) + 0.00012487512487512488*t110);
+    res[7] = ((-0.5*t113) - 0.5*n[1]*t21);
+    res[8] = ((-0.0011904761904761906*t117) - 0.0011904761904761906*t118 - 0.0011904761904761906*t123 - 0.0011904761904761906*t124 - 0.0011904761904761906*t125 + 0.025*n[0]*t119*t29*t38*t39*t40 + 0.025*n[1]*t119*t38*t39*t40*t78 + 0.005952380952380952*n[0]*t114*t38*t39*t40*t65 + 0.005952380952380952*n[1]*t114*t38*t39*t40*t72);
+    res[9] = ((-0.0005411255411255411*t126) + 0.0005411255411255411*t133);
+    res[10] = ((-0.0007575757575757576*t134) + 0.0007575757575757576*t140);
+    res[11] = ((-0.00012487512487512488*t141) + 0.00012487512487512488*t146);
     res[12] = 0.0;
     res[13] = t20;
-    res[14] = ((t26/2.0) + (n[0]*t147/2.0));
-    res[15] = ((t31/840.0) + (t80/840.0));
-    res[16] = ((t82/1848.0) + (t91/1848.0));
-    res[17] = ((t101/1320.0) + (t93/1320.0));
-    res[18] = ((t103/8008.0) + (t110/8008.0));
-    res[19] = ((t113/2.0) + (n[1]*t147/2.0));
-    res[20] = ((-(t117/840.0)) - (t118/840.0) - (t123/840.0) - (t124/840.0) + (t125/840.0) + (t148*t66/840.0) + (t148*t73/840.0) + (t149*t75/840.0) + (t149*t79/840.0));
-    res[21] = ((t126/1848.0) + (t133/1848.0));
-    res[22] = ((t134/1320.0) + (t140/1320.0));
-    res[23] = ((t141/8008.0) + (t146/8008.0));
+    res[14] = (0.5*t26 + 0.5*n[0]*t147);
+    res[15] = (0.0011904761904761906*t31 + 0.0011904761904761906*t80);
+    res[16] = (0.0005411255411255411*t82 + 0.0005411255411255411*t91);
+    res[17] = (0.0007575757575757576*t101 + 0.0007575757575757576*t93);
+    res[18] = (0.00012487512487512488*t103 + 0.00012487512487512488*t110);
+    res[19] = (0.5*t113 + 0.5*n[1]*t147);
+    res[20] = ((-0.0011904761904761906*t117) - 0.0011904761904761906*t118 - 0.0011904761904761906*t123 - 0.0011904761904761906*t124 + 0.0011904761904761906*t125 + 0.0011904761904761906*t148*t66 + 0.0011904761904761906*t148*t73 + 0.0011904761904761906*t149*t75 + 0.0011904761904761906*t149*t79);
+    res[21] = (0.0005411255411255411*t126 + 0.0005411255411255411*t133);
+    res[22] = (0.0007575757575757576*t134 + 0.0007575757575757576*t140);
+    res[23] = (0.00012487512487512488*t141 + 0.00012487512487512488*t146);
     return res;
     }
 
@@ -385,7 +385,7 @@ struct Numerics {
     {
     T t0 = std::max((T)1e-14, Q[1]);
     T t1 = (1.0/(t0));
-    T t2 = std::sqrt((((Q[3]*n[0] + Q[8]*n[1])*(Q[3]*n[0] + Q[8]*n[1])) + (((Q[11]*n[1] + Q[6]*n[0])*(Q[11]*n[1] + Q[6]*n[0]))/3.0) + (3.0/5.0)*((Q[4]*n[0] + Q[9]*n[1])*(Q[4]*n[0] + Q[9]*n[1])) + (3.0/7.0)*((Q[10]*n[1] + Q[5]*n[0])*(Q[10]*n[1] + Q[5]*n[0])) + (p[0]*std::max((T)0.0, (Q[1]*Q[1]*Q[1]*Q[1]*Q[1]))/(t0*t0))));
+    T t2 = std::sqrt((((Q[3]*n[0] + Q[8]*n[1])*(Q[3]*n[0] + Q[8]*n[1])) + 0.3333333333333333*((Q[11]*n[1] + Q[6]*n[0])*(Q[11]*n[1] + Q[6]*n[0])) + 0.6*((Q[4]*n[0] + Q[9]*n[1])*(Q[4]*n[0] + Q[9]*n[1])) + 0.42857142857142855*((Q[10]*n[1] + Q[5]*n[0])*(Q[10]*n[1] + Q[5]*n[0])) + (p[0]*std::max((T)0.0, (Q[1]*Q[1]*Q[1]*Q[1]*Q[1]))/(t0*t0))));
     T t3 = (Q[2]*n[0] + Q[7]*n[1]);
     SimpleArray<T, 1> res;
     res[0] = std::max(t1*std::fabs((t2 + t3)), t1*std::fabs((t2 - t3)));

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(PKG, "libzsme.so")
 
 ZSME_LIMITER_NONE, ZSME_LIMITER_TVD = 0, 1
 ZSME_GRADIENT_GREEN_GAUSS, ZSME_GRADIENT_LSQ = 0, 1
-KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step")
+KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step", "gather")
 
 
 class ZsmeMesh(ct.Structure):
@@ -102,6 +102,13 @@ def load():
     lib.zsme_set_profiling.argtypes = [vp, ct.c_int]
     lib.zsme_read_profile.argtypes = [vp, P, ct.POINTER(ct.c_int64)]
     lib.zsme_compute_dt_noalloc.argtypes = [ct.c_char_p, ct.c_int32, vp, vp, vp, vp, ct.c_double, vp, vp]
+    lib.zsme_batch_create.argtypes = [ct.c_char_p, ct.c_int32, vp, vp, P, ct.c_int, ct.POINTER(vp)]
+    lib.zsme_batch_size.argtypes = [vp, ct.POINTER(ct.c_int32)]
+    lib.zsme_batch_set_state.argtypes = [vp, ct.c_int32, P, ct.c_double]
+    lib.zsme_batch_get_state.argtypes = [vp, ct.c_int32, P]
+    lib.zsme_batch_get_time.argtypes = [vp, ct.c_int32, P, P]
+    lib.zsme_set_launch.argtypes = [vp, ct.POINTER(ct.c_int32)]
+    lib.zsme_get_launch.argtypes = [vp, ct.POINTER(ct.c_int32)]
     _lib = lib
     return lib
 

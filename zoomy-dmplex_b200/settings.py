@@ -3,9 +3,13 @@
 Mirrors ``Settings::from_json`` (reference ``Settings.hpp:73-138``) for the
 keys that change the SME step, with the same defaults, plus the model
 parameter overrides by name (``VirtualSolver.hpp:199-217``).  Two keys are
-additions of this implementation: ``solver.gradient`` (``"least_squares"``,
-the default, or ``"green_gauss"``, the gradient the reference's MUSCL path
-installs, ``ModularSolver.hpp:62-67``) and ``solver.block_size``.
+additions of this implementation: ``solver.gradient`` (``"green_gauss"``, the
+default and the gradient the reference's MUSCL path installs,
+``ModularSolver.hpp:62-67``, or ``"least_squares"``, the reference's
+``LeastSquaresGradient`` of ``Gradient.hpp:196-360``, which its MUSCL path
+never installs; its one-sided stencil at reflective walls lets wall cells
+grow without bound under inflow, so it is an option, not the default) and
+``solver.block_size``.
 
 How the reference interprets the strings, and so how they map here:
 * ``limiter``: only ``"none"`` changes anything; every other value (including
@@ -36,7 +40,7 @@ class SolverSettings:
     positivity: str = "none"
     wet_dry_eps: float = 1.0e-2
     ssp_stages: int = 5
-    gradient: str = "least_squares"
+    gradient: str = "green_gauss"
     block_size: int = 0
 
     def to_struct(self) -> native.ZsmeSettings:

@@ -171,3 +171,105 @@ class Solver:
         n = ct.c_int32()
         native.check(self.lib.zsme_launches_per_step(self.h, ct.byref(n)))
         return n.value
+
+
+class BatchSolver:
+    """An ensemble of independent instances (own mesh, parameters, time and
+    CFL dt) advanced together: every kernel launch of ``step`` covers all
+    instances (concatenated cell and face layout)."""
+
+    def __init__(self, model: str, meshes, settings: Union[SolverSettings, None] = None, params=None,
+                 device: int = 0):
+        from . import models as _m
+        self.lib = native.load()
+        self.model = model
+        self.info = native.model_info(model)
+        self.nq = self.info["n_dof_q"]
+        self.settings = settings or SolverSettings()
+        self.meshes = list(meshes)
+        self.n = len(self.meshes)
+        names, defaults = _m.parameter_table(model)
+        P = np.zeros((self.n, len(names)))
+        for i in range(self.n):
+            pi = params[i] if isinstance(params, (list, tuple)) else params
+            if pi is None or isinstance(pi, dict):
+                vals, unknown = resolve_parameters(names, defaults, pi or {})
+                if unknown:
+                    raise KeyError("parameters not defined by model %s: %s" % (model, unknown))
+                P[i] = vals
+            else:
+                P[i] = np.asarray(pi, dtype=np.float64)
+        self.params = np.ascontiguousarray(P)
+        self._keep = [native.make_mesh_struct(m.as_abi_arrays()) for m in self.meshes]
+        arr = (native.ZsmeMesh * self.n)(*[k[0] for k in self._keep])
+        self._arr = arr
+        self._st = self.settings.to_struct()
+        h = ct.c_void_p()
+        native.check(self.lib.zsme_batch_create(model.encode(), self.n, ct.addressof(arr), ct.addressof(self._st),
+                                                _p(self.params), int(device), ct.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.zsme_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, i: int, q: np.ndarray, t: float = 0.0):
+        q = np.ascontiguousarray(q, dtype=np.float64).reshape(self.meshes[i].n_cells, self.nq)
+        native.check(self.lib.zsme_batch_set_state(self.h, int(i), _p(q), float(t)))
+
+    def get_state(self, i: int) -> np.ndarray:
+        q = np.empty((self.meshes[i].n_cells, self.nq))
+        native.check(self.lib.zsme_batch_get_state(self.h, int(i), _p(q)))
+        return q
+
+    def time(self, i: int):
+        t, d = ct.c_double(), ct.c_double()
+        native.check(self.lib.zsme_batch_get_time(self.h, int(i), ct.byref(t), ct.byref(d)))
+        return t.value, d.value
+
+    def step(self, n: int = 1):
+        native.check(self.lib.zsme_step(self.h, int(n)))
+
+    def sync(self, check: bool = True) -> native.ZsmeDiag:
+        d = native.ZsmeDiag()
+        native.check(self.lib.zsme_get_diag(self.h, ct.byref(d)))
+        if check:
+            native.check(self.lib.zsme_sync(self.h))
+        return d
+
+    @property
+    def stream(self) -> int:
+        return self.lib.zsme_stream(self.h) or 0
+
+    def set_profiling(self, on: bool = True):
+        native.check(self.lib.zsme_set_profiling(self.h, int(bool(on))))
+
+    def launches_per_step(self) -> int:
+        n = ct.c_int32()
+        native.check(self.lib.zsme_launches_per_step(self.h, ct.byref(n)))
+        return n.value
+
+
+LAUNCH_KEYS = ("prep", "face", "gather", "finalize", "prep_occ", "face_occ")
+
+
+def set_launch(h, cfg):
+    """Launch configuration of a handle: dict with LAUNCH_KEYS (threads per
+    block of each kernel, register caps as blocks per SM)."""
+    lib = native.load()
+    b = (ct.c_int32 * 6)(*[int(cfg[k]) for k in LAUNCH_KEYS])
+    native.check(lib.zsme_set_launch(h, b))
+
+
+def get_launch(h):
+    lib = native.load()
+    b = (ct.c_int32 * 6)()
+    native.check(lib.zsme_get_launch(h, b))
+    return dict(zip(LAUNCH_KEYS, [int(x) for x in b]))
