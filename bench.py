@@ -4,11 +4,18 @@ roofline).
 
 Workload (default): SME level 4 (12 FP64 state slots) on the Hilbert-
 renumbered Delaunay mesh of a 1400x1400 jittered grid (3.91M triangles),
-16-Gaussian bathymetry, Navier-slip source; order 2 (least squares + Vacuum/
+16-Gaussian bathymetry, Navier-slip source; order 2 (Green-Gauss + Vacuum/
 TVD limiting), SSP-RK2, CFL 0.45.  A "step" is one full time step (two SSP
 stages, constraints, implicit source, CFL dt).  Inputs (375 MB of state +
 1.1 GB of face states) exceed the 126 MB L2, so no flush is needed between
-steps.
+steps.  The K timed steps run as CUDA graphs; a second, profiled pass of K
+steps (one CUDA event pair per kernel launch) gives the per-kernel times
+behind the roofline.
+
+``--workload ensemble``: SME level-2 instances on their own meshes (grid
+side log-uniform in [40, 400]) advanced by the batched path, then by a loop
+of single-instance solvers over the same instances; reports both times, the
+speed-up and the largest relative L2 difference between the two results.
 
 Launch: ``python bench.py [--gpus N --steps K --warmup W]``; for N > 1 one
 rank per GPU under torchrun, each rank advancing its own replica (the single
@@ -45,6 +52,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch configuration")
+    ap.add_argument("--workload", choices=["roofline", "ensemble"], default="roofline")
+    ap.add_argument("--instances", type=int, default=512, help="ensemble size per GPU (--workload ensemble)")
     return ap.parse_args()
 
 
@@ -164,6 +173,155 @@ def cpu_sample(side, steps, warm=1):
     return c.mesh.n_cells * steps / dt, nt, c.mesh.n_cells, dt
 
 
+def run_ensemble(a, dev, torch, dist, rank, world):
+    """Batched ensemble against the loop of single-instance solvers over the
+    same instances (each rank advances its own shard of instances)."""
+    import ctypes as ct
+
+    from zoomy_dmplex_b200 import autotune, cases, native
+    from zoomy_dmplex_b200.solver import BatchSolver, Solver, set_launch
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    n = a.instances
+    t0 = time.perf_counter()
+    members = cases.ensemble(n, first=rank * n)
+    build_s = time.perf_counter() - t0
+    model, st = members[0].model, members[0].settings
+    meshes = [c.mesh for c in members]
+    params = [params_of(c) for c in members]
+    C = sum(m.n_cells for m in meshes)
+    F = sum(m.n_faces for m in meshes)
+    B = BatchSolver(model, meshes, st, params, device=dev)
+
+    def reset_batch():
+        for i, c in enumerate(members):
+            B.set_state(i, c.q0)
+
+    reset_batch()
+    tuned = None
+    if not a.no_tune:
+        tuned = autotune.tune(B, model, C, steps=2, use_cache=False, write_cache=False)
+        reset_batch()
+    B.step(a.warmup)
+    B.sync()
+    reset_batch()
+    stream = torch.cuda.ExternalStream(B.stream, device=dev)
+    clk = ClockSampler(dev)
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
+    e0.record(stream)
+    B.step(a.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batch_wall = time.perf_counter() - w0
+    barrier()
+    clocks = clk.stop()
+    ms_batch = e0.elapsed_time(e1)
+    diag = B.sync(check=True)
+    got = [B.get_state(i) for i in range(n)]
+    t_batch = [B.time(i)[0] for i in range(n)]
+    launches = a.steps * B.launches_per_step()
+
+    # the same instances, one single-instance solver each, stepped one after the other
+    singles = [Solver(model, c.mesh, st, p, device=dev) for c, p in zip(members, params)]
+    for s, c in zip(singles, members):
+        if tuned:
+            set_launch(s.h, tuned)
+        s.set_state(c.q0)
+        s.step(a.warmup)
+    torch.cuda.synchronize()
+    for s, c in zip(singles, members):
+        s.set_state(c.q0)
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for s in singles:
+        s.step(a.steps)
+    torch.cuda.synchronize()          # every solver stream
+    loop_wall = time.perf_counter() - w0
+    barrier()
+    rel, t_diff = 0.0, 0.0
+    for i, s in enumerate(singles):
+        ref = s.get_state()
+        rel = max(rel, float(np.linalg.norm(got[i] - ref) / max(np.linalg.norm(ref), 1e-300)))
+        t_diff = max(t_diff, abs(s.time()[0] - t_batch[i]))
+    loop_launches = a.steps * sum(s.launches_per_step() for s in singles)
+    for s in singles:
+        s.close()
+
+    t = torch.tensor([ms_batch, loop_wall, batch_wall], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max, loop_max, bwall_max = (float(x) for x in t.tolist())
+    value = C * a.steps * world / (ms_max / 1e3)
+
+    # end to end through the public API: every instance's state from pinned host
+    # memory, one batched step, every state back
+    ne = min(a.steps, 3)
+    nq = B.nq
+    hosts = [torch.from_numpy(np.ascontiguousarray(c.q0)).pin_memory() for c in members]
+    outs = [torch.empty_like(h).pin_memory() for h in hosts]
+    lib = native.load()
+    P = ct.POINTER(ct.c_double)
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(ne):
+        for i in range(n):
+            native.check(lib.zsme_batch_set_state(B.h, i, ct.cast(hosts[i].data_ptr(), P), 0.0))
+        native.check(lib.zsme_step(B.h, 1))
+        for i in range(n):
+            native.check(lib.zsme_batch_get_state(B.h, i, ct.cast(outs[i].data_ptr(), P)))
+    e3.record(stream)
+    torch.cuda.synchronize()
+    t2 = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = C * ne * world / (float(t2.item()) / 1e3)
+    B.close()
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "ensemble of %d SME level-2 instances per GPU, jittered-Delaunay grid side "
+                                   "log-uniform in [40, 400] (%d cells, %d faces per GPU), order 2 Green-Gauss + "
+                                   "Vacuum/TVD, SSP-RK2, CFL 0.45 per instance, Navier-slip Newton source"
+                                   % (n, C, F),
+                       "model": model, "instances": n, "cells": C, "faces": F,
+                       "parallelism": "instance shards x%d" % world if world > 1 else "single GPU",
+                       "l2_flush": "not needed: state %.0f MB > 126 MB L2" % (C * nq * 8 / 1e6),
+                       "timing": "CUDA events on the batch stream around K graph-launched steps",
+                       "launch": tuned or "default", "mesh_build_s": build_s},
+            "ensemble": {"batched_ms_per_step": ms_max / a.steps,
+                         "batched_wall_ms_per_step": 1e3 * bwall_max / a.steps,
+                         "loop_wall_ms_per_step": 1e3 * loop_max / a.steps,
+                         "speedup_vs_loop": loop_max / bwall_max,
+                         "loop": "one single-instance solver per instance (own stream, CUDA graph per step), "
+                                 "K steps each, instances one after the other; host wall clock around the "
+                                 "loop and a device synchronize (the batched time beside it is taken the same way)",
+                         "max_rel_l2_vs_loop": rel, "max_time_diff_vs_loop": t_diff,
+                         "loop_gpu_launches": loop_launches},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C * nq * 8,
+                    "d2h_bytes_per_step": C * nq * 8, "steps": ne,
+                    "api": "zsme_batch_set_state x n (pinned host) + zsme_step(1) + zsme_batch_get_state x n"},
+            "gpu_launches": launches,
+            "diag": {"nonfinite": diag.n_nonfinite, "negative_depth": diag.n_negative_depth,
+                     "newton_unconverged": diag.n_newton_unconverged},
+            "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -179,7 +337,7 @@ def main():
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / max(1, a.steps),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": "sme2d_l4 jittered-Delaunay %dx%d (%d cells) order 2 LSQ+TVD SSP-RK2"
+                "config": {"workload": "sme2d_l4 jittered-Delaunay %dx%d (%d cells) order 2 Green-Gauss+TVD SSP-RK2"
                            % (a.cpu_side, a.cpu_side, C), "parallelism": "host threads"},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
                                  "sample": "%d steps of the CPU restatement on a %dx%d-grid mesh (%d cells)"
@@ -204,6 +362,9 @@ def main():
     from zoomy_dmplex_b200 import cases, native
     from zoomy_dmplex_b200.solver import Solver
 
+    if a.workload == "ensemble":
+        return run_ensemble(a, dev, torch, dist, rank, world)
+
     case = cases.roofline_l4(a.side)
     C, F = case.mesh.n_cells, case.mesh.n_faces
     g = Solver(case.model, case.mesh, case.settings, params_of(case), device=dev)
@@ -221,12 +382,9 @@ def main():
         if dist:
             dist.barrier()
 
-    # warm-up (graph path, then the profiled path once)
+    # warm-up on the graph path
     g.step(a.warmup)
-    g.set_profiling(True)
-    g.step(1)
     g.sync()
-    g.set_profiling(True)           # reset counters
 
     clk = ClockSampler(dev)
     clk.start()
@@ -241,6 +399,10 @@ def main():
     clocks = clk.stop()
     ms = e0.elapsed_time(e1)
     diag = g.sync(check=True)
+    # per-kernel durations: a second pass of K steps with one event pair per launch
+    g.set_profiling(True)
+    g.step(a.steps)
+    g.sync()
     prof = g.read_profile()
     g.set_profiling(False)
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -301,13 +463,14 @@ def main():
             "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "sme2d_l4 SME level 4, jittered-Delaunay %dx%d grid (%d cells, %d faces), "
-                                   "Hilbert-renumbered, order 2 LSQ + Vacuum/TVD, SSP-RK2, CFL 0.45, "
+                                   "Hilbert-renumbered, order 2 Green-Gauss + Vacuum/TVD, SSP-RK2, CFL 0.45, "
                                    "Navier-slip Newton source" % (a.side, a.side, C, F),
                        "model": case.model, "cells": C, "faces": F, "n_dof_q": nq,
                        "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
                        "l2_flush": "not needed: state %.0f MB + face states %.0f MB > 126 MB L2"
                                    % (C * nq * 8 / 1e6, C * nq * 3 * 8 / 1e6),
-                       "timing": "CUDA events on the solver stream around K steps; per-kernel events inside",
+                       "timing": "CUDA events on the solver stream around K graph-launched steps; "
+                                 "per-kernel events in a second, profiled pass of K steps",
                        "launch": tuned or "default"},
             "roofline": roofline, "roofline_step": roofline_step, "kernels": kernel_share,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,

@@ -157,13 +157,13 @@ def _member(args):
     return ensemble_member(i, seed=seed, side_range=(lo, hi))
 
 
-def ensemble(n: int = 512, seed: int = 3, side_range=(40, 400), processes: int = 0):
-    """The n instances of the level-2 ensemble, built in parallel worker
-    processes (spawned, so it is safe after CUDA has been initialised)."""
+def ensemble(n: int = 512, seed: int = 3, side_range=(40, 400), processes: int = 0, first: int = 0):
+    """Instances first .. first+n-1 of the level-2 ensemble, built in parallel
+    worker processes (spawned, so it is safe after CUDA has been initialised)."""
     import multiprocessing as mp
     import os
 
-    args = [(i, seed, side_range[0], side_range[1]) for i in range(n)]
+    args = [(i, seed, side_range[0], side_range[1]) for i in range(first, first + n)]
     procs = processes or min(n, os.cpu_count() or 1)
     if procs <= 1 or n < 4:
         return [_member(a) for a in args]
