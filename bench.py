@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch configuration")
     ap.add_argument("--workload", choices=["roofline", "ensemble"], default="roofline")
+    ap.add_argument("--launch", default="", help="launch configuration as JSON (keys of solver.LAUNCH_KEYS); "
+                    "skips the autotuner")
     ap.add_argument("--instances", type=int, default=512, help="ensemble size per GPU (--workload ensemble)")
     return ap.parse_args()
 
@@ -251,14 +253,25 @@ def run_ensemble(a, dev, torch, dist, rank, world):
         ref = s.get_state()
         rel = max(rel, float(np.linalg.norm(got[i] - ref) / max(np.linalg.norm(ref), 1e-300)))
         t_diff = max(t_diff, abs(s.time()[0] - t_batch[i]))
+    # the same loop, waiting for each instance before starting the next
+    for s, c in zip(singles, members):
+        s.set_state(c.q0)
+    torch.cuda.synchronize()
+    barrier()
+    w0 = time.perf_counter()
+    for s in singles:
+        s.step(a.steps)
+        s.sync(check=False)
+    sync_loop_wall = time.perf_counter() - w0
+    barrier()
     loop_launches = a.steps * sum(s.launches_per_step() for s in singles)
     for s in singles:
         s.close()
 
-    t = torch.tensor([ms_batch, loop_wall, batch_wall], dtype=torch.float64, device="cuda")
+    t = torch.tensor([ms_batch, loop_wall, batch_wall, sync_loop_wall], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max, loop_max, bwall_max = (float(x) for x in t.tolist())
+    ms_max, loop_max, bwall_max, sloop_max = (float(x) for x in t.tolist())
     value = C * a.steps * world / (ms_max / 1e3)
 
     # end to end through the public API: every instance's state from pinned host
@@ -303,9 +316,12 @@ def run_ensemble(a, dev, torch, dist, rank, world):
                          "batched_wall_ms_per_step": 1e3 * bwall_max / a.steps,
                          "loop_wall_ms_per_step": 1e3 * loop_max / a.steps,
                          "speedup_vs_loop": loop_max / bwall_max,
+                         "sync_loop_wall_ms_per_step": 1e3 * sloop_max / a.steps,
+                         "speedup_vs_sync_loop": sloop_max / bwall_max,
                          "loop": "one single-instance solver per instance (own stream, CUDA graph per step), "
                                  "K steps each, instances one after the other; host wall clock around the "
-                                 "loop and a device synchronize (the batched time beside it is taken the same way)",
+                                 "loop and a device synchronize (the batched time beside it is taken the same way); "
+                                 "sync loop: the same, waiting for each instance's K steps before the next",
                          "max_rel_l2_vs_loop": rel, "max_time_diff_vs_loop": t_diff,
                          "loop_gpu_launches": loop_launches},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C * nq * 8,
@@ -370,7 +386,12 @@ def main():
     g = Solver(case.model, case.mesh, case.settings, params_of(case), device=dev)
     g.set_state(case.q0)
     tuned = None
-    if not a.no_tune:
+    if a.launch:
+        from zoomy_dmplex_b200.solver import set_launch
+
+        tuned = json.loads(a.launch)
+        set_launch(g.h, tuned)
+    elif not a.no_tune:
         from zoomy_dmplex_b200 import autotune
 
         tuned = autotune.tune(g, case.model, case.mesh.n_cells, steps=2, use_cache=False, write_cache=False)

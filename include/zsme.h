@@ -179,12 +179,34 @@ int zsme_batch_set_state(zsme_handle* h, int32_t i, const double* q_aos, double 
 int zsme_batch_get_state(zsme_handle* h, int32_t i, double* q_aos);
 int zsme_batch_get_time(zsme_handle* h, int32_t i, double* t, double* dt);
 
-/* Launch configuration, 6 ints: threads per block {prep, face, gather,
- * finalize} (multiples of 32, <= 128) and the register caps {prep, face}
- * as resident blocks per SM (1 = uncapped .. 4): the knobs of the
- * autotuner (zoomy-dmplex_b200/autotune.py). */
+/* Launch configuration, 7 ints: threads per block {prep, face, gather,
+ * finalize} (multiples of 32, <= 128) and the register caps {prep, face,
+ * finalize} as resident blocks of 128 threads per SM (1 = uncapped; prep 2,
+ * 3, 4, 6 or 8, face and finalize 2..4): the knobs of the autotuner
+ * (zoomy-dmplex_b200/autotune.py). */
 int zsme_set_launch(zsme_handle* h, const int32_t* blocks);
 int zsme_get_launch(zsme_handle* h, int32_t* blocks);
+
+/* Discrete adjoint of nsteps steps from the resident state (single-instance
+ * handle).  No counterpart in the reference, which has no derivative path;
+ * it differentiates the zsme_step loop (MUSCLSolver.hpp:140-188) as
+ * written: the TVD limiter's branches, the clamps of update_variables and
+ * the implicit Newton source (SourceStep.hpp:125-209, by the implicit-
+ * function theorem at its converged state) included, with the CFL dt of each
+ * step recorded by the forward run and held fixed.
+ * Loss: sum_j w_j (Q_{obs_step[j]}[obs_cell[j], obs_comp[j]] - obs_target[j])^2,
+ * Q_k the state after k steps (0 = the resident state), cells in caller
+ * order; obs_weight may be NULL (all 1).  The forward run keeps a checkpoint
+ * every checkpoint_every steps and the reverse pass recomputes each segment.
+ * Outputs (host, any may be NULL): *loss; grad_q_aos [n_cells][n_dof_q], the
+ * gradient with respect to the resident state (its component 0 is the
+ * gradient with respect to the bathymetry b); grad_params [n_parameters];
+ * dts [nsteps], the dt sequence used.  The handle ends holding the state
+ * after nsteps steps, as zsme_step(h, nsteps) would leave it. */
+int zsme_adjoint(zsme_handle* h, int32_t nsteps, int32_t checkpoint_every, int32_t n_obs,
+                 const int32_t* obs_step, const int32_t* obs_cell, const int32_t* obs_comp,
+                 const double* obs_target, const double* obs_weight, double* loss, double* grad_q_aos,
+                 double* grad_params, double* dts);
 
 /* CFL time step of a caller-owned state with no device allocation.
  * No counterpart in the reference, which has no GPU path.  It serves callers

@@ -1,0 +1,177 @@
+"""The GPU discrete adjoint (zsme_adjoint) against the oracle.
+
+* loss: the adjoint's forward run is the plain step, so its misfit equals
+  the oracle's at the same dt sequence (the forward is bit-identical);
+* directional derivatives: <grad, d> against the dual-number tangent-linear
+  oracle run along d (the derivative of the same branches), for per-cell
+  white-noise directions in the bathymetry b and for the Manning coefficient;
+* central finite differences (eps = 1e-6) of the GPU forward with the
+  recorded dts, on smooth directions over a horizon where the step is smooth
+  on that scale;
+* the torch.autograd wrapper returns the same gradients.
+The case is the level-1 adjoint case (Manning friction, order 2, Green-Gauss,
+Vacuum + TVD limiting) on small meshes; checkpoint intervals that do not
+divide the step count exercise partial segments."""
+import numpy as np
+import pytest
+
+import oracle_py as O
+from zoomy_dmplex_b200 import adjoint as adj
+from zoomy_dmplex_b200 import cases, models
+from zoomy_dmplex_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(c):
+    names, vals = models.parameter_table(c.model)
+    for k, v in c.params.items():
+        vals[names.index(k)] = v
+    return np.array(vals), names
+
+
+def _smooth(mesh, rng, bumps=6):
+    x, y = mesh.cell_centroid[:, 0], mesh.cell_centroid[:, 1]
+    d = np.zeros_like(x)
+    for _ in range(bumps):
+        cx, cy = rng.uniform(0, 1, 2)
+        w = rng.uniform(0.02, 0.1)
+        d += rng.standard_normal() * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / w)
+    return d
+
+
+def _setup(n, nsteps, every_obs, ngauge, seed=0):
+    c = cases.adjoint_l1(n)
+    p, names = _params(c)
+    tgt = cases.adjoint_l1(n, target=True)
+    o = O.Oracle(tgt.model, tgt.mesh.as_abi_arrays(), tgt.settings.to_struct(), p)
+    o.set_state(tgt.q0)
+    steps = list(range(every_obs, nsteps + 1, every_obs))
+    cells = adj.gauges(c.mesh.n_cells, ngauge, seed)
+    targets = []
+    for k in range(1, nsteps + 1):
+        o.step(1)
+        if k in steps:
+            targets.append(o.get_state()[cells, 1])
+    obs = adj.depth_observations(cells, steps, np.array(targets))
+    return c, p, names, obs
+
+
+def _oracle_tlm(c, p, dts, obs, dq, dp):
+    """Misfit and its derivative along (dq, dp) from the tangent-linear oracle."""
+    st, ce, co, tg = obs
+    t = O.TangentOracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), p)
+    t.set_state(c.q0)
+    t.set_tangent(dq, dp)
+    L = dL = 0.0
+    for n in range(len(dts) + 1):
+        sel = np.nonzero(st == n)[0]
+        if sel.size:
+            q, tan = t.get_state(), t.get_tangent()
+            r = q[ce[sel], co[sel]] - tg[sel]
+            L += float(np.sum(r * r))
+            dL += float(np.sum(2.0 * r * tan[ce[sel], co[sel]]))
+        if n < len(dts):
+            t.step(1, dts=np.array([dts[n]]))
+    return L, dL
+
+
+@pytest.mark.parametrize("n,nsteps,every", [(16, 12, 5), (24, 30, 7)])
+def test_adjoint_matches_tangent_linear_oracle(n, nsteps, every):
+    c, p, names, obs = _setup(n, nsteps, 3, 24)
+    g = Solver(c.model, c.mesh, c.settings, p)
+    g.set_state(c.q0)
+    loss, gq, gp, dts = g.adjoint(nsteps, *obs, checkpoint_every=every)
+    # the handle ends at the state after nsteps plain steps
+    h = Solver(c.model, c.mesh, c.settings, p)
+    h.set_state(c.q0)
+    h.step(nsteps)
+    assert np.array_equal(g.get_state(), h.get_state())
+    rng = np.random.default_rng(7)
+    ni = names.index("n_manning")
+    for what in ("b", "b", "manning"):
+        dq = np.zeros_like(c.q0)
+        dp = np.zeros_like(p)
+        if what == "b":
+            dq[:, 0] = rng.standard_normal(c.mesh.n_cells)
+        else:
+            dp[ni] = 1.0
+        L, dL = _oracle_tlm(c, p, dts, obs, dq, dp)
+        assert abs(L - loss) <= 1e-12 * abs(L)
+        ad = float(np.sum(gq * dq) + np.sum(gp * dp))
+        assert abs(ad - dL) <= 1e-8 * max(abs(dL), 1e-30), (what, ad, dL)
+
+
+def test_adjoint_matches_central_differences():
+    n, nsteps = 16, 12
+    c, p, names, obs = _setup(n, nsteps, 3, 24)
+    g = Solver(c.model, c.mesh, c.settings, p)
+    g.set_state(c.q0)
+    loss, gq, gp, dts = g.adjoint(nsteps, *obs, checkpoint_every=5)
+    st, ce, co, tg = obs
+
+    def misfit(q0, pp):
+        s = Solver(c.model, c.mesh, c.settings, pp)
+        s.set_state(q0)
+        L = 0.0
+        for k in range(nsteps + 1):
+            sel = np.nonzero(st == k)[0]
+            if sel.size:
+                r = s.get_state()[ce[sel], co[sel]] - tg[sel]
+                L += float(np.sum(r * r))
+            if k < nsteps:
+                s.step(1, dts=dts[k:k + 1])
+        return L
+
+    assert abs(misfit(c.q0, p) - loss) <= 1e-13 * loss
+    eps = 1e-6
+    rng = np.random.default_rng(11)
+    for _ in range(3):
+        dq = np.zeros_like(c.q0)
+        dq[:, 0] = _smooth(c.mesh, rng) * 1e-2
+        fd = (misfit(c.q0 + eps * dq, p) - misfit(c.q0 - eps * dq, p)) / (2 * eps)
+        ad = float(np.sum(gq * dq))
+        assert abs(ad - fd) <= 1e-6 * abs(fd) + 1e-14, (ad, fd)
+    # The misfit's derivative in n is O(1e-7) here, and the Newton loop's
+    # tolerance-based stop (0 or 1 update) moves the map in steps of up to its
+    # 1e-8 tolerance, so central differences resolve it only to a few 1e-5
+    # (2.7e-5 measured); the tangent-linear comparison above checks the same
+    # derivative to 1e-8.
+    dp = np.zeros_like(p)
+    dp[names.index("n_manning")] = 1.0
+    fd = (misfit(c.q0, p + eps * dp) - misfit(c.q0, p - eps * dp)) / (2 * eps)
+    ad = float(np.sum(gp * dp))
+    assert abs(ad - fd) <= 1e-4 * abs(fd) + 1e-14, (ad, fd)
+
+
+def test_torch_autograd_wrapper():
+    import torch
+
+    n, nsteps = 16, 9
+    c, p, names, obs = _setup(n, nsteps, 3, 16)
+    g = Solver(c.model, c.mesh, c.settings, p)
+    b = torch.tensor(c.q0[:, 0], requires_grad=True)
+    pt = torch.tensor(p, requires_grad=True)
+    rest = torch.tensor(c.q0[:, 1:])
+    q0 = torch.cat([b[:, None], rest], dim=1)
+    loss = adj.gauge_loss(g, q0, pt, nsteps, obs, checkpoint_every=4)
+    (2.0 * loss).backward()
+    g2 = Solver(c.model, c.mesh, c.settings, p)
+    g2.set_state(c.q0)
+    L, gq, gp, _ = g2.adjoint(nsteps, *obs, checkpoint_every=4)
+    assert abs(float(loss.detach()) - L) <= 1e-14 * L
+    assert np.allclose(b.grad.numpy(), 2.0 * gq[:, 0], rtol=0, atol=0)
+    assert np.allclose(pt.grad.numpy(), 2.0 * gp, rtol=0, atol=0)
+
+
+def test_adjoint_rejects_bad_input():
+    from zoomy_dmplex_b200 import native
+
+    c = cases.adjoint_l1(12)
+    p, _ = _params(c)
+    g = Solver(c.model, c.mesh, c.settings, p)
+    g.set_state(c.q0)
+    with pytest.raises(native.ZsmeError):
+        g.adjoint(5, [9], [0], [1], [0.0])          # observation after the last step
+    with pytest.raises(native.ZsmeError):
+        g.adjoint(5, [1], [c.mesh.n_cells], [1], [0.0])

@@ -18,10 +18,10 @@ import os
 from . import native
 from .solver import LAUNCH_KEYS, get_launch, set_launch
 
-KNOBS = (("prep", (64, 128)), ("prep_occ", (1, 2, 3, 4)), ("face", (64, 128)), ("face_occ", (1, 2, 3, 4)),
-         ("gather", (64, 128)), ("finalize", (64, 128)))
+KNOBS = (("prep", (64, 128)), ("prep_occ", (1, 2, 3, 4, 6, 8)), ("face", (64, 128)), ("face_occ", (1, 2, 3, 4)),
+         ("gather", (64, 128)), ("finalize", (64, 128)), ("finalize_occ", (1, 2, 3, 4)))
 KERNEL_OF = {"prep": "prep", "prep_occ": "prep", "face": "flux", "face_occ": "flux", "gather": "gather",
-             "finalize": "finalize"}
+             "finalize": "finalize", "finalize_occ": "finalize"}
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_launch.json")
 
 

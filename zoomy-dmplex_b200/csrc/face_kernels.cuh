@@ -94,7 +94,8 @@ template <class M>
 __global__ void __launch_bounds__(128) gather_kernel(MeshDev m, Opts o, int c0, int cn,
                                                      const double* __restrict__ fb, int mode, const double* x_in,
                                                      double* x_out, double* base, const double* __restrict__ dt_step,
-                                                     const int* __restrict__ active) {
+                                                     const int* __restrict__ active, const double* __restrict__ aux,
+                                                     const double* __restrict__ params, double* __restrict__ xl_out) {
     constexpr int NQ = M::n_dof_q;
     const int C = m.C, F = m.F;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -140,7 +141,19 @@ __global__ void __launch_bounds__(128) gather_kernel(MeshDev m, Opts o, int c0, 
         case MODE_MID: {    // w += dt/(s-1) F (in place)
             const double a = h / (s - 1.);
 #pragma unroll
-            for (int i = 0; i < NQ; ++i) x_out[(size_t)i * C + c] = x_in[(size_t)i * C + c] + a * acc[i];
+            for (int i = 0; i < NQ; ++i) {
+                acc[i] = x_in[(size_t)i * C + c] + a * acc[i];
+                x_out[(size_t)i * C + c] = acc[i];
+            }
+            if (xl_out) {   // the next stage's clamped copy
+                constexpr int NA = M::n_dof_qaux;
+                double an[NA];
+#pragma unroll
+                for (int i = 0; i < NA; ++i) an[i] = aux[(size_t)i * C + c];
+                clamp_q<M>(acc, an, params + (size_t)I * m.np);
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) xl_out[(size_t)i * C + c] = acc[i];
+            }
             break;
         }
         case MODE_FINAL: {  // X = (s-1)/s w + dt/s F + 1/s X

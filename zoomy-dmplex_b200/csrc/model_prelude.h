@@ -36,6 +36,10 @@ struct SimpleArray {
 };
 #endif
 
+// dual numbers and their std:: overloads, visible before the plugins are
+// parsed (qualified std::sqrt etc. in a template bind at its definition)
+#include "dual.h"
+
 template <typename T>
 ZSME_HD inline T Heaviside(T x, double h0) {
     return x < T(0) ? T(0) : (x > T(0) ? T(1) : T(h0));
@@ -43,14 +47,23 @@ ZSME_HD inline T Heaviside(T x, double h0) {
 
 namespace zsme {
 
+// The scalar type T of a plugin instantiation Model<T> (double, or a dual
+// number for derivatives), so that the traits below detect the same
+// functions whatever the scalar.
+template <class M>
+struct ScalarOf { using type = double; };
+template <template <typename> class MT, typename T>
+struct ScalarOf<MT<T>> { using type = T; };
+
 // Trait detection mirroring the reference's SFINAE switches.
 // update_variables(Q, Qaux, p, dt) present?  (TransportStep.hpp:22-29)
 template <class M, typename = void>
 struct HasUpdateVariables : std::false_type {};
 template <class M>
 struct HasUpdateVariables<M, std::void_t<decltype(M::update_variables(
-    std::declval<const double*>(), std::declval<const double*>(),
-    std::declval<const double*>(), std::declval<const double>()))>> : std::true_type {};
+    std::declval<const typename ScalarOf<M>::type*>(), std::declval<const typename ScalarOf<M>::type*>(),
+    std::declval<const typename ScalarOf<M>::type*>(), std::declval<const typename ScalarOf<M>::type>()))>>
+    : std::true_type {};
 
 // Analytic dAux/dQ with the 3-argument signature?  (SourceStep.hpp:16-20)
 // A 5-argument update_aux_variables_jacobian_wrt_variables does not match,
@@ -59,6 +72,7 @@ template <class M, typename = void>
 struct HasAuxJacobian : std::false_type {};
 template <class M>
 struct HasAuxJacobian<M, std::void_t<decltype(M::update_aux_variables_jacobian_wrt_variables(
-    (const double*)nullptr, (const double*)nullptr, (const double*)nullptr))>> : std::true_type {};
+    (const typename ScalarOf<M>::type*)nullptr, (const typename ScalarOf<M>::type*)nullptr,
+    (const typename ScalarOf<M>::type*)nullptr))>> : std::true_type {};
 
 }  // namespace zsme

@@ -32,7 +32,8 @@ struct PreparedMesh {
 // Block sizes of the kernels (the autotuner's knobs).
 struct LaunchConfig {
     int prep, face, gather, finalize;  // threads per block
-    int prep_occ = 1, face_occ = 1;    // register cap: blocks per SM (1, 2, 3 or 4)
+    int prep_occ = 1, face_occ = 1;    // register cap, blocks per SM: prep 1, 2, 3, 4, 6, 8; face 1-4
+    int finalize_occ = 1;              // register cap of finalize, blocks of 128 per SM: 1-4
 };
 
 // Builds the layout (validates the connectivity; computes the least-squares
@@ -42,6 +43,17 @@ int prepare_mesh(const zsme_mesh& m, PreparedMesh& out);
 int concat_meshes(std::vector<PreparedMesh>& parts, PreparedMesh& out);
 
 int set_error(int code, const std::string& msg);
+
+// Least-squares observations of a discrete adjoint run (zsme_adjoint):
+// loss = sum_j weight_j (Q_{step_j}[cell_j, comp_j] - target_j)^2.
+struct AdjointSpec {
+    int nsteps = 0, every = 1, nobs = 0;
+    const int* obs_step = nullptr;
+    const int* obs_cell = nullptr;   // caller cell ids
+    const int* obs_comp = nullptr;
+    const double* obs_target = nullptr;
+    const double* obs_weight = nullptr;  // nullptr: all 1
+};
 
 class SolverBase {
   public:
@@ -66,6 +78,10 @@ class SolverBase {
     virtual int read_profile(double* ms, int64_t* n) = 0;
     virtual int set_launch(const LaunchConfig& lc) = 0;
     virtual LaunchConfig launch() const = 0;
+    // loss, gradient with respect to the state at call time (caller order, AoS),
+    // gradient with respect to the parameters, and the dt of every step
+    virtual int adjoint(const AdjointSpec& spec, double* loss, double* grad_q, double* grad_params,
+                        double* dts) = 0;
 };
 
 }  // namespace zsme

@@ -6,6 +6,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -17,6 +18,7 @@
 #include "step_kernels.cuh"
 #include "face_kernels.cuh"
 #include "source_kernels.cuh"
+#include "adjoint_kernels.cuh"
 #include "zsme.h"
 
 namespace zsme {
@@ -68,15 +70,20 @@ class Solver final : public SolverBase {
     DevBuf<int> cell_inst_, face_inst_;
     DevBuf<double> slot_dx_, slot_w_, vol_, rc_, fn_, farea_, fc_, fnr_;
     // state
-    DevBuf<double> x_, w_, aux_, fs_, fb_, tmp_a_, tmp_b_, params_, dts_;
+    DevBuf<double> x_, w_, wl_, aux_, fs_, fb_, tmp_a_, tmp_b_, params_, dts_;
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
     DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..3] diag
     DevBuf<unsigned long long> ratio_;
+    // discrete adjoint (allocated by the first zsme_adjoint call)
+    DevBuf<double> adj_ck_x_, adj_ck_a_, adj_tape_, adj_lam0_, adj_lam1_, adj_lam2_, adj_own_w_, adj_own_wl_;
+    DevBuf<double> adj_out_w_, adj_out_wl_, adj_gfs_, adj_lp_cell_, adj_lp_, adj_wl_, adj_oval_, adj_oseed_, adj_dts_;
+    DevBuf<int> adj_ocell_, adj_ocomp_;
     MeshDev md_{};
     Opts opts_{};
     // per-kernel CUDA-event timing (zsme_set_profiling)
     bool profiling_ = false;
+    bool x_clamped_ = true;  // x_ equals update_variables(x_)
     std::vector<cudaEvent_t> ev_pool_;
     std::vector<int> ev_kind_;
     size_t ev_used_ = 0;
@@ -141,8 +148,10 @@ class Solver final : public SolverBase {
     int set_launch(const LaunchConfig& lc) override {
         for (int b : {lc.prep, lc.face, lc.gather, lc.finalize})
             if (b < 32 || b > 128 || b % 32) return set_error(ZSME_ERR_ARG, "block sizes must be 32, 64, 96 or 128");
-        for (int o : {lc.prep_occ, lc.face_occ})
-            if (o < 1 || o > 4) return set_error(ZSME_ERR_ARG, "occupancy caps must be 1..4 blocks per SM");
+        if (lc.prep_occ < 1 || lc.prep_occ > 8 || lc.prep_occ == 5 || lc.prep_occ == 7)
+            return set_error(ZSME_ERR_ARG, "prep occupancy cap must be 1, 2, 3, 4, 6 or 8 blocks per SM");
+        if (lc.face_occ < 1 || lc.face_occ > 4 || lc.finalize_occ < 1 || lc.finalize_occ > 4)
+            return set_error(ZSME_ERR_ARG, "face and finalize occupancy caps must be 1..4 blocks per SM");
         lc_ = lc;
         if (graph_) {
             cudaGraphExecDestroy(graph_);
@@ -193,6 +202,7 @@ class Solver final : public SolverBase {
         opts_ = Opts{st_.reconstruction_order, st_.limiter, st_.gradient, st_.ssp_stages, st_.source};
         ZSME_CUDA(x_.alloc((size_t)NQ * C));
         ZSME_CUDA(w_.alloc((size_t)NQ * C));
+        ZSME_CUDA(wl_.alloc((size_t)NQ * C));
         ZSME_CUDA(aux_.alloc((size_t)NA * C));
         ZSME_CUDA(fs_.alloc((size_t)2 * NQ * F));
         ZSME_CUDA(fb_.alloc((size_t)3 * NQ * F));
@@ -259,8 +269,7 @@ class Solver final : public SolverBase {
         // constraints, then dt_start = max(ComputeTimeStep, min_dt)
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
-        finalize_kernel<M, N><<<blocks_for(cn, lc_.finalize), lc_.finalize, 0, stream_>>>(
-            md_, c0, cn, x_.p, aux_.p, params_.p, sd, nullptr, FIN_POST | FIN_WRITE | FIN_DT);
+        finalize_range(c0, cn, sd, nullptr, FIN_POST | FIN_WRITE | FIN_DT);
         ZSME_CUDA(cudaGetLastError());
         end_step_kernel<<<1, 32, 0, stream_>>>(step_dev(nullptr), inst, 1, 0, st_.min_dt, nullptr);
         ZSME_CUDA(cudaGetLastError());
@@ -288,23 +297,28 @@ class Solver final : public SolverBase {
     }
 
     // ---------------------------------------------------------- pieces
-    void launch_prep(const double* w, const int* active) {
+    // w: stage state, wl: its clamped copy (the same array where w is already clamped)
+    void launch_prep(const double* w, const double* wl, const int* active) {
         mark(ZSME_KERNEL_PREP, true);
         const int gb = blocks_for(pm_.C, lc_.prep);
         switch (lc_.prep_occ) {
 #define ZSME_PREP(OCC)                                                                                          \
     case OCC:                                                                                                   \
-        prep_kernel<M, OCC><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, aux_.p, params_.p, fs_.p,     \
-                                                          active);                                              \
+        if (pm_.K == 3)                                                                                         \
+            prep_kernel<M, OCC, 3><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, aux_.p, params_.p,\
+                                                                 fs_.p, active);                                \
+        else                                                                                                    \
+            prep_kernel<M, OCC, 4><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, aux_.p, params_.p,\
+                                                                 fs_.p, active);                                \
         break;
-            ZSME_PREP(2) ZSME_PREP(3) ZSME_PREP(4)
+            ZSME_PREP(2) ZSME_PREP(3) ZSME_PREP(4) ZSME_PREP(6) ZSME_PREP(8)
             default: ZSME_PREP(1)
 #undef ZSME_PREP
         }
         mark(ZSME_KERNEL_PREP, false);
     }
     void launch_flux(int mode, double t_host, const double* t_dev, double frac, const double* x_in, double* x_out,
-                     double* base, const double* dt, const int* active) {
+                     double* base, const double* dt, const int* active, double* xl_out = nullptr) {
         mark(ZSME_KERNEL_FLUX, true);
         const int gf = blocks_for(pm_.F, lc_.face);
         switch (lc_.face_occ) {
@@ -321,13 +335,25 @@ class Solver final : public SolverBase {
         mark(ZSME_KERNEL_GATHER, true);
         gather_kernel<M><<<blocks_for(pm_.C, lc_.gather), lc_.gather, 0, stream_>>>(md_, opts_, 0, pm_.C, fb_.p,
                                                                                    mode, x_in, x_out, base, dt,
-                                                                                   active);
+                                                                                   active, aux_.p, params_.p, xl_out);
         mark(ZSME_KERNEL_GATHER, false);
+    }
+    void finalize_range(int c0, int cn, const StepDev& sd, const double* dt_src, int flags) {
+        const int gb = blocks_for(cn, lc_.finalize);
+        switch (lc_.finalize_occ) {
+#define ZSME_FIN(OCC)                                                                                            \
+    case OCC:                                                                                                    \
+        finalize_kernel<M, N, OCC><<<gb, lc_.finalize, 0, stream_>>>(md_, c0, cn, x_.p, aux_.p, params_.p, sd,    \
+                                                                     dt_src, flags);                             \
+        break;
+            ZSME_FIN(2) ZSME_FIN(3) ZSME_FIN(4)
+            default: ZSME_FIN(1)
+#undef ZSME_FIN
+        }
     }
     void launch_finalize(const StepDev& sd, const double* dt_src, int flags) {
         mark(ZSME_KERNEL_FINALIZE, true);
-        finalize_kernel<M, N><<<blocks_for(pm_.C, lc_.finalize), lc_.finalize, 0, stream_>>>(
-            md_, 0, pm_.C, x_.p, aux_.p, params_.p, sd, dt_src, flags);
+        finalize_range(0, pm_.C, sd, dt_src, flags);
         mark(ZSME_KERNEL_FINALIZE, false);
     }
 
@@ -336,7 +362,8 @@ class Solver final : public SolverBase {
         const int C = pm_.C;
         ZSME_CUDA(cudaMemcpyAsync(tmp_b_.p, x_aos, (size_t)NQ * C * sizeof(double), cudaMemcpyHostToDevice, stream_));
         aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(tmp_b_.p, w_.p, old_of_new_.p, 0, C, C, NQ);
-        launch_prep(w_.p, nullptr);
+        clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, w_.p, aux_.p, params_.p, wl_.p);
+        launch_prep(w_.p, wl_.p, nullptr);
         launch_flux(MODE_RHS, t, nullptr, 0.0, nullptr, tmp_a_.p, nullptr, nullptr, nullptr);
         ZSME_CUDA(cudaGetLastError());
         return get_soa(0, tmp_a_.p, NQ, f_aos, false);
@@ -348,6 +375,7 @@ class Solver final : public SolverBase {
         launch_finalize(sd, nullptr, FIN_PRE | FIN_WRITE);
         ZSME_CUDA(cudaGetLastError());
         ZSME_CUDA(cudaStreamSynchronize(stream_));
+        x_clamped_ = true;
         return ZSME_OK;
     }
 
@@ -359,6 +387,7 @@ class Solver final : public SolverBase {
         launch_finalize(sd, dt_aux_.p, FIN_SOURCE | FIN_WRITE);
         ZSME_CUDA(cudaGetLastError());
         ZSME_CUDA(cudaStreamSynchronize(stream_));
+        x_clamped_ = false;     // the Newton result is not clamped until the next step
         return ZSME_OK;
     }
 
@@ -376,7 +405,11 @@ class Solver final : public SolverBase {
     }
 
     // One time step of every instance (MUSCLSolver.hpp:140-188).
-    void enqueue_step(const double* dts) {
+    // wl0: clamped copy of x_ for the first stage (x_ itself when x_ is constrained).
+    // tape (adjoint replay): NQ x C slots receiving each stage state W_1 .. W_{s-1}
+    // and the stage output X' before finalize (tape[0] = W_0 is the caller's copy)
+    void enqueue_step(const double* dts, const double* wl0, double* tape = nullptr) {
+        const size_t tape_n = (size_t)NQ * pm_.C;
         StepDev sd = step_dev(dts);
         const double* t = sd.t;
         const double* dt = sd.dt_step;
@@ -385,18 +418,27 @@ class Solver final : public SolverBase {
         begin_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_);
         mark(ZSME_KERNEL_BEGIN, false);
         if (st_.reconstruction_order < 2) {
-            launch_prep(x_.p, act);
+            launch_prep(x_.p, x_.p, act);
             launch_flux(MODE_EULER, 0.0, t, 0.0, nullptr, nullptr, x_.p, dt, act);
+            if (tape)
+                cudaMemcpyAsync(tape + tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
         } else {
             const int s = st_.ssp_stages;
             for (int i = 0; i < s - 1; ++i) {
                 const double frac = i / (s - 1.);
-                launch_prep(i == 0 ? x_.p : w_.p, act);
+                // later stages get their clamped copy from gather
+                launch_prep(i == 0 ? x_.p : w_.p, i == 0 ? wl0 : wl_.p, act);
                 launch_flux(i == 0 ? MODE_FIRST : MODE_MID, 0.0, t, frac, i == 0 ? x_.p : w_.p, w_.p, nullptr, dt,
-                            act);
+                            act, wl_.p);
+                if (tape)
+                    cudaMemcpyAsync(tape + (size_t)(i + 1) * tape_n, w_.p, tape_n * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, stream_);
             }
-            launch_prep(w_.p, act);
+            launch_prep(w_.p, wl_.p, act);
             launch_flux(MODE_FINAL, 0.0, t, 1.0, w_.p, nullptr, x_.p, dt, act);
+            if (tape)
+                cudaMemcpyAsync(tape + (size_t)s * tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                stream_);
         }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
         launch_finalize(sd, sd.dt_step, flags);
@@ -412,7 +454,15 @@ class Solver final : public SolverBase {
         if (nsteps <= 0) return ZSME_OK;
         if (dts_host && n_inst_ != 1) return set_error(ZSME_ERR_ARG, "imposed dts need a single-instance handle");
         ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 3 * sizeof(int), stream_));
-        if (dts_host || profiling_) {
+        // x_ is constrained after set_state, update_state and every step (update_variables is a
+        // projection: the clamp of a clamped state is that state), so it serves as its own
+        // clamped copy; after a bare source() the first step clamps a copy first, uncaptured
+        const bool unclamped = !x_clamped_ && st_.reconstruction_order >= 2;
+        x_clamped_ = true;
+        if (unclamped)
+            clamp_kernel<M><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, 0, pm_.C, x_.p, aux_.p, params_.p,
+                                                                        wl_.p);
+        if (dts_host || profiling_ || unclamped) {
             // imposed dts or per-kernel timing: plain launches (the step index
             // lives on the device)
             if (dts_host) {
@@ -420,7 +470,8 @@ class Solver final : public SolverBase {
                 ZSME_CUDA(cudaMemcpyAsync(dts_.p, dts_host, nsteps * sizeof(double), cudaMemcpyHostToDevice, stream_));
                 ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));
             }
-            for (int i = 0; i < nsteps; ++i) enqueue_step(dts_host ? dts_.p : nullptr);
+            for (int i = 0; i < nsteps; ++i)
+                enqueue_step(dts_host ? dts_.p : nullptr, (unclamped && i == 0) ? wl_.p : x_.p);
             ZSME_CUDA(cudaGetLastError());
             int rc = collect_profile();
             if (rc) return rc;
@@ -428,13 +479,218 @@ class Solver final : public SolverBase {
             if (!graph_) {
                 cudaGraph_t g = nullptr;
                 ZSME_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-                enqueue_step(nullptr);
+                enqueue_step(nullptr, x_.p);
                 ZSME_CUDA(cudaStreamEndCapture(stream_, &g));
                 ZSME_CUDA(cudaGraphInstantiate(&graph_, g, 0));
                 cudaGraphDestroy(g);
             }
             for (int i = 0; i < nsteps; ++i) ZSME_CUDA(cudaGraphLaunch(graph_, stream_));
         }
+        return ZSME_OK;
+    }
+
+    // ------------------------------------------------------ discrete adjoint
+    // R'(W)^T (scale * src) + c_src * src -> dst, for the stage state W at stage
+    // time t; W0: W is the step's start state (its own clamped copy, as in the
+    // forward stage).
+    void adj_apply_rt(const double* W, bool W0, double t, double scale, const double* src, double c_src,
+                      double* dst) {
+        const int C = pm_.C, F = pm_.F;
+        const double* wl = W;
+        if (!W0) {
+            clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, W, aux_.p, params_.p, adj_wl_.p);
+            wl = adj_wl_.p;
+        }
+        launch_prep(W, wl, nullptr);
+        adj_face_kernel<MT, NT><<<blocks_for(F, 128), 128, 0, stream_>>>(md_, fs_.p, aux_.p, params_.p, t, src, scale,
+                                                                         adj_gfs_.p);
+        if (pm_.K == 3)
+            adj_cell_kernel<MT, 3><<<blocks_for(C, 128), 128, 0, stream_>>>(
+                md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);
+        else
+            adj_cell_kernel<MT, 4><<<blocks_for(C, 128), 128, 0, stream_>>>(
+                md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);
+        adj_combine_kernel<MT><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, W, aux_.p, params_.p, adj_own_w_.p,
+                                                                        adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p,
+                                                                        src, c_src, dst);
+    }
+
+    // lam (adjoint of X_{n+1}) -> adjoint of X_n, from the tape of step n:
+    // tape[i] = W_i (i < s), tape[s] = X'.  Returns the buffer now holding it.
+    double* adj_step(double* lam, double* t1, double* t2, const double* tape, double dt, double tn) {
+        const int C = pm_.C;
+        const size_t nv = (size_t)NQ * C;
+        if (!(dt > 0.0)) return lam;  // inactive step: the identity
+        const int flags = FIN_PRE | FIN_POST | (st_.source ? FIN_SOURCE : 0);
+        const int s = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
+        adj_finalize_kernel<MT><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, tape + (size_t)s * nv, aux_.p,
+                                                                         params_.p, dt, flags, lam, t1,
+                                                                         adj_lp_cell_.p);
+        adj_param_reduce_kernel<<<NP, 256, 0, stream_>>>(adj_lp_cell_.p, C, adj_lp_.p);
+        // t1 = adjoint of X'
+        if (st_.reconstruction_order < 2) {  // X' = W0 + dt R(W0)
+            adj_apply_rt(tape, true, tn, dt, t1, 1.0, lam);
+            return lam;
+        }
+        // X' = (s-1)/s W_{s-1} + dt/s R(W_{s-1}) + 1/s W_0
+        adj_apply_rt(tape + (size_t)(s - 1) * nv, s - 1 == 0, tn + 1.0 * dt, dt / s, t1, (s - 1.) / s, t2);
+        double* cur = t2;
+        double* oth = lam;
+        const double a = dt / (s - 1.);
+        for (int i = s - 2; i >= 0; --i) {  // W_{i+1} = W_i + a R(W_i)
+            adj_apply_rt(tape + (size_t)i * nv, i == 0, tn + (i / (s - 1.)) * dt, a, cur, 1.0, oth);
+            std::swap(cur, oth);
+        }
+        axpby_kernel<<<blocks_for((long long)nv, 256), 256, 0, stream_>>>((long long)nv, 1.0 / s, t1, 1.0, cur);
+        return cur;
+    }
+
+    int adjoint(const AdjointSpec& A, double* loss, double* grad_q, double* grad_p, double* dts_out) override {
+        if (n_inst_ != 1) return set_error(ZSME_ERR_ARG, "the adjoint needs a single-instance handle");
+        if (A.nsteps < 0 || A.every < 1 || A.nobs < 0)
+            return set_error(ZSME_ERR_ARG, "adjoint: nsteps >= 0, checkpoint interval >= 1 and n_obs >= 0 required");
+        if (A.nobs && (!A.obs_step || !A.obs_cell || !A.obs_comp || !A.obs_target))
+            return set_error(ZSME_ERR_ARG, "adjoint: null observation array");
+        if (!x_clamped_)
+            return set_error(ZSME_ERR_STATE, "adjoint: the state is not constrained (call zsme_update_state)");
+        const int C = pm_.C, F = pm_.F, K = pm_.K, NS = A.nsteps;
+        const int s = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
+        const size_t nv = (size_t)NQ * C, na = (size_t)NA * C;
+        // observations in device numbering, grouped by step (stable)
+        std::vector<int> ord(A.nobs);
+        for (int j = 0; j < A.nobs; ++j) {
+            ord[j] = j;
+            if (A.obs_step[j] < 0 || A.obs_step[j] > NS || A.obs_cell[j] < 0 || A.obs_cell[j] >= C ||
+                A.obs_comp[j] < 0 || A.obs_comp[j] >= NQ)
+                return set_error(ZSME_ERR_ARG, "adjoint: observation " + std::to_string(j) + " out of range");
+        }
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return A.obs_step[x] < A.obs_step[y]; });
+        std::vector<int> first(NS + 2, 0), ocell(A.nobs), ocomp(A.nobs);
+        for (int r = 0; r < A.nobs; ++r) {
+            const int j = ord[r];
+            ocell[r] = pm_.new_of_old[A.obs_cell[j]];
+            ocomp[r] = A.obs_comp[j];
+            first[A.obs_step[j] + 1]++;
+        }
+        for (int n = 0; n <= NS; ++n) first[n + 1] += first[n];
+        const int nseg = (NS + A.every - 1) / A.every;
+        ZSME_CUDA(adj_ocell_.upload(ocell, stream_));
+        ZSME_CUDA(adj_ocomp_.upload(ocomp, stream_));
+        ZSME_CUDA(adj_oval_.alloc(std::max(1, A.nobs)));
+        ZSME_CUDA(adj_oseed_.alloc(std::max(1, A.nobs)));
+        ZSME_CUDA(adj_ck_x_.alloc((size_t)(nseg + 1) * nv));
+        ZSME_CUDA(adj_ck_a_.alloc((size_t)(nseg + 1) * na));
+        ZSME_CUDA(adj_tape_.alloc((size_t)std::min(A.every, std::max(NS, 1)) * (s + 1) * nv));
+        for (auto* b : {&adj_lam0_, &adj_lam1_, &adj_lam2_, &adj_own_w_, &adj_own_wl_, &adj_wl_})
+            ZSME_CUDA(b->alloc(nv));
+        ZSME_CUDA(adj_out_w_.alloc((size_t)K * nv));
+        ZSME_CUDA(adj_out_wl_.alloc((size_t)K * nv));
+        ZSME_CUDA(adj_gfs_.alloc((size_t)2 * NQ * F));
+        ZSME_CUDA(adj_lp_cell_.alloc((size_t)NP * C));
+        ZSME_CUDA(adj_lp_.alloc(NP));
+        ZSME_CUDA(adj_dts_.alloc(std::max(1, NS)));
+        auto obs_values = [&](int n) {
+            const int cnt = first[n + 1] - first[n];
+            if (cnt > 0)
+                obs_value_kernel<<<blocks_for(cnt, 128), 128, 0, stream_>>>(cnt, adj_ocell_.p + first[n],
+                                                                            adj_ocomp_.p + first[n], x_.p, C,
+                                                                            adj_oval_.p + first[n]);
+        };
+        auto save = [&](int slot) {
+            cudaMemcpyAsync(adj_ck_x_.p + (size_t)slot * nv, x_.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
+            cudaMemcpyAsync(adj_ck_a_.p + (size_t)slot * na, aux_.p, na * sizeof(double), cudaMemcpyDeviceToDevice,
+                            stream_);
+        };
+        auto restore = [&](int slot) {
+            cudaMemcpyAsync(x_.p, adj_ck_x_.p + (size_t)slot * nv, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
+            cudaMemcpyAsync(aux_.p, adj_ck_a_.p + (size_t)slot * na, na * sizeof(double), cudaMemcpyDeviceToDevice,
+                            stream_);
+        };
+        // ---- forward: CFL steps, checkpoints, observed values, dt record
+        double t0 = 0.0;
+        ZSME_CUDA(cudaMemcpyAsync(&t0, t_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ZSME_CUDA(cudaStreamSynchronize(stream_));
+        save(0);
+        for (int n = 0; n < NS; ++n) {
+            obs_values(n);
+            int rc = step(1, nullptr);
+            if (rc) return rc;
+            ZSME_CUDA(cudaMemcpyAsync(adj_dts_.p + n, dt_step_.p, sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            if ((n + 1) % A.every == 0 && n + 1 < NS) save((n + 1) / A.every);
+        }
+        obs_values(NS);
+        save(nseg);  // the final state, restored at the end
+        double t_fin = 0.0, dtc_fin = 0.0;
+        std::vector<double> dth(std::max(1, NS)), oval(std::max(1, A.nobs));
+        ZSME_CUDA(cudaMemcpyAsync(&t_fin, t_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ZSME_CUDA(cudaMemcpyAsync(&dtc_fin, dt_cfl_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ZSME_CUDA(cudaMemcpyAsync(dth.data(), adj_dts_.p, dth.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ZSME_CUDA(cudaMemcpyAsync(oval.data(), adj_oval_.p, oval.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                  stream_));
+        ZSME_CUDA(cudaStreamSynchronize(stream_));
+        std::vector<double> th(NS + 1);
+        th[0] = t0;
+        for (int n = 0; n < NS; ++n) th[n + 1] = th[n] + dth[n];
+        // loss in the caller's order; seeds 2 w (q - target) in device order
+        std::vector<double> val_of(A.nobs), seed(std::max(1, A.nobs));
+        for (int r = 0; r < A.nobs; ++r) val_of[ord[r]] = oval[r];
+        double L = 0.0;
+        for (int j = 0; j < A.nobs; ++j) {
+            const double wj = A.obs_weight ? A.obs_weight[j] : 1.0;
+            const double rr = val_of[j] - A.obs_target[j];
+            L += wj * rr * rr;
+        }
+        for (int r = 0; r < A.nobs; ++r) {
+            const int j = ord[r];
+            seed[r] = 2.0 * (A.obs_weight ? A.obs_weight[j] : 1.0) * (val_of[j] - A.obs_target[j]);
+        }
+        ZSME_CUDA(cudaMemcpyAsync(adj_oseed_.p, seed.data(), seed.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                  stream_));
+        // ---- reverse, segment by segment
+        double* lam = adj_lam0_.p;
+        ZSME_CUDA(cudaMemsetAsync(lam, 0, nv * sizeof(double), stream_));
+        ZSME_CUDA(cudaMemsetAsync(adj_lp_.p, 0, NP * sizeof(double), stream_));
+        auto seeds = [&](int n, double* l) {
+            const int cnt = first[n + 1] - first[n];
+            if (cnt > 0)
+                adj_seed_kernel<<<1, 1, 0, stream_>>>(cnt, adj_ocell_.p + first[n], adj_ocomp_.p + first[n],
+                                                      adj_oseed_.p + first[n], C, l);
+        };
+        seeds(NS, lam);
+        for (int seg = nseg - 1; seg >= 0; --seg) {
+            const int n0 = seg * A.every, n1 = std::min(NS, n0 + A.every);
+            restore(seg);
+            ZSME_CUDA(cudaMemcpyAsync(t_.p, &th[n0], sizeof(double), cudaMemcpyHostToDevice, stream_));
+            for (int n = n0; n < n1; ++n) {  // replay with the recorded dts, into the tape
+                double* tp = adj_tape_.p + (size_t)(n - n0) * (s + 1) * nv;
+                cudaMemcpyAsync(tp, x_.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
+                ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));
+                enqueue_step(adj_dts_.p + n, x_.p, tp);
+            }
+            for (int n = n1 - 1; n >= n0; --n) {
+                const double* tp = adj_tape_.p + (size_t)(n - n0) * (s + 1) * nv;
+                double* t1 = lam == adj_lam0_.p ? adj_lam1_.p : adj_lam0_.p;
+                double* t2 = (lam != adj_lam2_.p && t1 != adj_lam2_.p) ? adj_lam2_.p
+                             : (lam != adj_lam1_.p && t1 != adj_lam1_.p) ? adj_lam1_.p : adj_lam0_.p;
+                lam = adj_step(lam, t1, t2, tp, dth[n], th[n]);
+                seeds(n, lam);
+            }
+            ZSME_CUDA(cudaGetLastError());
+        }
+        // ---- outputs; the handle keeps the final state of the forward run
+        if (grad_q) {
+            int rc = get_soa(0, lam, NQ, grad_q, false);
+            if (rc) return rc;
+        }
+        if (grad_p) ZSME_CUDA(cudaMemcpyAsync(grad_p, adj_lp_.p, NP * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        restore(nseg);
+        ZSME_CUDA(cudaMemcpyAsync(t_.p, &t_fin, sizeof(double), cudaMemcpyHostToDevice, stream_));
+        ZSME_CUDA(cudaMemcpyAsync(dt_cfl_.p, &dtc_fin, sizeof(double), cudaMemcpyHostToDevice, stream_));
+        ZSME_CUDA(cudaStreamSynchronize(stream_));
+        if (loss) *loss = L;
+        if (dts_out)
+            for (int n = 0; n < NS; ++n) dts_out[n] = dth[n];
+        x_clamped_ = true;
         return ZSME_OK;
     }
 

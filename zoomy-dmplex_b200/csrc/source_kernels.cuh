@@ -184,8 +184,10 @@ __device__ __forceinline__ int newton_fast(double dtl, double* q, const double* 
     }
 }
 
+// iters (optional): Newton updates applied (0 when the first residual is below
+// the tolerance, so that q is returned unchanged)
 template <class M>
-__device__ __forceinline__ int newton_cell(double dtl, double* q, double* aux, const double* p) {
+__device__ __forceinline__ int newton_cell(double dtl, double* q, double* aux, const double* p, int* iters = nullptr) {
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
     const double X0[3] = {0.0, 0.0, 0.0};
     double q_old[NQ], res[NQ];
@@ -254,6 +256,7 @@ __device__ __forceinline__ int newton_cell(double dtl, double* q, double* aux, c
 #pragma unroll
         for (int i = 0; i < NQ; ++i) q[i] += xv[i];
     }
+    if (iters) *iters = iter;
     return iter >= 15 ? 1 : 0;
 }
 
@@ -266,8 +269,9 @@ enum FinalizeFlags {
 };
 
 // cells [c0, c0 + cn); dt_src: per-instance dt of the source step
-template <class M, class N>
-__global__ void __launch_bounds__(128) finalize_kernel(MeshDev m, int c0, int cn, double* __restrict__ x,
+// MINB: resident blocks of 128 threads per SM the register allocation must allow (1 = no cap)
+template <class M, class N, int MINB>
+__global__ void __launch_bounds__(128, MINB) finalize_kernel(MeshDev m, int c0, int cn, double* __restrict__ x,
                                                        double* __restrict__ aux, const double* __restrict__ params,
                                                        StepDev sd, const double* __restrict__ dt_src, int flags) {
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, DIM = M::dimension;

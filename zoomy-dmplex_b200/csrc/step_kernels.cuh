@@ -6,15 +6,16 @@
 // takes that instance's parameters, time, dt and activity.
 //
 // One SSP stage = prep_kernel + face_kernel + gather_kernel:
-//   prep_kernel   per cell: wet/dry clamp of the stage state, neighbour bounds
-//                 of the clamped state, gradient of the unclamped state (least
-//                 squares or Green-Gauss), limited linear reconstruction at each
-//                 of the cell's faces -> face-indexed face states
-//                 (TransportStep.hpp:196-230, 122-154, 339; Gradient.hpp;
-//                 Reconstruction.hpp:203-243)
+//   prep_kernel   per cell: neighbour bounds of the clamped stage state,
+//                 gradient of the unclamped one (least squares or Green-Gauss),
+//                 limited linear reconstruction at each of the cell's faces ->
+//                 face-indexed face states (TransportStep.hpp:196-230, 122-154,
+//                 339; Gradient.hpp; Reconstruction.hpp:203-243)
 //   face_kernel   per face, once: Riemann flux + fluctuations (face_kernels.cuh)
 //   gather_kernel per cell: face contributions in the reference's order, /
-//                 volume, SSP-RK(s,2) stage combination (face_kernels.cuh)
+//                 volume, SSP-RK(s,2) stage combination, and for the next
+//                 stage the state's wet/dry clamp (update_variables) beside
+//                 the state itself (face_kernels.cuh)
 // After the last stage:
 //   finalize_kernel per cell: constraints, implicit Newton source, constraints,
 //                 CFL ratio r_c / lambda_c, per-instance minimum (source_kernels.cuh)
@@ -99,138 +100,152 @@ __device__ __forceinline__ void constrain(double* q, double* a, const double* p)
     for (int i = 0; i < M::n_dof_qaux; ++i) a[i] = ra[i];
 }
 
+// The state part of constrain<M> alone: the aux update does not change q.
+template <class M>
+__device__ __forceinline__ void clamp_q(double* q, const double* a, const double* p) {
+    if constexpr (HasUpdateVariables<M>::value) {
+        auto r = M::update_variables(q, a, p, 0.0);
+#pragma unroll
+        for (int i = 0; i < M::n_dof_q; ++i) q[i] = r[i];
+    }
+}
+
 template <int NQ>
 __device__ __forceinline__ void load_q(const double* __restrict__ w, int C, int c, double* q) {
 #pragma unroll
     for (int i = 0; i < NQ; ++i) q[i] = w[(size_t)i * C + c];
 }
 
-// LinearReconstructor::Reconstruct with VacuumLimiter + TVDLimiter
-// (Reconstruction.hpp:25-36, 62-81, 203-243): one scalar alpha per face.
-template <int NQ, int DIM>
-__device__ __forceinline__ void reconstruct(const double* q, const double* g, const double* dx,
-                                            const double* qmin, const double* qmax, int limiter,
-                                            double* out) {
-    double delta[NQ];
-    double alpha = 1.0;
-    bool vac = limiter && NQ > 1 && qmin[1] < 1e-2;
+// wl = update_variables(w) for cells [c0, c0 + cn): the clamped copy of a
+// state given from outside (zsme_rhs).  Inside a step the gather kernel
+// writes it alongside each stage state.
+template <class M>
+__global__ void __launch_bounds__(128) clamp_kernel(MeshDev m, int c0, int cn, const double* __restrict__ w,
+                                                    const double* __restrict__ aux,
+                                                    const double* __restrict__ params, double* __restrict__ wl) {
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r, C = m.C;
+    const double* p = params + (size_t)cell_instance(m, c) * m.np;
+    double q[NQ], a[NA];
+    load_q<NQ>(w, C, c, q);
 #pragma unroll
-    for (int i = 0; i < NQ; ++i) {
-        double d = 0.0;
+    for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
+    clamp_q<M>(q, a, p);
 #pragma unroll
-        for (int k = 0; k < DIM; ++k) d += g[i * DIM + k] * dx[k];
-        delta[i] = d;
-        if (limiter) {
-            double qfu = q[i] + d;
-            double dq = qfu - q[i];
-            double al = 1.0;
-            if (!(fabs(dq) < 1e-12)) {
-                if (dq > 0) al = (qmax[i] > q[i]) ? fmin(1.0, (qmax[i] - q[i]) / dq) : 0.0;
-                else al = (qmin[i] < q[i]) ? fmin(1.0, (qmin[i] - q[i]) / dq) : 0.0;
-            }
-            // alpha = min over components of min(vacuum, tvd) (NaN-ignoring as "<")
-            if (al < alpha) alpha = al;
-        }
-    }
-    if (vac) alpha = 0.0 < alpha ? 0.0 : alpha;
-#pragma unroll
-    for (int i = 0; i < NQ; ++i) out[i] = q[i] + alpha * delta[i];
+    for (int i = 0; i < NQ; ++i) wl[(size_t)i * C + c] = q[i];
 }
 
 // ----------------------------------------------------------------- prep
 // cells [c0, c0 + cn)
+// w: the stage state (its gradient), wl: the same state after update_variables
+// (bounds and reconstruction base; TransportStep.hpp:326-339 clamp a local
+// copy and take the gradient of the unclamped global vector).  The kernel
+// works one component at a time and keeps only the gradient and one running
+// alpha per face in registers: the components meet only in the limiter's
+// alpha = min over components, so a first pass over the components lowers each
+// face's alpha and a second writes q + alpha * delta.  Every sum runs in the
+// reference's order (cone order for the bounds and least squares, original
+// face order for Green-Gauss), so the result is that of the whole-vector form.
 // MINB: resident blocks per SM the register allocation must allow (1 = no cap)
-template <class M, int MINB>
+// KM: face slots per cell, 3 = exactly three (triangles), 4 = up to four
+template <class M, int MINB, int KM>
 __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int c0, int cn, const double* __restrict__ w,
-                                                   const double* __restrict__ aux, const double* __restrict__ params,
-                                                   double* __restrict__ fs, const int* __restrict__ active) {
+                                                   const double* __restrict__ wl, const double* __restrict__ aux,
+                                                   const double* __restrict__ params, double* __restrict__ fs,
+                                                   const int* __restrict__ active) {
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, DIM = M::dimension;
-    const int C = m.C;
+    const int C = m.C, F = m.F;
+    const int K = KM == 3 ? 3 : m.K;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= cn) return;
     const int c = c0 + r;
     const int I = cell_instance(m, c);
     if (active && !active[I]) return;
     const double* p = params + (size_t)I * m.np;
-    double qg[NQ], ql[NQ], a[NA];
-    load_q<NQ>(w, C, c, qg);
-#pragma unroll
-    for (int i = 0; i < NQ; ++i) ql[i] = qg[i];
-#pragma unroll
-    for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
-    constrain<M>(ql, a, p);
     if (o.order < 2) {
-        for (int k = 0; k < m.K; ++k) {
+        double ql[NQ], a[NA];
+        load_q<NQ>(w, C, c, ql);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
+        clamp_q<M>(ql, a, p);
+        for (int k = 0; k < K; ++k) {
             const int f = m.slot_face[k * C + c];
             if (f < 0) continue;
             const int side = meta_isL(m.slot_meta[k * C + c]) ? 0 : 1;
 #pragma unroll
-            for (int i = 0; i < NQ; ++i) fs[((size_t)side * NQ + i) * m.F + f] = ql[i];
+            for (int i = 0; i < NQ; ++i) fs[((size_t)side * NQ + i) * F + f] = ql[i];
         }
         return;
     }
-    double mn[NQ], mx[NQ], g[NQ * DIM];
+    // the cell's slots in cone order
+    int nb[KM], ff[KM], sd[KM];
+    double dx[KM][DIM];
 #pragma unroll
-    for (int i = 0; i < NQ; ++i) {
-        mn[i] = ql[i];
-        mx[i] = ql[i];
+    for (int k = 0; k < KM; ++k) {
+        nb[k] = -2;
+        ff[k] = -1;
+        sd[k] = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dx[k][d] = 0.0;
+        if (k < K) {
+            nb[k] = m.slot_nbr[k * C + c];
+            ff[k] = m.slot_face[k * C + c];
+            sd[k] = meta_isL(m.slot_meta[k * C + c]) ? 0 : 1;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) dx[k][d] = m.slot_dx[((size_t)k * 2 + d) * C + c];
+        }
     }
+    // gradient of the unclamped stage state
+    double g[NQ * DIM];
 #pragma unroll
     for (int i = 0; i < NQ * DIM; ++i) g[i] = 0.0;
-    // neighbours in cone order: bounds of the clamped state, LSQ of the raw state
-    for (int k = 0; k < m.K; ++k) {
-        const int n = m.slot_nbr[k * C + c];
-        if (n < 0) continue;
-        double qn[NQ], an[NA];
-        load_q<NQ>(w, C, n, qn);
-        double wk[DIM];
+    if (o.gradient == 1) {
+        // least squares, cone order (Gradient.hpp:330-346)
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) wk[d] = m.slot_w[((size_t)k * 2 + d) * C + c];
-        if (o.gradient == 1) {
+        for (int k = 0; k < KM; ++k) {
+            if (nb[k] < 0) continue;
+            const int n = nb[k];
+            double wk[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) wk[d] = m.slot_w[((size_t)k * 2 + d) * C + c];
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
-                double du = qn[i] - qg[i];
+                const double du = w[(size_t)i * C + n] - w[(size_t)i * C + c];
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) g[i * DIM + d] += wk[d] * du;
             }
         }
-#pragma unroll
-        for (int i = 0; i < NA; ++i) an[i] = aux[(size_t)i * C + n];
-        constrain<M>(qn, an, p);
-#pragma unroll
-        for (int i = 0; i < NQ; ++i) {
-            if (qn[i] < mn[i]) mn[i] = qn[i];
-            if (qn[i] > mx[i]) mx[i] = qn[i];
-        }
-    }
-    if (o.gradient == 0) {
+    } else {
         // Green-Gauss in increasing original face order (Gradient.hpp:91-176)
         const int ord = m.order[c];
-        for (int j = 0; j < m.K; ++j) {
+        for (int j = 0; j < K; ++j) {
             const int k = (ord >> (2 * j)) & 3;
             const int f = m.slot_face[k * C + c];
             if (f < 0) continue;
             const int meta = m.slot_meta[k * C + c];
             const int n = m.slot_nbr[k * C + c];
-            const double Nf[2] = {m.fnr[f], m.fnr[m.F + f]};
+            const double Nf[2] = {m.fnr[f], m.fnr[F + f]};
             if (n >= 0) {
-                double qn[NQ];
-                load_q<NQ>(w, C, n, qn);
                 const bool isL = meta_isL(meta);
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) {
-                    double fv = 0.5 * (isL ? (qg[i] + qn[i]) : (qn[i] + qg[i]));
+                    const double qc = w[(size_t)i * C + c], qn = w[(size_t)i * C + n];
+                    const double fv = 0.5 * (isL ? (qc + qn) : (qn + qc));
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) {
-                        double v = fv * Nf[d];
+                        const double v = fv * Nf[d];
                         if (isL) g[i * DIM + d] += v;
                         else g[i * DIM + d] -= v;
                     }
                 }
             } else if (meta_bc(meta) >= 0) {
-                double nh[3] = {m.fn[f], m.fn[m.F + f], 0.0};
-                double xf[3] = {m.fc[f], m.fc[m.F + f], 0.0};
-                auto qb = M::boundary_conditions(meta_bc(meta), qg, (const double*)nullptr, p, nh, xf, 0.0, 0.0);
+                double qg[NQ];
+                load_q<NQ>(w, C, c, qg);
+                const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
+                const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
+                const auto qb = M::boundary_conditions(meta_bc(meta), qg, (const double*)nullptr, p, nh, xf, 0.0, 0.0);
 #pragma unroll
                 for (int i = 0; i < NQ; ++i)
 #pragma unroll
@@ -243,17 +258,76 @@ __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int 
             for (int i = 0; i < NQ * DIM; ++i) g[i] /= v;
         }
     }
-    for (int k = 0; k < m.K; ++k) {
-        const int f = m.slot_face[k * C + c];
-        if (f < 0) continue;
-        double dx[DIM];
+    // pass 1: each face's alpha = min over components of min(vacuum, tvd)
+    // (Reconstruction.hpp:25-36, 62-81, 224-238); "<" ignores NaN as there
+    double al[KM];
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) dx[d] = m.slot_dx[((size_t)k * 2 + d) * C + c];
-        double qf[NQ];
-        reconstruct<NQ, DIM>(ql, g, dx, mn, mx, o.limiter, qf);
-        const int side = meta_isL(m.slot_meta[k * C + c]) ? 0 : 1;
+    for (int k = 0; k < KM; ++k) al[k] = 1.0;
+    if (o.limiter) {
+        bool vac = false;
+        if (NQ > 1) {   // VacuumLimiter: minimum depth (component 1) over the cell and its neighbours
+            double mnh = wl[C + c];
 #pragma unroll
-        for (int i = 0; i < NQ; ++i) fs[((size_t)side * NQ + i) * m.F + f] = qf[i];
+            for (int k = 0; k < KM; ++k) {
+                if (nb[k] < 0) continue;
+                const double v = wl[(size_t)C + nb[k]];
+                if (v < mnh) mnh = v;
+            }
+            vac = mnh < 1e-2;
+        }
+        if (vac) {
+#pragma unroll
+            for (int k = 0; k < KM; ++k) al[k] = 0.0;
+        } else {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                const double q = wl[(size_t)i * C + c];
+                double mn = q, mx = q;
+#pragma unroll
+                for (int k = 0; k < KM; ++k) {
+                    if (nb[k] < 0) continue;
+                    const double v = wl[(size_t)i * C + nb[k]];
+                    if (v < mn) mn = v;
+                    if (v > mx) mx = v;
+                }
+#pragma unroll
+                for (int k = 0; k < KM; ++k) {
+                    if (ff[k] < 0) continue;
+                    double d = 0.0;
+#pragma unroll
+                    for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+                    const double qfu = q + d;
+                    const double dq = qfu - q;
+                    // fmin(1, r / dq) is exactly 1 when r >= dq > 0 (or r <= dq < 0): the
+                    // correctly rounded quotient of |r| >= |dq| is >= 1, so the
+                    // division is only taken where it can limit (NaN still takes it)
+                    double a = 1.0;
+                    if (!(fabs(dq) < 1e-12)) {
+                        if (dq > 0) {
+                            const double rr = mx - q;
+                            a = (mx > q) ? (rr >= dq ? 1.0 : fmin(1.0, rr / dq)) : 0.0;
+                        } else {
+                            const double rr = mn - q;
+                            a = (mn < q) ? (rr <= dq ? 1.0 : fmin(1.0, rr / dq)) : 0.0;
+                        }
+                    }
+                    if (a < al[k]) al[k] = a;
+                }
+            }
+        }
+    }
+    // pass 2: face states q + alpha * delta
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        const double q = wl[(size_t)i * C + c];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (ff[k] < 0) continue;
+            double d = 0.0;
+#pragma unroll
+            for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+            fs[((size_t)sd[k] * NQ + i) * F + ff[k]] = q + al[k] * d;
+        }
     }
 }
 

@@ -259,7 +259,23 @@ int zsme_batch_get_time(zsme_handle* h, int32_t i, double* t, double* dt) {
 int zsme_set_launch(zsme_handle* h, const int32_t* blocks) {
     CHECK_H(h);
     if (!blocks) return set_error(ZSME_ERR_ARG, "null block sizes");
-    return h->s->set_launch(zsme::LaunchConfig{blocks[0], blocks[1], blocks[2], blocks[3], blocks[4], blocks[5]});
+    return h->s->set_launch(
+        zsme::LaunchConfig{blocks[0], blocks[1], blocks[2], blocks[3], blocks[4], blocks[5], blocks[6]});
+}
+int zsme_adjoint(zsme_handle* h, int32_t nsteps, int32_t checkpoint_every, int32_t n_obs, const int32_t* obs_step,
+                 const int32_t* obs_cell, const int32_t* obs_comp, const double* obs_target,
+                 const double* obs_weight, double* loss, double* grad_q_aos, double* grad_params, double* dts) {
+    CHECK_SINGLE(h);
+    zsme::AdjointSpec a;
+    a.nsteps = nsteps;
+    a.every = checkpoint_every;
+    a.nobs = n_obs;
+    a.obs_step = obs_step;
+    a.obs_cell = obs_cell;
+    a.obs_comp = obs_comp;
+    a.obs_target = obs_target;
+    a.obs_weight = obs_weight;
+    return h->s->adjoint(a, loss, grad_q_aos, grad_params, dts);
 }
 int zsme_get_launch(zsme_handle* h, int32_t* blocks) {
     CHECK_H(h);
@@ -271,6 +287,7 @@ int zsme_get_launch(zsme_handle* h, int32_t* blocks) {
     blocks[3] = lc.finalize;
     blocks[4] = lc.prep_occ;
     blocks[5] = lc.face_occ;
+    blocks[6] = lc.finalize_occ;
     return ZSME_OK;
 }
 

@@ -109,6 +109,8 @@ def load():
     lib.zsme_batch_get_time.argtypes = [vp, ct.c_int32, P, P]
     lib.zsme_set_launch.argtypes = [vp, ct.POINTER(ct.c_int32)]
     lib.zsme_get_launch.argtypes = [vp, ct.POINTER(ct.c_int32)]
+    I32 = ct.POINTER(ct.c_int32)
+    lib.zsme_adjoint.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, I32, I32, I32, P, P, P, P, P, P]
     _lib = lib
     return lib
 

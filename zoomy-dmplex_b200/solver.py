@@ -134,6 +134,37 @@ class Solver:
             native.check(self.lib.zsme_sync(self.h))
         return d
 
+    def adjoint(self, nsteps: int, obs_step, obs_cell, obs_comp, obs_target, obs_weight=None,
+                checkpoint_every: int = 20):
+        """Discrete adjoint of ``nsteps`` steps from the current state.
+
+        Loss = sum_j w_j (Q_{obs_step[j]}[obs_cell[j], obs_comp[j]] - obs_target[j])^2
+        with Q_k the state after k steps (caller cell order).  Returns
+        ``(loss, grad_q [n_cells, n_dof_q], grad_params [n_parameters], dts
+        [nsteps])``: the gradients with respect to the current state (column 0
+        is the bathymetry) and the parameters, at the dt sequence of the
+        forward run (``dts``), which the derivative holds fixed.  Afterwards
+        the solver holds the state after ``nsteps`` steps.  Checkpoints every
+        ``checkpoint_every`` steps; the reverse pass recomputes in between."""
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        st, ce, co, tg = i32(obs_step), i32(obs_cell), i32(obs_comp), f64(obs_target)
+        n = st.size
+        if not (ce.size == co.size == tg.size == n):
+            raise ValueError("observation arrays differ in length")
+        wt = None if obs_weight is None else f64(obs_weight)
+        if wt is not None and wt.size != n:
+            raise ValueError("observation weights differ in length")
+        ip = lambda a: a.ctypes.data_as(ct.POINTER(ct.c_int32))
+        loss = np.zeros(1)
+        gq = np.zeros((self.mesh.n_cells, self.nq))
+        gp = np.zeros(self.info["n_parameters"])
+        dts = np.zeros(max(1, int(nsteps)))
+        native.check(self.lib.zsme_adjoint(self.h, int(nsteps), int(checkpoint_every), n, ip(st), ip(ce), ip(co),
+                                           _p(tg), _p(wt) if wt is not None else None, _p(loss), _p(gq), _p(gp),
+                                           _p(dts)))
+        return float(loss[0]), gq, gp, dts[:int(nsteps)]
+
     def time(self):
         t, d = ct.c_double(), ct.c_double()
         native.check(self.lib.zsme_get_time(self.h, ct.byref(t), ct.byref(d)))
@@ -257,19 +288,19 @@ class BatchSolver:
         return n.value
 
 
-LAUNCH_KEYS = ("prep", "face", "gather", "finalize", "prep_occ", "face_occ")
+LAUNCH_KEYS = ("prep", "face", "gather", "finalize", "prep_occ", "face_occ", "finalize_occ")
 
 
 def set_launch(h, cfg):
     """Launch configuration of a handle: dict with LAUNCH_KEYS (threads per
     block of each kernel, register caps as blocks per SM)."""
     lib = native.load()
-    b = (ct.c_int32 * 6)(*[int(cfg[k]) for k in LAUNCH_KEYS])
+    b = (ct.c_int32 * len(LAUNCH_KEYS))(*[int(cfg.get(k, 1 if k.endswith("_occ") else 128)) for k in LAUNCH_KEYS])
     native.check(lib.zsme_set_launch(h, b))
 
 
 def get_launch(h):
     lib = native.load()
-    b = (ct.c_int32 * 6)()
+    b = (ct.c_int32 * len(LAUNCH_KEYS))()
     native.check(lib.zsme_get_launch(h, b))
     return dict(zip(LAUNCH_KEYS, [int(x) for x in b]))
