@@ -52,10 +52,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch configuration")
-    ap.add_argument("--workload", choices=["roofline", "ensemble"], default="roofline")
+    ap.add_argument("--workload", choices=["roofline", "ensemble", "adjoint"], default="roofline")
     ap.add_argument("--launch", default="", help="launch configuration as JSON (keys of solver.LAUNCH_KEYS); "
                     "skips the autotuner")
     ap.add_argument("--instances", type=int, default=512, help="ensemble size per GPU (--workload ensemble)")
+    ap.add_argument("--adj-side", type=int, default=200, help="grid side of the adjoint workload")
+    ap.add_argument("--adj-steps", type=int, default=400, help="steps of the adjoint workload")
+    ap.add_argument("--adj-limiter", default="tvd", choices=["tvd", "none"], help="limiter of the adjoint workload")
     return ap.parse_args()
 
 
@@ -338,6 +341,136 @@ def run_ensemble(a, dev, torch, dist, rank, world):
     return 0
 
 
+def run_adjoint(a, dev, torch, dist, rank, world):
+    """SME level 1 on the 200x200 jittered grid, 400 steps; misfit of the depth
+    at 64 seeded gauge cells every 10th step against a run whose bathymetry
+    is raised by 0.02 exp(-|x - (0.6, 0.4)|^2 / 0.01); gradients with respect
+    to the per-cell bathymetry and the Manning coefficient, checkpoints every
+    20 steps.  Times the forward run and the adjoint call, and checks the
+    gradient against central differences (eps = 1e-6) of the forward run at the
+    recorded dts along 32 seeded smooth directions and the Manning direction.
+    Each rank runs its own replica."""
+    from zoomy_dmplex_b200 import adjoint as adj
+    from zoomy_dmplex_b200 import cases, models
+    from zoomy_dmplex_b200.solver import Solver
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    side, N, every, ngauge = a.adj_side, a.adj_steps, 20, 64
+    c = cases.adjoint_l1(side)
+    tgt = cases.adjoint_l1(side, target=True)
+    c.settings.limiter = tgt.settings.limiter = a.adj_limiter
+    p = params_of(c)
+    names, _ = models.parameter_table(c.model)
+    C, F = c.mesh.n_cells, c.mesh.n_faces
+    g = Solver(c.model, c.mesh, c.settings, p, device=dev)
+    cells = adj.gauges(C, ngauge, seed=0)
+    steps = list(range(10, N + 1, 10))
+    targets = adj.observe_run(g, tgt.q0, N, steps, cells)
+    obs = adj.depth_observations(cells, steps, targets)
+    stream = torch.cuda.ExternalStream(g.stream, device=dev)
+    # warm-up: forward graph, one adjoint call (allocations)
+    g.set_state(c.q0)
+    g.step(max(1, a.warmup))
+    g.set_state(c.q0)
+    g.adjoint(N, *obs, checkpoint_every=every)
+    # forward: N steps on the graph path
+    g.set_state(c.q0)
+    clk = ClockSampler(dev)
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.step(N)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    # the adjoint call (it synchronises): host wall clock
+    g.set_state(c.q0)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    loss, gq, gp, dts = g.adjoint(N, *obs, checkpoint_every=every)
+    adj_s = time.perf_counter() - w0
+    phases = g.adjoint_phases()
+    # end to end: initial state from the host, adjoint, gradients back
+    w0 = time.perf_counter()
+    g.set_state(c.q0)
+    g.adjoint(N, *obs, checkpoint_every=every)
+    e2e_s = time.perf_counter() - w0
+    clocks = clk.stop()
+    barrier()
+
+    # central differences of the forward run at the recorded dts
+    def misfit(q0, pp):
+        g.set_params(pp)
+        v = adj.observe_run(g, q0, N, steps, cells, dts=dts)
+        return float(np.sum((v - targets) ** 2))
+
+    rng = np.random.default_rng(2024)
+    eps = 1e-6
+    errs, pairs = [], []
+    for _ in range(32):
+        dq = np.zeros_like(c.q0)
+        dq[:, 0] = adj.smooth_direction(c.mesh, rng) * 1e-2
+        fd = (misfit(c.q0 + eps * dq, p) - misfit(c.q0 - eps * dq, p)) / (2 * eps)
+        ad = float(np.sum(gq * dq))
+        errs.append(abs(ad - fd) / max(abs(fd), 1e-300))
+        pairs.append((ad, fd))
+    ni = names.index("n_manning")
+    dp = np.zeros_like(p)
+    dp[ni] = 1.0
+    fd_n = (misfit(c.q0, p + eps * dp) - misfit(c.q0, p - eps * dp)) / (2 * eps)
+    g.set_params(p)
+    man_err = abs(gp[ni] - fd_n) / max(abs(fd_n), 1e-300)
+
+    t = torch.tensor([fwd_ms, adj_s, e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    fwd_ms, adj_s, e2e_s = (float(x) for x in t.tolist())
+    s = c.settings.ssp_stages
+    lps = g.launches_per_step()
+    rev_launches = 3 + s * 4 + (s - 1) + 1     # finalize, reduce, seeds; per stage prep/face/cell/combine; clamps; axpby
+    nv = C * g.nq * 8
+    line = {"metric": METRIC, "value": C * N * world / adj_s, "unit": UNIT, "n_gpus": world, "steps": N,
+            "warmup": a.warmup, "ms_per_step": 1e3 * adj_s / N, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "discrete adjoint of SME level 1 on the jittered-Delaunay %dx%d grid (%d cells, "
+                                   "%d faces), %d steps, depth misfit at %d gauge cells every 10th step, gradients "
+                                   "w.r.t. per-cell b and Manning n, checkpoints every %d steps, order 2 Green-Gauss "
+                                   "+ limiter %s, SSP-RK2, CFL 0.45" % (side, side, C, F, N, ngauge, every,
+                                                                        "Vacuum/TVD" if a.adj_limiter == "tvd" else
+                                                                        "none"),
+                       "model": c.model, "cells": C, "faces": F, "parallelism": "replicas x%d" % world if world > 1
+                       else "single GPU",
+                       "l2_flush": "not needed for the ratio: both runs see the same cache state",
+                       "timing": "forward: CUDA events around N graph-launched steps; adjoint: host wall clock "
+                                 "around the (synchronising) zsme_adjoint call, forward pass with checkpoints, "
+                                 "segment replays and reverse sweep included"},
+            "adjoint": {"forward_ms_per_step": fwd_ms / N, "adjoint_call_ms_per_step": 1e3 * adj_s / N,
+                        "adjoint_call_over_forward": 1e3 * adj_s / fwd_ms,
+                        "phases_ms_per_step": {k: v / N for k, v in phases.items()},
+                        "reverse_step_over_forward_step": phases["reverse"] / fwd_ms,
+                        "replay_plus_reverse_over_forward": (phases["replay"] + phases["reverse"]) / fwd_ms,
+                        "loss": loss, "grad_n_manning": float(gp[ni]), "grad_b_norm": float(np.linalg.norm(gq[:, 0])),
+                        "fd": {"directions": len(errs), "eps": eps, "kind": "smooth random b directions",
+                               "max_rel_err": float(max(errs)), "median_rel_err": float(np.median(errs)),
+                               "manning_rel_err": float(man_err), "first_pairs_adjoint_fd": pairs[:4],
+                               "manning_adjoint_fd": [float(gp[ni]), fd_n]}},
+            "e2e": {"value": C * N * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nv / N,
+                    "d2h_bytes_per_step": nv / N,
+                    "api": "zsme_set_state(host) + zsme_adjoint (host observations in, host gradients out)"},
+            "gpu_launches": N * (2 * lps + rev_launches) + 2 * len(steps) + 1,
+            "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -380,6 +513,8 @@ def main():
 
     if a.workload == "ensemble":
         return run_ensemble(a, dev, torch, dist, rank, world)
+    if a.workload == "adjoint":
+        return run_adjoint(a, dev, torch, dist, rank, world)
 
     case = cases.roofline_l4(a.side)
     C, F = case.mesh.n_cells, case.mesh.n_faces

@@ -207,6 +207,10 @@ int zsme_adjoint(zsme_handle* h, int32_t nsteps, int32_t checkpoint_every, int32
                  const int32_t* obs_step, const int32_t* obs_cell, const int32_t* obs_comp,
                  const double* obs_target, const double* obs_weight, double* loss, double* grad_q_aos,
                  double* grad_params, double* dts);
+/* Device time (ms) of the last zsme_adjoint call's three phases: the
+ * forward run with checkpoints, the segment replays into the tape, and the
+ * reverse sweep.  No counterpart in the reference. */
+int zsme_adjoint_phases(zsme_handle* h, double* ms3);
 
 /* CFL time step of a caller-owned state with no device allocation.
  * No counterpart in the reference, which has no GPU path.  It serves callers

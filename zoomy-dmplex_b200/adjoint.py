@@ -62,3 +62,33 @@ def depth_observations(cells, steps, targets):
     ce = np.tile(cells, steps.size)
     co = np.ones_like(ce)
     return st, ce, co, np.asarray(targets, dtype=np.float64).reshape(-1)
+
+
+def observe_run(solver, q0, nsteps: int, steps, cells, comp: int = 1, dts=None) -> np.ndarray:
+    """Values of component ``comp`` at ``cells`` after each of ``steps`` in a
+    plain run of ``solver`` from ``q0`` (CFL dts, or the given ``dts``):
+    targets for ``depth_observations``, or the misfit of a perturbed run."""
+    steps = sorted(int(s) for s in steps)
+    cells = np.asarray(cells)
+    solver.set_state(q0)
+    out = []
+    k = 0
+    for s in steps:
+        if s > k:
+            solver.step(s - k, None if dts is None else dts[k:s])
+            k = s
+        out.append(solver.get_state()[cells, comp])
+    return np.array(out)
+
+
+def smooth_direction(mesh, rng, bumps: int = 6) -> np.ndarray:
+    """A seeded random smooth per-cell field (a sum of Gaussians with random
+    centres, widths and signs): a direction along which the discrete step is
+    smooth on the scale of a finite-difference check."""
+    x, y = mesh.cell_centroid[:, 0], mesh.cell_centroid[:, 1]
+    d = np.zeros_like(x)
+    for _ in range(bumps):
+        cx, cy = rng.uniform(0, 1, 2)
+        w = rng.uniform(0.02, 0.1)
+        d += rng.standard_normal() * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / w)
+    return d

@@ -82,6 +82,8 @@ class SolverBase {
     // gradient with respect to the parameters, and the dt of every step
     virtual int adjoint(const AdjointSpec& spec, double* loss, double* grad_q, double* grad_params,
                         double* dts) = 0;
+    // device times of the last adjoint call's forward pass, replays and reverse sweep (ms)
+    virtual int adjoint_phases(double* ms) = 0;
 };
 
 }  // namespace zsme

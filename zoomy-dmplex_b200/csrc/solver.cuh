@@ -79,6 +79,7 @@ class Solver final : public SolverBase {
     DevBuf<double> adj_ck_x_, adj_ck_a_, adj_tape_, adj_lam0_, adj_lam1_, adj_lam2_, adj_own_w_, adj_own_wl_;
     DevBuf<double> adj_out_w_, adj_out_wl_, adj_gfs_, adj_lp_cell_, adj_lp_, adj_wl_, adj_oval_, adj_oseed_, adj_dts_;
     DevBuf<int> adj_ocell_, adj_ocomp_;
+    double adj_phase_ms_[3] = {0, 0, 0};  // last zsme_adjoint: forward pass, replays, reverse sweep
     MeshDev md_{};
     Opts opts_{};
     // per-kernel CUDA-event timing (zsme_set_profiling)
@@ -545,6 +546,10 @@ class Solver final : public SolverBase {
         return cur;
     }
 
+    int adjoint_phases(double* ms) override {
+        for (int i = 0; i < 3; ++i) ms[i] = adj_phase_ms_[i];
+        return ZSME_OK;
+    }
     int adjoint(const AdjointSpec& A, double* loss, double* grad_q, double* grad_p, double* dts_out) override {
         if (n_inst_ != 1) return set_error(ZSME_ERR_ARG, "the adjoint needs a single-instance handle");
         if (A.nsteps < 0 || A.every < 1 || A.nobs < 0)
@@ -606,10 +611,17 @@ class Solver final : public SolverBase {
             cudaMemcpyAsync(aux_.p, adj_ck_a_.p + (size_t)slot * na, na * sizeof(double), cudaMemcpyDeviceToDevice,
                             stream_);
         };
+        cudaEvent_t ev[4];
+        for (auto& e : ev) ZSME_CUDA(cudaEventCreate(&e));
+        struct EvGuard {
+            cudaEvent_t* e;
+            ~EvGuard() { for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]); }
+        } ev_guard{ev};
         // ---- forward: CFL steps, checkpoints, observed values, dt record
         double t0 = 0.0;
         ZSME_CUDA(cudaMemcpyAsync(&t0, t_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
+        ZSME_CUDA(cudaEventRecord(ev[0], stream_));
         save(0);
         for (int n = 0; n < NS; ++n) {
             obs_values(n);
@@ -620,6 +632,7 @@ class Solver final : public SolverBase {
         }
         obs_values(NS);
         save(nseg);  // the final state, restored at the end
+        ZSME_CUDA(cudaEventRecord(ev[1], stream_));
         double t_fin = 0.0, dtc_fin = 0.0;
         std::vector<double> dth(std::max(1, NS)), oval(std::max(1, A.nobs));
         ZSME_CUDA(cudaMemcpyAsync(&t_fin, t_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -628,6 +641,11 @@ class Solver final : public SolverBase {
         ZSME_CUDA(cudaMemcpyAsync(oval.data(), adj_oval_.p, oval.size() * sizeof(double), cudaMemcpyDeviceToHost,
                                   stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
+        {
+            float a0 = 0.f;
+            ZSME_CUDA(cudaEventElapsedTime(&a0, ev[0], ev[1]));
+            adj_phase_ms_[0] = a0;
+        }
         std::vector<double> th(NS + 1);
         th[0] = t0;
         for (int n = 0; n < NS; ++n) th[n + 1] = th[n] + dth[n];
@@ -657,8 +675,10 @@ class Solver final : public SolverBase {
                                                       adj_oseed_.p + first[n], C, l);
         };
         seeds(NS, lam);
+        float replay_ms = 0.f, reverse_ms = 0.f;
         for (int seg = nseg - 1; seg >= 0; --seg) {
             const int n0 = seg * A.every, n1 = std::min(NS, n0 + A.every);
+            ZSME_CUDA(cudaEventRecord(ev[2], stream_));
             restore(seg);
             ZSME_CUDA(cudaMemcpyAsync(t_.p, &th[n0], sizeof(double), cudaMemcpyHostToDevice, stream_));
             for (int n = n0; n < n1; ++n) {  // replay with the recorded dts, into the tape
@@ -667,6 +687,7 @@ class Solver final : public SolverBase {
                 ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));
                 enqueue_step(adj_dts_.p + n, x_.p, tp);
             }
+            ZSME_CUDA(cudaEventRecord(ev[3], stream_));
             for (int n = n1 - 1; n >= n0; --n) {
                 const double* tp = adj_tape_.p + (size_t)(n - n0) * (s + 1) * nv;
                 double* t1 = lam == adj_lam0_.p ? adj_lam1_.p : adj_lam0_.p;
@@ -676,7 +697,16 @@ class Solver final : public SolverBase {
                 seeds(n, lam);
             }
             ZSME_CUDA(cudaGetLastError());
+            ZSME_CUDA(cudaEventRecord(ev[1], stream_));
+            ZSME_CUDA(cudaEventSynchronize(ev[1]));
+            float a1 = 0.f, a2 = 0.f;
+            ZSME_CUDA(cudaEventElapsedTime(&a1, ev[2], ev[3]));
+            ZSME_CUDA(cudaEventElapsedTime(&a2, ev[3], ev[1]));
+            replay_ms += a1;
+            reverse_ms += a2;
         }
+        adj_phase_ms_[1] = replay_ms;
+        adj_phase_ms_[2] = reverse_ms;
         // ---- outputs; the handle keeps the final state of the forward run
         if (grad_q) {
             int rc = get_soa(0, lam, NQ, grad_q, false);

@@ -277,6 +277,11 @@ int zsme_adjoint(zsme_handle* h, int32_t nsteps, int32_t checkpoint_every, int32
     a.obs_weight = obs_weight;
     return h->s->adjoint(a, loss, grad_q_aos, grad_params, dts);
 }
+int zsme_adjoint_phases(zsme_handle* h, double* ms3) {
+    CHECK_SINGLE(h);
+    if (!ms3) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->adjoint_phases(ms3);
+}
 int zsme_get_launch(zsme_handle* h, int32_t* blocks) {
     CHECK_H(h);
     if (!blocks) return set_error(ZSME_ERR_ARG, "null output");

@@ -111,6 +111,7 @@ def load():
     lib.zsme_get_launch.argtypes = [vp, ct.POINTER(ct.c_int32)]
     I32 = ct.POINTER(ct.c_int32)
     lib.zsme_adjoint.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, I32, I32, I32, P, P, P, P, P, P]
+    lib.zsme_adjoint_phases.argtypes = [vp, P]
     _lib = lib
     return lib
 

@@ -165,6 +165,12 @@ class Solver:
                                            _p(dts)))
         return float(loss[0]), gq, gp, dts[:int(nsteps)]
 
+    def adjoint_phases(self):
+        """Device ms of the last adjoint call: forward pass, replays, reverse sweep."""
+        ms = np.zeros(3)
+        native.check(self.lib.zsme_adjoint_phases(self.h, _p(ms)))
+        return {"forward": float(ms[0]), "replay": float(ms[1]), "reverse": float(ms[2])}
+
     def time(self):
         t, d = ct.c_double(), ct.c_double()
         native.check(self.lib.zsme_get_time(self.h, ct.byref(t), ct.byref(d)))
