@@ -10,9 +10,9 @@
 //
 // R'(W)^T v is applied by four kernels (after prep_kernel has recomputed the
 // face states of W):
-//   adj_face_kernel    per face: the face states' adjoints g_f from the cells'
-//                      mu = v / V through the flux Jacobians (dual numbers,
-//                      one pass per face side);
+//   adj_face_kernel    per face side: the face state's adjoint g_f from the
+//                      cells' mu = v / V through the flux and fluctuation
+//                      Jacobians (dual numbers);
 //   adj_cell_kernel    per cell: replays the forward reconstruction and its
 //                      limiter branches (alpha_f, and for a ratio branch the
 //                      component and the neighbour that bounded it) and maps g_f
@@ -68,29 +68,38 @@ __device__ __forceinline__ void clamp_adjoint(const double* q, const double* a, 
 }
 
 // ---------------------------------------------------------------- faces
-// gfs[side][NQ][F] = adjoint of face state `side` (0: support[0], 1:
-// support[1]) given the cells' adjoint v of R scaled by `scale`.  t: stage
-// time (time-dependent boundary conditions only).
+// gfs[side][NQ][F]: the adjoint of face state `side` (0: support[0], 1:
+// support[1]), given the cells' adjoint v of R scaled by factor * dt, dt =
+// *dtp; stage time *tp + frac * dt (time-dependent boundary conditions only).
 template <template <typename> class MT, template <typename> class NT>
 __global__ void __launch_bounds__(128) adj_face_kernel(MeshDev m, const double* __restrict__ fs,
                                                        const double* __restrict__ aux,
-                                                       const double* __restrict__ params, double t,
-                                                       const double* __restrict__ v, double scale,
-                                                       double* __restrict__ gfs) {
+                                                       const double* __restrict__ params, const double* tp,
+                                                       double frac, const double* dtp, double factor,
+                                                       const double* __restrict__ v, double* __restrict__ gfs) {
     using M = MT<double>;
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, NP = M::n_parameters;
+    // One thread per (face, side), differentiating the numerical flux and the
+    // fluctuations together (they share the hydrostatic reconstruction) in all
+    // NQ directions of its side's face state.
     using D = Dual<NQ>;
     const int F = m.F, C = m.C;
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= F) return;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long long)F * 2) return;
+    const int f = (int)(tid >> 1);
+    const int side = (int)(tid & 1);
     const int R = m.face_R[f], bc = m.face_bc[f], L = m.face_L[f];
+    if (R < 0 && side == 1) return;  // a boundary face has one face state
     if (R < 0 && bc < 0) {  // no flux through this face
 #pragma unroll
-        for (int i = 0; i < NQ; ++i) gfs[(size_t)i * F + f] = 0.0;
+        for (int j = 0; j < NQ; ++j) gfs[(size_t)j * F + f] = 0.0;
         return;
     }
     const double* p = params + (size_t)face_instance(m, f) * m.np;
     const double area = m.farea[f];
+    const double dt = *dtp;
+    const double t = *tp + frac * dt;
+    const double scale = factor * dt;
     D pd[NP], nh[3], xf[3];
 #pragma unroll
     for (int k = 0; k < NP; ++k) pd[k] = D(p[k]);
@@ -118,69 +127,70 @@ __global__ void __launch_bounds__(128) adj_face_kernel(MeshDev m, const double* 
             }
         }
     }
-    const int sides = R >= 0 ? 2 : 1;
-    for (int side = 0; side < sides; ++side) {
-        D qL[NQ], aLc[NA], aL[NA];
-#pragma unroll
-        for (int i = 0; i < NQ; ++i) {
-            qL[i] = D(fs[(size_t)i * F + f]);
-            if (side == 0) qL[i].d[i] = 1.0;
-        }
-#pragma unroll
-        for (int i = 0; i < NA; ++i) aLc[i] = D(aux[(size_t)i * C + L]);
-        double g[NQ];
-        if (R >= 0) {
-            D qR[NQ], aRc[NA], aR[NA];
+    {
+        {
+            D qL[NQ], aLc[NA], aL[NA];
 #pragma unroll
             for (int i = 0; i < NQ; ++i) {
-                qR[i] = D(fs[((size_t)NQ + i) * F + f]);
-                if (side == 1) qR[i].d[i] = 1.0;
+                qL[i] = D(fs[(size_t)i * F + f]);
+                if (side == 0) qL[i].d[i] = 1.0;
             }
 #pragma unroll
-            for (int i = 0; i < NA; ++i) aRc[i] = D(aux[(size_t)i * C + R]);
-            {
-                const auto ra = MT<D>::update_aux_variables(qL, aLc, pd, D(0.0), xf);
-                const auto rb = MT<D>::update_aux_variables(qR, aRc, pd, D(0.0), xf);
+            for (int i = 0; i < NA; ++i) aLc[i] = D(aux[(size_t)i * C + L]);
+            double g[NQ];
+            if (R >= 0) {
+                D qR[NQ], aRc[NA], aR[NA];
 #pragma unroll
-                for (int i = 0; i < NA; ++i) { aL[i] = ra[i]; aR[i] = rb[i]; }
+                for (int i = 0; i < NQ; ++i) {
+                    qR[i] = D(fs[((size_t)NQ + i) * F + f]);
+                    if (side == 1) qR[i].d[i] = 1.0;
+                }
+#pragma unroll
+                for (int i = 0; i < NA; ++i) aRc[i] = D(aux[(size_t)i * C + R]);
+                {
+                    const auto ra = MT<D>::update_aux_variables(qL, aLc, pd, D(0.0), xf);
+                    const auto rb = MT<D>::update_aux_variables(qR, aRc, pd, D(0.0), xf);
+#pragma unroll
+                    for (int i = 0; i < NA; ++i) { aL[i] = ra[i]; aR[i] = rb[i]; }
+                }
+                // cell L gets -(nc_L + F) A, cell R gets (F - nc_R) A
+                const auto flux = NT<D>::numerical_flux(qL, qR, aL, aR, pd, nh);
+                const auto nc = NT<D>::numerical_fluctuations(qL, qR, aL, aR, pd, nh);
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    double sum = 0.0;
+#pragma unroll
+                    for (int i = 0; i < NQ; ++i)
+                        sum += (muR[i] - muL[i]) * area * flux[i].d[j] -
+                               area * (muL[i] * nc[NQ + i].d[j] + muR[i] * nc[i].d[j]);
+                    g[j] = sum;
+                }
+            } else {
+                {
+                    const auto ra = MT<D>::update_aux_variables(qL, aLc, pd, D(t), xf);
+#pragma unroll
+                    for (int i = 0; i < NA; ++i) aL[i] = ra[i];
+                }
+                const auto qR = MT<D>::boundary_conditions(bc, qL, aL, pd, nh, xf, D(t), D(0.0));
+                D aR[NA];
+                {
+                    const auto rb = MT<D>::update_aux_variables(qR.data, aL, pd, D(t), xf);
+#pragma unroll
+                    for (int i = 0; i < NA; ++i) aR[i] = rb[i];
+                }
+                const auto flux = NT<D>::numerical_flux(qL, qR.data, aL, aR, pd, nh);
+                const auto nc = NT<D>::numerical_fluctuations(qL, qR.data, aL, aR, pd, nh);
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    double sum = 0.0;
+#pragma unroll
+                    for (int i = 0; i < NQ; ++i) sum -= muL[i] * area * (nc[NQ + i].d[j] + flux[i].d[j]);
+                    g[j] = sum;
+                }
             }
-            const auto flux = NT<D>::numerical_flux(qL, qR, aL, aR, pd, nh);
-            const auto nc = NT<D>::numerical_fluctuations(qL, qR, aL, aR, pd, nh);
-            // cell L gets -(nc_L + F) A, cell R gets (F - nc_R) A
 #pragma unroll
-            for (int j = 0; j < NQ; ++j) {
-                double s = 0.0;
-#pragma unroll
-                for (int i = 0; i < NQ; ++i)
-                    s += muL[i] * (-area) * (nc[NQ + i].d[j] + flux[i].d[j]) +
-                         muR[i] * area * (flux[i].d[j] - nc[i].d[j]);
-                g[j] = s;
-            }
-        } else {
-            {
-                const auto ra = MT<D>::update_aux_variables(qL, aLc, pd, D(t), xf);
-#pragma unroll
-                for (int i = 0; i < NA; ++i) aL[i] = ra[i];
-            }
-            const auto qR = MT<D>::boundary_conditions(bc, qL, aL, pd, nh, xf, D(t), D(0.0));
-            D aR[NA];
-            {
-                const auto rb = MT<D>::update_aux_variables(qR.data, aL, pd, D(t), xf);
-#pragma unroll
-                for (int i = 0; i < NA; ++i) aR[i] = rb[i];
-            }
-            const auto flux = NT<D>::numerical_flux(qL, qR.data, aL, aR, pd, nh);
-            const auto nc = NT<D>::numerical_fluctuations(qL, qR.data, aL, aR, pd, nh);
-#pragma unroll
-            for (int j = 0; j < NQ; ++j) {
-                double s = 0.0;
-#pragma unroll
-                for (int i = 0; i < NQ; ++i) s += muL[i] * (-area) * (nc[NQ + i].d[j] + flux[i].d[j]);
-                g[j] = s;
-            }
+            for (int j = 0; j < NQ; ++j) gfs[((size_t)side * NQ + j) * F + f] = g[j];
         }
-#pragma unroll
-        for (int j = 0; j < NQ; ++j) gfs[((size_t)side * NQ + j) * F + f] = g[j];
     }
 }
 
@@ -233,7 +243,8 @@ __global__ void __launch_bounds__(128) adj_cell_kernel(MeshDev m, Opts o, const 
         for (int k = 0; k < KM; ++k) {
             if (ff[k] < 0) continue;
 #pragma unroll
-            for (int i = 0; i < NQ; ++i) owl[i] += gfs[((size_t)sd[k] * NQ + i) * F + ff[k]];
+            for (int i = 0; i < NQ; ++i)
+                owl[i] += gfs[((size_t)sd[k] * NQ + i) * F + ff[k]];
         }
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
@@ -520,19 +531,18 @@ __global__ void __launch_bounds__(128) adj_combine_kernel(MeshDev m, const doubl
 
 // --------------------------------------------------------------- finalize
 // lam_in = adjoint of the stage output X' given lam_out, the adjoint of the
-// step's result; lp_cell[NP][C] = this step's parameter adjoint per cell.
+// step's result; lp_part[NP][gridDim.x] = this step's parameter adjoint summed
+// over each block's cells (blockDim.x = 128, fixed-order tree).
+// One cell of adj_finalize_kernel; lp[k * lp_stride] receives the cell's
+// parameter adjoint k.
 template <template <typename> class MT>
-__global__ void __launch_bounds__(128) adj_finalize_kernel(MeshDev m, const double* __restrict__ xp,
-                                                           const double* __restrict__ aux,
-                                                           const double* __restrict__ params, double dt, int flags,
-                                                           const double* __restrict__ lam_out,
-                                                           double* __restrict__ lam_in,
-                                                           double* __restrict__ lp_cell) {
+__device__ __forceinline__ void adj_finalize_cell(const MeshDev& m, int c, const double* __restrict__ xp,
+                                                  const double* __restrict__ aux, const double* __restrict__ params,
+                                                  double dt, int flags, const double* __restrict__ lam_out,
+                                                  double* __restrict__ lam_in, double* lp, int lp_stride) {
     using M = MT<double>;
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, NP = M::n_parameters;
     const int C = m.C;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C) return;
     const double* p = params + (size_t)cell_instance(m, c) * m.np;
     // forward replay: q0 -(pre)-> q1 -(newton)-> q2 -(pre)-> q3 -(post)-> out
     double q0[NQ], a0[NA], q2[NQ], a2[NA], q3[NQ], a3[NA];
@@ -559,8 +569,6 @@ __global__ void __launch_bounds__(128) adj_finalize_kernel(MeshDev m, const doub
 #pragma unroll
         for (int i = 0; i < NQ; ++i) lam[i] = tmp[i];
     }
-#pragma unroll
-    for (int k = 0; k < NP; ++k) lp_cell[(size_t)k * C + c] = 0.0;
     if (flags & FIN_SOURCE) {
         if (flags & FIN_PRE) {
             clamp_adjoint<MT>(q2, a2, p, lam, tmp);
@@ -599,7 +607,7 @@ __global__ void __launch_bounds__(128) adj_finalize_kernel(MeshDev m, const doub
                     double s = 0.0;
 #pragma unroll
                     for (int i = 0; i < NQ; ++i) s += mu[i] * dt * S[i].d[NQ + k];
-                    lp_cell[(size_t)k * C + c] = s;
+                    lp[k * lp_stride] = s;
                 }
 #pragma unroll
                 for (int i = 0; i < NQ; ++i) lam[i] = mu[i];
@@ -615,15 +623,50 @@ __global__ void __launch_bounds__(128) adj_finalize_kernel(MeshDev m, const doub
     for (int i = 0; i < NQ; ++i) lam_in[(size_t)i * C + c] = lam[i];
 }
 
+template <template <typename> class MT>
+__global__ void __launch_bounds__(128) adj_finalize_kernel(MeshDev m, const double* __restrict__ xp,
+                                                           const double* __restrict__ aux,
+                                                           const double* __restrict__ params, const double* dtp,
+                                                           int flags, const double* __restrict__ lam_out,
+                                                           double* __restrict__ lam_in,
+                                                           double* __restrict__ lp_part) {
+    using M = MT<double>;
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, NP = M::n_parameters;
+    const int C = m.C;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double lp_sh[NP][128];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) lp_sh[k][threadIdx.x] = 0.0;
+    const double dt = *dtp;
+    if (c < C) {
+        if (dt > 0.0) {
+            adj_finalize_cell<MT>(m, c, xp, aux, params, dt, flags, lam_out, lam_in, &lp_sh[0][0] + threadIdx.x, 128);
+        } else {  // a step after t_end changed nothing
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) lam_in[(size_t)i * C + c] = lam_out[(size_t)i * C + c];
+        }
+    }
+    __syncthreads();
+    for (int h = 64; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h)
+#pragma unroll
+            for (int k = 0; k < NP; ++k) lp_sh[k][threadIdx.x] += lp_sh[k][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NP; ++k) lp_part[(size_t)k * gridDim.x + blockIdx.x] = lp_sh[k][0];
+}
+
 // ------------------------------------------------------------- small ones
-// lp_total[k] += sum over cells of lp_cell[k][.] (one block per parameter,
-// fixed order: deterministic)
-static __global__ void __launch_bounds__(256) adj_param_reduce_kernel(const double* __restrict__ lp_cell, int C,
+// lp_total[k] += sum of the nb block partials lp_part[k][.] (one block per
+// parameter, fixed order: deterministic)
+static __global__ void __launch_bounds__(256) adj_param_reduce_kernel(const double* __restrict__ lp_part, int nb,
                                                                       double* __restrict__ lp_total) {
     __shared__ double sh[256];
     const int k = blockIdx.x;
     double s = 0.0;
-    for (int c = threadIdx.x; c < C; c += blockDim.x) s += lp_cell[(size_t)k * C + c];
+    for (int c = threadIdx.x; c < nb; c += blockDim.x) s += lp_part[(size_t)k * nb + c];
     sh[threadIdx.x] = s;
     __syncthreads();
     for (int h = blockDim.x / 2; h > 0; h >>= 1) {
@@ -645,6 +688,15 @@ static __global__ void adj_seed_kernel(int n, const int* __restrict__ cell, cons
                                        const double* __restrict__ seed, int C, double* __restrict__ lam) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     for (int j = 0; j < n; ++j) lam[(size_t)comp[j] * C + cell[j]] += seed[j];
+}
+
+// the seeds of the observations of step *n0 + k (first: per-step CSR offsets)
+static __global__ void adj_seed_seg_kernel(const int* __restrict__ first, const int* __restrict__ n0, int k,
+                                           const int* __restrict__ cell, const int* __restrict__ comp,
+                                           const double* __restrict__ seed, int C, double* __restrict__ lam) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int n = *n0 + k;
+    for (int j = first[n]; j < first[n + 1]; ++j) lam[(size_t)comp[j] * C + cell[j]] += seed[j];
 }
 
 // y = a x + b y over n values

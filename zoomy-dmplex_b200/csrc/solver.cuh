@@ -36,6 +36,7 @@ struct DevBuf {
     size_t n = 0;
     ~DevBuf() { if (p) cudaFree(p); }
     cudaError_t alloc(size_t count) {
+        if (p && n == count) return cudaSuccess;  // same size: keep the allocation
         if (p) cudaFree(p);
         p = nullptr;
         n = count;
@@ -78,7 +79,9 @@ class Solver final : public SolverBase {
     // discrete adjoint (allocated by the first zsme_adjoint call)
     DevBuf<double> adj_ck_x_, adj_ck_a_, adj_tape_, adj_lam0_, adj_lam1_, adj_lam2_, adj_own_w_, adj_own_wl_;
     DevBuf<double> adj_out_w_, adj_out_wl_, adj_gfs_, adj_lp_cell_, adj_lp_, adj_wl_, adj_oval_, adj_oseed_, adj_dts_;
-    DevBuf<int> adj_ocell_, adj_ocomp_;
+    DevBuf<int> adj_ocell_, adj_ocomp_, adj_first_, adj_segn0_all_, adj_seg_n0_;
+    DevBuf<double> adj_th_, adj_seg_dt_, adj_seg_t_;
+    size_t adj_tstride_ = 0;
     double adj_phase_ms_[3] = {0, 0, 0};  // last zsme_adjoint: forward pass, replays, reverse sweep
     MeshDev md_{};
     Opts opts_{};
@@ -408,9 +411,17 @@ class Solver final : public SolverBase {
     // One time step of every instance (MUSCLSolver.hpp:140-188).
     // wl0: clamped copy of x_ for the first stage (x_ itself when x_ is constrained).
     // tape (adjoint replay): NQ x C slots receiving each stage state W_1 .. W_{s-1}
-    // and the stage output X' before finalize (tape[0] = W_0 is the caller's copy)
+    // and the stage output X' before finalize (tape[0] = W_0 is the caller's copy),
+    // then 2 NQ x F slots receiving each stage's face states
     void enqueue_step(const double* dts, const double* wl0, double* tape = nullptr) {
         const size_t tape_n = (size_t)NQ * pm_.C;
+        const size_t fs_n = (size_t)2 * NQ * pm_.F;
+        const int ns = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
+        auto tape_fs = [&](int i) {
+            if (tape)
+                cudaMemcpyAsync(tape + (size_t)(ns + 1) * tape_n + (size_t)i * fs_n, fs_.p, fs_n * sizeof(double),
+                                cudaMemcpyDeviceToDevice, stream_);
+        };
         StepDev sd = step_dev(dts);
         const double* t = sd.t;
         const double* dt = sd.dt_step;
@@ -420,6 +431,7 @@ class Solver final : public SolverBase {
         mark(ZSME_KERNEL_BEGIN, false);
         if (st_.reconstruction_order < 2) {
             launch_prep(x_.p, x_.p, act);
+            tape_fs(0);
             launch_flux(MODE_EULER, 0.0, t, 0.0, nullptr, nullptr, x_.p, dt, act);
             if (tape)
                 cudaMemcpyAsync(tape + tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
@@ -429,6 +441,7 @@ class Solver final : public SolverBase {
                 const double frac = i / (s - 1.);
                 // later stages get their clamped copy from gather
                 launch_prep(i == 0 ? x_.p : w_.p, i == 0 ? wl0 : wl_.p, act);
+                tape_fs(i);
                 launch_flux(i == 0 ? MODE_FIRST : MODE_MID, 0.0, t, frac, i == 0 ? x_.p : w_.p, w_.p, nullptr, dt,
                             act, wl_.p);
                 if (tape)
@@ -436,6 +449,7 @@ class Solver final : public SolverBase {
                                     cudaMemcpyDeviceToDevice, stream_);
             }
             launch_prep(w_.p, wl_.p, act);
+            tape_fs(s - 1);
             launch_flux(MODE_FINAL, 0.0, t, 1.0, w_.p, nullptr, x_.p, dt, act);
             if (tape)
                 cudaMemcpyAsync(tape + (size_t)s * tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -491,20 +505,21 @@ class Solver final : public SolverBase {
     }
 
     // ------------------------------------------------------ discrete adjoint
-    // R'(W)^T (scale * src) + c_src * src -> dst, for the stage state W at stage
-    // time t; W0: W is the step's start state (its own clamped copy, as in the
-    // forward stage).
-    void adj_apply_rt(const double* W, bool W0, double t, double scale, const double* src, double c_src,
-                      double* dst) {
+    // R'(W)^T (factor * dt * src) + c_src * src -> dst for the stage state W with
+    // face states fs.  dt = *dtp and the stage time *tp + frac * dt are device
+    // scalars of the step, so that the launches of one checkpoint segment are the
+    // same for every segment and replay as one CUDA graph.  W0: W is the step's
+    // start state (its own clamped copy, as in the forward stage).
+    void adj_apply_rt(const double* W, const double* fs, bool W0, const double* tp, double frac, const double* dtp,
+                      double factor, const double* src, double c_src, double* dst) {
         const int C = pm_.C, F = pm_.F;
         const double* wl = W;
         if (!W0) {
             clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, W, aux_.p, params_.p, adj_wl_.p);
             wl = adj_wl_.p;
         }
-        launch_prep(W, wl, nullptr);
-        adj_face_kernel<MT, NT><<<blocks_for(F, 128), 128, 0, stream_>>>(md_, fs_.p, aux_.p, params_.p, t, src, scale,
-                                                                         adj_gfs_.p);
+        adj_face_kernel<MT, NT><<<blocks_for((long long)F * 2, 128), 128, 0, stream_>>>(
+            md_, fs, aux_.p, params_.p, tp, frac, dtp, factor, src, adj_gfs_.p);
         if (pm_.K == 3)
             adj_cell_kernel<MT, 3><<<blocks_for(C, 128), 128, 0, stream_>>>(
                 md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);
@@ -516,40 +531,62 @@ class Solver final : public SolverBase {
                                                                         src, c_src, dst);
     }
 
-    // lam (adjoint of X_{n+1}) -> adjoint of X_n, from the tape of step n:
-    // tape[i] = W_i (i < s), tape[s] = X'.  Returns the buffer now holding it.
-    double* adj_step(double* lam, double* t1, double* t2, const double* tape, double dt, double tn) {
+    // Reverse of step k of the current segment (tape slot k: W_0 .. W_{s-1}, X',
+    // then each stage's face states): adj_lam0_ holds the adjoint of X_{n+1}
+    // and receives that of X_n, plus the seeds of the observations of X_n.
+    void adj_step(int k) {
         const int C = pm_.C;
-        const size_t nv = (size_t)NQ * C;
-        if (!(dt > 0.0)) return lam;  // inactive step: the identity
+        const size_t nv = (size_t)NQ * C, fs_n = (size_t)2 * NQ * pm_.F;
+        const double* tape = adj_tape_.p + (size_t)k * adj_tstride_;
+        const double* dtp = adj_seg_dt_.p + k;
+        const double* tp = adj_seg_t_.p + k;
+        double *lam = adj_lam0_.p, *t1 = adj_lam1_.p, *t2 = adj_lam2_.p;
         const int flags = FIN_PRE | FIN_POST | (st_.source ? FIN_SOURCE : 0);
         const int s = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
-        adj_finalize_kernel<MT><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, tape + (size_t)s * nv, aux_.p,
-                                                                         params_.p, dt, flags, lam, t1,
-                                                                         adj_lp_cell_.p);
-        adj_param_reduce_kernel<<<NP, 256, 0, stream_>>>(adj_lp_cell_.p, C, adj_lp_.p);
-        // t1 = adjoint of X'
+        const int nb = blocks_for(C, 128);
+        adj_finalize_kernel<MT><<<nb, 128, 0, stream_>>>(md_, tape + (size_t)s * nv, aux_.p, params_.p, dtp, flags,
+                                                         lam, t1, adj_lp_cell_.p);
+        adj_param_reduce_kernel<<<NP, 256, 0, stream_>>>(adj_lp_cell_.p, nb, adj_lp_.p);
+        const double* fst = tape + (size_t)(s + 1) * nv;
         if (st_.reconstruction_order < 2) {  // X' = W0 + dt R(W0)
-            adj_apply_rt(tape, true, tn, dt, t1, 1.0, lam);
-            return lam;
+            adj_apply_rt(tape, fst, true, tp, 0.0, dtp, 1.0, t1, 1.0, lam);
+        } else {
+            // X' = (s-1)/s W_{s-1} + dt/s R(W_{s-1}) + 1/s W_0
+            adj_apply_rt(tape + (size_t)(s - 1) * nv, fst + (size_t)(s - 1) * fs_n, s - 1 == 0, tp, 1.0, dtp,
+                         1.0 / s, t1, (s - 1.) / s, t2);
+            double* cur = t2;
+            double* oth = lam;
+            for (int i = s - 2; i >= 0; --i) {  // W_{i+1} = W_i + dt/(s-1) R(W_i)
+                adj_apply_rt(tape + (size_t)i * nv, fst + (size_t)i * fs_n, i == 0, tp, i / (s - 1.), dtp,
+                             1.0 / (s - 1.), cur, 1.0, oth);
+                std::swap(cur, oth);
+            }
+            axpby_kernel<<<blocks_for((long long)nv, 256), 256, 0, stream_>>>((long long)nv, 1.0 / s, t1, 1.0, cur);
+            if (cur != lam) cudaMemcpyAsync(lam, cur, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
         }
-        // X' = (s-1)/s W_{s-1} + dt/s R(W_{s-1}) + 1/s W_0
-        adj_apply_rt(tape + (size_t)(s - 1) * nv, s - 1 == 0, tn + 1.0 * dt, dt / s, t1, (s - 1.) / s, t2);
-        double* cur = t2;
-        double* oth = lam;
-        const double a = dt / (s - 1.);
-        for (int i = s - 2; i >= 0; --i) {  // W_{i+1} = W_i + a R(W_i)
-            adj_apply_rt(tape + (size_t)i * nv, i == 0, tn + (i / (s - 1.)) * dt, a, cur, 1.0, oth);
-            std::swap(cur, oth);
+        adj_seed_seg_kernel<<<1, 1, 0, stream_>>>(adj_first_.p, adj_seg_n0_.p, k, adj_ocell_.p, adj_ocomp_.p,
+                                                  adj_oseed_.p, C, lam);
+    }
+
+    // Replay of steps n0 .. n0+cnt-1 with the segment's dts into the tape.
+    void adj_replay(int cnt) {
+        const size_t nv = (size_t)NQ * pm_.C;
+        cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_);
+        for (int k = 0; k < cnt; ++k) {
+            double* tp = adj_tape_.p + (size_t)k * adj_tstride_;
+            cudaMemcpyAsync(tp, x_.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
+            enqueue_step(adj_seg_dt_.p, x_.p, tp);
         }
-        axpby_kernel<<<blocks_for((long long)nv, 256), 256, 0, stream_>>>((long long)nv, 1.0 / s, t1, 1.0, cur);
-        return cur;
+    }
+    void adj_reverse(int cnt) {
+        for (int k = cnt - 1; k >= 0; --k) adj_step(k);
     }
 
     int adjoint_phases(double* ms) override {
         for (int i = 0; i < 3; ++i) ms[i] = adj_phase_ms_[i];
         return ZSME_OK;
     }
+
     int adjoint(const AdjointSpec& A, double* loss, double* grad_q, double* grad_p, double* dts_out) override {
         if (n_inst_ != 1) return set_error(ZSME_ERR_ARG, "the adjoint needs a single-instance handle");
         if (A.nsteps < 0 || A.every < 1 || A.nobs < 0)
@@ -558,7 +595,7 @@ class Solver final : public SolverBase {
             return set_error(ZSME_ERR_ARG, "adjoint: null observation array");
         if (!x_clamped_)
             return set_error(ZSME_ERR_STATE, "adjoint: the state is not constrained (call zsme_update_state)");
-        const int C = pm_.C, F = pm_.F, K = pm_.K, NS = A.nsteps;
+        const int C = pm_.C, F = pm_.F, K = pm_.K, NS = A.nsteps, E = A.every;
         const int s = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
         const size_t nv = (size_t)NQ * C, na = (size_t)NA * C;
         // observations in device numbering, grouped by step (stable)
@@ -570,7 +607,7 @@ class Solver final : public SolverBase {
                 return set_error(ZSME_ERR_ARG, "adjoint: observation " + std::to_string(j) + " out of range");
         }
         std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return A.obs_step[x] < A.obs_step[y]; });
-        std::vector<int> first(NS + 2, 0), ocell(A.nobs), ocomp(A.nobs);
+        std::vector<int> first(NS + 2, 0), ocell(std::max(1, A.nobs), 0), ocomp(std::max(1, A.nobs), 0);
         for (int r = 0; r < A.nobs; ++r) {
             const int j = ord[r];
             ocell[r] = pm_.new_of_old[A.obs_cell[j]];
@@ -578,22 +615,32 @@ class Solver final : public SolverBase {
             first[A.obs_step[j] + 1]++;
         }
         for (int n = 0; n <= NS; ++n) first[n + 1] += first[n];
-        const int nseg = (NS + A.every - 1) / A.every;
+        const int nseg = (NS + E - 1) / E;
+        std::vector<int> seg_n0(std::max(1, nseg));
+        for (int g = 0; g < nseg; ++g) seg_n0[g] = g * E;
         ZSME_CUDA(adj_ocell_.upload(ocell, stream_));
         ZSME_CUDA(adj_ocomp_.upload(ocomp, stream_));
+        ZSME_CUDA(adj_first_.upload(first, stream_));
+        ZSME_CUDA(adj_segn0_all_.upload(seg_n0, stream_));
+        ZSME_CUDA(adj_seg_n0_.alloc(1));
         ZSME_CUDA(adj_oval_.alloc(std::max(1, A.nobs)));
         ZSME_CUDA(adj_oseed_.alloc(std::max(1, A.nobs)));
         ZSME_CUDA(adj_ck_x_.alloc((size_t)(nseg + 1) * nv));
         ZSME_CUDA(adj_ck_a_.alloc((size_t)(nseg + 1) * na));
-        ZSME_CUDA(adj_tape_.alloc((size_t)std::min(A.every, std::max(NS, 1)) * (s + 1) * nv));
+        adj_tstride_ = (size_t)(s + 1) * nv + (size_t)s * 2 * NQ * F;  // one step's tape
+        const int tape_steps = std::min(E, std::max(NS, 1));
+        ZSME_CUDA(adj_tape_.alloc((size_t)tape_steps * adj_tstride_));
         for (auto* b : {&adj_lam0_, &adj_lam1_, &adj_lam2_, &adj_own_w_, &adj_own_wl_, &adj_wl_})
             ZSME_CUDA(b->alloc(nv));
         ZSME_CUDA(adj_out_w_.alloc((size_t)K * nv));
         ZSME_CUDA(adj_out_wl_.alloc((size_t)K * nv));
         ZSME_CUDA(adj_gfs_.alloc((size_t)2 * NQ * F));
-        ZSME_CUDA(adj_lp_cell_.alloc((size_t)NP * C));
+        ZSME_CUDA(adj_lp_cell_.alloc((size_t)NP * blocks_for(C, 128)));  // per-block partial sums
         ZSME_CUDA(adj_lp_.alloc(NP));
         ZSME_CUDA(adj_dts_.alloc(std::max(1, NS)));
+        ZSME_CUDA(adj_th_.alloc((size_t)NS + 1));
+        ZSME_CUDA(adj_seg_dt_.alloc(tape_steps));
+        ZSME_CUDA(adj_seg_t_.alloc(tape_steps));
         auto obs_values = [&](int n) {
             const int cnt = first[n + 1] - first[n];
             if (cnt > 0)
@@ -628,7 +675,7 @@ class Solver final : public SolverBase {
             int rc = step(1, nullptr);
             if (rc) return rc;
             ZSME_CUDA(cudaMemcpyAsync(adj_dts_.p + n, dt_step_.p, sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-            if ((n + 1) % A.every == 0 && n + 1 < NS) save((n + 1) / A.every);
+            if ((n + 1) % E == 0 && n + 1 < NS) save((n + 1) / E);
         }
         obs_values(NS);
         save(nseg);  // the final state, restored at the end
@@ -646,11 +693,13 @@ class Solver final : public SolverBase {
             ZSME_CUDA(cudaEventElapsedTime(&a0, ev[0], ev[1]));
             adj_phase_ms_[0] = a0;
         }
+        // step start times as the device forms them (t += dt)
         std::vector<double> th(NS + 1);
         th[0] = t0;
         for (int n = 0; n < NS; ++n) th[n + 1] = th[n] + dth[n];
+        ZSME_CUDA(cudaMemcpyAsync(adj_th_.p, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
         // loss in the caller's order; seeds 2 w (q - target) in device order
-        std::vector<double> val_of(A.nobs), seed(std::max(1, A.nobs));
+        std::vector<double> val_of(A.nobs), seed(std::max(1, A.nobs), 0.0);
         for (int r = 0; r < A.nobs; ++r) val_of[ord[r]] = oval[r];
         double L = 0.0;
         for (int j = 0; j < A.nobs; ++j) {
@@ -664,37 +713,67 @@ class Solver final : public SolverBase {
         }
         ZSME_CUDA(cudaMemcpyAsync(adj_oseed_.p, seed.data(), seed.size() * sizeof(double), cudaMemcpyHostToDevice,
                                   stream_));
-        // ---- reverse, segment by segment
-        double* lam = adj_lam0_.p;
-        ZSME_CUDA(cudaMemsetAsync(lam, 0, nv * sizeof(double), stream_));
+        // ---- reverse, segment by segment; full segments replay captured graphs
+        ZSME_CUDA(cudaMemsetAsync(adj_lam0_.p, 0, nv * sizeof(double), stream_));
         ZSME_CUDA(cudaMemsetAsync(adj_lp_.p, 0, NP * sizeof(double), stream_));
-        auto seeds = [&](int n, double* l) {
-            const int cnt = first[n + 1] - first[n];
+        {
+            const int cnt = first[NS + 1] - first[NS];
             if (cnt > 0)
-                adj_seed_kernel<<<1, 1, 0, stream_>>>(cnt, adj_ocell_.p + first[n], adj_ocomp_.p + first[n],
-                                                      adj_oseed_.p + first[n], C, l);
+                adj_seed_kernel<<<1, 1, 0, stream_>>>(cnt, adj_ocell_.p + first[NS], adj_ocomp_.p + first[NS],
+                                                      adj_oseed_.p + first[NS], C, adj_lam0_.p);
+        }
+        const bool graphs = !profiling_;
+        cudaGraphExec_t g_replay = nullptr, g_reverse = nullptr;
+        struct GraphGuard {
+            cudaGraphExec_t* a;
+            cudaGraphExec_t* b;
+            ~GraphGuard() {
+                if (*a) cudaGraphExecDestroy(*a);
+                if (*b) cudaGraphExecDestroy(*b);
+            }
+        } graph_guard{&g_replay, &g_reverse};
+        auto capture = [&](cudaGraphExec_t* out, bool replay) -> int {
+            cudaGraph_t gr = nullptr;
+            ZSME_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            if (replay) adj_replay(E);
+            else adj_reverse(E);
+            ZSME_CUDA(cudaStreamEndCapture(stream_, &gr));
+            cudaError_t e = cudaGraphInstantiate(out, gr, 0);
+            cudaGraphDestroy(gr);
+            ZSME_CUDA(e);
+            return ZSME_OK;
         };
-        seeds(NS, lam);
         float replay_ms = 0.f, reverse_ms = 0.f;
         for (int seg = nseg - 1; seg >= 0; --seg) {
-            const int n0 = seg * A.every, n1 = std::min(NS, n0 + A.every);
+            const int n0 = seg * E, cnt = std::min(NS, n0 + E) - n0;
+            const bool full = cnt == E && graphs;
             ZSME_CUDA(cudaEventRecord(ev[2], stream_));
             restore(seg);
-            ZSME_CUDA(cudaMemcpyAsync(t_.p, &th[n0], sizeof(double), cudaMemcpyHostToDevice, stream_));
-            for (int n = n0; n < n1; ++n) {  // replay with the recorded dts, into the tape
-                double* tp = adj_tape_.p + (size_t)(n - n0) * (s + 1) * nv;
-                cudaMemcpyAsync(tp, x_.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
-                ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));
-                enqueue_step(adj_dts_.p + n, x_.p, tp);
+            ZSME_CUDA(cudaMemcpyAsync(t_.p, adj_th_.p + n0, sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(adj_seg_dt_.p, adj_dts_.p + n0, cnt * sizeof(double), cudaMemcpyDeviceToDevice,
+                                      stream_));
+            ZSME_CUDA(cudaMemcpyAsync(adj_seg_t_.p, adj_th_.p + n0, cnt * sizeof(double), cudaMemcpyDeviceToDevice,
+                                      stream_));
+            ZSME_CUDA(cudaMemcpyAsync(adj_seg_n0_.p, adj_segn0_all_.p + seg, sizeof(int), cudaMemcpyDeviceToDevice,
+                                      stream_));
+            if (full) {
+                if (!g_replay) {
+                    int rc = capture(&g_replay, true);
+                    if (rc) return rc;
+                }
+                ZSME_CUDA(cudaGraphLaunch(g_replay, stream_));
+            } else {
+                adj_replay(cnt);
             }
             ZSME_CUDA(cudaEventRecord(ev[3], stream_));
-            for (int n = n1 - 1; n >= n0; --n) {
-                const double* tp = adj_tape_.p + (size_t)(n - n0) * (s + 1) * nv;
-                double* t1 = lam == adj_lam0_.p ? adj_lam1_.p : adj_lam0_.p;
-                double* t2 = (lam != adj_lam2_.p && t1 != adj_lam2_.p) ? adj_lam2_.p
-                             : (lam != adj_lam1_.p && t1 != adj_lam1_.p) ? adj_lam1_.p : adj_lam0_.p;
-                lam = adj_step(lam, t1, t2, tp, dth[n], th[n]);
-                seeds(n, lam);
+            if (full) {
+                if (!g_reverse) {
+                    int rc = capture(&g_reverse, false);
+                    if (rc) return rc;
+                }
+                ZSME_CUDA(cudaGraphLaunch(g_reverse, stream_));
+            } else {
+                adj_reverse(cnt);
             }
             ZSME_CUDA(cudaGetLastError());
             ZSME_CUDA(cudaEventRecord(ev[1], stream_));
@@ -709,7 +788,7 @@ class Solver final : public SolverBase {
         adj_phase_ms_[2] = reverse_ms;
         // ---- outputs; the handle keeps the final state of the forward run
         if (grad_q) {
-            int rc = get_soa(0, lam, NQ, grad_q, false);
+            int rc = get_soa(0, adj_lam0_.p, NQ, grad_q, false);
             if (rc) return rc;
         }
         if (grad_p) ZSME_CUDA(cudaMemcpyAsync(grad_p, adj_lp_.p, NP * sizeof(double), cudaMemcpyDeviceToHost, stream_));
