@@ -95,12 +95,16 @@ def step_bytes_survey(nq):
     return 8 * (5 * me + 2) + 304
 
 
-def load_traffic():
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
-    return {}
+# DRAM bytes (read + write) per cell of one launch, from the ncu capture of
+# profiles/sme2d_l4_kernels_900.md (900x900 grid, 1,618,202 cells; the two
+# stage launches averaged).  The streams scale with the cell count, so a
+# 1400x1400 launch moves these figures times its cells.
+NCU_DRAM_BYTES_PER_CELL = {
+    "sme2d_l4/prep": (816.4e6 + 974.2e6) / 2 / 1618202,
+    "sme2d_l4/flux": 1199.9e6 / 1618202,
+    "sme2d_l4/gather": (1413.3e6 + 1338.9e6) / 2 / 1618202,
+    "sme2d_l4/finalize": 306.6e6 / 1618202,
+}
 
 
 # ------------------------------------------------------------------ clocks
@@ -577,11 +581,13 @@ def main():
     dom_ms = prof[dom][0] / prof[dom][1]
     alg = algorithmic_bytes(dom, C, F, nq, na, case.mesh.max_faces, case.settings.ssp_stages)
     achieved = alg / (dom_ms / 1e3) / 1e9
-    traffic = load_traffic().get("%s/%s" % (case.model, dom))
+    traffic = NCU_DRAM_BYTES_PER_CELL.get("%s/%s" % (case.model, dom))
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": alg,
-                "traffic": (traffic["dram_bytes_per_cell"] * C) if traffic else None,
+                "traffic": traffic * C if traffic else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell on the 900x900 grid, "
+                                  "scaled to this launch's cells" if traffic else None,
                 "kernel_ms": dom_ms}
     step_ms = ms_max / a.steps
     sb = step_bytes_survey(nq)
