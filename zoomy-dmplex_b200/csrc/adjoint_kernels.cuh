@@ -631,7 +631,7 @@ __global__ void __launch_bounds__(128) adj_finalize_kernel(MeshDev m, const doub
                                                            double* __restrict__ lam_in,
                                                            double* __restrict__ lp_part) {
     using M = MT<double>;
-    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, NP = M::n_parameters;
+    constexpr int NQ = M::n_dof_q, NP = M::n_parameters;
     const int C = m.C;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     __shared__ double lp_sh[NP][128];

@@ -298,19 +298,18 @@ __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int 
                     for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
                     const double qfu = q + d;
                     const double dq = qfu - q;
-                    // fmin(1, r / dq) is exactly 1 when r >= dq > 0 (or r <= dq < 0): the
-                    // correctly rounded quotient of |r| >= |dq| is >= 1, so the
-                    // division is only taken where it can limit (NaN still takes it)
-                    double a = 1.0;
-                    if (!(fabs(dq) < 1e-12)) {
-                        if (dq > 0) {
-                            const double rr = mx - q;
-                            a = (mx > q) ? (rr >= dq ? 1.0 : fmin(1.0, rr / dq)) : 0.0;
-                        } else {
-                            const double rr = mn - q;
-                            a = (mn < q) ? (rr <= dq ? 1.0 : fmin(1.0, rr / dq)) : 0.0;
-                        }
-                    }
+                    // TVDLimiter (Reconstruction.hpp:67-78) as selects: the bound on
+                    // dq's side, "0" when the cell is that side's extreme.  fmin(1,
+                    // r / dq) is exactly 1 when r >= dq > 0 (or r <= dq < 0): the
+                    // correctly rounded quotient of |r| >= |dq| is >= 1, so only the
+                    // rare limiting case divides (NaN still divides)
+                    const bool pos = dq > 0;
+                    const double rr = (pos ? mx : mn) - q;
+                    const bool room = pos ? (mx > q) : (mn < q);
+                    const bool lim = !(pos ? (rr >= dq) : (rr <= dq));
+                    const bool small = fabs(dq) < 1e-12;
+                    double a = small ? 1.0 : (room ? 1.0 : 0.0);
+                    if (!small && room && lim) a = fmin(1.0, rr / dq);
                     if (a < al[k]) al[k] = a;
                 }
             }
