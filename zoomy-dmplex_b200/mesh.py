@@ -109,9 +109,9 @@ class Mesh:
 def _faces_from_cells(cells: np.ndarray, nloc: int):
     """First-encounter face numbering (cell order, then local face order)."""
     C = cells.shape[0]
-    if nloc == 3:
-        a = cells[:, [0, 1, 2]]
-        b = cells[:, [1, 2, 0]]
+    if nloc >= 3:  # polygon edges (v_k, v_k+1)
+        a = cells[:, list(range(nloc))]
+        b = cells[:, [(k + 1) % nloc for k in range(nloc)]]
         lo = np.minimum(a, b).reshape(-1).astype(np.int64)
         hi = np.maximum(a, b).reshape(-1).astype(np.int64)
         key = lo * (int(cells.max()) + 1) + hi
@@ -167,6 +167,56 @@ def from_triangles(vertices: np.ndarray, tris: np.ndarray, name="mesh", boundary
     bc = np.where(face_cells[:, 1] < 0, boundary_bc, FACE_INTERIOR).astype(np.int32)
     return Mesh(2, vertices, tris.astype(np.int32), centroid, volume, cell_faces, face_cells,
                 fcent, normal, bc, name=name)
+
+
+def from_polygons(vertices: np.ndarray, polys: np.ndarray, name="mesh", boundary_bc=0) -> Mesh:
+    """Mesh of convex polygons with the same vertex count (counter-clockwise
+    or clockwise; re-oriented counter-clockwise): shoelace areas and
+    centroids, edge midpoints and outward edge normals."""
+    vertices = np.asarray(vertices, dtype=np.float64)[:, :2].copy()
+    polys = np.asarray(polys, dtype=np.int64).copy()
+    K = polys.shape[1]
+    P = vertices[polys]                                   # [C, K, 2]
+    Pn = np.roll(P, -1, axis=1)
+    cross = P[:, :, 0] * Pn[:, :, 1] - Pn[:, :, 0] * P[:, :, 1]
+    area2 = cross.sum(1)
+    neg = area2 < 0
+    polys[neg] = polys[neg][:, ::-1]
+    P = vertices[polys]
+    Pn = np.roll(P, -1, axis=1)
+    cross = P[:, :, 0] * Pn[:, :, 1] - Pn[:, :, 0] * P[:, :, 1]
+    area2 = cross.sum(1)
+    centroid = ((P + Pn) * cross[:, :, None]).sum(1) / (3.0 * area2[:, None])
+    volume = 0.5 * area2
+    cell_faces, face_cells, first = _faces_from_cells(polys, K)
+    loc = first % K
+    c0 = face_cells[:, 0]
+    xa = vertices[polys[c0, loc]]
+    xb = vertices[polys[c0, (loc + 1) % K]]
+    fcent = 0.5 * (xa + xb)
+    e = xb - xa
+    normal = np.stack([e[:, 1], -e[:, 0]], axis=1)
+    out = ((fcent - centroid[c0]) * normal).sum(1) < 0
+    normal[out] *= -1.0
+    bc = np.where(face_cells[:, 1] < 0, boundary_bc, FACE_INTERIOR).astype(np.int32)
+    return Mesh(2, vertices, polys.astype(np.int32), centroid, volume, cell_faces, face_cells,
+                fcent, normal, bc, name=name)
+
+
+def quad_strip(x: np.ndarray, height: float = 1.0, name="strip") -> Mesh:
+    """One row of rectangles [x_i, x_i+1] x [0, height] (walls all round):
+    with height 1 and a state uniform in y with v = 0, the 2-D scheme reduces
+    to the 1-D scheme on the interval mesh of the same nodes."""
+    x = np.asarray(x, dtype=np.float64)
+    n = x.size - 1
+    verts = np.concatenate([np.stack([x, np.zeros_like(x)], 1), np.stack([x, np.full_like(x, height)], 1)])
+    i = np.arange(n)
+    quads = np.stack([i, i + 1, n + 2 + i, n + 1 + i], axis=1)
+    m = from_polygons(verts, quads, name=name)
+    # rectangle measures formed exactly as interval() forms the 1-D ones
+    m.cell_volume = np.abs(x[1:] - x[:-1]) * height
+    m.cell_centroid = np.stack([0.5 * (x[:-1] + x[1:]), np.full(n, 0.5 * height)], axis=1)
+    return m
 
 
 def jittered_square(n: int, seed: int = 0, jitter: float = 0.2, name=None) -> Mesh:
