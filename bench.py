@@ -195,9 +195,11 @@ def run_ensemble(a, dev, torch, dist, rank, world):
         if dist:
             dist.barrier()
 
-    n = a.instances
+    # a.instances per GPU on average; ranks take greedy size-balanced shards
+    shard = cases.ensemble_shard(a.instances * world, world, rank)
+    n = len(shard)
     t0 = time.perf_counter()
-    members = cases.ensemble(n, first=rank * n)
+    members = cases.ensemble(indices=shard)
     build_s = time.perf_counter() - t0
     model, st = members[0].model, members[0].settings
     meshes = [c.mesh for c in members]

@@ -107,6 +107,33 @@ def roofline_l4(n: int = 1400, seed: int = 2, steps: int = 100, m: Optional[mesh
                 dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), steps)
 
 
+def ensemble_side(i: int, seed: int = 3, side_range=(40, 400)) -> int:
+    """Grid side of ensemble instance i (the first draw of its generator)."""
+    rng = np.random.default_rng([seed, i])
+    return int(round(np.exp(rng.uniform(np.log(side_range[0]), np.log(side_range[1])))))
+
+
+def shard_instances(cells, world: int):
+    """Instances over `world` ranks by greedy balance on their cell counts
+    (largest first, each to the least loaded rank; ties to the lower rank):
+    list of index lists, each in increasing order."""
+    order = sorted(range(len(cells)), key=lambda i: (-cells[i], i))
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += cells[i]
+        out[r].append(i)
+    return [sorted(o) for o in out]
+
+
+def ensemble_shard(n_total: int, world: int, rank: int, seed: int = 3, side_range=(40, 400)):
+    """The instance indices rank `rank` of `world` advances: greedy balance
+    on the cell counts 2 (side - 1)^2 of the Delaunay grids."""
+    cells = [2 * (ensemble_side(i, seed, side_range) - 1) ** 2 for i in range(n_total)]
+    return shard_instances(cells, world)[rank]
+
+
 def ensemble_member(i: int, seed: int = 3, side_range=(40, 400)) -> Case:
     """Instance i of the level-2 ensemble: grid side log-uniform in
     [40, 400], 1-4 Gaussian bumps (amplitude U[0.05,0.2], width
@@ -157,13 +184,17 @@ def _member(args):
     return ensemble_member(i, seed=seed, side_range=(lo, hi))
 
 
-def ensemble(n: int = 512, seed: int = 3, side_range=(40, 400), processes: int = 0, first: int = 0):
-    """Instances first .. first+n-1 of the level-2 ensemble, built in parallel
-    worker processes (spawned, so it is safe after CUDA has been initialised)."""
+def ensemble(n: int = 512, seed: int = 3, side_range=(40, 400), processes: int = 0, first: int = 0,
+             indices=None):
+    """Instances first .. first+n-1 (or the given indices) of the level-2
+    ensemble, built in parallel worker processes (spawned, so it is safe
+    after CUDA has been initialised)."""
     import multiprocessing as mp
     import os
 
-    args = [(i, seed, side_range[0], side_range[1]) for i in range(first, first + n)]
+    idx = list(indices) if indices is not None else list(range(first, first + n))
+    n = len(idx)
+    args = [(i, seed, side_range[0], side_range[1]) for i in idx]
     procs = processes or min(n, os.cpu_count() or 1)
     if procs <= 1 or n < 4:
         return [_member(a) for a in args]
