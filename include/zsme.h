@@ -63,6 +63,15 @@ typedef struct zsme_mesh {
 #define ZSME_LIMITER_TVD 1        /* VacuumLimiter + TVDLimiter (Reconstruction.hpp:170-175) */
 #define ZSME_GRADIENT_GREEN_GAUSS 0 /* GreenGaussGradient (Gradient.hpp:43-191) */
 #define ZSME_GRADIENT_LSQ 1       /* LeastSquaresGradient (Gradient.hpp:196-360) */
+/* settings.solver.positivity (Settings.hpp:24-27, ModularSolver.hpp:46-58) */
+#define ZSME_POSITIVITY_NONE 0      /* "none": LinearReconstructor with Vacuum + TVD limiting */
+#define ZSME_POSITIVITY_ZHANG_SHU 1 /* "zhang_shu": eta-well-balanced reconstruction, Venkatakrishnan
+                                       slopes and the Zhang-Shu theta (TransportStep.hpp:241-323,
+                                       Reconstruction.hpp:247-287); order 2 clamps CFL to 1/6
+                                       (MUSCLSolver.hpp:33-38) */
+#define ZSME_POSITIVITY_MOOD 2      /* "mood": the same reconstruction without theta, and cells whose
+                                       depth ends below -1e-10 redone by a first-order Euler step
+                                       (MUSCLSolver.hpp:130-171, 197-229) */
 
 /* The solver keys of the reference's Settings (Settings.hpp:13-40) that change
  * the step. */
@@ -76,7 +85,10 @@ typedef struct zsme_settings {
     int32_t ssp_stages;           /* s of SSP-RK(s,2), >= 2 */
     int32_t source;               /* 1: operator-split implicit source ("splitting") */
     int32_t block_size;           /* CUDA block size, 0 = library default */
-    int32_t reserved[6];
+    int32_t positivity;           /* ZSME_POSITIVITY_* */
+    int32_t reserved[5];
+    double wet_dry_eps;           /* solver.wet_dry_eps (reference default 1e-2): dry threshold of the
+                                     positivity variants, read only when positivity != NONE */
 } zsme_settings;
 
 /* Health counters of the last step (failure detection without faulting). */
@@ -87,7 +99,7 @@ typedef struct zsme_diag {
     int32_t n_nonfinite;          /* cells with a non-finite value */
     int32_t n_negative_depth;     /* cells with h < -1e-10 (MUSCLSolver.hpp:206) */
     int32_t n_newton_unconverged; /* cells whose Newton hit 15 iterations */
-    int32_t reserved;
+    int32_t n_mood_cells;         /* cells redone at first order by MOOD (ZSME_POSITIVITY_MOOD) */
 } zsme_diag;
 
 typedef struct zsme_handle zsme_handle;

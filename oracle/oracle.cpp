@@ -116,6 +116,7 @@ struct OracleBase {
     virtual void get_time(double* t, double* dt) const = 0;
     virtual void set_params(const double* p) = 0;
     virtual int newton_unconverged() const = 0;
+    virtual long long mood_cells() const = 0;
     virtual void gradient(const double* x, double* g) = 0;
     // tangent-linear (dual-number) instances only: seed / read directions
     virtual void set_tangent(const double*, const double*) {}
@@ -146,6 +147,7 @@ struct Oracle : OracleBase {
     std::vector<T> X, A, G;
     double time = 0.0, dt = 0.0;
     int n_unconv = 0;
+    long long n_troubled = 0;   // cells redone at first order by MOOD, all steps
 
     Oracle(const zsme_mesh* m, const zsme_settings* s, const double* p) {
         C = m->n_cells; F = m->n_faces; K = m->max_faces;
@@ -157,6 +159,9 @@ struct Oracle : OracleBase {
         fcell.assign(m->face_cells, m->face_cells + 2 * F);
         fbc.assign(m->face_bc, m->face_bc + F);
         st = *s;
+        // Zhang-Shu positivity holds for CFL <= 1/6 at order 2 (MUSCLSolver.hpp:33-38)
+        if (st.reconstruction_order >= 2 && st.positivity == ZSME_POSITIVITY_ZHANG_SHU && st.cfl > 1.0 / 6.0)
+            st.cfl = 1.0 / 6.0;
         auto dp = M::default_parameters();
         params.assign(dp.begin(), dp.end());
         if (p) params.assign(p, p + M::n_parameters);
@@ -171,6 +176,7 @@ struct Oracle : OracleBase {
     int naux() const override { return NA; }
     void set_params(const double* p) override { params.assign(p, p + M::n_parameters); }
     int newton_unconverged() const override { return n_unconv; }
+    long long mood_cells() const override { return n_troubled; }
 
     // SetupTopology (TransportStep.hpp:106-120): adjacency of a cell = the
     // other cells of its faces in cone order.
@@ -369,6 +375,112 @@ par_for(C, [&](int c, int) {
         for (int i = 0; i < NQ; ++i) out[i] = q[i] + alpha * delta[i];
     }
 
+    // ----------------------------------------------------- positivity (WB)
+    // TransportStep::LimitGradientsWB (TransportStep.hpp:241-323): per cell,
+    // Venkatakrishnan slopes on W = (b, eta = b + h, momenta) from the clamped
+    // local state, dry cells first order, b and momentum slopes tied to eta,
+    // the Zhang-Shu theta on the depth deviation (skipped under MOOD); the
+    // effective gradients replace the raw ones (b slot: grad b_eff, h slot:
+    // grad eta_eff, momenta: theta phi grad).
+    void limit_gradients_wb(const std::vector<T>& xl, std::vector<T>& g) {
+        const int B = 0, H = 1;
+        const bool skip_theta = st.positivity == ZSME_POSITIVITY_MOOD;
+        par_for(C, [&](int c, int) {
+            T* gc = &g[(size_t)c * NQ * DIM];
+            const T* qc = &xl[(size_t)c * NQ];
+            T gr[NQ * DIM], geta[3], Wc[NQ], Wmin[NQ], Wmax[NQ], phi[NQ];
+            for (int k = 0; k < NQ * DIM; ++k) gr[k] = gc[k];
+            for (int d = 0; d < DIM; ++d) geta[d] = gr[H * DIM + d] + gr[B * DIM + d];
+            const T h_bar = qc[H], b_bar = qc[B];
+            for (int i = 0; i < NQ; ++i) Wc[i] = (i == H) ? (b_bar + h_bar) : qc[i];
+            for (int i = 0; i < NQ; ++i) { Wmin[i] = Wc[i]; Wmax[i] = Wc[i]; }
+            for (int k = nb_off[c]; k < nb_off[c + 1]; ++k) {
+                const T* qn = &xl[(size_t)nb_list[k] * NQ];
+                for (int i = 0; i < NQ; ++i) {
+                    T w = (i == H) ? (qn[B] + qn[H]) : qn[i];
+                    if (w < Wmin[i]) Wmin[i] = w;
+                    if (w > Wmax[i]) Wmax[i] = w;
+                }
+            }
+            // vol^(2/dim) (TransportStep.hpp:279), written exactly for dim 1 and 2
+            const double eps2 = DIM == 2 ? vol[c] : DIM == 1 ? vol[c] * vol[c] : std::pow(vol[c], 2.0 / DIM);
+            for (int i = 0; i < NQ; ++i) phi[i] = 1.0;
+            for (int k = 0; k < K; ++k) {
+                const int f = cf[(size_t)c * K + k];
+                if (f < 0) continue;
+                double r[3];
+                for (int d = 0; d < DIM; ++d) r[d] = fc[2 * f + d] - cc[2 * c + d];
+                for (int i = 0; i < NQ; ++i) {
+                    T delta = 0.0;
+                    for (int d = 0; d < DIM; ++d) delta += ((i == H) ? geta[d] : gr[i * DIM + d]) * r[d];
+                    if (std::abs(delta) < 1e-14) continue;
+                    T dm = (delta > 0) ? (Wmax[i] - Wc[i]) : (Wmin[i] - Wc[i]);
+                    T num = dm * dm + eps2 + 2 * delta * dm, den = dm * dm + 2 * delta * delta + delta * dm + eps2;
+                    T pf = (den > 1e-30) ? num / den : (T)1.0;
+                    pf = std::max((T)0, std::min((T)1, pf));
+                    if (pf < phi[i]) phi[i] = pf;
+                }
+            }
+            if (h_bar < st.wet_dry_eps)
+                for (int i = 0; i < NQ; ++i) phi[i] = 0.0;
+            phi[B] = std::min(phi[B], phi[H]);
+            for (int i = 0; i < NQ; ++i)
+                if (i != B && i != H) phi[i] = std::min(phi[i], phi[H]);
+            T sh[3];
+            for (int d = 0; d < DIM; ++d) sh[d] = phi[H] * geta[d] - phi[B] * gr[B * DIM + d];
+            T hmin = h_bar;
+            for (int k = 0; k < K; ++k) {
+                const int f = cf[(size_t)c * K + k];
+                if (f < 0) continue;
+                T hf = h_bar;
+                for (int d = 0; d < DIM; ++d) hf += sh[d] * (fc[2 * f + d] - cc[2 * c + d]);
+                if (hf < hmin) hmin = hf;
+            }
+            T theta = 1.0;
+            if (!skip_theta && hmin < 0.0)
+                theta = std::max((T)0, std::min((T)1, h_bar / std::max(h_bar - hmin, (T)1e-14)));
+            for (int d = 0; d < DIM; ++d) {
+                gc[B * DIM + d] = phi[B] * gr[B * DIM + d];
+                gc[H * DIM + d] = phi[B] * gr[B * DIM + d] + theta * sh[d];
+            }
+            for (int i = 0; i < NQ; ++i)
+                if (i != B && i != H)
+                    for (int d = 0; d < DIM; ++d) gc[i * DIM + d] = theta * phi[i] * gr[i * DIM + d];
+        });
+    }
+
+    // WBPositivityReconstructor::Reconstruct (Reconstruction.hpp:264-286):
+    // eta_f and b_f from the effective gradients, h_f = max(eta_f - b_f, 0),
+    // momenta zeroed where h_f < wet_dry_eps.
+    void wb_reconstruct(const T* q, const T* g, const double* xc, const double* xf, T* out) const {
+        const int B = 0, H = 1;
+        T dx[3];
+        for (int d = 0; d < DIM; ++d) dx[d] = xf[d] - xc[d];
+        auto dot = [&](int slot) {
+            T sum = 0.0;
+            for (int d = 0; d < DIM; ++d) sum += g[slot * DIM + d] * dx[d];
+            return sum;
+        };
+        const T b_bar = q[B], h_bar = q[H];
+        const T b_f = b_bar + dot(B);
+        const T eta_f = (b_bar + h_bar) + dot(H);
+        const T h_f = std::max(eta_f - b_f, (T)0);
+        for (int i = 0; i < NQ; ++i) {
+            if (i == B) out[i] = b_f;
+            else if (i == H) out[i] = h_f;
+            else out[i] = (h_f < st.wet_dry_eps) ? (T)0 : (q[i] + dot(i));
+        }
+    }
+
+    // The face reconstruction of the configured path.
+    void recon(const T* q, const T* g, const double* xc, const double* xf, const T* qmin, const T* qmax,
+               T* out) const {
+        if (g && st.reconstruction_order >= 2 && st.positivity != ZSME_POSITIVITY_NONE)
+            wb_reconstruct(q, g, xc, xf, out);
+        else
+            reconstruct(q, g, xc, xf, qmin, qmax, out);
+    }
+
     // ------------------------------------------------------------- FormRHS
     void form_rhs(double t, const std::vector<T>& xg, std::vector<T>& f) {
         std::vector<T> xl = xg, al = A;          // local copies
@@ -393,6 +505,7 @@ par_for(C, [&](int c, int) {
             });
             // gradient of the UNCLAMPED global state (TransportStep.hpp:339)
             if (st.gradient == ZSME_GRADIENT_LSQ) gradient_lsq(xg, G); else gradient_gg(xg, G);
+            if (st.positivity != ZSME_POSITIVITY_NONE) limit_gradients_wb(xl, G);
         }
         // per-face contributions: nc into L, nc into R, flux (all * area)
         std::vector<T> fb((size_t)F * 3 * NQ, 0.0);
@@ -412,9 +525,9 @@ par_for(F, [&](int f, int) {
             T* fl = ncR + NQ;
             if (R >= 0) {
                 T qLf[NQ], qRf[NQ], aLf[NA], aRf[NA];
-                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
+                recon(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
                             o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
-                reconstruct(&xl[(size_t)R * NQ], o2 ? &G[(size_t)R * NQ * DIM] : nullptr, &cc[2 * R], &fc[2 * f],
+                recon(&xl[(size_t)R * NQ], o2 ? &G[(size_t)R * NQ * DIM] : nullptr, &cc[2 * R], &fc[2 * f],
                             o2 ? &vmin[(size_t)R * NQ] : nullptr, o2 ? &vmax[(size_t)R * NQ] : nullptr, qRf);
                 for (int i = 0; i < NA; ++i) { aLf[i] = al[(size_t)L * NA + i]; aRf[i] = al[(size_t)R * NA + i]; }
                 auto ra = M::update_aux_variables(qLf, aLf, params.data(), 0.0, xf);
@@ -431,7 +544,7 @@ par_for(F, [&](int f, int) {
                 active[f] = 1;
             } else if (fbc[f] >= 0) {
                 T qLf[NQ], aLf[NA], aRf[NA];
-                reconstruct(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
+                recon(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
                             o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
                 for (int i = 0; i < NA; ++i) aLf[i] = al[(size_t)L * NA + i];
                 auto ra = M::update_aux_variables(qLf, aLf, params.data(), t, xf);
@@ -662,15 +775,109 @@ par_for(C, [&](int c, int) {
         const double al = (s - 1.) / s, be = h / s, ga = 1. / s;
         for (size_t k = 0; k < n; ++k) X[k] = al * w[k] + be * F[k] + ga * X[k];
     }
+    // Local MOOD (MUSCLSolver.hpp:130-171, 197-229; TransportStep.hpp:363-381):
+    // cells whose depth ends below -1e-10 are overwritten by the first-order
+    // forward-Euler update from the step's start state Xs (piecewise constant
+    // states, fluxes of the faces touching a troubled cell), then the
+    // constraints are applied again.
+    void mood_override(double t0, double d0, const std::vector<T>& Xs) {
+        std::vector<char> bad(C, 0);
+        int nt = 0;
+        for (int c = 0; c < C; ++c)
+            if (X[(size_t)c * NQ + 1] < -1.0e-10) { bad[c] = 1; ++nt; }
+        if (!nt) return;
+        n_troubled += nt;
+        std::vector<T> xl = Xs, al = A;
+        update_state_vec(xl, al);
+        std::vector<T> fb((size_t)F * 3 * NQ, 0.0);
+        std::vector<char> active(F, 0);
+        par_for(F, [&](int f, int) {
+            const int L = fcell[2 * f], R = fcell[2 * f + 1];
+            if (!(bad[L] || (R >= 0 && bad[R]))) return;
+            const double* Nf = &fn[2 * f];
+            double area = 0;
+            for (int d = 0; d < DIM; ++d) area += Nf[d] * Nf[d];
+            area = std::sqrt(area);
+            if (area <= 1e-15) return;
+            T nh[3] = {0, 0, 0};
+            for (int d = 0; d < DIM; ++d) nh[d] = Nf[d] / area;
+            const T xf[3] = {fc[2 * f], fc[2 * f + 1], 0.0};
+            T* ncL = &fb[(size_t)f * 3 * NQ];
+            T* ncR = ncL + NQ;
+            T* fl = ncR + NQ;
+            T qLf[NQ], aLf[NA], aRf[NA];
+            for (int i = 0; i < NQ; ++i) qLf[i] = xl[(size_t)L * NQ + i];
+            for (int i = 0; i < NA; ++i) aLf[i] = al[(size_t)L * NA + i];
+            if (R >= 0) {
+                T qRf[NQ];
+                for (int i = 0; i < NQ; ++i) qRf[i] = xl[(size_t)R * NQ + i];
+                for (int i = 0; i < NA; ++i) aRf[i] = al[(size_t)R * NA + i];
+                auto ra = M::update_aux_variables(qLf, aLf, params.data(), 0.0, xf);
+                for (int i = 0; i < NA; ++i) aLf[i] = ra[i];
+                auto rb = M::update_aux_variables(qRf, aRf, params.data(), 0.0, xf);
+                for (int i = 0; i < NA; ++i) aRf[i] = rb[i];
+                auto flux = N::numerical_flux(qLf, qRf, aLf, aRf, params.data(), nh);
+                auto nc = N::numerical_fluctuations(qLf, qRf, aLf, aRf, params.data(), nh);
+                for (int i = 0; i < NQ; ++i) {
+                    ncL[i] = nc[NQ + i] * area;
+                    ncR[i] = nc[i] * area;
+                    fl[i] = flux[i] * area;
+                }
+                active[f] = 1;
+            } else if (fbc[f] >= 0) {
+                auto ra = M::update_aux_variables(qLf, aLf, params.data(), t0, xf);
+                for (int i = 0; i < NA; ++i) aLf[i] = ra[i];
+                auto qR = M::boundary_conditions(fbc[f], qLf, aLf, params.data(), nh, xf, t0, 0.0);
+                auto rb = M::update_aux_variables(qR.data, aLf, params.data(), t0, xf);
+                for (int i = 0; i < NA; ++i) aRf[i] = rb[i];
+                auto flux = N::numerical_flux(qLf, qR.data, aLf, aRf, params.data(), nh);
+                auto nc = N::numerical_fluctuations(qLf, qR.data, aLf, aRf, params.data(), nh);
+                for (int i = 0; i < NQ; ++i) {
+                    ncL[i] = nc[NQ + i] * area;
+                    fl[i] = flux[i] * area;
+                }
+                active[f] = 2;
+            }
+        });
+        par_for(C, [&](int c, int) {
+            if (!bad[c]) return;
+            T fcq[NQ];
+            for (int i = 0; i < NQ; ++i) fcq[i] = 0.0;
+            for (int k = 0; k < K; ++k) {
+                const int fi = cell_face_sorted[(size_t)c * K + k];
+                if (fi < 0) break;
+                if (!active[fi]) continue;
+                const T* ncL = &fb[(size_t)fi * 3 * NQ];
+                const T* ncR = ncL + NQ;
+                const T* fl = ncR + NQ;
+                if (fcell[2 * fi] == c) {
+                    for (int i = 0; i < NQ; ++i) fcq[i] -= ncL[i];
+                    for (int i = 0; i < NQ; ++i) fcq[i] -= fl[i];
+                } else {
+                    for (int i = 0; i < NQ; ++i) fcq[i] -= ncR[i];
+                    for (int i = 0; i < NQ; ++i) fcq[i] += fl[i];
+                }
+            }
+            if (vol[c] > 1e-15)
+                for (int i = 0; i < NQ; ++i) fcq[i] /= vol[c];
+            for (int i = 0; i < NQ; ++i) X[(size_t)c * NQ + i] = Xs[(size_t)c * NQ + i] + d0 * fcq[i];
+        });
+        update_state_vec(X, A);
+    }
+
     void step(int nsteps, const double* dts) override {
         for (int it = 0; it < nsteps; ++it) {
             if (!(time < st.t_end)) break;
             double t0 = time;
             double d0 = dts ? dts[it] : dt;
             if (t0 + d0 > st.t_end) d0 = st.t_end - t0;
+            const bool mood = st.positivity == ZSME_POSITIVITY_MOOD;
+            std::vector<T> Xs;
+            if (mood) Xs = X;
             ts_step(t0, d0);
             time = t0 + d0;
             update_state_vec(X, A);                            // EnforcePhysicalConstraints
+            if (mood) mood_override(t0, d0, Xs);
             if (st.source) {
                 source_solve(d0);
                 update_state_vec(X, A);
@@ -815,5 +1022,6 @@ int oracle_step_dt(void* h, int n, const double* dts) { ((OracleBase*)h)->step(n
 int oracle_get_time(void* h, double* t, double* dt) { ((OracleBase*)h)->get_time(t, dt); return 0; }
 int oracle_set_params(void* h, const double* p) { ((OracleBase*)h)->set_params(p); return 0; }
 int oracle_newton_unconverged(void* h) { return ((OracleBase*)h)->newton_unconverged(); }
+long long oracle_mood_cells(void* h) { return ((OracleBase*)h)->mood_cells(); }
 
 }  // extern "C"

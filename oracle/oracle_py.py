@@ -56,6 +56,8 @@ def load(ref: bool = False):
     lib.oracle_get_time.argtypes = [vp, P, P]
     lib.oracle_set_params.argtypes = [vp, P]
     lib.oracle_newton_unconverged.argtypes = [vp]
+    lib.oracle_mood_cells.argtypes = [vp]
+    lib.oracle_mood_cells.restype = ct.c_longlong
     lib.oracle_set_threads.argtypes = [ct.c_int]
     lib.oracle_model_info.argtypes = [ct.c_char_p] + [ct.POINTER(ct.c_int)] * 4
     lib.oracle_pointwise.argtypes = [ct.c_char_p, ct.c_int, P, P, P, P, P, P, ct.c_double, P]
@@ -176,6 +178,10 @@ class Oracle:
 
     def newton_unconverged(self):
         return self.lib.oracle_newton_unconverged(self.h)
+
+    def mood_cells(self):
+        """Cells redone at first order by MOOD over all steps so far."""
+        return self.lib.oracle_mood_cells(self.h)
 
 
 class TangentOracle(Oracle):

@@ -28,4 +28,7 @@ def test_rejects_out_of_path_strategies():
     with pytest.raises(ValueError):
         SolverSettings(time_integration="imex").to_struct()
     with pytest.raises(ValueError):
-        SolverSettings(positivity="mood").to_struct()
+        SolverSettings(positivity="bogus").to_struct()
+    assert SolverSettings(positivity="mood").to_struct().positivity == native.ZSME_POSITIVITY_MOOD
+    st = SolverSettings(positivity="zhang_shu", wet_dry_eps=0.05).to_struct()
+    assert st.positivity == native.ZSME_POSITIVITY_ZHANG_SHU and st.wet_dry_eps == 0.05

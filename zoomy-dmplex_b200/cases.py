@@ -107,6 +107,28 @@ def roofline_l4(n: int = 1400, seed: int = 2, steps: int = 100, m: Optional[mesh
                 dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), steps)
 
 
+def wet_dry_patchwork(n: int = 24, seed: int = 12, level: int = 0) -> Case:
+    """Wet/dry patchwork for the positivity variants: each cell dry with
+    probability 1/2, else depth U[0.01, 0.3] with velocities U[-3, 3]^2, over
+    three Gaussian bumps (amplitude U[0, 0.2], width^2 U[0.005, 0.03]); no
+    friction.  At CFL 1.5 the limited order-2 step drives depths negative
+    within the first steps, which the MOOD variant repairs."""
+    rng = np.random.default_rng(seed)
+    m = meshmod.jittered_square(n, seed=7)
+    x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
+    b = np.zeros_like(x)
+    for _ in range(3):
+        a = rng.uniform(0, 0.2)
+        c = rng.uniform(0, 1, 2)
+        b = b + a * _gauss(x, y, c[0], c[1], rng.uniform(0.005, 0.03))
+    h = np.where(rng.uniform(0, 1, x.size) < 0.5, 0.0, rng.uniform(0.01, 0.3, x.size))
+    u = rng.uniform(-3, 3, x.size)
+    v = rng.uniform(-3, 3, x.size)
+    q = _state(level, h, b, hu=[h * u] + [0 * h] * level, hv=[h * v] + [0 * h] * level)
+    return Case("wet_dry_patchwork_%d" % n, "sme2d_l%d" % level, m, q, default_settings(cfl=1.5),
+                dict(g=9.81, nu=0.0, n_manning=0.0), 20)
+
+
 def ensemble_side(i: int, seed: int = 3, side_range=(40, 400)) -> int:
     """Grid side of ensemble instance i (the first draw of its generator)."""
     rng = np.random.default_rng([seed, i])

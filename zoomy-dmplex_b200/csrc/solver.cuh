@@ -72,9 +72,10 @@ class Solver final : public SolverBase {
     DevBuf<double> slot_dx_, slot_w_, vol_, rc_, fn_, farea_, fc_, fnr_;
     // state
     DevBuf<double> x_, w_, wl_, aux_, fs_, fb_, tmp_a_, tmp_b_, params_, dts_;
+    DevBuf<double> xs_;  // MOOD: the state at the start of the step
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
-    DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..3] diag
+    DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag
     DevBuf<unsigned long long> ratio_;
     // discrete adjoint (allocated by the first zsme_adjoint call)
     DevBuf<double> adj_ck_x_, adj_ck_a_, adj_tape_, adj_lam0_, adj_lam1_, adj_lam2_, adj_own_w_, adj_own_wl_;
@@ -173,6 +174,11 @@ class Solver final : public SolverBase {
         if (pm_.dim != DIM) return set_error(ZSME_ERR_ARG, "mesh dimension does not match the model");
         if (st_.reconstruction_order >= 2 && st_.ssp_stages < 2)
             return set_error(ZSME_ERR_ARG, "ssp_stages must be >= 2");
+        if (st_.positivity != ZSME_POSITIVITY_NONE && (NQ < 3 || !(st_.wet_dry_eps >= 0)))
+            return set_error(ZSME_ERR_ARG, "positivity variants need a [b, h, momentum...] model and wet_dry_eps >= 0");
+        // Zhang-Shu positivity holds for CFL <= 1/6 at order 2 (MUSCLSolver.hpp:33-38)
+        if (st_.reconstruction_order >= 2 && st_.positivity == ZSME_POSITIVITY_ZHANG_SHU && st_.cfl > 1.0 / 6.0)
+            st_.cfl = 1.0 / 6.0;
         ZSME_CUDA(cudaSetDevice(device_));
         ZSME_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         LaunchConfig lc{128, 128, 128, 128};
@@ -208,6 +214,7 @@ class Solver final : public SolverBase {
         ZSME_CUDA(w_.alloc((size_t)NQ * C));
         ZSME_CUDA(wl_.alloc((size_t)NQ * C));
         ZSME_CUDA(aux_.alloc((size_t)NA * C));
+        if (st_.positivity == ZSME_POSITIVITY_MOOD) ZSME_CUDA(xs_.alloc((size_t)NQ * C));
         ZSME_CUDA(fs_.alloc((size_t)2 * NQ * F));
         ZSME_CUDA(fb_.alloc((size_t)3 * NQ * F));
         // staging for state (NQ per cell) and aux (NA per cell) conversions
@@ -305,6 +312,16 @@ class Solver final : public SolverBase {
     void launch_prep(const double* w, const double* wl, const int* active) {
         mark(ZSME_KERNEL_PREP, true);
         const int gb = blocks_for(pm_.C, lc_.prep);
+        if (st_.positivity != ZSME_POSITIVITY_NONE && st_.reconstruction_order >= 2) {
+            if (pm_.K == 3)
+                prep_wb_kernel<M, 3><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps,
+                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active);
+            else
+                prep_wb_kernel<M, 4><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps,
+                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active);
+            mark(ZSME_KERNEL_PREP, false);
+            return;
+        }
         switch (lc_.prep_occ) {
 #define ZSME_PREP(OCC)                                                                                          \
     case OCC:                                                                                                   \
@@ -429,6 +446,8 @@ class Solver final : public SolverBase {
         mark(ZSME_KERNEL_BEGIN, true);
         begin_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_);
         mark(ZSME_KERNEL_BEGIN, false);
+        const bool mood = st_.positivity == ZSME_POSITIVITY_MOOD;
+        if (mood) cudaMemcpyAsync(xs_.p, x_.p, xs_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
         if (st_.reconstruction_order < 2) {
             launch_prep(x_.p, x_.p, act);
             tape_fs(0);
@@ -455,6 +474,12 @@ class Solver final : public SolverBase {
                 cudaMemcpyAsync(tape + (size_t)s * tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice,
                                 stream_);
         }
+        if (mood) {   // a-posteriori first-order override of troubled cells
+            mark(ZSME_KERNEL_FINALIZE, true);
+            mood_kernel<M, N><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, 0, pm_.C, x_.p, xs_.p, aux_.p,
+                                                                          params_.p, sd);
+            mark(ZSME_KERNEL_FINALIZE, false);
+        }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
         launch_finalize(sd, sd.dt_step, flags);
         mark(ZSME_KERNEL_END, true);
@@ -462,13 +487,14 @@ class Solver final : public SolverBase {
         mark(ZSME_KERNEL_END, false);
     }
     int launches_per_step() const override {
-        return 3 + (st_.reconstruction_order < 2 ? 3 : 3 * st_.ssp_stages);
+        return 3 + (st_.reconstruction_order < 2 ? 3 : 3 * st_.ssp_stages) +
+               (st_.positivity == ZSME_POSITIVITY_MOOD ? 1 : 0);
     }
 
     int step(int nsteps, const double* dts_host) override {
         if (nsteps <= 0) return ZSME_OK;
         if (dts_host && n_inst_ != 1) return set_error(ZSME_ERR_ARG, "imposed dts need a single-instance handle");
-        ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 3 * sizeof(int), stream_));
+        ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 4 * sizeof(int), stream_));
         // x_ is constrained after set_state, update_state and every step (update_variables is a
         // projection: the clamp of a clamped state is that state), so it serves as its own
         // clamped copy; after a bare source() the first step clamps a copy first, uncaptured
@@ -595,6 +621,8 @@ class Solver final : public SolverBase {
             return set_error(ZSME_ERR_ARG, "adjoint: null observation array");
         if (!x_clamped_)
             return set_error(ZSME_ERR_STATE, "adjoint: the state is not constrained (call zsme_update_state)");
+        if (st_.positivity != ZSME_POSITIVITY_NONE)
+            return set_error(ZSME_ERR_ARG, "adjoint: the positivity variants are not differentiated (positivity none only)");
         const int C = pm_.C, F = pm_.F, K = pm_.K, NS = A.nsteps, E = A.every;
         const int s = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
         const size_t nv = (size_t)NQ * C, na = (size_t)NA * C;
@@ -819,7 +847,7 @@ class Solver final : public SolverBase {
             d->n_nonfinite = is[1];
             d->n_negative_depth = is[2];
             d->n_newton_unconverged = is[3];
-            d->reserved = 0;
+            d->n_mood_cells = is[4];
         }
         return ZSME_OK;
     }

@@ -138,50 +138,17 @@ __global__ void __launch_bounds__(128) clamp_kernel(MeshDev m, int c0, int cn, c
 }
 
 // ----------------------------------------------------------------- prep
-// cells [c0, c0 + cn)
-// w: the stage state (its gradient), wl: the same state after update_variables
-// (bounds and reconstruction base; TransportStep.hpp:326-339 clamp a local
-// copy and take the gradient of the unclamped global vector).  The kernel
-// works one component at a time and keeps only the gradient and one running
-// alpha per face in registers: the components meet only in the limiter's
-// alpha = min over components, so a first pass over the components lowers each
-// face's alpha and a second writes q + alpha * delta.  Every sum runs in the
-// reference's order (cone order for the bounds and least squares, original
-// face order for Green-Gauss), so the result is that of the whole-vector form.
-// MINB: resident blocks per SM the register allocation must allow (1 = no cap)
-// KM: face slots per cell, 3 = exactly three (triangles), 4 = up to four
-template <class M, int MINB, int KM>
-__global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int c0, int cn, const double* __restrict__ w,
-                                                   const double* __restrict__ wl, const double* __restrict__ aux,
-                                                   const double* __restrict__ params, double* __restrict__ fs,
-                                                   const int* __restrict__ active) {
-    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, DIM = M::dimension;
+// The cell's slots in cone order (neighbour, face, side of the face, face
+// centroid - cell centroid) and the gradient of the unclamped stage state w:
+// least squares in cone order (Gradient.hpp:330-346) or Green-Gauss in
+// increasing original face order (Gradient.hpp:91-176), / volume.
+template <class M, int KM>
+__device__ __forceinline__ void cell_slots_gradient(const MeshDev& m, const Opts& o, int c, int K,
+                                                    const double* __restrict__ w, const double* p, int (&nb)[KM],
+                                                    int (&ff)[KM], int (&sd)[KM], double (&dx)[KM][M::dimension],
+                                                    double (&g)[M::n_dof_q * M::dimension]) {
+    constexpr int NQ = M::n_dof_q, DIM = M::dimension;
     const int C = m.C, F = m.F;
-    const int K = KM == 3 ? 3 : m.K;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= cn) return;
-    const int c = c0 + r;
-    const int I = cell_instance(m, c);
-    if (active && !active[I]) return;
-    const double* p = params + (size_t)I * m.np;
-    if (o.order < 2) {
-        double ql[NQ], a[NA];
-        load_q<NQ>(w, C, c, ql);
-#pragma unroll
-        for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
-        clamp_q<M>(ql, a, p);
-        for (int k = 0; k < K; ++k) {
-            const int f = m.slot_face[k * C + c];
-            if (f < 0) continue;
-            const int side = meta_isL(m.slot_meta[k * C + c]) ? 0 : 1;
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) fs[((size_t)side * NQ + i) * F + f] = ql[i];
-        }
-        return;
-    }
-    // the cell's slots in cone order
-    int nb[KM], ff[KM], sd[KM];
-    double dx[KM][DIM];
 #pragma unroll
     for (int k = 0; k < KM; ++k) {
         nb[k] = -2;
@@ -198,7 +165,6 @@ __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int 
         }
     }
     // gradient of the unclamped stage state
-    double g[NQ * DIM];
 #pragma unroll
     for (int i = 0; i < NQ * DIM; ++i) g[i] = 0.0;
     if (o.gradient == 1) {
@@ -258,6 +224,52 @@ __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int 
             for (int i = 0; i < NQ * DIM; ++i) g[i] /= v;
         }
     }
+}
+
+// cells [c0, c0 + cn)
+// w: the stage state (its gradient), wl: the same state after update_variables
+// (bounds and reconstruction base; TransportStep.hpp:326-339 clamp a local
+// copy and take the gradient of the unclamped global vector).  The kernel
+// works one component at a time and keeps only the gradient and one running
+// alpha per face in registers: the components meet only in the limiter's
+// alpha = min over components, so a first pass over the components lowers each
+// face's alpha and a second writes q + alpha * delta.  Every sum runs in the
+// reference's order (cone order for the bounds and least squares, original
+// face order for Green-Gauss), so the result is that of the whole-vector form.
+// MINB: resident blocks per SM the register allocation must allow (1 = no cap)
+// KM: face slots per cell, 3 = exactly three (triangles), 4 = up to four
+template <class M, int MINB, int KM>
+__global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int c0, int cn, const double* __restrict__ w,
+                                                   const double* __restrict__ wl, const double* __restrict__ aux,
+                                                   const double* __restrict__ params, double* __restrict__ fs,
+                                                   const int* __restrict__ active) {
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, DIM = M::dimension;
+    const int C = m.C, F = m.F;
+    const int K = KM == 3 ? 3 : m.K;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    const int I = cell_instance(m, c);
+    if (active && !active[I]) return;
+    const double* p = params + (size_t)I * m.np;
+    if (o.order < 2) {
+        double ql[NQ], a[NA];
+        load_q<NQ>(w, C, c, ql);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
+        clamp_q<M>(ql, a, p);
+        for (int k = 0; k < K; ++k) {
+            const int f = m.slot_face[k * C + c];
+            if (f < 0) continue;
+            const int side = meta_isL(m.slot_meta[k * C + c]) ? 0 : 1;
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) fs[((size_t)side * NQ + i) * F + f] = ql[i];
+        }
+        return;
+    }
+    int nb[KM], ff[KM], sd[KM];
+    double dx[KM][DIM], g[NQ * DIM];
+    cell_slots_gradient<M, KM>(m, o, c, K, w, p, nb, ff, sd, dx, g);
     // pass 1: each face's alpha = min over components of min(vacuum, tvd)
     // (Reconstruction.hpp:25-36, 62-81, 224-238); "<" ignores NaN as there
     double al[KM];
@@ -328,6 +340,254 @@ __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int 
             fs[((size_t)sd[k] * NQ + i) * F + ff[k]] = q + al[k] * d;
         }
     }
+}
+
+// Venkatakrishnan eps^2 = vol^(2/dim) (TransportStep.hpp:279), exact in 1-D and 2-D.
+template <int DIM>
+__host__ __device__ __forceinline__ double venkat_eps2(double v) {
+    if constexpr (DIM == 2) return v;
+    else if constexpr (DIM == 1) return v * v;
+    else return pow(v, 2.0 / DIM);
+}
+
+// ---------------------------------------------------- prep, positivity variants
+// Order-2 face states of the positivity variants (zhang_shu, mood), cells
+// [c0, c0 + cn), layout [b, h, momenta...]:
+// 1. the raw gradient of the unclamped stage state w, as prep_kernel;
+// 2. TransportStep::LimitGradientsWB (TransportStep.hpp:241-323): per W
+//    component (b, eta = b + h, momenta; from the clamped state wl) the
+//    Venkatakrishnan factor phi = min over the cell's faces, phi = 0 in dry
+//    cells (h < wet_dry_eps), b and momentum factors capped by eta's, the
+//    Zhang-Shu theta from the smallest face depth of the depth deviation
+//    sh = phi_eta grad eta - phi_b grad b (theta = 1 under MOOD), and the
+//    effective gradients phi_b grad b, phi_b grad b + theta sh, theta phi grad m;
+// 3. WBPositivityReconstructor::Reconstruct (Reconstruction.hpp:264-286) at
+//    each face: b_f, eta_f from the effective gradients, h_f = max(eta_f - b_f, 0),
+//    momenta zero where h_f < wet_dry_eps.
+// std::min / std::max are written out as the selects they are, so NaN
+// propagates as in the reference.  positivity: ZSME_POSITIVITY_ZHANG_SHU or
+// _MOOD (no theta); eps: wet_dry_eps.
+template <class M, int KM>
+__global__ void __launch_bounds__(128) prep_wb_kernel(MeshDev m, Opts o, int positivity, double eps, int c0, int cn,
+                                                      const double* __restrict__ w, const double* __restrict__ wl,
+                                                      const double* __restrict__ params, double* __restrict__ fs,
+                                                      const int* __restrict__ active) {
+    constexpr int NQ = M::n_dof_q, DIM = M::dimension;
+    constexpr int B = 0, H = 1;
+    const int C = m.C, F = m.F;
+    const int K = KM == 3 ? 3 : m.K;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    const int I = cell_instance(m, c);
+    if (active && !active[I]) return;
+    const double* p = params + (size_t)I * m.np;
+    int nb[KM], ff[KM], sd[KM];
+    double dx[KM][DIM], g[NQ * DIM];
+    cell_slots_gradient<M, KM>(m, o, c, K, w, p, nb, ff, sd, dx, g);
+    double geta[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) geta[d] = g[H * DIM + d] + g[B * DIM + d];
+    const double h_bar = wl[(size_t)H * C + c], b_bar = wl[(size_t)B * C + c];
+    const double eps2 = venkat_eps2<DIM>(m.vol[c]);
+    double phi[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        const double wc = i == H ? (b_bar + h_bar) : wl[(size_t)i * C + c];
+        double wmn = wc, wmx = wc;
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (nb[k] < 0) continue;
+            const int n = nb[k];
+            const double wn = i == H ? (wl[(size_t)B * C + n] + wl[(size_t)H * C + n]) : wl[(size_t)i * C + n];
+            if (wn < wmn) wmn = wn;
+            if (wn > wmx) wmx = wn;
+        }
+        double ph = 1.0;
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (ff[k] < 0) continue;
+            double delta = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) delta += (i == H ? geta[d] : g[i * DIM + d]) * dx[k][d];
+            if (fabs(delta) < 1e-14) continue;
+            const double dm = (delta > 0) ? (wmx - wc) : (wmn - wc);
+            const double num = dm * dm + eps2 + 2 * delta * dm;
+            const double den = dm * dm + 2 * delta * delta + delta * dm + eps2;
+            double pf = (den > 1e-30) ? num / den : 1.0;
+            pf = (pf < 1.0) ? pf : 1.0;   // std::min(1, pf)
+            pf = (0.0 < pf) ? pf : 0.0;   // std::max(0, pf)
+            if (pf < ph) ph = pf;
+        }
+        phi[i] = ph;
+    }
+    if (h_bar < eps) {
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) phi[i] = 0.0;
+    }
+    phi[B] = (phi[H] < phi[B]) ? phi[H] : phi[B];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i)
+        if (i != B && i != H) phi[i] = (phi[H] < phi[i]) ? phi[H] : phi[i];
+    double sh[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) sh[d] = phi[H] * geta[d] - phi[B] * g[B * DIM + d];
+    double hmin = h_bar;
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        if (ff[k] < 0) continue;
+        double hf = h_bar;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) hf += sh[d] * dx[k][d];
+        if (hf < hmin) hmin = hf;
+    }
+    double theta = 1.0;
+    if (positivity != ZSME_POSITIVITY_MOOD && hmin < 0.0) {
+        const double gap = h_bar - hmin;
+        double th = h_bar / ((gap < 1e-14) ? 1e-14 : gap);
+        th = (th < 1.0) ? th : 1.0;
+        theta = (0.0 < th) ? th : 0.0;
+    }
+    // effective gradients in place: b slot grad b_eff, h slot grad eta_eff
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const double gb = g[B * DIM + d];
+        g[B * DIM + d] = phi[B] * gb;
+        g[H * DIM + d] = phi[B] * gb + theta * sh[d];
+    }
+#pragma unroll
+    for (int i = 0; i < NQ; ++i)
+        if (i != B && i != H)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) g[i * DIM + d] = theta * phi[i] * g[i * DIM + d];
+    // face states
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        if (ff[k] < 0) continue;
+        double* out = fs + (size_t)sd[k] * NQ * F + ff[k];
+        double db = 0.0, de = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) db += g[B * DIM + d] * dx[k][d];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) de += g[H * DIM + d] * dx[k][d];
+        const double b_f = b_bar + db;
+        const double eta_f = (b_bar + h_bar) + de;
+        const double hd = eta_f - b_f;
+        const double h_f = (hd < 0.0) ? 0.0 : hd;
+        out[(size_t)B * F] = b_f;
+        out[(size_t)H * F] = h_f;
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) {
+            if (i == B || i == H) continue;
+            double di = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) di += g[i * DIM + d] * dx[k][d];
+            out[(size_t)i * F] = (h_f < eps) ? 0.0 : (wl[(size_t)i * C + c] + di);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ MOOD
+// Local MOOD (MUSCLSolver.hpp:150-170, 197-229; TransportStep.hpp:363-381,
+// 412-418), cells [c0, c0 + cn): a cell whose depth after the transport step
+// is below -1e-10 is overwritten by its first-order forward-Euler update from
+// the step's start state xs -- piecewise-constant clamped states on every
+// face of the cell, the face contributions summed in increasing original
+// face order, / volume -- and counted in diag[3].  No other cell changes, so
+// each troubled cell evaluates its own faces and no face pass is needed.
+// Launched between the last stage and finalize, whose constraints follow
+// the override as EnforcePhysicalConstraints does.
+template <class M, class N>
+__global__ void __launch_bounds__(128) mood_kernel(MeshDev m, int c0, int cn, double* __restrict__ x,
+                                                   const double* __restrict__ xs, const double* __restrict__ aux,
+                                                   const double* __restrict__ params, StepDev sd) {
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
+    const int C = m.C, F = m.F;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    const int I = cell_instance(m, c);
+    if (sd.active && !sd.active[I]) return;
+    if (!(x[C + c] < -1.0e-10)) return;
+    atomicAdd(&sd.diag[3], 1);
+    const double* p = params + (size_t)I * m.np;
+    const double t = sd.t[I], h = sd.dt_step[I];
+    double qc[NQ], ac[NA];
+    load_q<NQ>(xs, C, c, qc);
+#pragma unroll
+    for (int i = 0; i < NA; ++i) ac[i] = aux[(size_t)i * C + c];
+    clamp_q<M>(qc, ac, p);
+    double acc[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) acc[i] = 0.0;
+    const int ord = m.order[c];
+    for (int j = 0; j < m.K; ++j) {
+        const int k = (ord >> (2 * j)) & 3;
+        const int f = m.slot_face[k * C + c];
+        if (f < 0) continue;
+        const int meta = m.slot_meta[k * C + c];
+        const int n = m.slot_nbr[k * C + c];
+        if (n < 0 && meta_bc(meta) < 0) continue;
+        const double area = m.farea[f];
+        const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
+        const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
+        if (n >= 0) {
+            double qn[NQ], an[NA];
+            load_q<NQ>(xs, C, n, qn);
+#pragma unroll
+            for (int i = 0; i < NA; ++i) an[i] = aux[(size_t)i * C + n];
+            clamp_q<M>(qn, an, p);
+            const bool isL = meta_isL(meta);
+            const double* qL = isL ? qc : qn;
+            const double* qR = isL ? qn : qc;
+            double aL[NA], aR[NA];
+            {
+                auto ra = M::update_aux_variables(qL, isL ? ac : an, p, 0.0, xf);
+                auto rb = M::update_aux_variables(qR, isL ? an : ac, p, 0.0, xf);
+#pragma unroll
+                for (int i = 0; i < NA; ++i) { aL[i] = ra[i]; aR[i] = rb[i]; }
+            }
+            const auto flux = N::numerical_flux(qL, qR, aL, aR, p, nh);
+            const auto nc = N::numerical_fluctuations(qL, qR, aL, aR, p, nh);
+            if (isL) {
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] -= nc[NQ + i] * area;
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] -= flux[i] * area;
+            } else {
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] -= nc[i] * area;
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] += flux[i] * area;
+            }
+        } else {
+            double aL[NA], aR[NA];
+            {
+                auto ra = M::update_aux_variables(qc, ac, p, t, xf);
+#pragma unroll
+                for (int i = 0; i < NA; ++i) aL[i] = ra[i];
+            }
+            const auto qR = M::boundary_conditions(meta_bc(meta), qc, aL, p, nh, xf, t, 0.0);
+            {
+                auto rb = M::update_aux_variables(qR.data, aL, p, t, xf);
+#pragma unroll
+                for (int i = 0; i < NA; ++i) aR[i] = rb[i];
+            }
+            const auto flux = N::numerical_flux(qc, qR.data, aL, aR, p, nh);
+            const auto nc = N::numerical_fluctuations(qc, qR.data, aL, aR, p, nh);
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= nc[NQ + i] * area;
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= flux[i] * area;
+        }
+    }
+    const double v = m.vol[c];
+    if (v > 1e-15) {
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) acc[i] /= v;
+    }
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) x[(size_t)i * C + c] = xs[(size_t)i * C + c] + h * acc[i];
 }
 
 // --------------------------------------------------------------- step ends

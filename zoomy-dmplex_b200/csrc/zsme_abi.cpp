@@ -86,6 +86,8 @@ int zsme_create(const char* model, const zsme_mesh* mesh, const zsme_settings* s
     if (settings->reconstruction_order < 1 || settings->reconstruction_order > 2)
         return set_error(ZSME_ERR_ARG, "reconstruction_order must be 1 or 2");
     if (!(settings->cfl > 0)) return set_error(ZSME_ERR_ARG, "cfl must be > 0");
+    if (settings->positivity < ZSME_POSITIVITY_NONE || settings->positivity > ZSME_POSITIVITY_MOOD)
+        return set_error(ZSME_ERR_ARG, "positivity must be ZSME_POSITIVITY_NONE, _ZHANG_SHU or _MOOD");
     zsme::PreparedMesh pm;
     int rc = zsme::prepare_mesh(*mesh, pm);
     if (rc) return rc;
@@ -215,6 +217,8 @@ int zsme_batch_create(const char* model, int32_t n, const zsme_mesh* meshes, con
     if (settings->reconstruction_order < 1 || settings->reconstruction_order > 2)
         return set_error(ZSME_ERR_ARG, "reconstruction_order must be 1 or 2");
     if (!(settings->cfl > 0)) return set_error(ZSME_ERR_ARG, "cfl must be > 0");
+    if (settings->positivity < ZSME_POSITIVITY_NONE || settings->positivity > ZSME_POSITIVITY_MOOD)
+        return set_error(ZSME_ERR_ARG, "positivity must be ZSME_POSITIVITY_NONE, _ZHANG_SHU or _MOOD");
     std::vector<zsme::PreparedMesh> parts(n);
     for (int i = 0; i < n; ++i) {
         int rc = zsme::prepare_mesh(meshes[i], parts[i]);

@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(PKG, "libzsme.so")
 
 ZSME_LIMITER_NONE, ZSME_LIMITER_TVD = 0, 1
 ZSME_GRADIENT_GREEN_GAUSS, ZSME_GRADIENT_LSQ = 0, 1
+ZSME_POSITIVITY_NONE, ZSME_POSITIVITY_ZHANG_SHU, ZSME_POSITIVITY_MOOD = 0, 1, 2
+POSITIVITY = {"none": ZSME_POSITIVITY_NONE, "zhang_shu": ZSME_POSITIVITY_ZHANG_SHU, "mood": ZSME_POSITIVITY_MOOD}
 KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step", "gather")
 
 
@@ -32,14 +34,14 @@ class ZsmeSettings(ct.Structure):
         ("cfl", ct.c_double), ("t_end", ct.c_double), ("min_dt", ct.c_double),
         ("reconstruction_order", ct.c_int32), ("limiter", ct.c_int32), ("gradient", ct.c_int32),
         ("ssp_stages", ct.c_int32), ("source", ct.c_int32), ("block_size", ct.c_int32),
-        ("reserved", ct.c_int32 * 6),
+        ("positivity", ct.c_int32), ("reserved", ct.c_int32 * 5), ("wet_dry_eps", ct.c_double),
     ]
 
 
 class ZsmeDiag(ct.Structure):
     _fields_ = [
         ("steps", ct.c_int64), ("time", ct.c_double), ("dt", ct.c_double), ("n_nonfinite", ct.c_int32),
-        ("n_negative_depth", ct.c_int32), ("n_newton_unconverged", ct.c_int32), ("reserved", ct.c_int32),
+        ("n_negative_depth", ct.c_int32), ("n_newton_unconverged", ct.c_int32), ("n_mood_cells", ct.c_int32),
     ]
 
 

@@ -18,7 +18,10 @@ How the reference interprets the strings, and so how they map here:
   (``MUSCLSolver.hpp:43``, ``Reconstruction.hpp:170-175``);
 * ``time_integration``: ``"splitting"`` (explicit transport + implicit source)
   is the only strategy of this path; ``"imex"``/``"implicit"`` are rejected;
-* ``positivity``: ``"none"`` only (``"zhang_shu"``/``"mood"`` are rejected).
+* ``positivity``: ``"none"`` (limited linear reconstruction), ``"zhang_shu"``
+  or ``"mood"`` (the eta-well-balanced reconstruction with the Zhang-Shu
+  theta, or with the a-posteriori first-order override of cells that end
+  with negative depth), with ``wet_dry_eps`` the dry threshold.
 """
 from __future__ import annotations
 
@@ -47,8 +50,8 @@ class SolverSettings:
         if self.time_integration != "splitting":
             raise ValueError("time_integration %r is not on this path (only 'splitting')"
                              % self.time_integration)
-        if self.positivity != "none":
-            raise ValueError("positivity %r is not supported (only 'none')" % self.positivity)
+        if self.positivity not in native.POSITIVITY:
+            raise ValueError("positivity must be one of %s" % sorted(native.POSITIVITY))
         if self.gradient not in ("least_squares", "green_gauss"):
             raise ValueError("gradient must be 'least_squares' or 'green_gauss'")
         if self.reconstruction_order >= 2 and self.ssp_stages < 2:
@@ -62,6 +65,8 @@ class SolverSettings:
         s.ssp_stages = int(self.ssp_stages)
         s.source = 1
         s.block_size = int(self.block_size)
+        s.positivity = native.POSITIVITY[self.positivity]
+        s.wet_dry_eps = float(self.wet_dry_eps)
         return s
 
 
