@@ -47,8 +47,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--side", type=int, default=1400, help="jittered grid side of the mesh")
-    ap.add_argument("--cpu-side", type=int, default=300, help="grid side of the bounded CPU sample")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-side", type=int, default=600, help="grid side of the bounded CPU sample")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="the CPU sample steps until this much time has passed")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch configuration")
@@ -60,7 +61,13 @@ def parse():
     ap.add_argument("--adj-steps", type=int, default=400, help="steps of the adjoint workload")
     ap.add_argument("--adj-limiter", default="tvd", choices=["tvd", "none"], help="limiter of the adjoint workload")
     ap.add_argument("--adj-fd", type=int, default=32, help="finite-difference directions of the adjoint check (0: none)")
+    ap.add_argument("--positivity", default="none", choices=["none", "zhang_shu", "mood"],
+                    help="positivity variant of the roofline workload")
     return ap.parse_args()
+
+
+POS_TEXT = {"none": "", "zhang_shu": ", eta-well-balanced reconstruction + Zhang-Shu theta (CFL clamped to 1/6)",
+            "mood": ", eta-well-balanced reconstruction + local MOOD"}
 
 
 # ------------------------------------------------------------------ roofline
@@ -165,22 +172,28 @@ def params_of(case):
     return np.array(vals)
 
 
-def cpu_sample(side, steps, warm=1):
+def cpu_sample(side, steps=0, warm=1, seconds=0.0, positivity="none"):
     """The oracle (CPU restatement of the reference step) on a bounded
-    sample of the workload: same model and physics on a side x side mesh."""
+    sample of the workload: same model and physics on a side x side mesh,
+    `steps` steps, or (steps = 0) one step at a time until `seconds` have
+    passed.  Returns (cell-steps/s, threads, cells, seconds, steps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
     from zoomy_dmplex_b200 import cases
 
     c = cases.roofline_l4(side)
+    c.settings.positivity = positivity
     nt = O.set_threads(0)
     o = O.Oracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), params_of(c))
     o.set_state(c.q0)
     o.step(warm)
     t0 = time.perf_counter()
-    o.step(steps)
+    n = 0
+    while (n < steps) if steps else (n == 0 or time.perf_counter() - t0 < seconds):
+        o.step(1)
+        n += 1
     dt = time.perf_counter() - t0
-    return c.mesh.n_cells * steps / dt, nt, c.mesh.n_cells, dt
+    return c.mesh.n_cells * n / dt, nt, c.mesh.n_cells, dt, n
 
 
 def run_ensemble(a, dev, torch, dist, rank, world):
@@ -339,7 +352,7 @@ def run_ensemble(a, dev, torch, dist, rank, world):
                     "api": "zsme_batch_set_state x n (pinned host) + zsme_step(1) + zsme_batch_get_state x n"},
             "gpu_launches": launches,
             "diag": {"nonfinite": diag.n_nonfinite, "negative_depth": diag.n_negative_depth,
-                     "newton_unconverged": diag.n_newton_unconverged},
+                     "newton_unconverged": diag.n_newton_unconverged, "mood_cells": diag.n_mood_cells},
             "clocks": clocks}
     if rank == 0:
         print(json.dumps(line))
@@ -491,7 +504,7 @@ def main():
         if rank != 0:
             return 0
         # warmup + K timed oracle steps on the bounded sample
-        v, nt, C, dt = cpu_sample(a.cpu_side, max(1, a.steps), warm=max(1, a.warmup))
+        v, nt, C, dt, _ = cpu_sample(a.cpu_side, max(1, a.steps), warm=max(1, a.warmup), positivity=a.positivity)
         line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / max(1, a.steps),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -527,6 +540,7 @@ def main():
         return run_adjoint(a, dev, torch, dist, rank, world)
 
     case = cases.roofline_l4(a.side)
+    case.settings.positivity = a.positivity
     C, F = case.mesh.n_cells, case.mesh.n_faces
     g = Solver(case.model, case.mesh, case.settings, params_of(case), device=dev)
     g.set_state(case.q0)
@@ -583,7 +597,7 @@ def main():
     dom_ms = prof[dom][0] / prof[dom][1]
     alg = algorithmic_bytes(dom, C, F, nq, na, case.mesh.max_faces, case.settings.ssp_stages)
     achieved = alg / (dom_ms / 1e3) / 1e9
-    traffic = NCU_DRAM_BYTES_PER_CELL.get("%s/%s" % (case.model, dom))
+    traffic = NCU_DRAM_BYTES_PER_CELL.get("%s/%s" % (case.model, dom)) if a.positivity == "none" else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": alg,
@@ -632,8 +646,8 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "sme2d_l4 SME level 4, jittered-Delaunay %dx%d grid (%d cells, %d faces), "
                                    "Hilbert-renumbered, order 2 Green-Gauss + Vacuum/TVD, SSP-RK2, CFL 0.45, "
-                                   "Navier-slip Newton source" % (a.side, a.side, C, F),
-                       "model": case.model, "cells": C, "faces": F, "n_dof_q": nq,
+                                   "Navier-slip Newton source%s" % (a.side, a.side, C, F, POS_TEXT[a.positivity]),
+                       "model": case.model, "cells": C, "faces": F, "n_dof_q": nq, "positivity": a.positivity,
                        "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
                        "l2_flush": "not needed: state %.0f MB + face states %.0f MB > 126 MB L2"
                                    % (C * nq * 8 / 1e6, C * nq * 3 * 8 / 1e6),
@@ -645,13 +659,13 @@ def main():
                     "steps": ne, "api": "zsme_set_state(pinned host) + zsme_step(1) + zsme_get_state(pinned host)"},
             "gpu_launches": a.steps * g.launches_per_step(),
             "diag": {"nonfinite": diag.n_nonfinite, "negative_depth": diag.n_negative_depth,
-                     "newton_unconverged": diag.n_newton_unconverged},
+                     "newton_unconverged": diag.n_newton_unconverged, "mood_cells": diag.n_mood_cells},
             "clocks": clocks}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        v, nt, Cs, dts = cpu_sample(a.cpu_side, a.cpu_steps)
+        v, nt, Cs, dts, ns = cpu_sample(a.cpu_side, seconds=a.cpu_seconds, positivity=a.positivity)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
                                 "sample": "%d steps of the CPU restatement (oracle) of the same model on a "
-                                          "%dx%d-grid mesh (%d cells), %.1f s" % (a.cpu_steps, a.cpu_side,
+                                          "%dx%d-grid mesh (%d cells), %.1f s" % (ns, a.cpu_side,
                                                                                  a.cpu_side, Cs, dts)}
     if rank == 0:
         print(json.dumps(line))
