@@ -259,47 +259,35 @@ def interval(x: np.ndarray, name="interval", bc_left=0, bc_right=0) -> Mesh:
                 fcent, normal, bc, name=name)
 
 
-# ---------------------------------------------------------------------------
-# gmsh 2.2 ASCII (the format of the reference's meshes, make_bump_case.py)
-# ---------------------------------------------------------------------------
-def write_msh(path: str, mesh: Mesh):
-    V = mesh.vertices.shape[0]
-    with open(path, "w") as f:
-        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % V)
-        for i, (x, y) in enumerate(mesh.vertices):
-            f.write("%d %.17g %.17g 0.0\n" % (i + 1, x, y))
-        f.write("$EndNodes\n$Elements\n%d\n" % mesh.n_cells)
-        etype = 2 if mesh.dim == 2 else 1
-        for i, c in enumerate(mesh.cells):
-            f.write("%d %d 2 1 1 %s\n" % (i + 1, etype, " ".join(str(int(v) + 1) for v in c)))
-        f.write("$EndElements\n")
+def face_vertices(mesh: Mesh) -> np.ndarray:
+    """Vertex ids of each face: [F, 2] (lower id first) in 2-D, [F] in 1-D.
+    A cell's local face k is its edge (v_k, v_k+1), or its vertex v_k in 1-D."""
+    C, K = mesh.cell_faces.shape
+    f = mesh.cell_faces.reshape(-1)
+    c = np.repeat(np.arange(C), K)
+    k = np.tile(np.arange(K), C)
+    a = mesh.cells[c, k].astype(np.int64)
+    if mesh.dim == 1:
+        out = np.empty(mesh.n_faces, dtype=np.int64)
+        out[f] = a
+        return out
+    b = mesh.cells[c, (k + 1) % K].astype(np.int64)
+    out = np.empty((mesh.n_faces, 2), dtype=np.int64)
+    out[f, 0] = np.minimum(a, b)
+    out[f, 1] = np.maximum(a, b)
+    return out
 
 
-def read_msh(path: str, boundary_bc=0) -> Mesh:
-    """Read a gmsh 2.2 ASCII mesh (triangles, or segments for 1-D)."""
-    with open(path) as f:
-        lines = [ln.strip() for ln in f]
-    i = lines.index("$Nodes")
-    nv = int(lines[i + 1])
-    ids, xy = [], []
-    for ln in lines[i + 2: i + 2 + nv]:
-        t = ln.split()
-        ids.append(int(t[0]))
-        xy.append((float(t[1]), float(t[2])))
-    idmap = {v: k for k, v in enumerate(ids)}
-    xy = np.array(xy)
-    i = lines.index("$Elements")
-    ne = int(lines[i + 1])
-    tris, segs = [], []
-    for ln in lines[i + 2: i + 2 + ne]:
-        t = [int(v) for v in ln.split()]
-        et, nt = t[1], t[2]
-        nodes = [idmap[v] for v in t[3 + nt:]]
-        if et == 2:
-            tris.append(nodes)
-        elif et == 1:
-            segs.append(nodes)
-    if tris:
-        return from_triangles(xy, np.array(tris), name=path, boundary_bc=boundary_bc)
-    xs = np.unique(xy[np.array(segs).reshape(-1), 0])
-    return interval(xs, name=path, bc_left=boundary_bc, bc_right=boundary_bc)
+# ---------------------------------------------------------------------------
+# gmsh 2.2 ASCII (the format of the reference's meshes): see caseio
+# ---------------------------------------------------------------------------
+def write_msh(path: str, mesh: Mesh, **kw):
+    from .caseio import write_gmsh
+
+    write_gmsh(path, mesh, **kw)
+
+
+def read_msh(path: str, boundary_tags=("default",)) -> Mesh:
+    from .caseio import read_gmsh
+
+    return read_gmsh(path, boundary_tags)

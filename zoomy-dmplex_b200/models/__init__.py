@@ -32,3 +32,11 @@ def constants(model: str):
     for k in ("n_dof_q", "n_dof_qaux", "n_parameters", "dimension"):
         out[k] = int(re.search(r"static constexpr int %s\s*=\s*(\d+);" % k, src).group(1))
     return out
+
+
+def boundary_tags(model: str):
+    """The model's boundary tag names (Model::get_boundary_tags), in bc-index order."""
+    with open(header_path(model)) as f:
+        src = f.read()
+    body = re.search(r"get_boundary_tags\(\) \{ return \{ (.*?) \}; \}", src).group(1)
+    return [t.strip().strip('"') for t in body.split(",")]
