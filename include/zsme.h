@@ -173,7 +173,9 @@ int zsme_launches_per_step(zsme_handle* h, int32_t* n);
 #define ZSME_KERNEL_FINALIZE 3  /* constraints + source + CFL partials */
 #define ZSME_KERNEL_END 4       /* dt reduction + time advance */
 #define ZSME_KERNEL_GATHER 5    /* per-cell sum of face contributions + stage update */
-#define ZSME_KERNEL_KINDS 6
+#define ZSME_KERNEL_FALLBACK 6  /* finalize of the cells whose Newton update needs the full-size GEPP */
+#define ZSME_KERNEL_MOOD 7      /* MOOD first-order override (ZSME_POSITIVITY_MOOD) */
+#define ZSME_KERNEL_KINDS 8
 int zsme_set_profiling(zsme_handle* h, int enable);
 /* ms[ZSME_KERNEL_KINDS]: summed milliseconds; n[...]: launches. */
 int zsme_read_profile(zsme_handle* h, double* ms, int64_t* n);

@@ -209,3 +209,21 @@ def test_device_pointer_state_roundtrip():
     g.get_state_device(out.data_ptr())
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), g.get_state())
+
+
+def test_profile_kinds_per_step():
+    """Per-kernel timing attributes every launch of a step to its own kind:
+    two SSP stages (prep, flux, gather each), finalize and its fallback, the
+    step ends; launches_per_step counts the same kernels."""
+    c = CASES["l2"]
+    g, _ = pair(c)
+    g.set_profiling(True)
+    g.step(2)
+    g.sync()
+    prof = g.read_profile()
+    g.set_profiling(False)
+    n = {k: v[1] for k, v in prof.items()}
+    assert n == {"begin_step": 2, "prep": 4, "flux": 4, "finalize": 2, "end_step": 2, "gather": 4,
+                 "finalize_fallback": 2, "mood": 0}
+    assert all(v[0] > 0 for k, v in prof.items() if n[k])
+    assert g.launches_per_step() == sum(n.values()) // 2

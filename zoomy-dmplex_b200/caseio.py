@@ -253,7 +253,8 @@ def write_vtu(path: str, mesh: Mesh, q: np.ndarray, aux: Optional[np.ndarray] = 
 
 
 def read_vtu_cell_data(path: str) -> Dict[str, np.ndarray]:
-    """The cell data arrays of a file written by write_vtu ([C, ncomp] each)."""
+    """The binary arrays of a file written by write_vtu by name; arrays with a
+    component count come back as [n, ncomp] (cell data "Q", "Aux", points)."""
     root = ET.parse(path).getroot()
     out = {}
     for a in root.iter("DataArray"):
@@ -263,8 +264,8 @@ def read_vtu_cell_data(path: str) -> Dict[str, np.ndarray]:
         n = int(np.frombuffer(raw[:8], dtype=np.uint64)[0])
         dt = {"Float64": np.float64, "Int64": np.int64, "UInt8": np.uint8}[a.get("type")]
         v = np.frombuffer(raw[8: 8 + n], dtype=dt)
-        nc = int(a.get("NumberOfComponents", "1"))
-        out[a.get("Name")] = v.reshape(-1, nc) if nc > 1 else v
+        nc = a.get("NumberOfComponents")
+        out[a.get("Name")] = v.reshape(-1, int(nc)) if nc is not None else v
     return out
 
 

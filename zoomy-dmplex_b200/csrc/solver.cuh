@@ -75,7 +75,9 @@ class Solver final : public SolverBase {
     DevBuf<double> xs_;  // MOOD: the state at the start of the step
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
-    DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag
+    DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag, [5] deferred finalize cells
+    DevBuf<int> fin_list_;        // [C] cells deferred to the generic Newton path
+    int sm_count_ = 148;
     DevBuf<unsigned long long> ratio_;
     // discrete adjoint (allocated by the first zsme_adjoint call)
     DevBuf<double> adj_ck_x_, adj_ck_a_, adj_tape_, adj_lam0_, adj_lam1_, adj_lam2_, adj_own_w_, adj_own_wl_;
@@ -226,6 +228,8 @@ class Solver final : public SolverBase {
             ZSME_CUDA(b->alloc(n_inst_));
             ZSME_CUDA(cudaMemsetAsync(b->p, 0, n_inst_ * sizeof(double), stream_));
         }
+        ZSME_CUDA(fin_list_.alloc((size_t)C));
+        ZSME_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
         ZSME_CUDA(active_.alloc(n_inst_));
         ZSME_CUDA(cudaMemsetAsync(active_.p, 0, n_inst_ * sizeof(int), stream_));
         ZSME_CUDA(iscal_.alloc(8));
@@ -245,7 +249,7 @@ class Solver final : public SolverBase {
 
     StepDev step_dev(const double* dts) {
         return StepDev{t_.p, dt_cfl_.p, dt_step_.p, active_.p, ratio_.p, dts, iscal_.p + 0, n_inst_,
-                       st_.t_end, st_.cfl, M::dt_max, iscal_.p + 1};
+                       st_.t_end, st_.cfl, M::dt_max, iscal_.p + 1, fin_list_.p, iscal_.p + 5};
     }
 
     int set_params(const double* params) override {
@@ -361,6 +365,8 @@ class Solver final : public SolverBase {
     }
     void finalize_range(int c0, int cn, const StepDev& sd, const double* dt_src, int flags) {
         const int gb = blocks_for(cn, lc_.finalize);
+        if (flags & FIN_SOURCE) cudaMemsetAsync(sd.n_fallback, 0, sizeof(int), stream_);
+        mark(ZSME_KERNEL_FINALIZE, true);
         switch (lc_.finalize_occ) {
 #define ZSME_FIN(OCC)                                                                                            \
     case OCC:                                                                                                    \
@@ -371,11 +377,16 @@ class Solver final : public SolverBase {
             default: ZSME_FIN(1)
 #undef ZSME_FIN
         }
+        mark(ZSME_KERNEL_FINALIZE, false);
+        if (flags & FIN_SOURCE) {   // the cells whose Newton update needs the generic GEPP (usually none)
+            mark(ZSME_KERNEL_FALLBACK, true);
+            finalize_fallback_kernel<M, N><<<std::min(blocks_for(cn, 64), 8 * sm_count_), 64, 0, stream_>>>(
+                md_, x_.p, aux_.p, params_.p, sd, dt_src, flags);
+            mark(ZSME_KERNEL_FALLBACK, false);
+        }
     }
     void launch_finalize(const StepDev& sd, const double* dt_src, int flags) {
-        mark(ZSME_KERNEL_FINALIZE, true);
         finalize_range(0, pm_.C, sd, dt_src, flags);
-        mark(ZSME_KERNEL_FINALIZE, false);
     }
 
     int rhs(double t, const double* x_aos, double* f_aos) override {
@@ -475,10 +486,10 @@ class Solver final : public SolverBase {
                                 stream_);
         }
         if (mood) {   // a-posteriori first-order override of troubled cells
-            mark(ZSME_KERNEL_FINALIZE, true);
+            mark(ZSME_KERNEL_MOOD, true);
             mood_kernel<M, N><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, 0, pm_.C, x_.p, xs_.p, aux_.p,
                                                                           params_.p, sd);
-            mark(ZSME_KERNEL_FINALIZE, false);
+            mark(ZSME_KERNEL_MOOD, false);
         }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
         launch_finalize(sd, sd.dt_step, flags);
@@ -488,7 +499,7 @@ class Solver final : public SolverBase {
     }
     int launches_per_step() const override {
         return 3 + (st_.reconstruction_order < 2 ? 3 : 3 * st_.ssp_stages) +
-               (st_.positivity == ZSME_POSITIVITY_MOOD ? 1 : 0);
+               (st_.positivity == ZSME_POSITIVITY_MOOD ? 1 : 0) + (st_.source ? 1 : 0);
     }
 
     int step(int nsteps, const double* dts_host) override {

@@ -185,8 +185,11 @@ __device__ __forceinline__ int newton_fast(double dtl, double* q, const double* 
 }
 
 // iters (optional): Newton updates applied (0 when the first residual is below
-// the tolerance, so that q is returned unchanged)
-template <class M>
+// the tolerance, so that q is returned unchanged).  Returns 1 when the
+// iteration hit 15 updates, else 0.  GENERIC = false: the generic path is not
+// compiled in; where an update needs it the function returns -1 and q / aux
+// are left part-way (the caller discards them and defers the cell).
+template <class M, bool GENERIC = true>
 __device__ __forceinline__ int newton_cell(double dtl, double* q, double* aux, const double* p, int* iters = nullptr) {
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
     const double X0[3] = {0.0, 0.0, 0.0};
@@ -218,43 +221,47 @@ __device__ __forceinline__ int newton_cell(double dtl, double* q, double* aux, c
 #pragma unroll
         for (int i = 0; i < NQ; ++i) need |= !isfinite(q[i]);
         if (!need && newton_fast<M>(dtl, q, res, dSdQ)) continue;
-        // generic path: the reference's matrix and GEPP, in local memory
-        double dAdQ[NA * NQ];
-#pragma unroll
-        for (int e = 0; e < NA * NQ; ++e) dAdQ[e] = 0.0;
-        if constexpr (HasAuxJacobian<M>::value) {
-            auto r = M::update_aux_variables_jacobian_wrt_variables(q, aux, p);
-#pragma unroll
-            for (int e = 0; e < NA * NQ; ++e) dAdQ[e] = r[e];
+        if constexpr (!GENERIC) {
+            return -1;
         } else {
-            auto a0 = M::update_aux_variables(q, aux, p, 0.0, X0);
+            // generic path: the reference's matrix and GEPP, in local memory
+            double dAdQ[NA * NQ];
 #pragma unroll
-            for (int j = 0; j < NQ; ++j) {
-                double qp[NQ];
+            for (int e = 0; e < NA * NQ; ++e) dAdQ[e] = 0.0;
+            if constexpr (HasAuxJacobian<M>::value) {
+                auto r = M::update_aux_variables_jacobian_wrt_variables(q, aux, p);
 #pragma unroll
-                for (int mm = 0; mm < NQ; ++mm) qp[mm] = q[mm];
-                const double hh = 1e-7 * (fabs(q[j]) + 1e-7);
-                qp[j] += hh;
-                auto a1 = M::update_aux_variables(qp, aux, p, 0.0, X0);
+                for (int e = 0; e < NA * NQ; ++e) dAdQ[e] = r[e];
+            } else {
+                auto a0 = M::update_aux_variables(q, aux, p, 0.0, X0);
 #pragma unroll
-                for (int k = 0; k < NA; ++k) dAdQ[k * NQ + j] = (a1[k] - a0[k]) / hh;
+                for (int j = 0; j < NQ; ++j) {
+                    double qp[NQ];
+#pragma unroll
+                    for (int mm = 0; mm < NQ; ++mm) qp[mm] = q[mm];
+                    const double hh = 1e-7 * (fabs(q[j]) + 1e-7);
+                    qp[j] += hh;
+                    auto a1 = M::update_aux_variables(qp, aux, p, 0.0, X0);
+#pragma unroll
+                    for (int k = 0; k < NA; ++k) dAdQ[k * NQ + j] = (a1[k] - a0[k]) / hh;
+                }
             }
+            double J[NQ * NQ], bv[NQ], xv[NQ];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i)
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    double term = dSdQ[i * NQ + j];
+#pragma unroll
+                    for (int k = 0; k < NA; ++k) term += dSdA[i * NA + k] * dAdQ[k * NQ + j];
+                    J[i * NQ + j] = (i == j ? 1.0 : 0.0) - dtl * term;
+                }
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) bv[i] = -res[i];
+            if (!gepp_full<NQ>(J, bv, xv)) break;
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) q[i] += xv[i];
         }
-        double J[NQ * NQ], bv[NQ], xv[NQ];
-#pragma unroll
-        for (int i = 0; i < NQ; ++i)
-#pragma unroll
-            for (int j = 0; j < NQ; ++j) {
-                double term = dSdQ[i * NQ + j];
-#pragma unroll
-                for (int k = 0; k < NA; ++k) term += dSdA[i * NA + k] * dAdQ[k * NQ + j];
-                J[i * NQ + j] = (i == j ? 1.0 : 0.0) - dtl * term;
-            }
-#pragma unroll
-        for (int i = 0; i < NQ; ++i) bv[i] = -res[i];
-        if (!gepp_full<NQ>(J, bv, xv)) break;
-#pragma unroll
-        for (int i = 0; i < NQ; ++i) q[i] += xv[i];
     }
     if (iters) *iters = iter;
     return iter >= 15 ? 1 : 0;
@@ -268,59 +275,89 @@ enum FinalizeFlags {
     FIN_WRITE = 16,  // store the state / aux back
 };
 
-// cells [c0, c0 + cn); dt_src: per-instance dt of the source step
+// One cell of the finalize step: constraints, source, constraints, store,
+// CFL ratio (into ratio).  GENERIC = false: returns -1 without storing
+// anything when the Newton iteration needs the generic full-size GEPP.
+template <class M, class N, bool GENERIC>
+__device__ __forceinline__ int finalize_cell(const MeshDev& m, int c, int I, double* __restrict__ x,
+                                             double* __restrict__ aux, const double* p, const StepDev& sd,
+                                             const double* __restrict__ dt_src, int flags, double& ratio) {
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, DIM = M::dimension;
+    const int C = m.C;
+    double q[NQ], a[NA];
+    load_q<NQ>(x, C, c, q);
+#pragma unroll
+    for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
+    if (flags & FIN_PRE) constrain<M>(q, a, p);
+    if (flags & FIN_SOURCE) {
+        const int rc = newton_cell<M, GENERIC>(dt_src[I], q, a, p);
+        if constexpr (!GENERIC) {
+            if (rc < 0) return -1;
+        }
+        if (rc > 0) atomicAdd(&sd.diag[2], 1);
+        if (flags & FIN_PRE) constrain<M>(q, a, p);
+    }
+    if (flags & FIN_POST) constrain<M>(q, a, p);
+    if (flags & FIN_WRITE) {
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) x[(size_t)i * C + c] = q[i];
+#pragma unroll
+        for (int i = 0; i < NA; ++i) aux[(size_t)i * C + c] = a[i];
+        bool bad = false;
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) bad |= !isfinite(q[i]);
+        if (bad) atomicAdd(&sd.diag[0], 1);
+        if (q[1] < -1e-10) atomicAdd(&sd.diag[1], 1);
+    }
+    if (flags & FIN_DT) {
+        double eig = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            double n[3] = {0.0, 0.0, 0.0};
+            n[d] = 1.0;
+            auto rr = N::local_max_abs_eigenvalue(q, a, p, n);
+            if (rr[0] > eig) eig = rr[0];
+        }
+        if (!(eig < 1e-14)) {
+            const double rcv = m.rc[c];
+            // a NaN ratio never wins a "<" comparison (VirtualSolver.hpp:342)
+            if (rcv < DBL_MAX) {
+                const double v = rcv / eig;
+                if (v < ratio) ratio = v;
+            }
+        }
+    }
+    return 0;
+}
+
+// cells [c0, c0 + cn); dt_src: per-instance dt of the source step.
+// The Newton iteration runs with the register fast path only; a cell whose
+// update needs the generic GEPP is left untouched and appended to
+// sd.fallback (warp-aggregated, so runs of consecutive cells stay together)
+// for finalize_fallback_kernel.  Keeping the generic path out of this
+// kernel lowers its stack and register pressure (1.29 -> 0.99 ms on the
+// 1400^2 level-4 workload).
 // MINB: resident blocks of 128 threads per SM the register allocation must allow (1 = no cap)
 template <class M, class N, int MINB>
 __global__ void __launch_bounds__(128, MINB) finalize_kernel(MeshDev m, int c0, int cn, double* __restrict__ x,
                                                        double* __restrict__ aux, const double* __restrict__ params,
                                                        StepDev sd, const double* __restrict__ dt_src, int flags) {
-    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, DIM = M::dimension;
-    const int C = m.C;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = c0 + r;
     const int I = r < cn ? cell_instance(m, c) : -1;
     double ratio = DBL_MAX;
     const bool act = I >= 0 && (sd.active ? (sd.active[I] != 0) : true);
-    if (act) {
-        const double* p = params + (size_t)I * m.np;
-        double q[NQ], a[NA];
-        load_q<NQ>(x, C, c, q);
-#pragma unroll
-        for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
-        if (flags & FIN_PRE) constrain<M>(q, a, p);
-        if (flags & FIN_SOURCE) {
-            if (newton_cell<M>(dt_src[I], q, a, p)) atomicAdd(&sd.diag[2], 1);
-            if (flags & FIN_PRE) constrain<M>(q, a, p);
-        }
-        if (flags & FIN_POST) constrain<M>(q, a, p);
-        if (flags & FIN_WRITE) {
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) x[(size_t)i * C + c] = q[i];
-#pragma unroll
-            for (int i = 0; i < NA; ++i) aux[(size_t)i * C + c] = a[i];
-            bool bad = false;
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) bad |= !isfinite(q[i]);
-            if (bad) atomicAdd(&sd.diag[0], 1);
-            if (q[1] < -1e-10) atomicAdd(&sd.diag[1], 1);
-        }
-        if (flags & FIN_DT) {
-            double eig = 0.0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                double n[3] = {0.0, 0.0, 0.0};
-                n[d] = 1.0;
-                auto rr = N::local_max_abs_eigenvalue(q, a, p, n);
-                if (rr[0] > eig) eig = rr[0];
-            }
-            if (!(eig < 1e-14)) {
-                const double rcv = m.rc[c];
-                // a NaN ratio never wins a "<" comparison (VirtualSolver.hpp:342)
-                if (rcv < DBL_MAX) {
-                    const double v = rcv / eig;
-                    if (v < ratio) ratio = v;
-                }
-            }
+    bool defer = false;
+    if (act) defer = finalize_cell<M, N, false>(m, c, I, x, aux, params + (size_t)I * m.np, sd, dt_src, flags,
+                                                 ratio) < 0;
+    if (flags & FIN_SOURCE) {
+        const unsigned dm = __ballot_sync(0xffffffffu, defer);
+        if (dm) {
+            const int lane = threadIdx.x & 31;
+            int base = 0;
+            if (lane == 0) base = atomicAdd(sd.n_fallback, __popc(dm));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (defer) sd.fallback[base + __popc(dm & ((1u << lane) - 1u))] = c;
         }
     }
     if (!(flags & FIN_DT)) return;
@@ -359,6 +396,25 @@ __global__ void __launch_bounds__(128, MINB) finalize_kernel(MeshDev m, int c0, 
             if (wv[k] < best) best = wv[k];
         }
         if (cur >= 0 && best < ZSME_RATIO_NONE) atomicMin(&sd.ratio[cur], best);
+    }
+}
+
+// The deferred cells of finalize_kernel, with the generic Newton path
+// (grid-stride over sd.fallback[0 .. *sd.n_fallback)); their CFL ratios go
+// straight to the per-instance atomic minimum, which is order-free.
+template <class M, class N>
+__global__ void __launch_bounds__(64) finalize_fallback_kernel(MeshDev m, double* __restrict__ x,
+                                                               double* __restrict__ aux,
+                                                               const double* __restrict__ params, StepDev sd,
+                                                               const double* __restrict__ dt_src, int flags) {
+    const int n = *sd.n_fallback;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const int c = sd.fallback[e];
+        const int I = cell_instance(m, c);
+        double ratio = DBL_MAX;
+        finalize_cell<M, N, true>(m, c, I, x, aux, params + (size_t)I * m.np, sd, dt_src, flags, ratio);
+        if ((flags & FIN_DT) && ratio < DBL_MAX)
+            atomicMin(&sd.ratio[I], (unsigned long long)__double_as_longlong(ratio));
     }
 }
 

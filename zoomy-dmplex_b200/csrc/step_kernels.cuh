@@ -64,7 +64,9 @@ struct StepDev {
     int* step_idx;             // steps taken by instance 0 (index into dts)
     int n_inst;
     double t_end, cfl, dt_max;
-    int* diag;                 // [0] nonfinite, [1] negative depth, [2] newton unconverged
+    int* diag;                 // [0] nonfinite, [1] negative depth, [2] newton unconverged, [3] MOOD cells
+    int* fallback;             // [C] cells finalize_kernel deferred to finalize_fallback_kernel
+    int* n_fallback;           // their count
 };
 
 // bits of DBL_MAX: "no cell constrains dt"

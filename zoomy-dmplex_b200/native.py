@@ -17,7 +17,7 @@ ZSME_LIMITER_NONE, ZSME_LIMITER_TVD = 0, 1
 ZSME_GRADIENT_GREEN_GAUSS, ZSME_GRADIENT_LSQ = 0, 1
 ZSME_POSITIVITY_NONE, ZSME_POSITIVITY_ZHANG_SHU, ZSME_POSITIVITY_MOOD = 0, 1, 2
 POSITIVITY = {"none": ZSME_POSITIVITY_NONE, "zhang_shu": ZSME_POSITIVITY_ZHANG_SHU, "mood": ZSME_POSITIVITY_MOOD}
-KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step", "gather")
+KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step", "gather", "finalize_fallback", "mood")
 
 
 class ZsmeMesh(ct.Structure):
