@@ -107,10 +107,10 @@ def step_bytes_survey(nq):
 # stage launches averaged).  The streams scale with the cell count, so a
 # 1400x1400 launch moves these figures times its cells.
 NCU_DRAM_BYTES_PER_CELL = {
-    "sme2d_l4/prep": (816.4e6 + 974.2e6) / 2 / 1618202,
-    "sme2d_l4/flux": 1199.9e6 / 1618202,
-    "sme2d_l4/gather": (1413.3e6 + 1338.9e6) / 2 / 1618202,
-    "sme2d_l4/finalize": 306.6e6 / 1618202,
+    "sme2d_l4/prep": ((375.8 + 430.0) + (520.6 + 427.1)) * 1e6 / 2 / 1618202,
+    "sme2d_l4/flux": (544.7 + 654.2) * 1e6 / 1618202,
+    "sme2d_l4/gather": ((1106.1 + 282.5) + (1188.4 + 141.4)) * 1e6 / 2 / 1618202,
+    "sme2d_l4/finalize": (181.4 + 148.5) * 1e6 / 1618202,
 }
 
 
