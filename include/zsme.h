@@ -133,6 +133,23 @@ int zsme_get_aux(zsme_handle* h, double* a_aos);
 /* Same with device pointers (zero-copy from torch), caller order. */
 int zsme_set_state_device(zsme_handle* h, const double* d_q_aos, double t);
 int zsme_get_state_device(zsme_handle* h, double* d_q_aos);
+/* Asynchronous forms of zsme_set_state / zsme_get_state for pipelined calls
+ * (single-instance handles; no counterpart in the reference, whose state
+ * stays in host memory).  They return at once.  The copies run on two copy
+ * streams of the handle, one per direction, through double-buffered device
+ * staging, ordered against the handle's stream.  A read-back can therefore
+ * overlap the next state's upload and the steps in between.  With
+ * page-locked host buffers (cudaHostAlloc / cudaHostRegister) the copies
+ * are truly asynchronous.  The caller keeps q_aos unchanged, and does not
+ * read the output buffer, until zsme_sync (which waits for the copies too)
+ * has returned.  Two reads in a row must go to different host buffers if
+ * the first is read before zsme_sync.  zsme_stream_wait_copies makes the
+ * handle's stream wait (on the device) for every copy issued so far, e.g.
+ * before recording a timing event on zsme_stream.  The staging buffers
+ * (4 x n_cells x n_dof_q doubles) are allocated by the first call. */
+int zsme_set_state_async(zsme_handle* h, const double* q_aos, double t);
+int zsme_get_state_async(zsme_handle* h, double* q_aos);
+int zsme_stream_wait_copies(zsme_handle* h);
 
 /* F = dQ/dt of the transport for state X (TransportStep::FormRHS,
  * TransportStep.hpp:325-357).  Host AoS buffers, caller order. */

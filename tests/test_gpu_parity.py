@@ -227,3 +227,34 @@ def test_profile_kinds_per_step():
                  "finalize_fallback": 2, "mood": 0}
     assert all(v[0] > 0 for k, v in prof.items() if n[k])
     assert g.launches_per_step() == sum(n.values()) // 2
+
+
+def test_async_state_io_matches_blocking_calls():
+    """Three independent one-step problems pipelined through the asynchronous
+    state calls (page-locked host buffers, copies on their own streams) give
+    the blocking calls' results bit for bit."""
+    import torch
+
+    c = CASES["l2"]
+    g, _ = pair(c)
+    qs = []
+    for k in range(3):
+        q = c.q0.copy()
+        q[:, 2:] += 0.01 * k * q[:, 1:2]
+        qs.append(q)
+    ref = []
+    for q in qs:
+        g.set_state(q)
+        g.step(1)
+        ref.append(g.get_state())
+    ins = [torch.from_numpy(q).pin_memory() for q in qs]
+    outs = [torch.zeros(c.q0.shape, dtype=torch.float64).pin_memory() for _ in qs]
+    for k in range(3):
+        g.set_state_async(ins[k].data_ptr(), 0.0)
+        g.step(1)
+        g.get_state_async(outs[k].data_ptr())
+    g.stream_wait_copies()
+    g.sync()
+    for k in range(3):
+        assert np.array_equal(outs[k].numpy(), ref[k]), k
+    assert np.array_equal(g.get_state(), ref[2])

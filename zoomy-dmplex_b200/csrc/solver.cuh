@@ -92,6 +92,11 @@ class Solver final : public SolverBase {
     bool profiling_ = false;
     bool x_clamped_ = true;  // x_ equals update_variables(x_)
     std::vector<cudaEvent_t> ev_pool_;
+    // asynchronous state I/O (zsme_set_state_async / zsme_get_state_async)
+    cudaStream_t h2d_ = nullptr, d2h_ = nullptr;
+    DevBuf<double> in_stage_[2], out_stage_[2];
+    cudaEvent_t ev_h2d_[2] = {}, ev_in_used_[2] = {}, ev_out_[2] = {}, ev_d2h_[2] = {};
+    int in_k_ = 0, out_k_ = 0, last_d2h_ = 0;
     std::vector<int> ev_kind_;
     size_t ev_used_ = 0;
     double prof_ms_[ZSME_KERNEL_KINDS] = {0};
@@ -101,6 +106,14 @@ class Solver final : public SolverBase {
     ~Solver() override {
         if (graph_) cudaGraphExecDestroy(graph_);
         for (auto e : ev_pool_) cudaEventDestroy(e);
+        if (h2d_) {
+            cudaStreamSynchronize(h2d_);
+            cudaStreamSynchronize(d2h_);
+            for (int j = 0; j < 2; ++j)
+                for (cudaEvent_t e : {ev_h2d_[j], ev_in_used_[j], ev_out_[j], ev_d2h_[j]}) cudaEventDestroy(e);
+            cudaStreamDestroy(h2d_);
+            cudaStreamDestroy(d2h_);
+        }
         if (stream_) cudaStreamDestroy(stream_);
     }
 
@@ -276,19 +289,85 @@ class Solver final : public SolverBase {
         }
         aos_to_soa_kernel<<<blocks_for(cn, 128), 128, 0, stream_>>>(src, x_.p, old_of_new_.p, c0, cn, pm_.C, NQ);
         ZSME_CUDA(cudaGetLastError());
+        set_time_kernel<<<1, 1, 0, stream_>>>(t_.p + inst, t);
+        rc = enqueue_loaded(inst, c0, cn);
+        if (rc) return rc;
+        ZSME_CUDA(cudaStreamSynchronize(stream_));
+        return ZSME_OK;
+    }
+    // After a state (and its time) is in place: aux reset, constraints, then
+    // dt_start = max(ComputeTimeStep, min_dt) (MUSCLSolver.hpp:51-54, 103).
+    int enqueue_loaded(int inst, int c0, int cn) {
         for (int k = 0; k < NA; ++k)
             ZSME_CUDA(cudaMemsetAsync(aux_.p + (size_t)k * pm_.C + c0, 0, cn * sizeof(double), stream_));
-        ZSME_CUDA(cudaMemcpyAsync(t_.p + inst, &t, sizeof(double), cudaMemcpyHostToDevice, stream_));
         ZSME_CUDA(cudaMemsetAsync(active_.p + inst, 0, sizeof(int), stream_));
         if (inst == 0) ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, 8 * sizeof(int), stream_));
-        // constraints, then dt_start = max(ComputeTimeStep, min_dt)
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
         finalize_range(c0, cn, sd, nullptr, FIN_POST | FIN_WRITE | FIN_DT);
         ZSME_CUDA(cudaGetLastError());
         end_step_kernel<<<1, 32, 0, stream_>>>(step_dev(nullptr), inst, 1, 0, st_.min_dt, nullptr);
         ZSME_CUDA(cudaGetLastError());
-        ZSME_CUDA(cudaStreamSynchronize(stream_));
+        x_clamped_ = true;
+        return ZSME_OK;
+    }
+
+    // ------------------------------------------------ asynchronous state I/O
+    // Host <-> device state copies on two copy streams (one per direction)
+    // through double-buffered device staging, ordered against the handle's
+    // stream by events: a copy in one direction, the other direction's copy
+    // and the steps in between can all be in flight at once.
+    int async_setup() {
+        if (h2d_) return ZSME_OK;
+        const size_t n = (size_t)NQ * pm_.C;
+        for (int j = 0; j < 2; ++j) {
+            ZSME_CUDA(in_stage_[j].alloc(n));
+            ZSME_CUDA(out_stage_[j].alloc(n));
+            for (cudaEvent_t* e : {&ev_h2d_[j], &ev_in_used_[j], &ev_out_[j], &ev_d2h_[j]})
+                ZSME_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        }
+        ZSME_CUDA(cudaStreamCreateWithFlags(&d2h_, cudaStreamNonBlocking));
+        ZSME_CUDA(cudaStreamCreateWithFlags(&h2d_, cudaStreamNonBlocking));
+        return ZSME_OK;
+    }
+    int set_state_async(const double* q, double t) override {
+        int rc = async_setup();
+        if (rc) return rc;
+        const int j = in_k_;
+        in_k_ ^= 1;
+        const int C = pm_.C;
+        // staging buffer j is free once the conversion of two calls ago has read it
+        ZSME_CUDA(cudaStreamWaitEvent(h2d_, ev_in_used_[j], 0));
+        ZSME_CUDA(cudaMemcpyAsync(in_stage_[j].p, q, (size_t)NQ * C * sizeof(double), cudaMemcpyHostToDevice, h2d_));
+        ZSME_CUDA(cudaEventRecord(ev_h2d_[j], h2d_));
+        ZSME_CUDA(cudaStreamWaitEvent(stream_, ev_h2d_[j], 0));
+        aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(in_stage_[j].p, x_.p, old_of_new_.p, 0, C, C, NQ);
+        ZSME_CUDA(cudaGetLastError());
+        ZSME_CUDA(cudaEventRecord(ev_in_used_[j], stream_));
+        set_time_kernel<<<1, 1, 0, stream_>>>(t_.p, t);
+        return enqueue_loaded(0, 0, C);
+    }
+    int get_state_async(double* q) override {
+        int rc = async_setup();
+        if (rc) return rc;
+        const int j = out_k_;
+        out_k_ ^= 1;
+        const int C = pm_.C;
+        // staging buffer j is free once its copy of two calls ago has left the device
+        ZSME_CUDA(cudaStreamWaitEvent(stream_, ev_d2h_[j], 0));
+        soa_to_aos_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(x_.p, out_stage_[j].p, old_of_new_.p, 0, C, C, NQ);
+        ZSME_CUDA(cudaGetLastError());
+        ZSME_CUDA(cudaEventRecord(ev_out_[j], stream_));
+        ZSME_CUDA(cudaStreamWaitEvent(d2h_, ev_out_[j], 0));
+        ZSME_CUDA(cudaMemcpyAsync(q, out_stage_[j].p, (size_t)NQ * C * sizeof(double), cudaMemcpyDeviceToHost, d2h_));
+        ZSME_CUDA(cudaEventRecord(ev_d2h_[j], d2h_));
+        last_d2h_ = j;
+        return ZSME_OK;
+    }
+    int stream_wait_copies() override {
+        if (!h2d_) return ZSME_OK;
+        ZSME_CUDA(cudaStreamWaitEvent(stream_, ev_d2h_[last_d2h_], 0));
+        ZSME_CUDA(cudaStreamWaitEvent(stream_, ev_h2d_[in_k_ ^ 1], 0));
         return ZSME_OK;
     }
 
@@ -846,6 +925,10 @@ class Solver final : public SolverBase {
         int rc = check_inst(inst);
         if (rc) return rc;
         ZSME_CUDA(cudaStreamSynchronize(stream_));
+        if (h2d_) {
+            ZSME_CUDA(cudaStreamSynchronize(h2d_));
+            ZSME_CUDA(cudaStreamSynchronize(d2h_));
+        }
         double tt = 0, dd = 0;
         int is[8];
         ZSME_CUDA(cudaMemcpy(&tt, t_.p + inst, sizeof(double), cudaMemcpyDeviceToHost));

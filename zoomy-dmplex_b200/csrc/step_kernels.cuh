@@ -633,6 +633,7 @@ static __global__ void end_step_kernel(StepDev sd, int i0, int ni, int mode, dou
 // AoS (caller order within an instance) <-> SoA (Hilbert order): cells
 // [c0, c0 + cn) of the SoA arrays (row stride C) are instance-local rows
 // old_of_new[c] of the AoS buffer.
+static __global__ void set_time_kernel(double* t, double v) { *t = v; }
 static __global__ void aos_to_soa_kernel(const double* __restrict__ aos, double* __restrict__ soa,
                                          const int* __restrict__ old_of_new, int c0, int cn, int C, int nq) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;

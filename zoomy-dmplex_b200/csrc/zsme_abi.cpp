@@ -128,6 +128,20 @@ int zsme_get_state_device(zsme_handle* h, double* q) {
     if (!q) return set_error(ZSME_ERR_ARG, "null output");
     return h->s->get_state(0, q, true);
 }
+int zsme_set_state_async(zsme_handle* h, const double* q, double t) {
+    CHECK_SINGLE(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null state");
+    return h->s->set_state_async(q, t);
+}
+int zsme_get_state_async(zsme_handle* h, double* q) {
+    CHECK_SINGLE(h);
+    if (!q) return set_error(ZSME_ERR_ARG, "null output");
+    return h->s->get_state_async(q);
+}
+int zsme_stream_wait_copies(zsme_handle* h) {
+    CHECK_SINGLE(h);
+    return h->s->stream_wait_copies();
+}
 int zsme_get_aux(zsme_handle* h, double* a) {
     CHECK_SINGLE(h);
     if (!a) return set_error(ZSME_ERR_ARG, "null output");

@@ -88,6 +88,9 @@ def load():
     lib.zsme_get_aux.argtypes = [vp, P]
     lib.zsme_set_state_device.argtypes = [vp, vp, ct.c_double]
     lib.zsme_get_state_device.argtypes = [vp, vp]
+    lib.zsme_set_state_async.argtypes = [vp, vp, ct.c_double]
+    lib.zsme_get_state_async.argtypes = [vp, vp]
+    lib.zsme_stream_wait_copies.argtypes = [vp]
     lib.zsme_rhs.argtypes = [vp, ct.c_double, P, P]
     lib.zsme_update_state.argtypes = [vp]
     lib.zsme_source.argtypes = [vp, ct.c_double]

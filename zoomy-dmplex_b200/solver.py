@@ -93,6 +93,22 @@ class Solver:
     def get_state_device(self, q_dev_ptr: int):
         native.check(self.lib.zsme_get_state_device(self.h, ct.c_void_p(q_dev_ptr)))
 
+    def set_state_async(self, q_host_ptr: int, t: float = 0.0):
+        """zsme_set_state_async: the state at host address q_host_ptr (AoS,
+        caller order; page-locked for a truly asynchronous copy) becomes the
+        state at time t once the handle's stream reaches it.  The buffer must
+        stay unchanged until sync()."""
+        native.check(self.lib.zsme_set_state_async(self.h, ct.c_void_p(q_host_ptr), float(t)))
+
+    def get_state_async(self, q_host_ptr: int):
+        """zsme_get_state_async: the current state is copied to host address
+        q_host_ptr; valid after sync()."""
+        native.check(self.lib.zsme_get_state_async(self.h, ct.c_void_p(q_host_ptr)))
+
+    def stream_wait_copies(self):
+        """The handle's stream waits (on the device) for the asynchronous copies issued so far."""
+        native.check(self.lib.zsme_stream_wait_copies(self.h))
+
     def get_aux(self) -> np.ndarray:
         a = np.empty((self.C, self.naux))
         native.check(self.lib.zsme_get_aux(self.h, _p(a)))
