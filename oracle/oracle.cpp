@@ -894,7 +894,9 @@ par_for(C, [&](int c, int) {
 // source_jacobian_wrt_variables, 5 source_jacobian_wrt_aux_variables, 6
 // update_variables, 7 update_aux_variables, 8 boundary_conditions(bc 0),
 // 9 eigenvalues, 10 flux, 11 solver-side dAux/dQ (SourceStep.hpp:26-53),
-// 12 nonconservative_matrix.
+// 12 nonconservative_matrix, 13 the Jacobian of [numerical_flux,
+// numerical_fluctuations] (3 nq rows) with respect to [qL, qR] (2 nq
+// columns), row-major, by dual numbers.
 template <template <typename> class MT, template <typename> class NT>
 int pointwise(int fn, const double* qL, const double* qR, const double* aL, const double* aR,
               const double* p, const double* n, double s, double* out) {
@@ -922,8 +924,39 @@ int pointwise(int fn, const double* qL, const double* qR, const double* aL, cons
             return na * nq;
         }
         case 12: return put(M::nonconservative_matrix(qL, aL, p), nq * nq * dim);
+        case 13: {
+            using D = zsme::Dual<nq>;
+            for (int side = 0; side < 2; ++side) {
+                D dl[nq], dr[nq], dal[na], dar[na], dp[M::n_parameters], dn[3];
+                for (int i = 0; i < nq; ++i) {
+                    dl[i] = side == 0 ? D::seed(qL[i], i) : D(qL[i]);
+                    dr[i] = side == 1 ? D::seed(qR[i], i) : D(qR[i]);
+                }
+                for (int i = 0; i < na; ++i) { dal[i] = D(aL[i]); dar[i] = D(aR[i]); }
+                for (int i = 0; i < M::n_parameters; ++i) dp[i] = D(p[i]);
+                for (int i = 0; i < 3; ++i) dn[i] = D(n[i]);
+                const auto fl = NT<D>::numerical_flux(dl, dr, dal, dar, dp, dn);
+                const auto nc = NT<D>::numerical_fluctuations(dl, dr, dal, dar, dp, dn);
+                for (int r = 0; r < 3 * nq; ++r)
+                    for (int j = 0; j < nq; ++j)
+                        out[r * 2 * nq + side * nq + j] = r < nq ? fl[r].d[j] : nc[r - nq].d[j];
+            }
+            return 6 * nq * nq;
+        }
     }
     return -1;
+}
+
+// The generated reverse-mode face derivative, or -1 where the plugin has none.
+template <template <typename> class MT, template <typename> class NT>
+int flux_vjp(const double* qL, const double* qR, const double* aL, const double* aR, const double* p,
+             const double* n, const double* w, double* g) {
+    if constexpr (zsme::HasFluxVJP<NT<double>>::value) {
+        NT<double>::numerical_flux_fluct_vjp(qL, qR, aL, aR, p, n, w, g);
+        return 2 * MT<double>::n_dof_q;
+    } else {
+        return -1;
+    }
 }
 
 struct Entry {
@@ -931,6 +964,8 @@ struct Entry {
     OracleBase* (*make)(const zsme_mesh*, const zsme_settings*, const double*);
     int (*pw)(int, const double*, const double*, const double*, const double*, const double*,
               const double*, double, double*);
+    int (*vjp)(const double*, const double*, const double*, const double*, const double*, const double*,
+               const double*, double*);
     int nq, na, np, dim;
     OracleBase* (*make_tlm)(const zsme_mesh*, const zsme_settings*, const double*);
 };
@@ -946,6 +981,7 @@ OracleBase* make_tlm(const zsme_mesh* m, const zsme_settings* s, const double* p
 
 #define ORACLE_ENTRY(NS)                                                                   \
     Entry{#NS, &make_oracle<NS::Model, NS::Numerics>, &pointwise<NS::Model, NS::Numerics>,   \
+          &flux_vjp<NS::Model, NS::Numerics>,                                              \
           NS::Model<double>::n_dof_q,                                                      \
           NS::Model<double>::n_dof_qaux, NS::Model<double>::n_parameters,                  \
           NS::Model<double>::dimension, &make_tlm<NS::Model, NS::Numerics>}
@@ -993,6 +1029,12 @@ int oracle_pointwise(const char* model, int fn, const double* qL, const double* 
                      const double* aR, const double* p, const double* n, double s, double* out) {
     for (auto& e : kEntries)
         if (!std::strcmp(e.name, model)) return e.pw(fn, qL, qR, aL, aR, p, n, s, out);
+    return fail(-ZSME_ERR_MODEL, std::string("unknown model ") + model);
+}
+int oracle_flux_vjp(const char* model, const double* qL, const double* qR, const double* aL, const double* aR,
+                    const double* p, const double* n, const double* w, double* g) {
+    for (auto& e : kEntries)
+        if (!std::strcmp(e.name, model)) return e.vjp(qL, qR, aL, aR, p, n, w, g);
     return fail(-ZSME_ERR_MODEL, std::string("unknown model ") + model);
 }
 // Tangent-linear instance: the same restatement on Dual<1> numbers.

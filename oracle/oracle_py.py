@@ -61,6 +61,7 @@ def load(ref: bool = False):
     lib.oracle_set_threads.argtypes = [ct.c_int]
     lib.oracle_model_info.argtypes = [ct.c_char_p] + [ct.POINTER(ct.c_int)] * 4
     lib.oracle_pointwise.argtypes = [ct.c_char_p, ct.c_int, P, P, P, P, P, P, ct.c_double, P]
+    lib.oracle_flux_vjp.argtypes = [ct.c_char_p, P, P, P, P, P, P, P, P]
     _libs[path] = lib
     return lib
 
@@ -91,6 +92,31 @@ def pointwise(model: str, fn: str, qL, aL, p, n=None, qR=None, aR=None, s=0.0, r
     if k < 0:
         raise ValueError(lib.oracle_last_error().decode())
     return out[:k].copy()
+
+
+def face_jacobian(model: str, qL, qR, p, n, aL=None, aR=None):
+    """d[numerical_flux, numerical_fluctuations] / d[qL, qR] by dual numbers:
+    (3 nq) x (2 nq)."""
+    lib = load(False)
+    f = lambda a: np.ascontiguousarray(a if a is not None else np.zeros(16), dtype=np.float64)
+    nq = len(qL)
+    out = np.zeros(6 * nq * nq)
+    k = lib.oracle_pointwise(model.encode(), 13, _p(f(qL)), _p(f(qR)), _p(f(aL)), _p(f(aR)), _p(f(p)), _p(f(n)),
+                             0.0, _p(out))
+    if k < 0:
+        raise ValueError(lib.oracle_last_error().decode())
+    return out.reshape(3 * nq, 2 * nq)
+
+
+def flux_vjp(model: str, qL, qR, p, n, w, aL=None, aR=None):
+    """g = w^T d[numerical_flux, numerical_fluctuations] / d[qL, qR] from the
+    plugin's generated reverse sweep, or None if the plugin has none."""
+    lib = load(False)
+    f = lambda a: np.ascontiguousarray(a if a is not None else np.zeros(16), dtype=np.float64)
+    g = np.zeros(2 * len(qL))
+    k = lib.oracle_flux_vjp(model.encode(), _p(f(qL)), _p(f(qR)), _p(f(aL)), _p(f(aR)), _p(f(p)), _p(f(n)),
+                            _p(f(w)), _p(g))
+    return None if k < 0 else g[:k].copy()
 
 
 def set_threads(n: int = 0, ref: bool = False) -> int:

@@ -175,3 +175,37 @@ def test_adjoint_rejects_bad_input():
         g.adjoint(5, [9], [0], [1], [0.0])          # observation after the last step
     with pytest.raises(native.ZsmeError):
         g.adjoint(5, [1], [c.mesh.n_cells], [1], [0.0])
+
+
+def test_dual_number_face_path_on_reference_style_header():
+    """A plugin without a generated face VJP (the 1-D model mirrors the
+    reference's shipped header) is differentiated by the dual-number face
+    kernel: adjoint against the tangent-linear oracle."""
+    from test_gpu_parity import case_1d
+
+    c = case_1d()
+    p, names = _params(c)
+    nsteps = 20
+    o = O.Oracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), p)
+    q_tgt = c.q0.copy()
+    q_tgt[:, 1] += 0.01 * np.exp(-(c.mesh.cell_centroid[:, 0] - 0.4) ** 2 / 0.02)
+    o.set_state(q_tgt)
+    steps = [5, 10, 15, 20]
+    cells = adj.gauges(c.mesh.n_cells, 12, 3)
+    targets = []
+    for k in range(1, nsteps + 1):
+        o.step(1)
+        if k in steps:
+            targets.append(o.get_state()[cells, 1])
+    obs = adj.depth_observations(cells, steps, np.array(targets))
+    g = Solver(c.model, c.mesh, c.settings, p)
+    g.set_state(c.q0)
+    loss, gq, gp, dts = g.adjoint(nsteps, *obs, checkpoint_every=7)
+    rng = np.random.default_rng(5)
+    for _ in range(2):
+        dq = np.zeros_like(c.q0)
+        dq[:, 0] = rng.standard_normal(c.mesh.n_cells)
+        L, dL = _oracle_tlm(c, p, dts, obs, dq, np.zeros_like(p))
+        assert abs(L - loss) <= 1e-12 * abs(L)
+        ad = float(np.sum(gq * dq))
+        assert abs(ad - dL) <= 1e-8 * max(abs(dL), 1e-30), (ad, dL)

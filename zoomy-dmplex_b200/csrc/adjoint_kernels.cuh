@@ -194,6 +194,130 @@ __global__ void __launch_bounds__(128) adj_face_kernel(MeshDev m, const double* 
     }
 }
 
+// A boundary face's ghost state, as the face kernel forms it: qR =
+// boundary_conditions(bc, qL, aux(qL)) at time t, with its aux.  With g
+// non-null the adjoint instead: g[0 .. NQ) += (dqR / dqL)^T g[NQ .. 2 NQ)
+// (dual numbers through update_aux_variables and boundary_conditions).
+// Out of line, so that its dual arithmetic does not weigh on the caller's
+// registers.
+template <template <typename> class MT>
+__device__ __noinline__ void ghost_state(const double* qL, const double* aLc, const double* p, const double* nh,
+                                         const double* xf, double t, int bc, double* qR, double* aL, double* aR,
+                                         double* g) {
+    using M = MT<double>;
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, NP = M::n_parameters;
+    if (!g) {
+        const auto ra = M::update_aux_variables(qL, aLc, p, t, xf);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) aL[i] = ra[i];
+        const auto qb = M::boundary_conditions(bc, qL, aL, p, nh, xf, t, 0.0);
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) qR[i] = qb[i];
+        const auto rb = M::update_aux_variables(qR, aL, p, t, xf);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) aR[i] = rb[i];
+        return;
+    }
+    using D = Dual<NQ>;
+    D qd[NQ], ad[NA], pd[NP], nd[3], xd[3];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) qd[i] = D::seed(qL[i], i);
+#pragma unroll
+    for (int i = 0; i < NA; ++i) ad[i] = D(aLc[i]);
+#pragma unroll
+    for (int k = 0; k < NP; ++k) pd[k] = D(p[k]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { nd[d] = D(nh[d]); xd[d] = D(xf[d]); }
+    const auto ra = MT<D>::update_aux_variables(qd, ad, pd, D(t), xd);
+    D ald[NA];
+#pragma unroll
+    for (int i = 0; i < NA; ++i) ald[i] = ra[i];
+    const auto qb = MT<D>::boundary_conditions(bc, qd, ald, pd, nd, xd, D(t), D(0.0));
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) s += g[NQ + i] * qb[i].d[j];
+        g[j] += s;
+    }
+}
+
+// adj_face_kernel in one reverse sweep per face, for plugins with a
+// generated numerical_flux_fluct_vjp: w^T J for both face states at once,
+// w the weights adj_face_kernel contracts its dual-number Jacobian with
+// (flux: (mu_R - mu_L) A; fluctuations into R: -mu_R A, into L: -mu_L A;
+// at a boundary face mu_R = 0 and the fluctuations into the ghost count for
+// nothing), the ghost state's dependence on the inner one pulled back by
+// ghost_state.
+template <template <typename> class MT, template <typename> class NT>
+__global__ void __launch_bounds__(128) adj_face_vjp_kernel(MeshDev m, const double* __restrict__ fs,
+                                                           const double* __restrict__ aux,
+                                                           const double* __restrict__ params, const double* tp,
+                                                           double frac, const double* dtp, double factor,
+                                                           const double* __restrict__ v, double* __restrict__ gfs) {
+    using M = MT<double>;
+    using N = NT<double>;
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
+    const int F = m.F, C = m.C;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= F) return;
+    const int R = m.face_R[f], L = m.face_L[f], bc = m.face_bc[f];
+    if (R < 0 && bc < 0) {  // no flux through this face
+#pragma unroll
+        for (int j = 0; j < NQ; ++j) gfs[(size_t)j * F + f] = 0.0;
+        return;
+    }
+    const double* p = params + (size_t)face_instance(m, f) * m.np;
+    const double area = m.farea[f];
+    const double dt = *dtp;
+    const double scale = factor * dt;
+    const double vL = m.vol[L], vR = R >= 0 ? m.vol[R] : 0.0;
+    double w[3 * NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        double muL = scale * v[(size_t)i * C + L];
+        if (vL > 1e-15) muL /= vL;
+        double muR = 0.0;
+        if (R >= 0) {
+            muR = scale * v[(size_t)i * C + R];
+            if (vR > 1e-15) muR /= vR;
+        }
+        w[i] = (muR - muL) * area;
+        w[NQ + i] = -(area * muR);
+        w[2 * NQ + i] = -(area * muL);
+    }
+    const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
+    const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
+    double qL[NQ], qR[NQ], aL[NA], aR[NA], aLc[NA];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) qL[i] = fs[(size_t)i * F + f];
+#pragma unroll
+    for (int i = 0; i < NA; ++i) aLc[i] = aux[(size_t)i * C + L];
+    const double t = *tp + frac * dt;
+    if (R >= 0) {
+        double aRc[NA];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) qR[i] = fs[((size_t)NQ + i) * F + f];
+#pragma unroll
+        for (int i = 0; i < NA; ++i) aRc[i] = aux[(size_t)i * C + R];
+        const auto ra = M::update_aux_variables(qL, aLc, p, 0.0, xf);
+        const auto rb = M::update_aux_variables(qR, aRc, p, 0.0, xf);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) { aL[i] = ra[i]; aR[i] = rb[i]; }
+    } else {
+        ghost_state<MT>(qL, aLc, p, nh, xf, t, bc, qR, aL, aR, nullptr);
+    }
+    double g[2 * NQ];
+    N::numerical_flux_fluct_vjp(qL, qR, aL, aR, p, nh, w, g);
+    if (R < 0) ghost_state<MT>(qL, aLc, p, nh, xf, t, bc, qR, aL, aR, g);
+#pragma unroll
+    for (int j = 0; j < NQ; ++j) gfs[(size_t)j * F + f] = g[j];
+    if (R >= 0) {
+#pragma unroll
+        for (int j = 0; j < NQ; ++j) gfs[((size_t)NQ + j) * F + f] = g[NQ + j];
+    }
+}
+
 // ---------------------------------------------------------------- cells
 // own_w / own_wl [NQ][C]: adjoint of the cell's raw / clamped stage state
 // from its own face states; out_w / out_wl [K][NQ][C]: what the cell owes

@@ -75,4 +75,17 @@ struct HasAuxJacobian<M, std::void_t<decltype(M::update_aux_variables_jacobian_w
     (const typename ScalarOf<M>::type*)nullptr, (const typename ScalarOf<M>::type*)nullptr,
     (const typename ScalarOf<M>::type*)nullptr))>> : std::true_type {};
 
+// A generated numerical_flux_fluct_vjp(Q_minus, Q_plus, Qaux_minus,
+// Qaux_plus, p, n, w, g): g = w^T d[numerical_flux, numerical_fluctuations]
+// / d[Q_minus, Q_plus] in one reverse sweep.  Headers without it (the
+// reference's own) are differentiated with dual numbers.
+template <class N, typename = void>
+struct HasFluxVJP : std::false_type {};
+template <class N>
+struct HasFluxVJP<N, std::void_t<decltype(N::numerical_flux_fluct_vjp(
+    (const typename ScalarOf<N>::type*)nullptr, (const typename ScalarOf<N>::type*)nullptr,
+    (const typename ScalarOf<N>::type*)nullptr, (const typename ScalarOf<N>::type*)nullptr,
+    (const typename ScalarOf<N>::type*)nullptr, (const typename ScalarOf<N>::type*)nullptr,
+    (const typename ScalarOf<N>::type*)nullptr, (typename ScalarOf<N>::type*)nullptr))>> : std::true_type {};
+
 }  // namespace zsme

@@ -634,8 +634,13 @@ class Solver final : public SolverBase {
             clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, W, aux_.p, params_.p, adj_wl_.p);
             wl = adj_wl_.p;
         }
-        adj_face_kernel<MT, NT><<<blocks_for((long long)F * 2, 128), 128, 0, stream_>>>(
-            md_, fs, aux_.p, params_.p, tp, frac, dtp, factor, src, adj_gfs_.p);
+        if constexpr (HasFluxVJP<N>::value) {   // the plugin's generated reverse sweep
+            adj_face_vjp_kernel<MT, NT><<<blocks_for(F, 128), 128, 0, stream_>>>(md_, fs, aux_.p, params_.p, tp,
+                                                                                frac, dtp, factor, src, adj_gfs_.p);
+        } else {
+            adj_face_kernel<MT, NT><<<blocks_for((long long)F * 2, 128), 128, 0, stream_>>>(
+                md_, fs, aux_.p, params_.p, tp, frac, dtp, factor, src, adj_gfs_.p);
+        }
         if (pm_.K == 3)
             adj_cell_kernel<MT, 3><<<blocks_for(C, 128), 128, 0, stream_>>>(
                 md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);

@@ -164,6 +164,12 @@ class Printer:
             return s
         if isinstance(e, sp.Abs):
             return "std::fabs(" + self.p(e.args[0]) + ")"
+        if isinstance(e, Sel):
+            a, b, x, y = e.args
+            return "((%s < %s) ? %s : %s)" % (self._arg(a), self._arg(b), self._arg(x), self._arg(y))
+        if isinstance(e, SelNZ):
+            a, x, y = e.args
+            return "((%s != %s) ? %s : %s)" % (self._arg(a), self._arg(sp.Integer(0)), self._arg(x), self._arg(y))
         if isinstance(e, sp.Heaviside):
             h0 = e.args[1] if len(e.args) > 1 else sp.Rational(1, 2)
             return "Heaviside(" + self.p(e.args[0]) + ", " + _num(h0) + ")"
@@ -194,6 +200,110 @@ def emit_body(exprs, res_name="res", size=None, indent="    "):
 
 def arr(name, n):
     return [sp.Symbol("%s[%d]" % (name, i)) for i in range(n)]
+
+
+# --------------------------------------------------------------------------
+# Reverse-mode derivatives (vector-Jacobian products) of printed code
+# --------------------------------------------------------------------------
+class Sel(sp.Function):
+    """Sel(a, b, x, y) = (a < b) ? x : y, printed as a conditional."""
+    nargs = 4
+
+
+class SelNZ(sp.Function):
+    """SelNZ(a, x, y) = (a != 0) ? x : y, printed as a conditional."""
+    nargs = 3
+
+
+def _vjp(e, a, acc):
+    """Add the adjoint a of expression e to its leaf symbols (acc: symbol ->
+    list of terms).  The rules differentiate the C++ this module's Printer
+    emits for e, with the conventions of the dual numbers (csrc/dual.h): a
+    max / min takes the derivative of the argument std::max / std::min
+    returns (the first one on a tie), d|x| = +dx at x = 0, and a square or
+    cube root has a zero derivative where it is 0."""
+    if e.is_Symbol:
+        acc.setdefault(e, []).append(a)
+    elif e.is_Number:
+        return
+    elif isinstance(e, sp.Add):
+        for t in e.args:
+            _vjp(t, a, acc)
+    elif isinstance(e, sp.Mul):
+        args = e.args
+        for i, f in enumerate(args):
+            if not f.is_Number:
+                _vjp(f, a * sp.Mul(*(args[:i] + args[i + 1:])), acc)
+    elif isinstance(e, sp.Pow):
+        b, x = e.base, e.exp
+        if x.is_Integer:
+            _vjp(b, a * x * b ** (x - 1), acc)
+        elif x == sp.Rational(1, 2):                       # std::sqrt(b)
+            _vjp(b, a * Sel(0, e, sp.Rational(1, 2) / e, 0), acc)
+        elif x == sp.Rational(-1, 2):                      # 1.0/std::sqrt(b)
+            s = sp.sqrt(b)
+            _vjp(b, -a * e ** 2 * Sel(0, s, sp.Rational(1, 2) / s, 0), acc)
+        elif x.is_Rational and x.q == 2 and x > 0:         # b*...*b*std::sqrt(b)
+            k = (x.p - 1) // 2
+            s = sp.sqrt(b)
+            _vjp(b, a * (k * b ** (k - 1) * s + b ** k * Sel(0, s, sp.Rational(1, 2) / s, 0)), acc)
+        elif x == sp.Rational(1, 3):                       # std::cbrt(b)
+            _vjp(b, a * SelNZ(e, 1 / (3 * e * e), 0), acc)
+        elif x == sp.Rational(-1, 3):                      # 1.0/std::cbrt(b)
+            c = sp.cbrt(b)
+            _vjp(b, -a * e ** 2 * SelNZ(c, 1 / (3 * c * c), 0), acc)
+        else:                                              # std::pow(b, x)
+            _vjp(b, a * SelNZ(b, x * b ** (x - 1), 0), acc)
+    elif isinstance(e, (sp.Max, sp.Min)):
+        args = sorted(e.args, key=lambda t: 0 if t.is_Number else 1)    # the printer's nesting
+        _vjp_minmax(isinstance(e, sp.Max), args, a, acc)
+    elif isinstance(e, sp.Abs):                            # std::fabs(x)
+        x = e.args[0]
+        _vjp(x, Sel(x, 0, -a, a), acc)
+    elif isinstance(e, sp.Heaviside):
+        return
+    else:
+        raise NotImplementedError(type(e), e)
+
+
+def _vjp_minmax(is_max, args, a, acc):
+    # fn(args[0], fn(args[1], ... fn(args[-2], args[-1])))
+    if len(args) == 1:
+        _vjp(args[0], a, acc)
+        return
+    x, rest = args[0], args[1:]
+    y = rest[0] if len(rest) == 1 else (sp.Max if is_max else sp.Min)(*rest, evaluate=False)
+    if is_max:      # std::max(x, y) = (x < y) ? y : x
+        _vjp(x, Sel(x, y, 0, a), acc)
+        _vjp_minmax(True, rest, Sel(x, y, a, 0), acc)
+    else:           # std::min(x, y) = (y < x) ? y : x
+        _vjp(x, Sel(y, x, 0, a), acc)
+        _vjp_minmax(False, rest, Sel(y, x, a, 0), acc)
+
+
+def emit_vjp_body(exprs, inputs, w_name="w", g_name="g", indent="    "):
+    """g[j] = sum_k w[k] d exprs[k] / d inputs[j]: the outputs' SSA (CSE)
+    followed by its reverse sweep, one adjoint per SSA value."""
+    exprs = [sp.sympify(e) for e in exprs]
+    w = arr(w_name, len(exprs))
+    repl, red = sp.cse(exprs, symbols=sp.numbered_symbols("t"), optimizations="basic")
+    acc = {}
+    for k, e in enumerate(red):
+        _vjp(e, w[k], acc)
+    adj = []
+    for s, e in reversed(repl):
+        terms = acc.pop(s, [])
+        if not terms:
+            continue
+        a_s = sp.Symbol("a_" + s.name)
+        adj.append((a_s, sp.Add(*terms)))
+        _vjp(e, a_s, acc)
+    pr = Printer()
+    lines = ["%sT %s = %s;" % (indent, s.name, pr.p(e)) for s, e in repl]
+    lines += ["%sT %s = %s;" % (indent, s.name, pr.p(e)) for s, e in adj]
+    for j, x in enumerate(inputs):
+        lines.append("%s%s[%d] = %s;" % (indent, g_name, j, pr.p(sp.Add(*acc.get(x, [])))))
+    return "\n".join(lines)
 
 
 # --------------------------------------------------------------------------
@@ -525,6 +635,21 @@ def gen_numerics(S):
         right[i0] += n[d] * (-QR[1] ** 2 * half_g + half_g * hsR ** 2)
         left[i0] += n[d] * (QL[1] ** 2 * half_g - half_g * hsL ** 2)
     fn("numerical_fluctuations", args6, right + left)
+
+    # w^T of the Jacobian of [numerical_flux, numerical_fluctuations] with
+    # respect to both face states (the adjoint of a face; no counterpart in
+    # the reference's headers, which the GPU adjoint differentiates with dual
+    # numbers instead): g[0 .. nq) = d/dQ_minus, g[nq .. 2 nq) = d/dQ_plus.
+    # The variant that mirrors the reference's shipped header goes without,
+    # like that header.
+    if S.variant != "malpasset":
+        assert not any(str(s).startswith("Qaux") for e in flux + right + left for s in e.free_symbols)
+        w("    PORTABLE_FN static inline void numerical_flux_fluct_vjp(")
+        w(",\n".join("        " + a for a in args6 + ["const T* w", "T* g"]) + ")")
+        w("    {")
+        w(emit_vjp_body(flux + right + left, QL + QR))
+        w("    }")
+        w("")
 
     Q, Qa = arr("Q", nq), arr("Qaux", S.n_aux)
     hreg = sp.Max(sp.Float(1e-14), Q[1])
