@@ -57,6 +57,8 @@ typedef struct zsme_mesh {
     const double* face_normal;    /* [n_faces][2] area-weighted, support[0] -> support[1] */
     const int32_t* face_bc;       /* [n_faces] ZSME_FACE_INTERIOR, bc index >= 0, or
                                      ZSME_FACE_NO_CONDITION */
+    const uint8_t* cell_cfl_skip; /* [n_cells] nonzero: the cell does not constrain the CFL dt
+                                     (the halo cells of a mesh partition); NULL: none */
 } zsme_mesh;
 
 #define ZSME_LIMITER_NONE 0       /* settings.solver.limiter == "none" */
@@ -147,6 +149,14 @@ int zsme_get_state_device(zsme_handle* h, double* d_q_aos);
  * handle's stream wait (on the device) for every copy issued so far, e.g.
  * before recording a timing event on zsme_stream.  The staging buffers
  * (4 x n_cells x n_dof_q doubles) are allocated by the first call. */
+/* The state of n selected cells (caller ids; single-instance handles), for
+ * the halo exchange of a partitioned mesh (no counterpart in the reference,
+ * where PETSc's ghost-point scatters do this): q_aos [n][n_dof_q].  With
+ * on_device the cell list and q_aos are device pointers, else host.
+ * zsme_set_cells also recomputes those cells' aux variables; time, dt and
+ * the other cells are left alone. */
+int zsme_get_cells(zsme_handle* h, int32_t n, const int32_t* cells, double* q_aos, int32_t on_device);
+int zsme_set_cells(zsme_handle* h, int32_t n, const int32_t* cells, const double* q_aos, int32_t on_device);
 int zsme_set_state_async(zsme_handle* h, const double* q_aos, double t);
 int zsme_get_state_async(zsme_handle* h, double* q_aos);
 int zsme_stream_wait_copies(zsme_handle* h);

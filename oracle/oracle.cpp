@@ -148,6 +148,7 @@ struct Oracle : OracleBase {
     double time = 0.0, dt = 0.0;
     int n_unconv = 0;
     long long n_troubled = 0;   // cells redone at first order by MOOD, all steps
+    std::vector<unsigned char> cfl_skip;   // cells left out of the CFL minimum
 
     Oracle(const zsme_mesh* m, const zsme_settings* s, const double* p) {
         C = m->n_cells; F = m->n_faces; K = m->max_faces;
@@ -158,6 +159,7 @@ struct Oracle : OracleBase {
         cf.assign(m->cell_faces, m->cell_faces + K * C);
         fcell.assign(m->face_cells, m->face_cells + 2 * F);
         fbc.assign(m->face_bc, m->face_bc + F);
+        if (m->cell_cfl_skip) cfl_skip.assign(m->cell_cfl_skip, m->cell_cfl_skip + C);
         st = *s;
         // Zhang-Shu positivity holds for CFL <= 1/6 at order 2 (MUSCLSolver.hpp:33-38)
         if (st.reconstruction_order >= 2 && st.positivity == ZSME_POSITIVITY_ZHANG_SHU && st.cfl > 1.0 / 6.0)
@@ -692,6 +694,7 @@ par_for(C, [&](int c, int) {
                 if (r[0] > eig) eig = r[0];
             }
             if (eig < 1e-14) return;
+            if (!cfl_skip.empty() && cfl_skip[c]) return;   // a halo cell of a partition
             double rc = std::numeric_limits<double>::max();
             for (int k = 0; k < K; ++k) {
                 int f = cf[(size_t)c * K + k];

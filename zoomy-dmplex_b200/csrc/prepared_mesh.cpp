@@ -236,6 +236,10 @@ int prepare_mesh(const zsme_mesh& m, PreparedMesh& out) {
     p.n_inst = 1;
     p.inst_cell_off = {0, C};
     p.inst_face_off = {0, F};
+    // cells left out of the CFL minimum: no distance constrains them
+    if (m.cell_cfl_skip)
+        for (int c = 0; c < C; ++c)
+            if (m.cell_cfl_skip[p.old_of_new[c]]) p.rc[c] = DBL_MAX;
     return ZSME_OK;
 }
 

@@ -65,6 +65,8 @@ class SolverBase {
     virtual int set_params(const double* params) = 0;
     virtual int set_state(int inst, const double* q, double t, bool device) = 0;
     virtual int get_state(int inst, double* q, bool device) = 0;
+    virtual int get_cells(int n, const int* cells, double* q, bool device) = 0;
+    virtual int set_cells(int n, const int* cells, const double* q, bool device) = 0;
     virtual int set_state_async(const double* q, double t) = 0;
     virtual int get_state_async(double* q) = 0;
     virtual int stream_wait_copies() = 0;

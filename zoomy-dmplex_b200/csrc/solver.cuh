@@ -68,6 +68,7 @@ class Solver final : public SolverBase {
     cudaGraphExec_t graph_ = nullptr;
     // mesh
     DevBuf<int> slot_nbr_, slot_meta_, slot_face_, order_, old_of_new_, face_L_, face_R_, face_bc_;
+    DevBuf<int> new_of_old_, cells_tmp_;  // single-instance handles: caller -> device cell ids; zsme_*_cells staging
     DevBuf<int> cell_inst_, face_inst_;
     DevBuf<double> slot_dx_, slot_w_, vol_, rc_, fn_, farea_, fc_, fnr_;
     // state
@@ -206,6 +207,7 @@ class Solver final : public SolverBase {
         ZSME_CUDA(slot_face_.upload(pm_.slot_face, stream_));
         ZSME_CUDA(order_.upload(pm_.order, stream_));
         ZSME_CUDA(old_of_new_.upload(pm_.old_of_new, stream_));
+        if (n_inst_ == 1) ZSME_CUDA(new_of_old_.upload(pm_.new_of_old, stream_));
         ZSME_CUDA(slot_dx_.upload(pm_.slot_dx, stream_));
         ZSME_CUDA(slot_w_.upload(pm_.slot_w, stream_));
         ZSME_CUDA(vol_.upload(pm_.vol, stream_));
@@ -310,6 +312,47 @@ class Solver final : public SolverBase {
         ZSME_CUDA(cudaGetLastError());
         x_clamped_ = true;
         return ZSME_OK;
+    }
+
+    // ------------------------------------------------ cell subsets (halo exchange)
+    int cells_io(int n, const int* cells, double* q_get, const double* q_set, bool device) {
+        const int C = pm_.C;
+        if (n < 0 || n > C) return set_error(ZSME_ERR_ARG, "cell count out of range");
+        if (n == 0) return ZSME_OK;
+        const int* dc = cells;
+        double* dq = q_get ? q_get : const_cast<double*>(q_set);
+        if (!device) {
+            for (int e = 0; e < n; ++e)
+                if (cells[e] < 0 || cells[e] >= C) return set_error(ZSME_ERR_ARG, "cell id out of range");
+            ZSME_CUDA(cells_tmp_.alloc((size_t)C));
+            ZSME_CUDA(cudaMemcpyAsync(cells_tmp_.p, cells, n * sizeof(int), cudaMemcpyHostToDevice, stream_));
+            dc = cells_tmp_.p;
+            dq = tmp_a_.p;
+            if (q_set)
+                ZSME_CUDA(cudaMemcpyAsync(tmp_a_.p, q_set, (size_t)n * NQ * sizeof(double), cudaMemcpyHostToDevice,
+                                          stream_));
+        }
+        if (q_get) {
+            get_cells_kernel<<<blocks_for(n, 128), 128, 0, stream_>>>(x_.p, C, NQ, new_of_old_.p, dc, n, dq);
+            ZSME_CUDA(cudaGetLastError());
+            if (!device) {
+                ZSME_CUDA(cudaMemcpyAsync(q_get, tmp_a_.p, (size_t)n * NQ * sizeof(double), cudaMemcpyDeviceToHost,
+                                          stream_));
+                ZSME_CUDA(cudaStreamSynchronize(stream_));
+            }
+        } else {
+            set_cells_kernel<M><<<blocks_for(n, 128), 128, 0, stream_>>>(x_.p, aux_.p, C, new_of_old_.p, dc, n, dq,
+                                                                        params_.p);
+            ZSME_CUDA(cudaGetLastError());
+            if (!device) ZSME_CUDA(cudaStreamSynchronize(stream_));
+        }
+        return ZSME_OK;
+    }
+    int get_cells(int n, const int* cells, double* q, bool device) override {
+        return cells_io(n, cells, q, nullptr, device);
+    }
+    int set_cells(int n, const int* cells, const double* q, bool device) override {
+        return cells_io(n, cells, nullptr, q, device);
     }
 
     // ------------------------------------------------ asynchronous state I/O

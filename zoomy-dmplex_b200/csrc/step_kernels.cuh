@@ -634,6 +634,41 @@ static __global__ void end_step_kernel(StepDev sd, int i0, int ni, int mode, dou
 // [c0, c0 + cn) of the SoA arrays (row stride C) are instance-local rows
 // old_of_new[c] of the AoS buffer.
 static __global__ void set_time_kernel(double* t, double v) { *t = v; }
+// q_aos[e] = state of caller cell cells[e] (ids outside [0, C) are skipped)
+static __global__ void get_cells_kernel(const double* __restrict__ soa, int C, int nq,
+                                        const int* __restrict__ new_of_old, const int* __restrict__ cells, int n,
+                                        double* __restrict__ q_aos) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int o = cells[e];
+    if (o < 0 || o >= C) return;
+    const int c = new_of_old[o];
+    for (int i = 0; i < nq; ++i) q_aos[(size_t)e * nq + i] = soa[(size_t)i * C + c];
+}
+// the state of caller cell cells[e] = q_aos[e], and its aux recomputed
+template <class M>
+__global__ void set_cells_kernel(double* __restrict__ x, double* __restrict__ aux, int C,
+                                 const int* __restrict__ new_of_old, const int* __restrict__ cells, int n,
+                                 const double* __restrict__ q_aos, const double* __restrict__ params) {
+    constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int o = cells[e];
+    if (o < 0 || o >= C) return;
+    const int c = new_of_old[o];
+    double q[NQ], a[NA];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        q[i] = q_aos[(size_t)e * NQ + i];
+        x[(size_t)i * C + c] = q[i];
+    }
+#pragma unroll
+    for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
+    const double X0[3] = {0.0, 0.0, 0.0};
+    const auto ra = M::update_aux_variables(q, a, params, 0.0, X0);
+#pragma unroll
+    for (int i = 0; i < NA; ++i) aux[(size_t)i * C + c] = ra[i];
+}
 static __global__ void aos_to_soa_kernel(const double* __restrict__ aos, double* __restrict__ soa,
                                          const int* __restrict__ old_of_new, int c0, int cn, int C, int nq) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;

@@ -128,6 +128,16 @@ int zsme_get_state_device(zsme_handle* h, double* q) {
     if (!q) return set_error(ZSME_ERR_ARG, "null output");
     return h->s->get_state(0, q, true);
 }
+int zsme_get_cells(zsme_handle* h, int32_t n, const int32_t* cells, double* q, int32_t on_device) {
+    CHECK_SINGLE(h);
+    if (n > 0 && (!cells || !q)) return set_error(ZSME_ERR_ARG, "null cell list or state");
+    return h->s->get_cells(n, cells, q, on_device != 0);
+}
+int zsme_set_cells(zsme_handle* h, int32_t n, const int32_t* cells, const double* q, int32_t on_device) {
+    CHECK_SINGLE(h);
+    if (n > 0 && (!cells || !q)) return set_error(ZSME_ERR_ARG, "null cell list or state");
+    return h->s->set_cells(n, cells, q, on_device != 0);
+}
 int zsme_set_state_async(zsme_handle* h, const double* q, double t) {
     CHECK_SINGLE(h);
     if (!q) return set_error(ZSME_ERR_ARG, "null state");

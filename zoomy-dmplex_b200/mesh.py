@@ -27,6 +27,7 @@ as well.
 from __future__ import annotations
 
 import dataclasses
+from typing import Optional
 
 import numpy as np
 
@@ -47,6 +48,7 @@ class Mesh:
     face_normal: np.ndarray       # [F, 2] area-weighted, oriented cells[0] -> cells[1]
     face_bc: np.ndarray           # [F] int32: -1 interior, >= 0 bc index, -2 none
     name: str = "mesh"
+    cell_cfl_skip: Optional[np.ndarray] = None   # [C] nonzero: left out of the CFL minimum (halo cells)
 
     @property
     def n_cells(self):
@@ -100,6 +102,8 @@ class Mesh:
             face_centroid=np.ascontiguousarray(self.face_centroid, dtype=np.float64),
             face_normal=np.ascontiguousarray(self.face_normal, dtype=np.float64),
             face_bc=np.ascontiguousarray(self.face_bc, dtype=np.int32),
+            **({} if self.cell_cfl_skip is None
+               else {"cell_cfl_skip": np.ascontiguousarray(self.cell_cfl_skip, dtype=np.uint8)}),
         )
 
 

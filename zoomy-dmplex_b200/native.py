@@ -25,7 +25,7 @@ class ZsmeMesh(ct.Structure):
         ("dim", ct.c_int32), ("n_cells", ct.c_int32), ("n_faces", ct.c_int32), ("max_faces", ct.c_int32),
         ("cell_centroid", ct.c_void_p), ("cell_volume", ct.c_void_p), ("cell_faces", ct.c_void_p),
         ("face_cells", ct.c_void_p), ("face_centroid", ct.c_void_p), ("face_normal", ct.c_void_p),
-        ("face_bc", ct.c_void_p),
+        ("face_bc", ct.c_void_p), ("cell_cfl_skip", ct.c_void_p),
     ]
 
 
@@ -54,6 +54,9 @@ def make_mesh_struct(abi: dict):
     for k in ("cell_centroid", "cell_volume", "cell_faces", "face_cells", "face_centroid", "face_normal",
               "face_bc"):
         setattr(m, k, keep[k].ctypes.data)
+    if "cell_cfl_skip" in keep:
+        keep["cell_cfl_skip"] = np.ascontiguousarray(keep["cell_cfl_skip"], dtype=np.uint8)
+        m.cell_cfl_skip = keep["cell_cfl_skip"].ctypes.data
     return (m, keep)
 
 
@@ -88,6 +91,8 @@ def load():
     lib.zsme_get_aux.argtypes = [vp, P]
     lib.zsme_set_state_device.argtypes = [vp, vp, ct.c_double]
     lib.zsme_get_state_device.argtypes = [vp, vp]
+    lib.zsme_get_cells.argtypes = [vp, ct.c_int32, vp, vp, ct.c_int32]
+    lib.zsme_set_cells.argtypes = [vp, ct.c_int32, vp, vp, ct.c_int32]
     lib.zsme_set_state_async.argtypes = [vp, vp, ct.c_double]
     lib.zsme_get_state_async.argtypes = [vp, vp]
     lib.zsme_stream_wait_copies.argtypes = [vp]

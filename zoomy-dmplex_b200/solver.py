@@ -93,6 +93,20 @@ class Solver:
     def get_state_device(self, q_dev_ptr: int):
         native.check(self.lib.zsme_get_state_device(self.h, ct.c_void_p(q_dev_ptr)))
 
+    def get_cells(self, cells) -> np.ndarray:
+        """zsme_get_cells: the state of the given cells (caller ids), [n, nq]."""
+        c = np.ascontiguousarray(cells, dtype=np.int32)
+        q = np.empty((len(c), self.nq))
+        native.check(self.lib.zsme_get_cells(self.h, len(c), c.ctypes.data_as(ct.c_void_p), _p(q), 0))
+        return q
+
+    def set_cells(self, cells, q):
+        """zsme_set_cells: the state of the given cells (caller ids) and their
+        aux variables; time and dt unchanged."""
+        c = np.ascontiguousarray(cells, dtype=np.int32)
+        q = np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(len(c), self.nq))
+        native.check(self.lib.zsme_set_cells(self.h, len(c), c.ctypes.data_as(ct.c_void_p), _p(q), 0))
+
     def set_state_async(self, q_host_ptr: int, t: float = 0.0):
         """zsme_set_state_async: the state at host address q_host_ptr (AoS,
         caller order; page-locked for a truly asynchronous copy) becomes the
