@@ -74,9 +74,10 @@ class Solver final : public SolverBase {
     // state
     DevBuf<double> x_, w_, wl_, aux_, fs_, fb_, tmp_a_, tmp_b_, params_, dts_;
     DevBuf<double> xs_;  // MOOD: the state at the start of the step
+    DevBuf<int> mood_list_;  // MOOD: the troubled cells of the step (count in iscal_[6])
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
-    DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag, [5] deferred finalize cells
+    DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag, [5] deferred finalize cells, [6] MOOD cells
     DevBuf<int> fin_list_;        // [C] cells deferred to the generic Newton path
     int sm_count_ = 148;
     DevBuf<unsigned long long> ratio_;
@@ -231,7 +232,10 @@ class Solver final : public SolverBase {
         ZSME_CUDA(w_.alloc((size_t)NQ * C));
         ZSME_CUDA(wl_.alloc((size_t)NQ * C));
         ZSME_CUDA(aux_.alloc((size_t)NA * C));
-        if (st_.positivity == ZSME_POSITIVITY_MOOD) ZSME_CUDA(xs_.alloc((size_t)NQ * C));
+        if (st_.positivity == ZSME_POSITIVITY_MOOD) {
+            ZSME_CUDA(xs_.alloc((size_t)NQ * C));
+            ZSME_CUDA(mood_list_.alloc((size_t)C));
+        }
         ZSME_CUDA(fs_.alloc((size_t)2 * NQ * F));
         ZSME_CUDA(fb_.alloc((size_t)3 * NQ * F));
         // staging for state (NQ per cell) and aux (NA per cell) conversions
@@ -439,12 +443,20 @@ class Solver final : public SolverBase {
         mark(ZSME_KERNEL_PREP, true);
         const int gb = blocks_for(pm_.C, lc_.prep);
         if (st_.positivity != ZSME_POSITIVITY_NONE && st_.reconstruction_order >= 2) {
-            if (pm_.K == 3)
-                prep_wb_kernel<M, 3><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps,
-                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active);
-            else
-                prep_wb_kernel<M, 4><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps,
-                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active);
+            switch (lc_.prep_occ) {
+#define ZSME_PREPWB(OCC)                                                                                        \
+    case OCC:                                                                                                   \
+        if (pm_.K == 3)                                                                                         \
+            prep_wb_kernel<M, 3, OCC><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps, \
+                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active); \
+        else                                                                                                    \
+            prep_wb_kernel<M, 4, OCC><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps, \
+                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active); \
+        break;
+                ZSME_PREPWB(2) ZSME_PREPWB(3) ZSME_PREPWB(4) ZSME_PREPWB(6) ZSME_PREPWB(8)
+                default: ZSME_PREPWB(1)
+#undef ZSME_PREPWB
+            }
             mark(ZSME_KERNEL_PREP, false);
             return;
         }
@@ -608,9 +620,14 @@ class Solver final : public SolverBase {
                                 stream_);
         }
         if (mood) {   // a-posteriori first-order override of troubled cells
+            cudaMemsetAsync(iscal_.p + 6, 0, sizeof(int), stream_);
             mark(ZSME_KERNEL_MOOD, true);
-            mood_kernel<M, N><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, 0, pm_.C, x_.p, xs_.p, aux_.p,
-                                                                          params_.p, sd);
+            mood_detect_kernel<<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, 0, pm_.C, x_.p, sd, mood_list_.p,
+                                                                           iscal_.p + 6);
+            mark(ZSME_KERNEL_MOOD, false);
+            mark(ZSME_KERNEL_MOOD, true);
+            mood_kernel<M, N><<<std::min(blocks_for(pm_.C, 64), 8 * sm_count_), 64, 0, stream_>>>(
+                md_, x_.p, xs_.p, aux_.p, params_.p, sd, mood_list_.p, iscal_.p + 6);
             mark(ZSME_KERNEL_MOOD, false);
         }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
@@ -621,7 +638,7 @@ class Solver final : public SolverBase {
     }
     int launches_per_step() const override {
         return 3 + (st_.reconstruction_order < 2 ? 3 : 3 * st_.ssp_stages) +
-               (st_.positivity == ZSME_POSITIVITY_MOOD ? 1 : 0) + (st_.source ? 1 : 0);
+               (st_.positivity == ZSME_POSITIVITY_MOOD ? 2 : 0) + (st_.source ? 1 : 0);
     }
 
     int step(int nsteps, const double* dts_host) override {

@@ -368,9 +368,9 @@ __host__ __device__ __forceinline__ double venkat_eps2(double v) {
 //    momenta zero where h_f < wet_dry_eps.
 // std::min / std::max are written out as the selects they are, so NaN
 // propagates as in the reference.  positivity: ZSME_POSITIVITY_ZHANG_SHU or
-// _MOOD (no theta); eps: wet_dry_eps.
-template <class M, int KM>
-__global__ void __launch_bounds__(128) prep_wb_kernel(MeshDev m, Opts o, int positivity, double eps, int c0, int cn,
+// _MOOD (no theta); eps: wet_dry_eps.  MINB: the register cap, as prep_kernel's.
+template <class M, int KM, int MINB>
+__global__ void __launch_bounds__(128, MINB) prep_wb_kernel(MeshDev m, Opts o, int positivity, double eps, int c0, int cn,
                                                       const double* __restrict__ w, const double* __restrict__ wl,
                                                       const double* __restrict__ params, double* __restrict__ fs,
                                                       const int* __restrict__ active) {
@@ -491,27 +491,45 @@ __global__ void __launch_bounds__(128) prep_wb_kernel(MeshDev m, Opts o, int pos
 
 // ------------------------------------------------------------------ MOOD
 // Local MOOD (MUSCLSolver.hpp:150-170, 197-229; TransportStep.hpp:363-381,
-// 412-418), cells [c0, c0 + cn): a cell whose depth after the transport step
-// is below -1e-10 is overwritten by its first-order forward-Euler update from
-// the step's start state xs -- piecewise-constant clamped states on every
-// face of the cell, the face contributions summed in increasing original
-// face order, / volume -- and counted in diag[3].  No other cell changes, so
-// each troubled cell evaluates its own faces and no face pass is needed.
-// Launched between the last stage and finalize, whose constraints follow
-// the override as EnforcePhysicalConstraints does.
+// 412-418): a cell whose depth after the transport step is below -1e-10 is
+// overwritten by its first-order forward-Euler update from the step's start
+// state xs -- piecewise-constant clamped states on every face of the cell,
+// the face contributions summed in increasing original face order, / volume
+// -- and counted in diag[3].  No other cell changes, so each troubled cell
+// evaluates its own faces and no face pass is needed.  mood_detect_kernel
+// lists the troubled cells of [c0, c0 + cn) (warp-aggregated, so a light
+// kernel scans the mesh) and mood_kernel overrides the listed ones; both run
+// between the last stage and finalize, whose constraints follow the
+// override as EnforcePhysicalConstraints does.
+static __global__ void __launch_bounds__(128) mood_detect_kernel(MeshDev m, int c0, int cn, const double* __restrict__ x,
+                                                          StepDev sd, int* __restrict__ list, int* __restrict__ count) {
+    const int C = m.C;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = c0 + r;
+    bool bad = false;
+    if (r < cn) {
+        const int I = cell_instance(m, c);
+        bad = (!sd.active || sd.active[I]) && x[C + c] < -1.0e-10;
+    }
+    const unsigned bm = __ballot_sync(0xffffffffu, bad);
+    if (!bm) return;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) {
+        base = atomicAdd(count, __popc(bm));
+        atomicAdd(&sd.diag[3], __popc(bm));
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (bad) list[base + __popc(bm & ((1u << lane) - 1u))] = c;
+}
+
 template <class M, class N>
-__global__ void __launch_bounds__(128) mood_kernel(MeshDev m, int c0, int cn, double* __restrict__ x,
-                                                   const double* __restrict__ xs, const double* __restrict__ aux,
-                                                   const double* __restrict__ params, StepDev sd) {
+__device__ __forceinline__ void mood_cell(const MeshDev& m, int c, double* __restrict__ x,
+                                          const double* __restrict__ xs, const double* __restrict__ aux,
+                                          const double* __restrict__ params, const StepDev& sd) {
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
     const int C = m.C, F = m.F;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= cn) return;
-    const int c = c0 + r;
     const int I = cell_instance(m, c);
-    if (sd.active && !sd.active[I]) return;
-    if (!(x[C + c] < -1.0e-10)) return;
-    atomicAdd(&sd.diag[3], 1);
     const double* p = params + (size_t)I * m.np;
     const double t = sd.t[I], h = sd.dt_step[I];
     double qc[NQ], ac[NA];
@@ -590,6 +608,16 @@ __global__ void __launch_bounds__(128) mood_kernel(MeshDev m, int c0, int cn, do
     }
 #pragma unroll
     for (int i = 0; i < NQ; ++i) x[(size_t)i * C + c] = xs[(size_t)i * C + c] + h * acc[i];
+}
+
+template <class M, class N>
+__global__ void __launch_bounds__(64) mood_kernel(MeshDev m, double* __restrict__ x, const double* __restrict__ xs,
+                                                  const double* __restrict__ aux, const double* __restrict__ params,
+                                                  StepDev sd, const int* __restrict__ list,
+                                                  const int* __restrict__ count) {
+    const int n = *count;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+        mood_cell<M, N>(m, list[e], x, xs, aux, params, sd);
 }
 
 // --------------------------------------------------------------- step ends
