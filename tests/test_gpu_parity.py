@@ -258,3 +258,34 @@ def test_async_state_io_matches_blocking_calls():
     for k in range(3):
         assert np.array_equal(outs[k].numpy(), ref[k]), k
     assert np.array_equal(g.get_state(), ref[2])
+
+
+def test_failure_detection_without_a_fault():
+    """Health counters and zsme_sync's error: negative depths from the
+    limited step at CFL 1.5 on a wet/dry patchwork, and a non-finite value
+    planted in the state, are counted on the device and reported by
+    zsme_sync as ZSME_ERR_STATE; the handle stays usable."""
+    from zoomy_dmplex_b200.native import ZsmeError
+
+    c = cases.wet_dry_patchwork(24)
+    g = Solver(c.model, c.mesh, c.settings, params(c.model, c.params))
+    g.set_state(c.q0)
+    g.step(20)
+    d = g.sync(check=False)
+    assert d.n_negative_depth > 0 and d.n_nonfinite == 0
+    with pytest.raises(ZsmeError, match="negative-depth"):
+        g.sync()
+    # a non-finite depth survives the constraints (a non-finite momentum does
+    # not: the clamp max(-t, min(hu, t)), written as std::max / std::min
+    # selects, returns its bound for NaN, as in the reference)
+    q = c.q0.copy()
+    q[7, 1] = np.nan
+    g.set_state(q)
+    g.step(1)
+    d = g.sync(check=False)
+    assert d.n_nonfinite > 0
+    with pytest.raises(ZsmeError, match="non-finite"):
+        g.sync()
+    g.set_state(c.q0)                    # the handle is usable again
+    g.step(1)
+    assert np.all(np.isfinite(g.get_state()))
