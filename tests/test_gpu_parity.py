@@ -199,6 +199,23 @@ def test_config0_full_run():
     assert abs((q[:, 1] * vol).sum() - (c.q0[:, 1] * vol).sum()) < 1e-13
 
 
+def test_config1_full_run_per_step():
+    """Configuration 1 as specified: SME level 2 on the 240x240 jittered
+    grid, 500 steps, every step against the oracle (its dt imposed), bit for
+    bit -- the level-2 plugins call no cbrt."""
+    c = cases.level2(240)
+    g, o = pair(c)
+    for k in range(500):
+        _, dt = o.time()
+        o.step(1)
+        g.step(1, dts=[dt])
+        assert np.array_equal(g.get_state(), o.get_state()), "step %d" % k
+    q = g.get_state()
+    assert q[:, 1].min() >= 0
+    d = g.sync()
+    assert d.n_nonfinite == 0 and d.n_negative_depth == 0
+
+
 def test_device_pointer_state_roundtrip():
     torch = pytest.importorskip("torch")
     c = CASES["l2"]
