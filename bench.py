@@ -46,7 +46,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--side", type=int, default=1400, help="jittered grid side of the mesh")
+    ap.add_argument("--side", type=int, default=0, help="jittered grid side of the mesh (0: the case's own)")
+    ap.add_argument("--case", default="roofline_l4", choices=["roofline_l4", "level2", "plain_l0"],
+                    help="plain-step case: SME level 4 on 1400^2 (default), level 2 on 240^2, level 0 on 60^2")
     ap.add_argument("--cpu-side", type=int, default=600, help="grid side of the bounded CPU sample")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="the CPU sample steps until this much time has passed")
@@ -66,6 +68,10 @@ def parse():
     return ap.parse_args()
 
 
+CASE_SIDE = {"roofline_l4": 1400, "level2": 240, "plain_l0": 60}
+CASE_TEXT = {"roofline_l4": ("sme2d_l4 SME level 4", "Navier-slip Newton source"),
+             "level2": ("sme2d_l2 SME level 2", "Navier-slip Newton source"),
+             "plain_l0": ("sme2d_l0 SME level 0 (shallow water)", "Manning friction Newton source")}
 POS_TEXT = {"none": "", "zhang_shu": ", eta-well-balanced reconstruction + Zhang-Shu theta (CFL clamped to 1/6)",
             "mood": ", eta-well-balanced reconstruction + local MOOD"}
 
@@ -172,7 +178,7 @@ def params_of(case):
     return np.array(vals)
 
 
-def cpu_sample(side, steps=0, warm=1, seconds=0.0, positivity="none"):
+def cpu_sample(side, steps=0, warm=1, seconds=0.0, positivity="none", case="roofline_l4"):
     """The oracle (CPU restatement of the reference step) on a bounded
     sample of the workload: same model and physics on a side x side mesh,
     `steps` steps, or (steps = 0) one step at a time until `seconds` have
@@ -181,7 +187,7 @@ def cpu_sample(side, steps=0, warm=1, seconds=0.0, positivity="none"):
     import oracle_py as O
     from zoomy_dmplex_b200 import cases
 
-    c = cases.roofline_l4(side)
+    c = getattr(cases, case)(side)
     c.settings.positivity = positivity
     nt = O.set_threads(0)
     o = O.Oracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), params_of(c))
@@ -504,13 +510,14 @@ def main():
         if rank != 0:
             return 0
         # warmup + K timed oracle steps on the bounded sample
-        v, nt, C, dt, _ = cpu_sample(a.cpu_side, max(1, a.steps), warm=max(1, a.warmup), positivity=a.positivity)
+        v, nt, C, dt, _ = cpu_sample(a.cpu_side, max(1, a.steps), warm=max(1, a.warmup), positivity=a.positivity,
+                                     case=a.case)
         line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / max(1, a.steps),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": "sme2d_l4 jittered-Delaunay %dx%d (%d cells) order 2 Green-Gauss+TVD SSP-RK2"
-                           % (a.cpu_side, a.cpu_side, C), "parallelism": "host threads"},
+                "config": {"workload": "%s, jittered-Delaunay %dx%d (%d cells) order 2 Green-Gauss+TVD SSP-RK2"
+                           % (CASE_TEXT[a.case][0], a.cpu_side, a.cpu_side, C), "parallelism": "host threads"},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
                                  "sample": "%d steps of the CPU restatement on a %dx%d-grid mesh (%d cells)"
                                            % (a.steps, a.cpu_side, a.cpu_side, C)},
@@ -539,7 +546,8 @@ def main():
     if a.workload == "adjoint":
         return run_adjoint(a, dev, torch, dist, rank, world)
 
-    case = cases.roofline_l4(a.side)
+    side = a.side or CASE_SIDE[a.case]
+    case = getattr(cases, a.case)(side)
     case.settings.positivity = a.positivity
     C, F = case.mesh.n_cells, case.mesh.n_faces
     g = Solver(case.model, case.mesh, case.settings, params_of(case), device=dev)
@@ -673,13 +681,16 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "sme2d_l4 SME level 4, jittered-Delaunay %dx%d grid (%d cells, %d faces), "
+            "config": {"workload": "%s, jittered-Delaunay %dx%d grid (%d cells, %d faces), "
                                    "Hilbert-renumbered, order 2 Green-Gauss + Vacuum/TVD, SSP-RK2, CFL 0.45, "
-                                   "Navier-slip Newton source%s" % (a.side, a.side, C, F, POS_TEXT[a.positivity]),
+                                   "%s%s" % (CASE_TEXT[a.case][0], side, side, C, F, CASE_TEXT[a.case][1],
+                                             POS_TEXT[a.positivity]),
                        "model": case.model, "cells": C, "faces": F, "n_dof_q": nq, "positivity": a.positivity,
                        "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
-                       "l2_flush": "not needed: state %.0f MB + face states %.0f MB > 126 MB L2"
-                                   % (C * nq * 8 / 1e6, C * nq * 3 * 8 / 1e6),
+                       "l2_flush": ("not needed: state %.0f MB + face states %.0f MB > 126 MB L2"
+                                    % (C * nq * 8 / 1e6, C * nq * 3 * 8 / 1e6)) if C * nq * 32 > 126e6 else
+                                   ("not flushed: state %.1f MB and face states fit in L2 (a latency-bound size)"
+                                    % (C * nq * 8 / 1e6)),
                        "timing": "CUDA events on the solver stream around K graph-launched steps; "
                                  "per-kernel events in a second, profiled pass of K steps",
                        "launch": tuned or "default"},
@@ -697,7 +708,7 @@ def main():
                      "newton_unconverged": diag.n_newton_unconverged, "mood_cells": diag.n_mood_cells},
             "clocks": clocks}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        v, nt, Cs, dts, ns = cpu_sample(a.cpu_side, seconds=a.cpu_seconds, positivity=a.positivity)
+        v, nt, Cs, dts, ns = cpu_sample(a.cpu_side, seconds=a.cpu_seconds, positivity=a.positivity, case=a.case)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
                                 "sample": "%d steps of the CPU restatement (oracle) of the same model on a "
                                           "%dx%d-grid mesh (%d cells), %.1f s" % (ns, a.cpu_side,
