@@ -23,6 +23,7 @@ mesh is not partitioned: replicas, weak scaling).  ``--impl reference`` times
 the CPU restatement of the reference step (the oracle) on the host cores.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -118,6 +119,36 @@ NCU_DRAM_BYTES_PER_CELL = {
     "sme2d_l4/gather": ((1106.1 + 282.5) + (1188.4 + 141.4)) * 1e6 / 2 / 1618202,
     "sme2d_l4/finalize": (181.4 + 148.5) * 1e6 / 1618202,
 }
+
+
+# Algorithmic FP64 operations per unit of each kernel: +, -, *, /, sqrt,
+# cbrt and pow on state and parameter values (selects, min / max and fabs
+# are not counted), counted by the CPU restatement of the reference step on
+# an operation-counting scalar over 2 steps of each configuration's 40x40
+# grid (tests/test_flop_count.py recounts them).  prep and gather: per cell
+# and stage; flux: per face and stage (the grid's mean over interior and
+# wall faces); finalize: per cell and step (constraints, Newton source,
+# CFL dt).
+FP64_FLOPS = {
+    "sme2d_l4": {"prep": 579.524, "flux": 1256.84, "gather": 126.0, "finalize": 2829.0},
+    "sme2d_l2": {"prep": 392.726, "flux": 528.504, "gather": 84.0, "finalize": 1268.0},
+    "sme2d_l0": {"prep": 204.313, "flux": 204.168, "gather": 42.0, "finalize": 126.0},
+    "sme2d_l1": {"prep": 311.716, "flux": 332.336, "gather": 63.0, "finalize": 523.766},
+}
+
+
+def fp64_flops(kind, model, C, F, stages):
+    """Algorithmic FP64 operations of one launch of a step kernel (None
+    where the table has no figure)."""
+    t = FP64_FLOPS.get(model, {})
+    if kind not in t:
+        return None
+    return t[kind] * (F if kind == "flux" else C)
+
+
+def fp64_flops_per_cell_step(model, C, F, stages):
+    t = FP64_FLOPS[model]
+    return stages * (t["prep"] + t["gather"] + t["flux"] * F / C) + t["finalize"]
 
 
 # ------------------------------------------------------------------ clocks
@@ -620,6 +651,35 @@ def main():
     kernel_share = {k: {"ms_per_launch": v[0] / v[1], "launches": v[1], "share": v[0] / max(1e-30, sum(
         x[0] for x in prof.values()))} for k, v in prof.items() if v[1]}
 
+    # FP64 roofline: the step does ~10 algorithmic flops per algorithmic byte,
+    # above the FP64 ridge, so its kernels are also held against the measured
+    # FP64 rate (FMA chains, 2 flops per FMA).  The kernels compile without
+    # FMA contraction (bit-identical rounding), one add or multiply per
+    # instruction: half that rate is their ceiling ("unfused").
+    roofline_fp64 = None
+    fp64_step = None
+    if case.model in FP64_FLOPS and a.positivity == "none":
+        pk = ctypes.c_double()
+        native.check(native.load().zsme_fp64_fma_peak(dev, ctypes.byref(pk)))
+        peak_tf = pk.value
+        s_ = case.settings.ssp_stages
+        for k, v in kernel_share.items():
+            fl = fp64_flops(k, case.model, C, F, s_)
+            if fl is not None:
+                v["fp64_tflops"] = fl / (v["ms_per_launch"] / 1e3) / 1e12
+        fk = max((k for k in kernel_share if "fp64_tflops" in kernel_share[k]),
+                 key=lambda k: kernel_share[k]["fp64_tflops"])
+        fl = fp64_flops(fk, case.model, C, F, s_)
+        ach = kernel_share[fk]["fp64_tflops"]
+        roofline_fp64 = {"bound": "fp64", "kernel": fk, "achieved": ach, "peak": peak_tf, "unit": "TFLOP/s",
+                         "frac": ach / peak_tf, "frac_of_unfused": ach / (peak_tf / 2),
+                         "flops_per_launch": fl,
+                         "peak_source": "measured on this GPU: zsme_fp64_fma_peak (FMA chains, 2 flops per FMA)"}
+        fc = fp64_flops_per_cell_step(case.model, C, F, s_)
+        ach_s = fc * C / (step_ms / 1e3) / 1e12
+        fp64_step = {"flops_per_cell_step": fc, "flop_per_byte": fc / sb, "achieved": ach_s, "peak": peak_tf,
+                     "unit": "TFLOP/s", "frac": ach_s / peak_tf, "frac_of_unfused": ach_s / (peak_tf / 2)}
+
     # end to end through the public API: pinned host state in, one step, state out
     ne = a.e2e_steps or a.steps
     q_host = torch.from_numpy(np.ascontiguousarray(case.q0)).pin_memory()
@@ -694,7 +754,8 @@ def main():
                        "timing": "CUDA events on the solver stream around K graph-launched steps; "
                                  "per-kernel events in a second, profiled pass of K steps",
                        "launch": tuned or "default"},
-            "roofline": roofline, "roofline_step": roofline_step, "kernels": kernel_share,
+            "roofline": roofline, "roofline_step": roofline_step, "roofline_fp64": roofline_fp64,
+            "fp64_step": fp64_step, "kernels": kernel_share,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "steps": ne,
                     "api": "per step: zsme_set_state_async(pinned host) + zsme_step(1) + "

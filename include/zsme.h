@@ -274,6 +274,15 @@ int zsme_compute_dt_noalloc(const char* model, int32_t n_cells, const double* d_
                             const double* d_aux_aos, const double* d_rc, const double* d_params,
                             double cfl, double* d_dt, void* stream);
 
+/* Measured FP64 rate of GPU `device`, for the FP64 roofline of the step's
+ * arithmetic-bound kernels.  No counterpart in the reference.  Runs
+ * independent chains of fused multiply-adds on every SM for a few
+ * milliseconds and writes the best of five timed launches, counting two
+ * flops per FMA, to *tflops (TFLOP/s).  The step's kernels compile without
+ * FMA contraction and issue one add or multiply per instruction, so half of
+ * this rate bounds them. */
+int zsme_fp64_fma_peak(int device, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,6 +28,7 @@
 // pinned only by this restatement.
 #include "model_prelude.h"
 #include "dual.h"
+#include "flopcount.h"
 #include "zsme.h"
 
 #include <cstdio>
@@ -123,9 +124,10 @@ struct OracleBase {
     virtual void get_tangent(double*) const {}
 };
 
-// S: the scalar of state and parameters -- double, or Dual<1> for the
+// S: the scalar of state and parameters -- double, Dual<1> for the
 // tangent-linear run (derivative along one seeded direction, the branches
-// decided by the values exactly as in the double run).
+// decided by the values exactly as in the double run), or Counted to count
+// the step's floating-point operations (flopcount.h).
 template <template <typename> class MT, template <typename> class NT, class Scalar = double>
 struct Oracle : OracleBase {
     using T = Scalar;
@@ -176,6 +178,10 @@ struct Oracle : OracleBase {
 
     int nq() const override { return NQ; }
     int naux() const override { return NA; }
+    // the phase the operation counters of a Counted instance charge
+    static void ph(int p) {
+        if constexpr (std::is_same<T, zsme::Counted>::value) zsme_flops::phase = p;
+    }
     void set_params(const double* p) override { params.assign(p, p + M::n_parameters); }
     int newton_unconverged() const override { return n_unconv; }
     long long mood_cells() const override { return n_troubled; }
@@ -485,6 +491,7 @@ par_for(C, [&](int c, int) {
 
     // ------------------------------------------------------------- FormRHS
     void form_rhs(double t, const std::vector<T>& xg, std::vector<T>& f) {
+        ph(zsme_flops::PREP);
         std::vector<T> xl = xg, al = A;          // local copies
         update_state_vec(xl, al);
         const bool o2 = st.reconstruction_order >= 2;
@@ -527,10 +534,12 @@ par_for(F, [&](int f, int) {
             T* fl = ncR + NQ;
             if (R >= 0) {
                 T qLf[NQ], qRf[NQ], aLf[NA], aRf[NA];
+                ph(zsme_flops::PREP);
                 recon(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
                             o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
                 recon(&xl[(size_t)R * NQ], o2 ? &G[(size_t)R * NQ * DIM] : nullptr, &cc[2 * R], &fc[2 * f],
                             o2 ? &vmin[(size_t)R * NQ] : nullptr, o2 ? &vmax[(size_t)R * NQ] : nullptr, qRf);
+                ph(zsme_flops::FACE);
                 for (int i = 0; i < NA; ++i) { aLf[i] = al[(size_t)L * NA + i]; aRf[i] = al[(size_t)R * NA + i]; }
                 auto ra = M::update_aux_variables(qLf, aLf, params.data(), 0.0, xf);
                 for (int i = 0; i < NA; ++i) aLf[i] = ra[i];
@@ -546,8 +555,10 @@ par_for(F, [&](int f, int) {
                 active[f] = 1;
             } else if (fbc[f] >= 0) {
                 T qLf[NQ], aLf[NA], aRf[NA];
+                ph(zsme_flops::PREP);
                 recon(&xl[(size_t)L * NQ], o2 ? &G[(size_t)L * NQ * DIM] : nullptr, &cc[2 * L], &fc[2 * f],
                             o2 ? &vmin[(size_t)L * NQ] : nullptr, o2 ? &vmax[(size_t)L * NQ] : nullptr, qLf);
+                ph(zsme_flops::FACE);
                 for (int i = 0; i < NA; ++i) aLf[i] = al[(size_t)L * NA + i];
                 auto ra = M::update_aux_variables(qLf, aLf, params.data(), t, xf);
                 for (int i = 0; i < NA; ++i) aLf[i] = ra[i];
@@ -564,6 +575,7 @@ par_for(F, [&](int f, int) {
             }
         });
         // per cell: accumulate in increasing face order, then / volume
+        ph(zsme_flops::GATHER);
         f.assign((size_t)C * NQ, 0.0);
 par_for(C, [&](int c, int) {
             T* fcq = &f[(size_t)c * NQ];
@@ -745,13 +757,13 @@ par_for(C, [&](int c, int) {
     // Seed the tangent direction of the (constrained) state and of the
     // parameters; read the state's tangent.  Dual<1> instances only.
     void set_tangent(const double* dq, const double* dp) override {
-        if constexpr (!std::is_same<T, double>::value) {
+        if constexpr (std::is_same<T, zsme::Dual<1>>::value) {
             for (size_t i = 0; i < X.size(); ++i) X[i].d[0] = dq ? dq[i] : 0.0;
             for (size_t k = 0; k < params.size(); ++k) params[k].d[0] = dp ? dp[k] : 0.0;
         }
     }
     void get_tangent(double* dq) const override {
-        if constexpr (!std::is_same<T, double>::value)
+        if constexpr (std::is_same<T, zsme::Dual<1>>::value)
             for (size_t i = 0; i < X.size(); ++i) dq[i] = X[i].d[0];
     }
     void update_state() override { update_state_vec(X, A); }
@@ -763,6 +775,7 @@ par_for(C, [&](int c, int) {
         const size_t n = X.size();
         if (st.reconstruction_order < 2) {
             form_rhs(t0, X, F);
+            ph(zsme_flops::GATHER);
             for (size_t i = 0; i < n; ++i) X[i] = X[i] + h * F[i];
             return;
         }
@@ -771,10 +784,12 @@ par_for(C, [&](int c, int) {
         for (int i = 0; i < s - 1; ++i) {
             double stage_time = t0 + h * (i / (s - 1.));
             form_rhs(stage_time, w, F);
+            ph(zsme_flops::GATHER);
             const double a = h / (s - 1.);
             for (size_t k = 0; k < n; ++k) w[k] = w[k] + a * F[k];
         }
         form_rhs(t0 + h, w, F);
+        ph(zsme_flops::GATHER);
         const double al = (s - 1.) / s, be = h / s, ga = 1. / s;
         for (size_t k = 0; k < n; ++k) X[k] = al * w[k] + be * F[k] + ga * X[k];
     }
@@ -878,6 +893,7 @@ par_for(C, [&](int c, int) {
             std::vector<T> Xs;
             if (mood) Xs = X;
             ts_step(t0, d0);
+            ph(zsme_flops::FINAL);
             time = t0 + d0;
             update_state_vec(X, A);                            // EnforcePhysicalConstraints
             if (mood) mood_override(t0, d0, Xs);
@@ -971,6 +987,7 @@ struct Entry {
                const double*, double*);
     int nq, na, np, dim;
     OracleBase* (*make_tlm)(const zsme_mesh*, const zsme_settings*, const double*);
+    OracleBase* (*make_counting)(const zsme_mesh*, const zsme_settings*, const double*);
 };
 
 template <template <typename> class MT, template <typename> class NT>
@@ -981,13 +998,18 @@ template <template <typename> class MT, template <typename> class NT>
 OracleBase* make_tlm(const zsme_mesh* m, const zsme_settings* s, const double* p) {
     return new Oracle<MT, NT, zsme::Dual<1>>(m, s, p);
 }
+template <template <typename> class MT, template <typename> class NT>
+OracleBase* make_counting(const zsme_mesh* m, const zsme_settings* s, const double* p) {
+    return new Oracle<MT, NT, zsme::Counted>(m, s, p);
+}
 
 #define ORACLE_ENTRY(NS)                                                                   \
     Entry{#NS, &make_oracle<NS::Model, NS::Numerics>, &pointwise<NS::Model, NS::Numerics>,   \
           &flux_vjp<NS::Model, NS::Numerics>,                                              \
           NS::Model<double>::n_dof_q,                                                      \
           NS::Model<double>::n_dof_qaux, NS::Model<double>::n_parameters,                  \
-          NS::Model<double>::dimension, &make_tlm<NS::Model, NS::Numerics>}
+          NS::Model<double>::dimension, &make_tlm<NS::Model, NS::Numerics>,                 \
+          &make_counting<NS::Model, NS::Numerics>}
 
 const Entry kEntries[] = {
     ORACLE_ENTRY(sme1d_l0_malpasset), ORACLE_ENTRY(sme2d_l0), ORACLE_ENTRY(sme2d_l1),
@@ -1050,6 +1072,29 @@ int oracle_create_tlm(const char* model, const zsme_mesh* mesh, const zsme_setti
             return 0;
         }
     return fail(ZSME_ERR_MODEL, std::string("unknown model ") + model);
+}
+// Operation-counting instance (flopcount.h): the same restatement on
+// Counted numbers; run it with one oracle thread.
+int oracle_create_counting(const char* model, const zsme_mesh* mesh, const zsme_settings* s, const double* params,
+                           void** out) {
+    for (auto& e : kEntries)
+        if (!std::strcmp(e.name, model)) {
+            if (mesh->dim != e.dim) return fail(ZSME_ERR_ARG, "mesh dim != model dimension");
+            *out = e.make_counting(mesh, s, params);
+            return 0;
+        }
+    return fail(ZSME_ERR_MODEL, std::string("unknown model ") + model);
+}
+// out[phase * NOPS + op] (flopcount.h's Phase x Op), counted since the last reset
+int oracle_flop_counts(long long* out) {
+    for (int p = 0; p < zsme_flops::NPH; ++p)
+        for (int o = 0; o < zsme_flops::NOPS; ++o) out[p * zsme_flops::NOPS + o] = zsme_flops::counts[p][o];
+    return zsme_flops::NPH * zsme_flops::NOPS;
+}
+int oracle_flop_reset() {
+    for (auto& r : zsme_flops::counts)
+        for (auto& v : r) v = 0;
+    return 0;
 }
 int oracle_set_tangent(void* h, const double* dq, const double* dp) { ((OracleBase*)h)->set_tangent(dq, dp); return 0; }
 int oracle_get_tangent(void* h, double* dq) { ((OracleBase*)h)->get_tangent(dq); return 0; }

@@ -62,6 +62,8 @@ def load(ref: bool = False):
     lib.oracle_model_info.argtypes = [ct.c_char_p] + [ct.POINTER(ct.c_int)] * 4
     lib.oracle_pointwise.argtypes = [ct.c_char_p, ct.c_int, P, P, P, P, P, P, ct.c_double, P]
     lib.oracle_flux_vjp.argtypes = [ct.c_char_p, P, P, P, P, P, P, P, P]
+    lib.oracle_create_counting.argtypes = [ct.c_char_p, vp, vp, P, ct.POINTER(vp)]
+    lib.oracle_flop_counts.argtypes = [ct.POINTER(ct.c_longlong)]
     _libs[path] = lib
     return lib
 
@@ -208,6 +210,42 @@ class Oracle:
     def mood_cells(self):
         """Cells redone at first order by MOOD over all steps so far."""
         return self.lib.oracle_mood_cells(self.h)
+
+
+FLOP_PHASES = ("prep", "face", "gather", "final")
+FLOP_OPS = ("add", "mul", "div", "sqrt", "other")
+
+
+def flop_counts(model: str, mesh_abi: dict, settings_struct, params, q0, steps: int = 1, ref=False):
+    """The floating-point operations of `steps` oracle steps from q0, counted
+    by the Counted-scalar instance (flopcount.h): {phase: {op: count}} with
+    phases prep / face / gather / final and ops add (+ and -), mul, div, sqrt,
+    other (cbrt, pow).  set_state's constraints and initial dt are not in
+    the count.  Runs the oracle on one thread (the counters are global) and
+    restores all threads afterwards."""
+    from zoomy_dmplex_b200 import native
+
+    lib = load(ref)
+    keep = native.make_mesh_struct(mesh_abi)
+    pr = np.ascontiguousarray(params, dtype=np.float64)
+    h = ct.c_void_p()
+    if lib.oracle_create_counting(model.encode(), ct.addressof(keep[0]), ct.addressof(settings_struct), _p(pr),
+                                  ct.byref(h)):
+        raise RuntimeError(lib.oracle_last_error().decode())
+    lib.oracle_set_threads(1)
+    try:
+        q = np.ascontiguousarray(q0, dtype=np.float64)
+        lib.oracle_set_state(h, _p(q), 0.0)
+        lib.oracle_flop_reset()
+        lib.oracle_step(h, int(steps))
+        out = (ct.c_longlong * (len(FLOP_PHASES) * len(FLOP_OPS)))()
+        lib.oracle_flop_counts(out)
+    finally:
+        lib.oracle_destroy(h)
+        lib.oracle_set_threads(0)
+    v = list(out)
+    n = len(FLOP_OPS)
+    return {ph: dict(zip(FLOP_OPS, v[i * n:(i + 1) * n])) for i, ph in enumerate(FLOP_PHASES)}
 
 
 class TangentOracle(Oracle):

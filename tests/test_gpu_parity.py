@@ -306,3 +306,15 @@ def test_failure_detection_without_a_fault():
     g.set_state(c.q0)                    # the handle is usable again
     g.step(1)
     assert np.all(np.isfinite(g.get_state()))
+
+
+def test_fp64_fma_peak_is_measured():
+    """zsme_fp64_fma_peak times FMA chains on every SM; a B200's FP64 rate
+    lies in the tens of TFLOP/s."""
+    import ctypes as ct
+
+    from zoomy_dmplex_b200 import native
+
+    v = ct.c_double()
+    native.check(native.load().zsme_fp64_fma_peak(0, ct.byref(v)))
+    assert 5.0 < v.value < 200.0, v.value

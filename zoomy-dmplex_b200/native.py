@@ -112,6 +112,7 @@ def load():
     lib.zsme_set_profiling.argtypes = [vp, ct.c_int]
     lib.zsme_read_profile.argtypes = [vp, P, ct.POINTER(ct.c_int64)]
     lib.zsme_compute_dt_noalloc.argtypes = [ct.c_char_p, ct.c_int32, vp, vp, vp, vp, ct.c_double, vp, vp]
+    lib.zsme_fp64_fma_peak.argtypes = [ct.c_int, P]
     lib.zsme_batch_create.argtypes = [ct.c_char_p, ct.c_int32, vp, vp, P, ct.c_int, ct.POINTER(vp)]
     lib.zsme_batch_size.argtypes = [vp, ct.POINTER(ct.c_int32)]
     lib.zsme_batch_set_state.argtypes = [vp, ct.c_int32, P, ct.c_double]
