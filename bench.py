@@ -153,16 +153,66 @@ def fp64_flops_per_cell_step(model, C, F, stages):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
+    """SM clock, power and clock-event reasons of the timed GPU, sampled
+    while the timed region runs: NVML every 10 ms (the GPU found by its UUID,
+    so CUDA_VISIBLE_DEVICES does not matter; start() returns after the
+    first sample and stop() takes a last one), else nvidia-smi every 200 ms.
+    Read-only queries."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.nv = None
         self.lines = []
+        self.samples = []
+
+    def _nvml_handle(self, nv):
+        import torch
+
+        pr = torch.cuda.get_device_properties(self.index)
+        try:
+            return nv.nvmlDeviceGetHandleByUUID("GPU-" + str(pr.uuid))
+        except Exception:
+            return nv.nvmlDeviceGetHandleByPciBusId_v2("%08X:%02X:%02X.0" % (
+                pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id))
+
+    def _nvml_sample(self):
+        nv, h = self.nv, self.h
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), nv.nvmlDeviceGetPowerUsage(h) / 1e3,
+                             tuple(n for n, b in zip(self.NAMES, bits) if r & b)))
+
+    def _poll(self):
+        while not self.done.is_set():
+            try:
+                self._nvml_sample()
+            except Exception:
+                break
+            self.first.set()
+            self.done.wait(0.01)
+        self.first.set()
 
     def start(self):
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = self._nvml_handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.done, self.first = threading.Event(), threading.Event()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            self.first.wait(2.0)
+            return
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -177,6 +227,19 @@ class ClockSampler:
             self.lines.append(ln.strip())
 
     def stop(self):
+        if self.nv is not None:
+            self.done.set()
+            self.t.join(timeout=2.0)
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
+            if not self.samples:
+                return None
+            return {"sm_mhz": statistics.median(x[0] for x in self.samples), "sm_max_mhz": self.max_mhz,
+                    "power_w_median": statistics.median(x[1] for x in self.samples),
+                    "reasons": sorted({n for x in self.samples for n in x[2]}), "samples": len(self.samples),
+                    "source": "NVML, 10 ms"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -193,10 +256,9 @@ class ClockSampler:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 # ------------------------------------------------------------------ cases
