@@ -74,6 +74,7 @@ def small_cases():
         "l2": cases.level2(40),
         "l4": cases.roofline_l4(40),
         "1d": case_1d(),
+        "mixed": cases.mixed_level2(24),      # triangles + quadrilaterals, empty face slots
     }
 
 
@@ -92,7 +93,7 @@ def test_rhs_one_step_map(name, order, grad):
     assert_close(fg, fo, what="rhs %s o%d %s" % (name, order, grad))
 
 
-@pytest.mark.parametrize("name", ["l2", "l4", "1d"])
+@pytest.mark.parametrize("name", ["l2", "l4", "1d", "mixed"])
 def test_rhs_bitwise_without_cbrt(name):
     """No FMA contraction + IEEE sqrt/div: identical rounding."""
     c = CASES[name]
@@ -118,7 +119,8 @@ def test_constraints_source_dt(name):
     assert_close(g.get_state(), o.get_state(), what="update_state")
 
 
-@pytest.mark.parametrize("name,steps", [("l0", 200), ("l1", 60), ("l2", 60), ("l4", 30), ("1d", 100)])
+@pytest.mark.parametrize("name,steps", [("l0", 200), ("l1", 60), ("l2", 60), ("l4", 30), ("1d", 100),
+                                        ("mixed", 60)])
 def test_trajectory_per_step(name, steps):
     """Free-running oracle; the GPU takes the oracle's dt each step; every
     step is compared."""

@@ -13,9 +13,10 @@ from test_gpu_parity import params
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,nparts", [("l2", 2), ("l2", 4), ("l4", 3)])
+@pytest.mark.parametrize("name,nparts", [("l2", 2), ("l2", 4), ("l4", 3), ("mixed", 3)])
 def test_partitioned_equals_undivided(name, nparts):
-    c = cases.level2(40) if name == "l2" else cases.roofline_l4(36)
+    c = {"l2": lambda: cases.level2(40), "l4": lambda: cases.roofline_l4(36),
+         "mixed": lambda: cases.mixed_level2(30)}[name]()
     p = params(c.model, c.params)
     g = Solver(c.model, c.mesh, c.settings, p)
     g.set_state(c.q0)

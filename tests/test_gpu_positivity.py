@@ -41,6 +41,7 @@ CASES = {
     "patch_l1": cases.wet_dry_patchwork(24, seed=5, level=1),
     "l2": cases.level2(40),
     "l4": cases.roofline_l4(40),
+    "mixed": cases.mixed_level2(24),
 }
 
 
@@ -54,7 +55,7 @@ def test_rhs_bitwise(name, pos):
 
 
 @pytest.mark.parametrize("pos", ["zhang_shu", "mood"])
-@pytest.mark.parametrize("name", ["patch_l0", "patch_l1", "l2"])
+@pytest.mark.parametrize("name", ["patch_l0", "patch_l1", "l2", "mixed"])
 def test_trajectory_per_step(name, pos):
     """Free-running oracle; the GPU takes the oracle's dt each step."""
     c = CASES[name]

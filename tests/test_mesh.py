@@ -66,3 +66,54 @@ def test_interval_and_msh_roundtrip(tmp_path):
     M.write_msh(str(p), m2)
     m3 = M.read_msh(str(p))
     assert m3.n_cells == m2.n_cells and np.allclose(m3.cell_volume.sum(), 1.0)
+
+
+def test_mixed_triangles_and_quadrilaterals():
+    """Ragged cells: -1 padded rows (triangles among quadrilaterals) have
+    an empty face slot; the geometry is closed and consistently oriented,
+    the numbering is first-encounter as for uniform meshes, and a gmsh file
+    of the mesh reads back bit for bit."""
+    m = M.mixed_square(10, seed=2)
+    nv = (m.cells >= 0).sum(1)
+    assert set(nv) == {3, 4} and m.max_faces == 4
+    assert np.array_equal(m.cell_faces < 0, m.cells < 0)     # one empty slot per triangle
+    assert abs(m.cell_volume.sum() - 1.0) < 1e-12 and (m.cell_volume > 0).all()
+    C = m.n_cells
+    s = np.zeros((C, 2))
+    for k in range(m.max_faces):
+        f = m.cell_faces[:, k]
+        ok = f >= 0
+        sign = np.where(m.face_cells[f[ok], 0] == np.arange(C)[ok], 1.0, -1.0)
+        s[ok] += sign[:, None] * m.face_normal[f[ok]]
+    assert np.abs(s).max() < 1e-14
+    d = m.face_centroid - m.cell_centroid[m.face_cells[:, 0]]
+    assert ((d * m.face_normal).sum(1) > 0).all()
+    assert m.n_faces == C + m.vertices.shape[0] - 1                 # Euler, disc-like
+    first = np.full(m.n_faces, -1)
+    for c in range(C):
+        for f in m.cell_faces[c]:
+            if f >= 0 and first[f] < 0:
+                first[f] = c
+    assert (first == m.face_cells[:, 0]).all()
+    fcs = m.cell_faces
+    interior = (fcs >= 0) & (m.face_cells[np.maximum(fcs, 0), 1] >= 0)
+    assert np.array_equal((m.cell_nbrs() >= 0).sum(1), interior.sum(1))
+
+
+def test_mixed_mesh_gmsh_roundtrip(tmp_path):
+    from zoomy_dmplex_b200 import caseio
+
+    m = M.mixed_square(7, seed=4)
+    p = str(tmp_path / "mixed.msh")
+    caseio.write_gmsh(p, m, np.where(m.face_cells[:, 1] < 0, 1, 0), {1: "default"})
+    r = caseio.read_gmsh(p)
+    for a in ("cells", "cell_centroid", "cell_volume", "cell_faces", "face_cells", "face_centroid",
+              "face_normal", "face_bc"):
+        assert np.array_equal(getattr(m, a), getattr(r, a)), a
+    v = str(tmp_path / "mixed.vtu")
+    caseio.write_vtu(v, m, np.zeros((m.n_cells, 3)))
+    d = caseio.read_vtu_cell_data(v)
+    nv = (m.cells >= 0).sum(1)
+    assert np.array_equal(d["offsets"], np.cumsum(nv))
+    assert np.array_equal(d["types"], np.where(nv == 3, 5, 9))
+    assert np.array_equal(d["connectivity"], m.cells[m.cells >= 0])

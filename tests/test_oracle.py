@@ -87,3 +87,23 @@ def test_source_newton_converges():
     o = make(c)
     o.source(1e-2)
     assert o.newton_unconverged() == 0
+
+
+def test_mixed_mesh_conservation_and_rest():
+    """Triangles and quadrilaterals in one mesh (empty face slots): mass is
+    conserved to rounding with walls, depths stay positive, and the lake at
+    rest stays at rest at first order."""
+    c = cases.mixed_level2(16)
+    o = make(c)
+    m0 = (c.q0[:, 1] * c.mesh.cell_volume).sum()
+    o.step(40)
+    q = o.get_state()
+    assert abs((q[:, 1] * c.mesh.cell_volume).sum() - m0) < 1e-14
+    assert q[:, 1].min() > 0.0
+    c.q0[:, 1] = 1.0 - c.q0[:, 0]
+    c.q0[:, 2:] = 0.0
+    o = make(c, reconstruction_order=1)
+    o.step(20)
+    q = o.get_state()
+    assert np.abs(q[:, 0] + q[:, 1] - 1.0).max() < 1e-14
+    assert np.abs(q[:, 2:]).max() < 1e-14

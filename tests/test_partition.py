@@ -84,9 +84,9 @@ def _oracle_partitioned(case, nparts, steps):
     return out, ors[0].time()[0]
 
 
-@pytest.mark.parametrize("nparts", [2, 4])
-def test_partitioned_oracle_equals_undivided(nparts):
-    c = cases.level2(24)
+@pytest.mark.parametrize("nparts,mixed", [(2, False), (4, False), (3, True)])
+def test_partitioned_oracle_equals_undivided(nparts, mixed):
+    c = cases.mixed_level2(18) if mixed else cases.level2(24)
     steps = 15
     o = O.Oracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), params(c))
     o.set_state(c.q0)

@@ -102,9 +102,10 @@ def boundary_map(names: Dict[str, tuple], boundary_tags: Sequence[str], dim: int
 
 
 def read_gmsh(path: str, boundary_tags: Sequence[str] = ("default",)) -> Mesh:
-    """A gmsh 2.2 ASCII mesh: triangles or quadrilaterals (2-D) or segments
-    (1-D) as cells, in file order; boundary faces carry the model boundary
-    index of their element's physical tag, or FACE_NO_CONDITION."""
+    """A gmsh 2.2 ASCII mesh: triangles and/or quadrilaterals (2-D; a mixed
+    mesh becomes -1 padded [C, 4] cells) or segments (1-D) as cells, in file
+    order; boundary faces carry the model boundary index of their element's
+    physical tag, or FACE_NO_CONDITION."""
     sec = _sections(path)
     fmt = sec.get("MeshFormat", ["2.2 0 8"])[0].split()
     if not fmt[0].startswith("2") or (len(fmt) > 1 and fmt[1] != "0"):
@@ -133,12 +134,11 @@ def read_gmsh(path: str, boundary_tags: Sequence[str] = ("default",)) -> Mesh:
     cells = by_dim[dim]
     if dim == 2:
         types = {e[0] for e in cells}
-        if len(types) != 1:
-            raise ValueError("%s: mixed triangles and quadrilaterals are not supported" % path)
-        conn = np.array([e[2] for e in cells], dtype=np.int64)
         if types == {2}:
+            conn = np.array([e[2] for e in cells], dtype=np.int64)
             m = meshmod.from_triangles(xy, conn, name=path, boundary_bc=FACE_NO_CONDITION)
-        else:
+        else:   # quadrilaterals, or a mix with triangles padded by -1
+            conn = np.array([e[2] + [-1] * (4 - len(e[2])) for e in cells], dtype=np.int64)
             m = meshmod.from_polygons(xy, conn, name=path, boundary_bc=FACE_NO_CONDITION)
     else:
         seg = np.array([e[2] for e in cells], dtype=np.int64)
@@ -181,11 +181,12 @@ def write_gmsh(path: str, mesh: Mesh, face_tags: Optional[np.ndarray] = None,
     fv = meshmod.face_vertices(mesh)
     bfaces = [f for f in range(F) if bnd[f] and face_tags[f] > 0]
     V = mesh.vertices.shape[0]
+    nvc = (mesh.cells >= 0).sum(1)
     if mesh.dim == 2:
-        ctype = {3: 2, 4: 3}[mesh.cells.shape[1]]
+        ctypes = [{3: 2, 4: 3}[int(n)] for n in nvc]      # triangle, quadrilateral
         btype = 1
     else:
-        ctype, btype = 1, 15
+        ctypes, btype = [1] * mesh.n_cells, 15
     with open(path, "w") as f:
         f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n")
         f.write("$PhysicalNames\n%d\n" % (len(names) + 1))
@@ -202,8 +203,8 @@ def write_gmsh(path: str, mesh: Mesh, face_tags: Optional[np.ndarray] = None,
             f.write("%d %d 2 %d %d %s\n" % (k, btype, face_tags[fc], face_tags[fc],
                                             " ".join(str(int(v) + 1) for v in vs)))
             k += 1
-        for c in mesh.cells:
-            f.write("%d %d 2 %d %d %s\n" % (k, ctype, dom_tag, dom_tag, " ".join(str(int(v) + 1) for v in c)))
+        for c, ct in zip(mesh.cells, ctypes):
+            f.write("%d %d 2 %d %d %s\n" % (k, ct, dom_tag, dom_tag, " ".join(str(int(v) + 1) for v in c if v >= 0)))
             k += 1
         f.write("$EndElements\n")
 
@@ -241,9 +242,10 @@ def write_vtu(path: str, mesh: Mesh, q: np.ndarray, aux: Optional[np.ndarray] = 
     pe = ET.SubElement(piece, "Points")
     arr(pe, "Points", pts, 3)
     ce = ET.SubElement(piece, "Cells")
-    arr(ce, "connectivity", mesh.cells.astype(np.int64), vtype="Int64")
-    arr(ce, "offsets", (np.arange(1, C + 1) * K).astype(np.int64), vtype="Int64")
-    arr(ce, "types", np.full(C, _VTK_TYPE[(mesh.dim, K)], dtype=np.uint8), vtype="UInt8")
+    nvc = (mesh.cells >= 0).sum(1)                      # -1 padded rows: mixed cells
+    arr(ce, "connectivity", mesh.cells[mesh.cells >= 0].astype(np.int64), vtype="Int64")
+    arr(ce, "offsets", np.cumsum(nvc).astype(np.int64), vtype="Int64")
+    arr(ce, "types", np.array([_VTK_TYPE[(mesh.dim, int(n))] for n in nvc], dtype=np.uint8), vtype="UInt8")
     cd = ET.SubElement(piece, "CellData", Scalars="Q")
     arr(cd, "Q", q, q.shape[1])
     if aux is not None:

@@ -86,6 +86,19 @@ def level2(n: int = 240, seed: int = 1, steps: int = 500) -> Case:
                 dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), steps)
 
 
+def mixed_level2(n: int = 24, seed: int = 5, steps: int = 60) -> Case:
+    """The level-2 problem (bathymetry, hump, u = 0.5, alpha_1 = 0.1, Navier
+    slip) on a mesh of mixed triangles and quadrilaterals (mesh.mixed_square:
+    -1 padded cells, so triangles have an empty face slot)."""
+    m = meshmod.mixed_square(n, seed=seed)
+    x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
+    b = 0.2 * _gauss(x, y, 0.5, 0.5, 0.01)
+    h = 1.0 - b + 0.05 * _gauss(x, y, 0.3, 0.3, 0.005)
+    q = _state(2, h, b, hu=[0.5 * h, 0.1 * h, 0 * h], hv=[0 * h] * 3)
+    return Case("mixed_level2_%d" % n, "sme2d_l2", m, q, default_settings(),
+                dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), steps)
+
+
 def roofline_l4(n: int = 1400, seed: int = 2, steps: int = 100, m: Optional[meshmod.Mesh] = None) -> Case:
     """SME level 4 at roofline size: bathymetry = 16 seeded Gaussians
     (amplitude U[0.02,0.1], width U[0.02,0.08], centre U[0,1]^2),

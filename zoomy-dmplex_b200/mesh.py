@@ -39,7 +39,7 @@ FACE_NO_CONDITION = -2
 class Mesh:
     dim: int                      # 1 or 2
     vertices: np.ndarray          # [V, 2]
-    cells: np.ndarray             # [C, K] vertex ids (K = 2 segments, 3 triangles)
+    cells: np.ndarray             # [C, K] vertex ids (K = 2 segments, 3 triangles, 4 quadrilaterals; -1 padded)
     cell_centroid: np.ndarray     # [C, 2]
     cell_volume: np.ndarray       # [C]
     cell_faces: np.ndarray        # [C, K] int32, cone order
@@ -110,25 +110,45 @@ class Mesh:
 # ---------------------------------------------------------------------------
 # construction
 # ---------------------------------------------------------------------------
+def _vertex_counts(cells: np.ndarray) -> np.ndarray:
+    """Vertices of each polygon in a -1 padded [C, K] array (padding only at
+    the end of a row)."""
+    ok = cells >= 0
+    nv = ok.sum(1)
+    if not np.array_equal(ok, np.arange(cells.shape[1])[None, :] < nv[:, None]):
+        raise ValueError("polygon rows must list their vertices first and pad with -1")
+    return nv
+
+
 def _faces_from_cells(cells: np.ndarray, nloc: int):
-    """First-encounter face numbering (cell order, then local face order)."""
+    """First-encounter face numbering (cell order, then local face order).
+    2-D: local face k of a cell is its edge (v_k, v_(k+1) mod n) over its n
+    vertices (rows of -1 padded polygons have fewer faces; their missing
+    slots get face -1).  Returns the [C, nloc] face ids, the [F, 2] support
+    and, per face, the flat index c * nloc + k of its first encounter."""
     C = cells.shape[0]
     if nloc >= 3:  # polygon edges (v_k, v_k+1)
-        a = cells[:, list(range(nloc))]
-        b = cells[:, [(k + 1) % nloc for k in range(nloc)]]
-        lo = np.minimum(a, b).reshape(-1).astype(np.int64)
-        hi = np.maximum(a, b).reshape(-1).astype(np.int64)
+        nv = _vertex_counts(cells)
+        k = np.arange(nloc)[None, :]
+        valid = k < nv[:, None]
+        a = np.where(valid, cells, 0)
+        b = np.take_along_axis(a, (k + 1) % nv[:, None], axis=1)
+        pos = np.nonzero(valid.reshape(-1))[0]
+        lo = np.minimum(a, b).reshape(-1)[pos].astype(np.int64)
+        hi = np.maximum(a, b).reshape(-1)[pos].astype(np.int64)
         key = lo * (int(cells.max()) + 1) + hi
     else:  # 1-D: faces are the vertices
+        pos = np.arange(C * nloc)
         key = cells.reshape(-1).astype(np.int64)
     uniq, first, inv = np.unique(key, return_index=True, return_inverse=True)
     order = np.argsort(first, kind="stable")           # face ids by first encounter
     rank = np.empty_like(order)
     rank[order] = np.arange(order.size)
-    fid = rank[inv].reshape(C, nloc)                    # [C, nloc]
+    fid = np.full(C * nloc, -1, dtype=np.int64)
+    fid[pos] = rank[inv]
     F = uniq.size
-    flat_c = np.repeat(np.arange(C), nloc)
-    flat_f = fid.reshape(-1)
+    flat_c = pos // nloc
+    flat_f = fid[pos]
     # support: the encountering cells in cell order
     srt = np.lexsort((flat_c, flat_f))
     ff, cc = flat_f[srt], flat_c[srt]
@@ -140,7 +160,7 @@ def _faces_from_cells(cells: np.ndarray, nloc: int):
         raise ValueError("non-manifold mesh: a face has more than two cells")
     two = cnt == 2
     face_cells[two, 1] = cc[start[two] + 1]
-    return fid.astype(np.int32), face_cells.astype(np.int32), first[order]
+    return fid.reshape(C, nloc).astype(np.int32), face_cells.astype(np.int32), pos[first[order]]
 
 
 def from_triangles(vertices: np.ndarray, tris: np.ndarray, name="mesh", boundary_bc=0) -> Mesh:
@@ -174,21 +194,32 @@ def from_triangles(vertices: np.ndarray, tris: np.ndarray, name="mesh", boundary
 
 
 def from_polygons(vertices: np.ndarray, polys: np.ndarray, name="mesh", boundary_bc=0) -> Mesh:
-    """Mesh of convex polygons with the same vertex count (counter-clockwise
-    or clockwise; re-oriented counter-clockwise): shoelace areas and
-    centroids, edge midpoints and outward edge normals."""
+    """Mesh of convex polygons, [C, K] vertex ids, rows with fewer than K
+    vertices padded with -1 at the end (mixed triangles and quadrilaterals;
+    such a cell has -1 face slots).  Counter-clockwise or clockwise
+    (re-oriented counter-clockwise): shoelace areas and centroids, edge
+    midpoints and outward edge normals."""
     vertices = np.asarray(vertices, dtype=np.float64)[:, :2].copy()
     polys = np.asarray(polys, dtype=np.int64).copy()
     K = polys.shape[1]
-    P = vertices[polys]                                   # [C, K, 2]
-    Pn = np.roll(P, -1, axis=1)
-    cross = P[:, :, 0] * Pn[:, :, 1] - Pn[:, :, 0] * P[:, :, 1]
-    area2 = cross.sum(1)
-    neg = area2 < 0
-    polys[neg] = polys[neg][:, ::-1]
-    P = vertices[polys]
-    Pn = np.roll(P, -1, axis=1)
-    cross = P[:, :, 0] * Pn[:, :, 1] - Pn[:, :, 0] * P[:, :, 1]
+    nv = _vertex_counts(polys)
+    if (nv < 3).any():
+        raise ValueError("a polygon needs at least 3 vertices")
+    k = np.arange(K)[None, :]
+    valid = k < nv[:, None]
+    nxt = (k + 1) % nv[:, None]
+
+    def shoelace(pl):
+        P = vertices[np.where(valid, pl, 0)]              # [C, K, 2]
+        Pn = np.take_along_axis(P, np.broadcast_to(nxt[..., None], P.shape), axis=1)
+        cross = np.where(valid, P[:, :, 0] * Pn[:, :, 1] - Pn[:, :, 0] * P[:, :, 1], 0.0)
+        return P, Pn, cross
+
+    _, _, cross = shoelace(polys)
+    neg = cross.sum(1) < 0
+    rev = np.where(valid, nv[:, None] - 1 - k, k)         # reverse the listed vertices
+    polys[neg] = np.take_along_axis(polys[neg], rev[neg], axis=1)
+    P, Pn, cross = shoelace(polys)
     area2 = cross.sum(1)
     centroid = ((P + Pn) * cross[:, :, None]).sum(1) / (3.0 * area2[:, None])
     volume = 0.5 * area2
@@ -196,7 +227,7 @@ def from_polygons(vertices: np.ndarray, polys: np.ndarray, name="mesh", boundary
     loc = first % K
     c0 = face_cells[:, 0]
     xa = vertices[polys[c0, loc]]
-    xb = vertices[polys[c0, (loc + 1) % K]]
+    xb = vertices[polys[c0, (loc + 1) % nv[c0]]]
     fcent = 0.5 * (xa + xb)
     e = xb - xa
     normal = np.stack([e[:, 1], -e[:, 0]], axis=1)
@@ -205,6 +236,35 @@ def from_polygons(vertices: np.ndarray, polys: np.ndarray, name="mesh", boundary
     bc = np.where(face_cells[:, 1] < 0, boundary_bc, FACE_INTERIOR).astype(np.int32)
     return Mesh(2, vertices, polys.astype(np.int32), centroid, volume, cell_faces, face_cells,
                 fcent, normal, bc, name=name)
+
+
+def mixed_square(n: int, seed: int = 0, jitter: float = 0.2, name=None) -> Mesh:
+    """Mixed triangles and quadrilaterals on the unit square: an n x n grid
+    with interior nodes jittered by +-jitter * spacing (seeded), every other
+    quadrilateral (checkerboard) split into two triangles along alternating
+    diagonals; -1 padded [C, 4] cells, so triangle cells have one empty face
+    slot."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(0.0, 1.0, n + 1)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    h = 1.0 / n
+    inner = np.zeros_like(X, dtype=bool)
+    inner[1:-1, 1:-1] = True
+    X = X + np.where(inner, rng.uniform(-jitter, jitter, X.shape) * h, 0.0)
+    Y = Y + np.where(inner, rng.uniform(-jitter, jitter, Y.shape) * h, 0.0)
+    verts = np.stack([X.reshape(-1), Y.reshape(-1)], 1)
+    idx = lambda i, j: i * (n + 1) + j
+    polys = []
+    for i in range(n):
+        for j in range(n):
+            a, b, c, d = idx(i, j), idx(i + 1, j), idx(i + 1, j + 1), idx(i, j + 1)
+            if (i + j) % 2 == 0:
+                polys.append([a, b, c, d])
+            elif (i // 2 + j) % 2 == 0:
+                polys += [[a, b, c, -1], [a, c, d, -1]]
+            else:
+                polys += [[a, b, d, -1], [b, c, d, -1]]
+    return from_polygons(verts, np.array(polys), name=name or "mixed%d" % n)
 
 
 def quad_strip(x: np.ndarray, height: float = 1.0, name="strip") -> Mesh:
@@ -265,17 +325,21 @@ def interval(x: np.ndarray, name="interval", bc_left=0, bc_right=0) -> Mesh:
 
 def face_vertices(mesh: Mesh) -> np.ndarray:
     """Vertex ids of each face: [F, 2] (lower id first) in 2-D, [F] in 1-D.
-    A cell's local face k is its edge (v_k, v_k+1), or its vertex v_k in 1-D."""
+    A cell's local face k is its edge (v_k, v_(k+1) mod n) over its n
+    vertices (-1 padded rows), or its vertex v_k in 1-D."""
     C, K = mesh.cell_faces.shape
     f = mesh.cell_faces.reshape(-1)
     c = np.repeat(np.arange(C), K)
     k = np.tile(np.arange(K), C)
+    ok = f >= 0
+    f, c, k = f[ok], c[ok], k[ok]
     a = mesh.cells[c, k].astype(np.int64)
     if mesh.dim == 1:
         out = np.empty(mesh.n_faces, dtype=np.int64)
         out[f] = a
         return out
-    b = mesh.cells[c, (k + 1) % K].astype(np.int64)
+    nv = (mesh.cells >= 0).sum(1)
+    b = mesh.cells[c, (k + 1) % nv[c]].astype(np.int64)
     out = np.empty((mesh.n_faces, 2), dtype=np.int64)
     out[f, 0] = np.minimum(a, b)
     out[f, 1] = np.maximum(a, b)
