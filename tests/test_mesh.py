@@ -117,3 +117,25 @@ def test_mixed_mesh_gmsh_roundtrip(tmp_path):
     assert np.array_equal(d["offsets"], np.cumsum(nv))
     assert np.array_equal(d["types"], np.where(nv == 3, 5, 9))
     assert np.array_equal(d["connectivity"], m.cells[m.cells >= 0])
+
+
+def test_pad_face_slots_keeps_the_mesh():
+    """A triangle mesh taken to 4 face slots: empty slots added, geometry and
+    numbering untouched, and the oracle step bit-identical."""
+    import oracle_py as O
+    from zoomy_dmplex_b200 import cases, models
+
+    c = cases.level2(12)
+    p = M.pad_face_slots(c.mesh, 4)
+    assert p.max_faces == 4 and (p.cell_faces[:, 3] == -1).all() and (p.cells[:, 3] == -1).all()
+    assert np.array_equal(p.cell_faces[:, :3], c.mesh.cell_faces)
+    names, vals = models.parameter_table(c.model)
+    for k, v in c.params.items():
+        vals[names.index(k)] = v
+    out = []
+    for m in (c.mesh, p):
+        o = O.Oracle(c.model, m.as_abi_arrays(), c.settings.to_struct(), np.array(vals))
+        o.set_state(c.q0)
+        o.step(5)
+        out.append(o.get_state())
+    assert np.array_equal(out[0], out[1])

@@ -238,6 +238,21 @@ def from_polygons(vertices: np.ndarray, polys: np.ndarray, name="mesh", boundary
                 fcent, normal, bc, name=name)
 
 
+def pad_face_slots(mesh: Mesh, K: int) -> Mesh:
+    """The same mesh with K face slots per cell: cells and cell_faces padded
+    with -1 columns (a triangle mesh taken to K = 4 joins quadrilateral or
+    mixed meshes in one ensemble).  The geometry, face numbering and each
+    cell's faces are unchanged, so the step is unchanged too."""
+    k0 = mesh.max_faces
+    if K == k0:
+        return mesh
+    if K < k0 or mesh.dim != 2:
+        raise ValueError("can only add face slots to a 2-D mesh (%d -> %d)" % (k0, K))
+    pad = np.full((mesh.n_cells, K - k0), -1, dtype=np.int32)
+    return dataclasses.replace(mesh, cells=np.concatenate([mesh.cells.astype(np.int32), pad], 1),
+                               cell_faces=np.concatenate([mesh.cell_faces.astype(np.int32), pad], 1))
+
+
 def mixed_square(n: int, seed: int = 0, jitter: float = 0.2, name=None) -> Mesh:
     """Mixed triangles and quadrilaterals on the unit square: an n x n grid
     with interior nodes jittered by +-jitter * spacing (seeded), every other

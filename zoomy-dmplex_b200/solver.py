@@ -255,6 +255,12 @@ class BatchSolver:
         self.settings = settings or SolverSettings()
         self.meshes = list(meshes)
         self.n = len(self.meshes)
+        # instances with fewer face slots (triangles beside quadrilaterals)
+        # get empty slots, so every instance has the same max_faces
+        kmax = max(m.max_faces for m in self.meshes)
+        if any(m.max_faces != kmax for m in self.meshes):
+            from .mesh import pad_face_slots
+            self.meshes = [pad_face_slots(m, kmax) for m in self.meshes]
         names, defaults = _m.parameter_table(model)
         P = np.zeros((self.n, len(names)))
         for i in range(self.n):
