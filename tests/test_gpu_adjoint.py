@@ -40,10 +40,10 @@ def _smooth(mesh, rng, bumps=6):
     return d
 
 
-def _setup(n, nsteps, every_obs, ngauge, seed=0):
-    c = cases.adjoint_l1(n)
+def _setup(n, nsteps, every_obs, ngauge, seed=0, mesh=None):
+    c = cases.adjoint_l1(n, m=mesh)
     p, names = _params(c)
-    tgt = cases.adjoint_l1(n, target=True)
+    tgt = cases.adjoint_l1(n, target=True, m=mesh)
     o = O.Oracle(tgt.model, tgt.mesh.as_abi_arrays(), tgt.settings.to_struct(), p)
     o.set_state(tgt.q0)
     steps = list(range(every_obs, nsteps + 1, every_obs))
@@ -76,9 +76,12 @@ def _oracle_tlm(c, p, dts, obs, dq, dp):
     return L, dL
 
 
-@pytest.mark.parametrize("n,nsteps,every", [(16, 12, 5), (24, 30, 7)])
-def test_adjoint_matches_tangent_linear_oracle(n, nsteps, every):
-    c, p, names, obs = _setup(n, nsteps, 3, 24)
+@pytest.mark.parametrize("n,nsteps,every,mixed", [(16, 12, 5, False), (24, 30, 7, False), (14, 20, 6, True)])
+def test_adjoint_matches_tangent_linear_oracle(n, nsteps, every, mixed):
+    """mixed: triangles and quadrilaterals in one mesh (empty face slots)."""
+    from zoomy_dmplex_b200 import mesh as meshmod
+
+    c, p, names, obs = _setup(n, nsteps, 3, 24, mesh=meshmod.mixed_square(n, seed=6) if mixed else None)
     g = Solver(c.model, c.mesh, c.settings, p)
     g.set_state(c.q0)
     loss, gq, gp, dts = g.adjoint(nsteps, *obs, checkpoint_every=every)

@@ -189,7 +189,8 @@ def ensemble_member(i: int, seed: int = 3, side_range=(40, 400)) -> Case:
                 dict(g=9.81, nu=1e-3, **{"lambda": 0.1}, n_manning=0.0), 200)
 
 
-def adjoint_l1(n: int = 200, seed: int = 4, steps: int = 400, target: bool = False) -> Case:
+def adjoint_l1(n: int = 200, seed: int = 4, steps: int = 400, target: bool = False,
+               m: Optional[meshmod.Mesh] = None) -> Case:
     """SME level 1 adjoint case, Manning n = 0.03; the target run perturbs b by
     +0.02 exp(-((x-0.6)^2+(y-0.4)^2)/0.01).
 
@@ -198,8 +199,10 @@ def adjoint_l1(n: int = 200, seed: int = 4, steps: int = 400, target: bool = Fal
     component is flat to round-off (a TVD ratio with |dq| just above the
     reference's 1e-12 cut-off has an arbitrarily large slope); every velocity
     and moment is non-zero (|u| at u = 0 is a kink of the Rusanov speed), with
-    the flow tapered towards the reflective walls."""
-    m = meshmod.jittered_square(n, seed=seed)
+    the flow tapered towards the reflective walls.  m: another mesh of the
+    unit square (default: the jittered n x n triangulation)."""
+    if m is None:
+        m = meshmod.jittered_square(n, seed=seed)
     x, y = m.cell_centroid[:, 0], m.cell_centroid[:, 1]
     b = 0.2 * _gauss(x, y, 0.5, 0.5, 0.01) + 0.1 * ((x - 0.4) ** 2 + (y - 0.55) ** 2)
     if target:
