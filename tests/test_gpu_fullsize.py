@@ -1,0 +1,78 @@
+"""Configuration 2 at its full size: SME level 4 on the 1400x1400 jittered
+grid (3,914,402 cells), the bench's workload.
+
+* one step from the initial state against the oracle on the same mesh, bit
+  for bit (the oracle finishes one step at this size in seconds);
+* the configuration's 100 steps, through size-independent properties: mass
+  conserved to rounding with reflective walls, depths non-negative and
+  finite, the bathymetry untouched, the health counters clean;
+* the lake at rest stays at rest at first order to 1e-14.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import oracle_py as O
+from zoomy_dmplex_b200 import cases, models
+from zoomy_dmplex_b200.solver import Solver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    return cases.roofline_l4(1400)
+
+
+def _params(c):
+    names, vals = models.parameter_table(c.model)
+    for k, v in c.params.items():
+        vals[names.index(k)] = v
+    return np.array(vals)
+
+
+def test_one_step_bitwise_against_oracle(case):
+    p = _params(case)
+    O.set_threads(0)
+    o = O.Oracle(case.model, case.mesh.as_abi_arrays(), case.settings.to_struct(), p)
+    o.set_state(case.q0)
+    _, dt = o.time()
+    o.step(1)
+    g = Solver(case.model, case.mesh, case.settings, p)
+    g.set_state(case.q0)
+    assert g.time()[1] == pytest.approx(dt, rel=1e-12)
+    g.step(1, dts=[dt])
+    assert np.array_equal(g.get_state(), o.get_state())
+    assert g.time()[0] == o.time()[0]
+    assert g.time()[1] == pytest.approx(o.time()[1], rel=1e-12)
+    g.close()
+
+
+def test_hundred_steps_conserve_mass(case):
+    g = Solver(case.model, case.mesh, case.settings, _params(case))
+    g.set_state(case.q0)
+    vol = case.mesh.cell_volume
+    m0 = np.sum(g.get_state()[:, 1] * vol)
+    g.step(100)
+    d = g.sync()
+    assert d.n_nonfinite == 0 and d.n_negative_depth == 0 and d.n_newton_unconverged == 0
+    q = g.get_state()
+    assert np.all(np.isfinite(q)) and q[:, 1].min() >= 0.0
+    assert np.array_equal(q[:, 0], case.q0[:, 0])                     # b is not evolved
+    assert abs(np.sum(q[:, 1] * vol) - m0) <= 1e-12 * m0
+    g.close()
+
+
+def test_lake_at_rest_first_order(case):
+    q = case.q0.copy()
+    q[:, 1] = 1.0 - q[:, 0]
+    q[:, 2:] = 0.0
+    st = dataclasses.replace(case.settings, reconstruction_order=1)
+    g = Solver(case.model, case.mesh, st, _params(case))
+    g.set_state(q)
+    g.step(5)
+    r = g.get_state()
+    assert np.abs(r[:, 0] + r[:, 1] - 1.0).max() < 1e-14
+    assert np.abs(r[:, 2:]).max() < 1e-14
+    g.close()
