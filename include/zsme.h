@@ -12,7 +12,11 @@
  * Conventions (mirroring PETSc's): every function returns an int status,
  * ZSME_OK (0) on success; on failure zsme_last_error() describes it.  The
  * caller owns host buffers; the library owns device buffers.  A handle is
- * single-threaded and stream-ordered (one CUDA stream per handle).  States
+ * single-threaded and stream-ordered (one CUDA stream per handle).  A handle
+ * lives on the device given to zsme_create; every call on it makes that
+ * device current for the call's duration and restores the calling thread's
+ * current device before returning, so handles on several GPUs may be driven
+ * from one thread in any order.  States
  * cross the boundary cell-major/interleaved ("AoS", [n_cells][n_dof_q], the
  * layout of the reference's PETSc Vec with block size n_dof_q) in the
  * caller's cell order; inside, the library renumbers cells along a Hilbert
@@ -102,6 +106,8 @@ typedef struct zsme_diag {
     int32_t n_negative_depth;     /* cells with h < -1e-10 (MUSCLSolver.hpp:206) */
     int32_t n_newton_unconverged; /* cells whose Newton hit 15 iterations */
     int32_t n_mood_cells;         /* cells redone at first order by MOOD (ZSME_POSITIVITY_MOOD) */
+    int32_t n_newton_deferred;    /* cell updates whose Newton solve left the register fast path for the
+                                     full pivoted elimination (summed over the last zsme_step call) */
 } zsme_diag;
 
 typedef struct zsme_handle zsme_handle;
@@ -188,6 +194,8 @@ int zsme_get_time(zsme_handle* h, double* t, double* dt);
 int zsme_set_params(zsme_handle* h, const double* params);
 /* The CUDA stream (cudaStream_t) the handle launches on. */
 void* zsme_stream(zsme_handle* h);
+/* The CUDA device ordinal the handle lives on (zsme_create's `device`). */
+int zsme_device(zsme_handle* h, int32_t* device);
 /* Kernel launches of one zsme_step step. */
 int zsme_launches_per_step(zsme_handle* h, int32_t* n);
 
@@ -262,13 +270,15 @@ int zsme_adjoint_phases(zsme_handle* h, double* ms3);
  * every GPU that loads the library holds until the process exits.
  * All pointers are device pointers, cells in any order (the same in all
  * arrays): d_q_aos [n_cells][n_dof_q], d_aux_aos [n_cells][n_dof_qaux],
- * d_rc [n_cells] (min over the cell's faces of |x_c - x_f|), d_params
+ * d_rc [n_cells] (min over the cell's faces of |x_c - x_f|; a cell whose
+ * d_rc is >= DBL_MAX, +inf included, is left out of the minimum -- the way
+ * a partitioned caller keeps its halo cells out of the CFL dt), d_params
  * [n_parameters]; dt (cfl * min r_c/lambda_c, or the model's dt_max) is
  * written to *d_dt in stream order on `stream` (a cudaStream_t; NULL = the
  * default stream).  n_cells > ZSME_NOALLOC_MAX_CELLS returns ZSME_ERR_LIMIT.
- * The first call on a device looks the scratch address up and must come
- * before any stream capture on that device.  All calls share the scratch:
- * calls that overlap on the GPU race. */
+ * The first call on a device (and in each CUDA context on it) looks the
+ * scratch address up and must come before any stream capture on that
+ * device.  All calls share the scratch: calls that overlap on the GPU race. */
 #define ZSME_NOALLOC_MAX_CELLS (1 << 24)
 int zsme_compute_dt_noalloc(const char* model, int32_t n_cells, const double* d_q_aos,
                             const double* d_aux_aos, const double* d_rc, const double* d_params,

@@ -3,7 +3,7 @@ shipped Model.H / Numerics.H (1-D SME level 0), compiled from the reference
 tree into oracle/_ref/liboracle_ref.so, on seeded random inputs (wet, dry
 and near-dry states).  Run in a container where the reference is mounted:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=<reference source tree> && python tests/golden/make_golden.py
 """
 import os
 import sys

@@ -19,9 +19,12 @@
 //    must be serialised by the caller;
 //  * the array keeps the last call's contents; every entry a call reads is
 //    written earlier in the same call, so nothing needs clearing;
-//  * the first call on each device looks up the array's device address
-//    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture begins on the device.
+//  * the first call on each device (and in each CUDA context on it) looks up
+//    the array's device address (cudaGetSymbolAddress) with that device
+//    current; make that first call before any stream capture begins on the
+//    device, and again after cudaDeviceReset or a context switch of its own;
+//  * cells whose d_rc is >= DBL_MAX (or +inf) are left out of the minimum,
+//    which is how a partitioned caller keeps its halo cells out of the CFL dt.
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -86,9 +89,16 @@ __global__ void __launch_bounds__(kBlock) dt_partial_kernel(int C, const double*
             auto r = N::local_max_abs_eigenvalue(qc, ac, p, n);
             if (r[0] > eig) eig = r[0];
         }
+        // a cell without wave speed, or with rc >= DBL_MAX (a halo cell left out
+        // of the minimum), does not constrain dt; a ratio enters the minimum
+        // only by winning a "<" comparison, so a NaN never masks another cell
+        // (VirtualSolver.hpp:326, 341-344)
         if (!(eig < 1e-14)) {
             const double rcv = rc[c];
-            if (rcv < DBL_MAX) ratio = rcv / eig;
+            if (rcv < DBL_MAX) {
+                const double v = rcv / eig;
+                if (v < ratio) ratio = v;
+            }
         }
     }
     __shared__ double red[kBlock / 32];
@@ -126,22 +136,65 @@ __global__ void __launch_bounds__(kBlock) dt_final_kernel(const double* partial,
     }
 }
 
-// Device address of g_dt_partial, looked up once per device.
-constexpr int kMaxDevices = 64;
+// Device address of g_dt_partial, looked up once per (device, CUDA context).
+// The context is part of the key because the array's address belongs to the
+// module loaded in one context: after cudaDeviceReset, or under a driver-API
+// context that the host code made current itself (PETSc can create one), the
+// same ordinal needs a fresh lookup.  The current context is read through the
+// runtime's driver entry point, so the library still links the runtime only;
+// where that entry point is unavailable the key is the ordinal alone.  A new
+// context that happens to reuse a destroyed one's handle value is not told
+// apart from it.
+using CtxGetCurrent = int (*)(void**);
+constexpr int kMaxEntries = 64;
 std::mutex g_mu;
-double* g_addr[kMaxDevices] = {nullptr};
+struct ScratchEntry {
+    int dev;
+    void* ctx;
+    double* addr;
+};
+ScratchEntry g_entries[kMaxEntries];
+int g_n_entries = 0;
+CtxGetCurrent g_ctx_fn = nullptr;
+bool g_ctx_fn_looked_up = false;
+
+void* current_context() {
+    if (!g_ctx_fn_looked_up) {
+        g_ctx_fn_looked_up = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_fn = reinterpret_cast<CtxGetCurrent>(fn);
+        else
+            cudaGetLastError();
+    }
+    void* ctx = nullptr;
+    if (g_ctx_fn && g_ctx_fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
 
 int scratch_address(int dev, double** out) {
-    if (dev < 0 || dev >= kMaxDevices) return zsme::set_error(ZSME_ERR_ARG, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        double* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_dt_partial);
-        if (e != cudaSuccess)
-            return zsme::set_error(ZSME_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_addr[dev] = p;
+    void* ctx = current_context();
+    for (int i = 0; i < g_n_entries; ++i)
+        if (g_entries[i].dev == dev && g_entries[i].ctx == ctx) {
+            *out = g_entries[i].addr;
+            return ZSME_OK;
+        }
+    double* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_dt_partial);
+    if (e != cudaSuccess)
+        return zsme::set_error(ZSME_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    // the lookup makes the device's primary context current on a thread that had none
+    if (!ctx) ctx = current_context();
+    // keep the newest entries when the table is full (contexts that came and went)
+    if (g_n_entries == kMaxEntries) {
+        for (int i = 1; i < kMaxEntries; ++i) g_entries[i - 1] = g_entries[i];
+        g_n_entries--;
     }
-    *out = g_addr[dev];
+    g_entries[g_n_entries++] = ScratchEntry{dev, ctx, p};
+    *out = p;
     return ZSME_OK;
 }
 

@@ -61,6 +61,8 @@ class SolverBase {
     virtual int n_dof_q() const = 0;
     virtual int n_dof_qaux() const = 0;
     virtual int n_instances() const = 0;
+    // the CUDA device the handle's buffers and stream live on
+    virtual int device() const = 0;
     virtual int init(PreparedMesh&& pm, const zsme_settings& st, const double* params, int device) = 0;
     virtual int set_params(const double* params) = 0;
     virtual int set_state(int inst, const double* q, double t, bool device) = 0;

@@ -122,6 +122,7 @@ class Solver final : public SolverBase {
     int n_dof_q() const override { return NQ; }
     int n_dof_qaux() const override { return NA; }
     int n_instances() const override { return n_inst_; }
+    int device() const override { return device_; }
 
     // ------------------------------------------------------- profiling
     void mark(int kind, bool start) {
@@ -645,6 +646,7 @@ class Solver final : public SolverBase {
         if (nsteps <= 0) return ZSME_OK;
         if (dts_host && n_inst_ != 1) return set_error(ZSME_ERR_ARG, "imposed dts need a single-instance handle");
         ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 4 * sizeof(int), stream_));
+        ZSME_CUDA(cudaMemsetAsync(iscal_.p + 7, 0, sizeof(int), stream_));
         // x_ is constrained after set_state, update_state and every step (update_variables is a
         // projection: the clamp of a clamped state is that state), so it serves as its own
         // clamped copy; after a bare source() the first step clamps a copy first, uncaptured
@@ -1007,6 +1009,7 @@ class Solver final : public SolverBase {
             d->n_negative_depth = is[2];
             d->n_newton_unconverged = is[3];
             d->n_mood_cells = is[4];
+            d->n_newton_deferred = is[7];
         }
         return ZSME_OK;
     }

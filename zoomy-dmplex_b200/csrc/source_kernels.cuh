@@ -408,6 +408,7 @@ __global__ void __launch_bounds__(64) finalize_fallback_kernel(MeshDev m, double
                                                                const double* __restrict__ params, StepDev sd,
                                                                const double* __restrict__ dt_src, int flags) {
     const int n = *sd.n_fallback;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&sd.diag[6], n);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
         const int c = sd.fallback[e];
         const int I = cell_instance(m, c);

@@ -64,7 +64,8 @@ struct StepDev {
     int* step_idx;             // steps taken by instance 0 (index into dts)
     int n_inst;
     double t_end, cfl, dt_max;
-    int* diag;                 // [0] nonfinite, [1] negative depth, [2] newton unconverged, [3] MOOD cells
+    int* diag;                 // [0] nonfinite, [1] negative depth, [2] newton unconverged, [3] MOOD cells,
+                               // [6] cells deferred to the generic Newton path (summed over steps)
     int* fallback;             // [C] cells finalize_kernel deferred to finalize_fallback_kernel
     int* n_fallback;           // their count
 };

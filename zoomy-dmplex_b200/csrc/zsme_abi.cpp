@@ -1,5 +1,9 @@
 // C ABI of the library (include/zsme.h): model registry, argument checks,
-// error reporting.  Each entry point forwards to the model's Solver.
+// error reporting.  Each entry point forwards to the model's Solver with the
+// handle's device current, and gives the caller's current device back on
+// return, so handles on different GPUs can be used from one thread.
+#include <cuda_runtime.h>
+
 #include <cstring>
 #include <string>
 
@@ -46,17 +50,48 @@ struct zsme_handle {
 
 using zsme::set_error;
 
+namespace {
+// Makes `dev` the current device for the guard's scope and restores the
+// device that was current before (cudaSetDevice is per host thread).
+class DeviceGuard {
+  public:
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev_) != cudaSuccess) {
+            err_ = cudaGetLastError();
+            return;
+        }
+        if (prev_ != dev) {
+            err_ = cudaSetDevice(dev);
+            set_ = err_ == cudaSuccess;
+        }
+    }
+    ~DeviceGuard() {
+        if (set_) cudaSetDevice(prev_);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+    int check() const {
+        if (err_ == cudaSuccess) return ZSME_OK;
+        return set_error(ZSME_ERR_CUDA, std::string("selecting the handle's device: ") + cudaGetErrorString(err_));
+    }
+
+  private:
+    int prev_ = 0;
+    bool set_ = false;
+    cudaError_t err_ = cudaSuccess;
+};
+}  // namespace
+
+// a valid handle, with its device current until the entry point returns
 #define CHECK_H(h)                                                          \
-    do {                                                                    \
-        if (!(h) || !(h)->s) return set_error(ZSME_ERR_ARG, "null handle"); \
-    } while (0)
+    if (!(h) || !(h)->s) return set_error(ZSME_ERR_ARG, "null handle");     \
+    DeviceGuard dev_guard_((h)->s->device());                               \
+    if (int dev_rc_ = dev_guard_.check()) return dev_rc_
 // calls that address "the" state need a single-instance handle
-#define CHECK_SINGLE(h)                                                                              \
-    do {                                                                                             \
-        CHECK_H(h);                                                                                  \
-        if ((h)->s->n_instances() != 1)                                                              \
-            return set_error(ZSME_ERR_ARG, "batch handle: use the zsme_batch_* state functions");   \
-    } while (0)
+#define CHECK_SINGLE(h)                                                                          \
+    CHECK_H(h);                                                                                  \
+    if ((h)->s->n_instances() != 1)                                                              \
+    return set_error(ZSME_ERR_ARG, "batch handle: use the zsme_batch_* state functions")
 
 extern "C" {
 
@@ -91,6 +126,8 @@ int zsme_create(const char* model, const zsme_mesh* mesh, const zsme_settings* s
     zsme::PreparedMesh pm;
     int rc = zsme::prepare_mesh(*mesh, pm);
     if (rc) return rc;
+    DeviceGuard dev_guard(device);
+    if ((rc = dev_guard.check())) return rc;
     zsme::SolverBase* s = e->make();
     rc = s->init(std::move(pm), *settings, params, device);
     if (rc) {
@@ -103,7 +140,10 @@ int zsme_create(const char* model, const zsme_mesh* mesh, const zsme_settings* s
 
 int zsme_destroy(zsme_handle* h) {
     if (!h) return ZSME_OK;
-    delete h->s;
+    if (h->s) {
+        DeviceGuard dev_guard(h->s->device());
+        delete h->s;
+    }
     delete h;
     return ZSME_OK;
 }
@@ -217,6 +257,11 @@ int zsme_set_params(zsme_handle* h, const double* p) {
     return h->s->set_params(p);
 }
 void* zsme_stream(zsme_handle* h) { return (h && h->s) ? h->s->stream() : nullptr; }
+int zsme_device(zsme_handle* h, int32_t* device) {
+    if (!h || !h->s) return set_error(ZSME_ERR_ARG, "null handle");
+    if (device) *device = h->s->device();
+    return ZSME_OK;
+}
 int zsme_launches_per_step(zsme_handle* h, int32_t* n) {
     CHECK_H(h);
     if (n) *n = h->s->launches_per_step();
@@ -251,6 +296,8 @@ int zsme_batch_create(const char* model, int32_t n, const zsme_mesh* meshes, con
     zsme::PreparedMesh pm;
     int rc = zsme::concat_meshes(parts, pm);
     if (rc) return rc;
+    DeviceGuard dev_guard(device);
+    if ((rc = dev_guard.check())) return rc;
     zsme::SolverBase* s = e->make();
     rc = s->init(std::move(pm), *settings, params, device);
     if (rc) {

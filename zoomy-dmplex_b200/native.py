@@ -42,6 +42,7 @@ class ZsmeDiag(ct.Structure):
     _fields_ = [
         ("steps", ct.c_int64), ("time", ct.c_double), ("dt", ct.c_double), ("n_nonfinite", ct.c_int32),
         ("n_negative_depth", ct.c_int32), ("n_newton_unconverged", ct.c_int32), ("n_mood_cells", ct.c_int32),
+        ("n_newton_deferred", ct.c_int32),
     ]
 
 
@@ -108,6 +109,7 @@ def load():
     lib.zsme_set_params.argtypes = [vp, P]
     lib.zsme_stream.argtypes = [vp]
     lib.zsme_stream.restype = vp
+    lib.zsme_device.argtypes = [vp, ct.POINTER(ct.c_int32)]
     lib.zsme_launches_per_step.argtypes = [vp, ct.POINTER(ct.c_int32)]
     lib.zsme_set_profiling.argtypes = [vp, ct.c_int]
     lib.zsme_read_profile.argtypes = [vp, P, ct.POINTER(ct.c_int64)]
