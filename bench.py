@@ -50,16 +50,20 @@ def parse():
     ap.add_argument("--side", type=int, default=0, help="jittered grid side of the mesh (0: the case's own)")
     ap.add_argument("--case", default="roofline_l4", choices=["roofline_l4", "level2", "plain_l0"],
                     help="plain-step case: SME level 4 on 1400^2 (default), level 2 on 240^2, level 0 on 60^2")
-    ap.add_argument("--cpu-side", type=int, default=600, help="grid side of the bounded CPU sample")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
-                    help="the CPU sample steps until this much time has passed")
+                    help="the CPU baseline (oracle on the same mesh) steps until this much time has passed")
+    ap.add_argument("--ref-seconds", type=float, default=240.0,
+                    help="--impl reference: the timed oracle steps end once this much time has passed")
+    ap.add_argument("--lsq-steps", type=int, default=5,
+                    help="steps timed with the least-squares gradient beside the default Green-Gauss (0: none)")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch configuration")
     ap.add_argument("--workload", choices=["roofline", "ensemble", "adjoint"], default="roofline")
     ap.add_argument("--launch", default="", help="launch configuration as JSON (keys of solver.LAUNCH_KEYS); "
                     "skips the autotuner")
-    ap.add_argument("--instances", type=int, default=512, help="ensemble size per GPU (--workload ensemble)")
+    ap.add_argument("--instances", type=int, default=512,
+                    help="ensemble size in all, split across the ranks (--workload ensemble)")
     ap.add_argument("--adj-side", type=int, default=200, help="grid side of the adjoint workload")
     ap.add_argument("--adj-steps", type=int, default=400, help="steps of the adjoint workload")
     ap.add_argument("--adj-limiter", default="tvd", choices=["tvd", "none"], help="limiter of the adjoint workload")
@@ -73,6 +77,8 @@ CASE_SIDE = {"roofline_l4": 1400, "level2": 240, "plain_l0": 60}
 CASE_TEXT = {"roofline_l4": ("sme2d_l4 SME level 4", "Navier-slip Newton source"),
              "level2": ("sme2d_l2 SME level 2", "Navier-slip Newton source"),
              "plain_l0": ("sme2d_l0 SME level 0 (shallow water)", "Manning friction Newton source")}
+GRAD_TEXT = {"green_gauss": "order 2 Green-Gauss + Vacuum/TVD",
+             "least_squares": "order 2 least squares + Vacuum/TVD (Barth-Jespersen)"}
 POS_TEXT = {"none": "", "zhang_shu": ", eta-well-balanced reconstruction + Zhang-Shu theta (CFL clamped to 1/6)",
             "mood": ", eta-well-balanced reconstruction + local MOOD"}
 
@@ -132,7 +138,7 @@ NCU_DRAM_BYTES_PER_CELL = {
 FP64_FLOPS = {
     "sme2d_l4": {"prep": 579.524, "flux": 1256.84, "gather": 126.0, "finalize": 2829.0},
     "sme2d_l2": {"prep": 392.726, "flux": 528.504, "gather": 84.0, "finalize": 1268.0},
-    "sme2d_l0": {"prep": 204.313, "flux": 204.168, "gather": 42.0, "finalize": 126.0},
+    "sme2d_l0": {"prep": 183.089, "flux": 204.168, "gather": 42.0, "finalize": 126.0},   # least squares
     "sme2d_l1": {"prep": 311.716, "flux": 332.336, "gather": 63.0, "finalize": 523.766},
 }
 
@@ -271,16 +277,19 @@ def params_of(case):
     return np.array(vals)
 
 
-def cpu_sample(side, steps=0, warm=1, seconds=0.0, positivity="none", case="roofline_l4"):
-    """The oracle (CPU restatement of the reference step) on a bounded
-    sample of the workload: same model and physics on a side x side mesh,
-    `steps` steps, or (steps = 0) one step at a time until `seconds` have
-    passed.  Returns (cell-steps/s, threads, cells, seconds, steps)."""
+def cpu_sample(side, steps=0, warm=1, seconds=0.0, positivity="none", case="roofline_l4", built=None,
+               max_seconds=0.0):
+    """The oracle (CPU restatement of the reference step) on the workload's
+    own mesh (`built`: the case already built by the GPU arm; else the case
+    on a side x side grid): `steps` steps, or (steps = 0) one step at a time
+    until `seconds` have passed; max_seconds > 0 ends a `steps` run early once
+    that much time has passed (the run stays bounded on slow hosts).
+    Returns (cell-steps/s, threads, cells, seconds, steps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
     from zoomy_dmplex_b200 import cases
 
-    c = getattr(cases, case)(side)
+    c = built if built is not None else getattr(cases, case)(side)
     c.settings.positivity = positivity
     nt = O.set_threads(0)
     o = O.Oracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), params_of(c))
@@ -288,7 +297,13 @@ def cpu_sample(side, steps=0, warm=1, seconds=0.0, positivity="none", case="roof
     o.step(warm)
     t0 = time.perf_counter()
     n = 0
-    while (n < steps) if steps else (n == 0 or time.perf_counter() - t0 < seconds):
+    while True:
+        el = time.perf_counter() - t0
+        if steps:
+            if n >= steps or (max_seconds > 0 and n > 0 and el >= max_seconds):
+                break
+        elif n > 0 and el >= seconds:
+            break
         o.step(1)
         n += 1
     dt = time.perf_counter() - t0
@@ -307,8 +322,9 @@ def run_ensemble(a, dev, torch, dist, rank, world):
         if dist:
             dist.barrier()
 
-    # a.instances per GPU on average; ranks take greedy size-balanced shards
-    shard = cases.ensemble_shard(a.instances * world, world, rank)
+    # the configuration's a.instances instances in all, dealt to the ranks in
+    # greedy size-balanced shards (total work fixed as N grows)
+    shard = cases.ensemble_shard(a.instances, world, rank)
     n = len(shard)
     t0 = time.perf_counter()
     members = cases.ensemble(indices=shard)
@@ -394,7 +410,17 @@ def run_ensemble(a, dev, torch, dist, rank, world):
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max, loop_max, bwall_max, sloop_max = (float(x) for x in t.tolist())
-    value = C * a.steps * world / (ms_max / 1e3)
+    # the whole job: every rank's cells over the slowest rank's time
+    tc = torch.tensor([float(C), float(F), rel, t_diff], dtype=torch.float64, device="cuda")
+    if dist:
+        tc0 = tc[:2].clone()
+        dist.all_reduce(tc0, op=dist.ReduceOp.SUM)
+        tc1 = tc[2:].clone()
+        dist.all_reduce(tc1, op=dist.ReduceOp.MAX)
+        tc = torch.cat([tc0, tc1])
+    C_all, F_all, rel_all, t_diff_all = (float(x) for x in tc.tolist())
+    identical = rel_all == 0.0 and t_diff_all == 0.0
+    value = C_all * a.steps / (ms_max / 1e3)
 
     # end to end through the public API: every instance's state from pinned host
     # memory, one batched step, every state back
@@ -419,17 +445,19 @@ def run_ensemble(a, dev, torch, dist, rank, world):
     t2 = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_value = C * ne * world / (float(t2.item()) / 1e3)
+    e2e_value = C_all * ne / (float(t2.item()) / 1e3)
     B.close()
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "ensemble of %d SME level-2 instances per GPU, jittered-Delaunay grid side "
-                                   "log-uniform in [40, 400] (%d cells, %d faces per GPU), order 2 Green-Gauss + "
+            "config": {"workload": "ensemble of %d SME level-2 instances (%d on rank 0), jittered-Delaunay grid "
+                                   "side log-uniform in [40, 400] (%d cells, %d faces in all), order 2 Green-Gauss + "
                                    "Vacuum/TVD, SSP-RK2, CFL 0.45 per instance, Navier-slip Newton source"
-                                   % (n, C, F),
-                       "model": model, "instances": n, "cells": C, "faces": F,
+                                   % (a.instances, n, int(C_all), int(F_all)),
+                       "model": model, "instances": a.instances, "instances_rank0": n, "cells": int(C_all),
+                       "faces": int(F_all),
                        "parallelism": "instance shards x%d" % world if world > 1 else "single GPU",
                        "l2_flush": "not needed: state %.0f MB > 126 MB L2" % (C * nq * 8 / 1e6),
                        "timing": "CUDA events on the batch stream around K graph-launched steps",
@@ -444,7 +472,8 @@ def run_ensemble(a, dev, torch, dist, rank, world):
                                  "K steps each, instances one after the other; host wall clock around the "
                                  "loop and a device synchronize (the batched time beside it is taken the same way); "
                                  "sync loop: the same, waiting for each instance's K steps before the next",
-                         "max_rel_l2_vs_loop": rel, "max_time_diff_vs_loop": t_diff,
+                         "max_rel_l2_vs_loop": rel_all, "max_time_diff_vs_loop": t_diff_all,
+                         "bit_identical_to_loop": identical,
                          "loop_gpu_launches": loop_launches},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": C * nq * 8,
                     "d2h_bytes_per_step": C * nq * 8, "steps": ne,
@@ -457,7 +486,8 @@ def run_ensemble(a, dev, torch, dist, rank, world):
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
-    return 0
+    # every instance must end bit-identical (state and time) to its own plain solve
+    return 0 if identical else 3
 
 
 def run_adjoint(a, dev, torch, dist, rank, world):
@@ -602,18 +632,31 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return 0
-        # warmup + K timed oracle steps on the bounded sample
-        v, nt, C, dt, _ = cpu_sample(a.cpu_side, max(1, a.steps), warm=max(1, a.warmup), positivity=a.positivity,
-                                     case=a.case)
+        from zoomy_dmplex_b200 import cases
+
+        # the GPU arm's own workload (same mesh, model, settings); warm-up and
+        # timed steps of the oracle, the timed loop bounded to --ref-seconds
+        side = a.side or CASE_SIDE[a.case]
+        built = getattr(cases, a.case)(side)
+        warm = max(1, min(a.warmup, 2))
+        v, nt, C, dt, n = cpu_sample(side, max(1, a.steps), warm=warm, positivity=a.positivity, built=built,
+                                     max_seconds=a.ref_seconds)
         line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
-                "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / max(1, a.steps),
+                "steps": n, "warmup": warm, "ms_per_step": 1e3 * dt / n,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": "%s, jittered-Delaunay %dx%d (%d cells) order 2 Green-Gauss+TVD SSP-RK2"
-                           % (CASE_TEXT[a.case][0], a.cpu_side, a.cpu_side, C), "parallelism": "host threads"},
+                "config": {"workload": "%s, jittered-Delaunay %dx%d grid (%d cells, %d faces), Hilbert-renumbered, "
+                                       "%s, SSP-RK2, CFL 0.45, %s%s"
+                                       % (CASE_TEXT[a.case][0], side, side, C, built.mesh.n_faces,
+                                          GRAD_TEXT[built.settings.gradient], CASE_TEXT[a.case][1],
+                                          POS_TEXT[a.positivity]),
+                           "model": built.model, "cells": C, "parallelism": "host threads",
+                           "same_config_as_gpu_arm": True},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
-                                 "sample": "%d steps of the CPU restatement on a %dx%d-grid mesh (%d cells)"
-                                           % (a.steps, a.cpu_side, a.cpu_side, C)},
+                                 "sample": "%d timed steps (after %d warm-up) of the CPU restatement (oracle) on the "
+                                           "GPU arm's own %dx%d-grid mesh (%d cells), %.1f s; requested %d steps, "
+                                           "bounded to %.0f s" % (n, warm, side, side, C, dt, a.steps,
+                                                                 a.ref_seconds)},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -742,6 +785,41 @@ def main():
         fp64_step = {"flops_per_cell_step": fc, "flop_per_byte": fc / sb, "achieved": ach_s, "peak": peak_tf,
                      "unit": "TFLOP/s", "frac": ach_s / peak_tf, "frac_of_unfused": ach_s / (peak_tf / 2)}
 
+    # the other gradient of the same workload (least squares where the case
+    # runs Green-Gauss, and the reverse), same launch configuration
+    variants = {}
+    if a.lsq_steps > 0 and a.positivity == "none":
+        import dataclasses
+
+        from zoomy_dmplex_b200.solver import set_launch
+
+        other = "least_squares" if case.settings.gradient == "green_gauss" else "green_gauss"
+        g2 = Solver(case.model, case.mesh, dataclasses.replace(case.settings, gradient=other), params_of(case),
+                    device=dev)
+        if tuned:
+            set_launch(g2.h, tuned)
+        g2.set_state(case.q0)
+        g2.step(2)
+        g2.sync()
+        s2 = torch.cuda.ExternalStream(g2.stream, device=dev)
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(s2)
+        g2.step(a.lsq_steps)
+        f1.record(s2)
+        torch.cuda.synchronize()
+        d2 = g2.sync(check=False)
+        t4 = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t4, op=dist.ReduceOp.MAX)
+        ms2 = float(t4.item()) / a.lsq_steps
+        variants[other] = {"ms_per_step": ms2, "value": C * world / (ms2 / 1e3), "unit": UNIT,
+                           "steps": a.lsq_steps, "gradient": GRAD_TEXT[other],
+                           "timing": "CUDA events around graph-launched steps after 2 warm-up steps",
+                           "diag": {"nonfinite": d2.n_nonfinite, "negative_depth": d2.n_negative_depth}}
+        g2.close()
+
     # end to end through the public API: pinned host state in, one step, state out
     ne = a.e2e_steps or a.steps
     q_host = torch.from_numpy(np.ascontiguousarray(case.q0)).pin_memory()
@@ -804,8 +882,9 @@ def main():
             "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "%s, jittered-Delaunay %dx%d grid (%d cells, %d faces), "
-                                   "Hilbert-renumbered, order 2 Green-Gauss + Vacuum/TVD, SSP-RK2, CFL 0.45, "
-                                   "%s%s" % (CASE_TEXT[a.case][0], side, side, C, F, CASE_TEXT[a.case][1],
+                                   "Hilbert-renumbered, %s, SSP-RK2, CFL 0.45, "
+                                   "%s%s" % (CASE_TEXT[a.case][0], side, side, C, F,
+                                             GRAD_TEXT[case.settings.gradient], CASE_TEXT[a.case][1],
                                              POS_TEXT[a.positivity]),
                        "model": case.model, "cells": C, "faces": F, "n_dof_q": nq, "positivity": a.positivity,
                        "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
@@ -817,6 +896,7 @@ def main():
                                  "per-kernel events in a second, profiled pass of K steps",
                        "launch": tuned or "default"},
             "roofline": roofline, "roofline_step": roofline_step, "roofline_fp64": roofline_fp64,
+            "variants": variants,
             "fp64_step": fp64_step, "kernels": kernel_share,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "steps": ne,
@@ -831,11 +911,10 @@ def main():
                      "newton_unconverged": diag.n_newton_unconverged, "mood_cells": diag.n_mood_cells},
             "clocks": clocks}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        v, nt, Cs, dts, ns = cpu_sample(a.cpu_side, seconds=a.cpu_seconds, positivity=a.positivity, case=a.case)
+        v, nt, Cs, dts, ns = cpu_sample(side, seconds=a.cpu_seconds, positivity=a.positivity, built=case)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nt, "kind": "port",
-                                "sample": "%d steps of the CPU restatement (oracle) of the same model on a "
-                                          "%dx%d-grid mesh (%d cells), %.1f s" % (ns, a.cpu_side,
-                                                                                 a.cpu_side, Cs, dts)}
+                                "sample": "%d steps of the CPU restatement (oracle) on the same %dx%d-grid mesh "
+                                          "(%d cells), state and settings, %.1f s" % (ns, side, side, Cs, dts)}
     if rank == 0:
         print(json.dumps(line))
     g.close()

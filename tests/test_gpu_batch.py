@@ -90,3 +90,27 @@ def test_batch_mixes_triangle_and_quadrilateral_meshes():
         g.step(25)
         assert np.array_equal(b.get_state(i), g.get_state()), i
         assert b.time(i) == g.time()
+
+
+def test_config3_members_batch_equals_loop():
+    """The first 64 members of configuration 3's ensemble as specified (grid
+    sides log-uniform in [40, 400], their own bumps, humps and CFL dt): one
+    batched handle against one plain solver per member, 20 steps, every
+    member bit-identical in state and time."""
+    members = cases.ensemble(64)
+    sides = [cases.ensemble_side(i) for i in range(64)]
+    assert min(sides) < 80 and max(sides) > 250
+    st = members[0].settings
+    b = BatchSolver(members[0].model, [c.mesh for c in members], st, [_params(c) for c in members])
+    for i, c in enumerate(members):
+        b.set_state(i, c.q0)
+    b.step(20)
+    d = b.sync()
+    assert d.n_nonfinite == 0 and d.n_negative_depth == 0
+    for i, c in enumerate(members):
+        g = Solver(c.model, c.mesh, st, _params(c))
+        g.set_state(c.q0)
+        g.step(20)
+        assert np.array_equal(b.get_state(i), g.get_state()), i
+        assert b.time(i) == g.time(), i
+        g.close()
