@@ -92,12 +92,18 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes(kind, C, F, nq, na, K, stages):
+def algorithmic_bytes(kind, C, F, nq, na, K, stages, fused=False):
     """Compulsory HBM bytes of one launch of each kernel when every array it
-    touches is read or written exactly once (neighbour re-reads are free)."""
+    touches is read or written exactly once (neighbour re-reads are free).
+    fused: "flux" is the fused face + gather tile kernel (face states,
+    geometry and support in, the stage's state in and out; no face
+    contributions in device memory)."""
     d = 2
     if kind == "prep":      # state + aux + slot tables in, two face states per face out
         return C * (8 * nq + 8 * na + 12 * K + 16 * d * K) + F * 16 * nq
+    if kind == "flux" and fused:
+        state_passes = (2 * (stages - 1) + 3) / stages      # FIRST/MID: in+out (+ clamped copy), FINAL: in+base+out
+        return F * (16 * nq + 8 * (2 * d + 1) + 12) + C * (8 * na + 4 * K + 8 + 8 * nq * state_passes)
     if kind == "flux":      # face kernel: two face states + geometry + support in, 3 NQ contributions out
         return F * (16 * nq + 8 * (2 * d + 1) + 12 + 24 * nq) + C * 8 * na
     if kind == "gather":    # 3 NQ contributions per face in, state in/out
@@ -143,12 +149,15 @@ FP64_FLOPS = {
 }
 
 
-def fp64_flops(kind, model, C, F, stages):
+def fp64_flops(kind, model, C, F, stages, fused=False):
     """Algorithmic FP64 operations of one launch of a step kernel (None
-    where the table has no figure)."""
+    where the table has no figure); fused: "flux" is the fused face + gather
+    tile kernel, which does both kernels' work."""
     t = FP64_FLOPS.get(model, {})
     if kind not in t:
         return None
+    if kind == "flux" and fused:
+        return t["flux"] * F + t["gather"] * C
     return t[kind] * (F if kind == "flux" else C)
 
 
@@ -685,6 +694,7 @@ def main():
     side = a.side or CASE_SIDE[a.case]
     case = getattr(cases, a.case)(side)
     case.settings.positivity = a.positivity
+    tune_trace = None
     C, F = case.mesh.n_cells, case.mesh.n_faces
     g = Solver(case.model, case.mesh, case.settings, params_of(case), device=dev)
     g.set_state(case.q0)
@@ -698,6 +708,7 @@ def main():
         from zoomy_dmplex_b200 import autotune
 
         tuned = autotune.tune(g, case.model, case.mesh.n_cells, steps=2, use_cache=False, write_cache=False)
+        tune_trace = autotune.last_trace
         g.set_state(case.q0)          # tuning advanced the state: start again from the initial condition
     nq, na = g.nq, g.naux
     stream = torch.cuda.ExternalStream(g.stream, device=dev)
@@ -737,11 +748,16 @@ def main():
 
     # roofline of the dominant kernel (algorithmic bytes / live average duration)
     hbm, peak_src = peaks()
+    from zoomy_dmplex_b200.solver import get_launch
+
+    launch_cfg = get_launch(g.h)
+    fused = launch_cfg["tile_faces"] > 0
     dom = max((k for k in prof if prof[k][1] > 0), key=lambda k: prof[k][0])
     dom_ms = prof[dom][0] / prof[dom][1]
-    alg = algorithmic_bytes(dom, C, F, nq, na, case.mesh.max_faces, case.settings.ssp_stages)
+    alg = algorithmic_bytes(dom, C, F, nq, na, case.mesh.max_faces, case.settings.ssp_stages, fused)
     achieved = alg / (dom_ms / 1e3) / 1e9
-    traffic = NCU_DRAM_BYTES_PER_CELL.get("%s/%s" % (case.model, dom)) if a.positivity == "none" else None
+    traffic = NCU_DRAM_BYTES_PER_CELL.get("%s/%s%s" % (case.model, dom, "/fused" if fused and dom == "flux" else "")) \
+        if a.positivity == "none" else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": alg,
@@ -769,12 +785,12 @@ def main():
         peak_tf = pk.value
         s_ = case.settings.ssp_stages
         for k, v in kernel_share.items():
-            fl = fp64_flops(k, case.model, C, F, s_)
+            fl = fp64_flops(k, case.model, C, F, s_, fused)
             if fl is not None:
                 v["fp64_tflops"] = fl / (v["ms_per_launch"] / 1e3) / 1e12
         fk = max((k for k in kernel_share if "fp64_tflops" in kernel_share[k]),
                  key=lambda k: kernel_share[k]["fp64_tflops"])
-        fl = fp64_flops(fk, case.model, C, F, s_)
+        fl = fp64_flops(fk, case.model, C, F, s_, fused)
         ach = kernel_share[fk]["fp64_tflops"]
         roofline_fp64 = {"bound": "fp64", "kernel": fk, "achieved": ach, "peak": peak_tf, "unit": "TFLOP/s",
                          "frac": ach / peak_tf, "frac_of_unfused": ach / (peak_tf / 2),
@@ -894,7 +910,7 @@ def main():
                                     % (C * nq * 8 / 1e6)),
                        "timing": "CUDA events on the solver stream around K graph-launched steps; "
                                  "per-kernel events in a second, profiled pass of K steps",
-                       "launch": tuned or "default"},
+                       "launch": launch_cfg, "tuning_trace": tune_trace},
             "roofline": roofline, "roofline_step": roofline_step, "roofline_fp64": roofline_fp64,
             "variants": variants,
             "fp64_step": fp64_step, "kernels": kernel_share,

@@ -130,6 +130,13 @@ int zsme_model_info(const char* model, int32_t* n_dof_q, int32_t* n_dof_qaux,
 int zsme_create(const char* model, const zsme_mesh* mesh, const zsme_settings* settings,
                 const double* params, int device, zsme_handle** out);
 int zsme_destroy(zsme_handle* h);
+/* Host-only inspection of the tiling the fused face + gather kernel uses for
+ * `mesh` at tile_faces (see zsme_set_launch); no device is touched.  No
+ * counterpart in the reference.  stats[5]: tiles, most faces evaluated by a
+ * tile, incoming faces (faces evaluated a second time by the tile of their
+ * higher cell), faces covered by the tiles' own ranges (= n_faces), and the
+ * cell-face incidences that carry a flux. */
+int zsme_mesh_tiles(const zsme_mesh* mesh, int32_t tile_faces, int32_t* stats);
 
 /* Load Q (host, AoS, caller order) as the state at time t, apply the physical
  * constraints and compute the first dt = max(ComputeTimeStep, min_dt)
@@ -228,11 +235,16 @@ int zsme_batch_set_state(zsme_handle* h, int32_t i, const double* q_aos, double 
 int zsme_batch_get_state(zsme_handle* h, int32_t i, double* q_aos);
 int zsme_batch_get_time(zsme_handle* h, int32_t i, double* t, double* dt);
 
-/* Launch configuration, 7 ints: threads per block {prep, face, gather,
- * finalize} (multiples of 32, <= 128) and the register caps {prep, face,
+/* Launch configuration, 8 ints: threads per block {prep, face, gather,
+ * finalize} (multiples of 32, <= 128), the register caps {prep, face,
  * finalize} as resident blocks of 128 threads per SM (1 = uncapped; prep 2,
- * 3, 4, 6 or 8, face and finalize 2..4): the knobs of the autotuner
- * (zoomy-dmplex_b200/autotune.py). */
+ * 3, 4, 6 or 8, face and finalize 2..4), tile_faces: 0 runs the face
+ * fluxes and the per-cell gather as two kernels with the face contributions
+ * in device memory; 64..1024 runs them as one kernel over tiles of
+ * consecutive cells evaluating at most that many faces each, the
+ * contributions kept in shared memory (the face block size and cap apply).
+ * The knobs of the autotuner (zoomy-dmplex_b200/autotune.py).  Setting them
+ * outside stream capture only: a new tile_faces rebuilds the tiles. */
 int zsme_set_launch(zsme_handle* h, const int32_t* blocks);
 int zsme_get_launch(zsme_handle* h, int32_t* blocks);
 

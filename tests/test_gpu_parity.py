@@ -250,20 +250,25 @@ def test_device_pointer_state_roundtrip():
     assert np.array_equal(out.cpu().numpy(), g.get_state())
 
 
-def test_profile_kinds_per_step():
+@pytest.mark.parametrize("tile_faces", [0, 128])
+def test_profile_kinds_per_step(tile_faces):
     """Per-kernel timing attributes every launch of a step to its own kind:
-    two SSP stages (prep, flux, gather each), finalize and its fallback, the
+    two SSP stages (prep, flux and, with the separate kernels, gather each;
+    the fused tile kernel counts as flux), finalize and its fallback, the
     step ends; launches_per_step counts the same kernels."""
+    from zoomy_dmplex_b200.solver import set_launch
+
     c = CASES["l2"]
     g, _ = pair(c)
+    set_launch(g.h, {"tile_faces": tile_faces})
     g.set_profiling(True)
     g.step(2)
     g.sync()
     prof = g.read_profile()
     g.set_profiling(False)
     n = {k: v[1] for k, v in prof.items()}
-    assert n == {"begin_step": 2, "prep": 4, "flux": 4, "finalize": 2, "end_step": 2, "gather": 4,
-                 "finalize_fallback": 2, "mood": 0}
+    assert n == {"begin_step": 2, "prep": 4, "flux": 4, "finalize": 2, "end_step": 2,
+                 "gather": 0 if tile_faces else 4, "finalize_fallback": 2, "mood": 0}
     assert all(v[0] > 0 for k, v in prof.items() if n[k])
     assert g.launches_per_step() == sum(n.values()) // 2
 

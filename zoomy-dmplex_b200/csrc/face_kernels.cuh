@@ -15,26 +15,25 @@
 
 namespace zsme {
 
-// faces [f0, f0 + fcount)
-// MINB: resident blocks per SM the register allocation must allow (1 = no cap)
-template <class M, class N, int MINB>
-__global__ void __launch_bounds__(128, MINB) face_kernel(MeshDev m, int f0, int fcount, const double* __restrict__ fs,
-                                                   const double* __restrict__ aux,
-                                                   const double* __restrict__ params, double t_host,
-                                                   const double* t_dev, double stage_frac,
-                                                   const double* __restrict__ dt_step, double* __restrict__ fb,
-                                                   const int* __restrict__ active) {
+// One face's contributions (TransportStep.hpp:420-552): out[r * ostride] for
+// r in [0, NQ) the fluctuation into the left cell, [NQ, 2 NQ) into the right
+// cell (interior faces only), [2 NQ, 3 NQ) the flux, each times the area.
+// Returns false, writing nothing, for an exterior face without a condition
+// (no flux) and for a face of an inactive instance.
+template <class M, class N>
+__device__ __forceinline__ bool face_contrib(const MeshDev& m, int f, const double* __restrict__ fs,
+                                             const double* __restrict__ aux, const double* __restrict__ params,
+                                             double t_host, const double* t_dev, double stage_frac,
+                                             const double* __restrict__ dt_step, const int* __restrict__ active,
+                                             double* __restrict__ out, size_t ostride) {
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
     const int F = m.F, C = m.C;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= fcount) return;
-    const int f = f0 + r;
     const int I = face_instance(m, f);
-    if (active && !active[I]) return;
+    if (active && !active[I]) return false;
     const double* p = params + (size_t)I * m.np;
     const int R = m.face_R[f];
     const int bc = m.face_bc[f];
-    if (R < 0 && bc < 0) return;  // exterior face without a condition: no flux
+    if (R < 0 && bc < 0) return false;  // exterior face without a condition: no flux
     const int L = m.face_L[f];
     // stage time t0 + dt * i/(s-1) (only time-dependent BCs / aux see it)
     const double t = t_dev ? (t_dev[I] + stage_frac * (dt_step ? dt_step[I] : 0.0)) : t_host;
@@ -63,9 +62,9 @@ __global__ void __launch_bounds__(128, MINB) face_kernel(MeshDev m, int f0, int 
         const auto nc = N::numerical_fluctuations(qL, qR, aL, aR, p, nh);
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
-            fb[(size_t)i * F + f] = nc[NQ + i] * area;
-            fb[((size_t)NQ + i) * F + f] = nc[i] * area;
-            fb[((size_t)2 * NQ + i) * F + f] = flux[i] * area;
+            out[i * ostride] = nc[NQ + i] * area;
+            out[(NQ + i) * ostride] = nc[i] * area;
+            out[(2 * NQ + i) * ostride] = flux[i] * area;
         }
     } else {
         {
@@ -83,48 +82,38 @@ __global__ void __launch_bounds__(128, MINB) face_kernel(MeshDev m, int f0, int 
         const auto nc = N::numerical_fluctuations(qL, qR.data, aL, aR, p, nh);
 #pragma unroll
         for (int i = 0; i < NQ; ++i) {
-            fb[(size_t)i * F + f] = nc[NQ + i] * area;
-            fb[((size_t)2 * NQ + i) * F + f] = flux[i] * area;
+            out[i * ostride] = nc[NQ + i] * area;
+            out[(2 * NQ + i) * ostride] = flux[i] * area;
         }
     }
+    return true;
 }
 
-// cells [c0, c0 + cn)
-template <class M>
-__global__ void __launch_bounds__(128) gather_kernel(MeshDev m, Opts o, int c0, int cn,
-                                                     const double* __restrict__ fb, int mode, const double* x_in,
-                                                     double* x_out, double* base, const double* __restrict__ dt_step,
-                                                     const int* __restrict__ active, const double* __restrict__ aux,
-                                                     const double* __restrict__ params, double* __restrict__ xl_out) {
-    constexpr int NQ = M::n_dof_q;
-    const int C = m.C, F = m.F;
+// faces [f0, f0 + fcount)
+// MINB: resident blocks per SM the register allocation must allow (1 = no cap)
+template <class M, class N, int MINB>
+__global__ void __launch_bounds__(128, MINB) face_kernel(MeshDev m, int f0, int fcount, const double* __restrict__ fs,
+                                                   const double* __restrict__ aux,
+                                                   const double* __restrict__ params, double t_host,
+                                                   const double* t_dev, double stage_frac,
+                                                   const double* __restrict__ dt_step, double* __restrict__ fb,
+                                                   const int* __restrict__ active) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= cn) return;
-    const int c = c0 + r;
-    const int I = cell_instance(m, c);
-    if (active && !active[I]) return;
-    double acc[NQ];
-#pragma unroll
-    for (int i = 0; i < NQ; ++i) acc[i] = 0.0;
-    const int ord = m.order[c];
-    for (int j = 0; j < m.K; ++j) {
-        const int k = (ord >> (2 * j)) & 3;
-        const int f = m.slot_face[k * C + c];
-        if (f < 0) continue;
-        const int meta = m.slot_meta[k * C + c];
-        if (m.slot_nbr[k * C + c] < 0 && meta_bc(meta) < 0) continue;
-        if (meta_isL(meta)) {
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) acc[i] -= fb[(size_t)i * F + f];
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)2 * NQ + i) * F + f];
-        } else {
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)NQ + i) * F + f];
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) acc[i] += fb[((size_t)2 * NQ + i) * F + f];
-        }
-    }
+    if (r >= fcount) return;
+    const int f = f0 + r;
+    face_contrib<M, N>(m, f, fs, aux, params, t_host, t_dev, stage_frac, dt_step, active, fb + f, (size_t)m.F);
+}
+
+// Division by the volume (TransportStep.hpp:555-560) and the SSP-RK(s,2)
+// stage combination of PETSc's TSSSP "rks2" for cell c of instance I, whose
+// summed face contributions are acc.
+template <class M>
+__device__ __forceinline__ void stage_update(const MeshDev& m, const Opts& o, int c, int I, double* acc, int mode,
+                                             const double* x_in, double* x_out, double* base,
+                                             const double* __restrict__ dt_step, const double* __restrict__ aux,
+                                             const double* __restrict__ params, double* __restrict__ xl_out) {
+    constexpr int NQ = M::n_dof_q;
+    const int C = m.C;
     const double v = m.vol[c];
     if (v > 1e-15) {
 #pragma unroll
@@ -173,6 +162,115 @@ __global__ void __launch_bounds__(128) gather_kernel(MeshDev m, Opts o, int c0, 
             }
             break;
         }
+    }
+}
+
+// cells [c0, c0 + cn)
+template <class M>
+__global__ void __launch_bounds__(128) gather_kernel(MeshDev m, Opts o, int c0, int cn,
+                                                     const double* __restrict__ fb, int mode, const double* x_in,
+                                                     double* x_out, double* base, const double* __restrict__ dt_step,
+                                                     const int* __restrict__ active, const double* __restrict__ aux,
+                                                     const double* __restrict__ params, double* __restrict__ xl_out) {
+    constexpr int NQ = M::n_dof_q;
+    const int C = m.C, F = m.F;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    const int I = cell_instance(m, c);
+    if (active && !active[I]) return;
+    double acc[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) acc[i] = 0.0;
+    const int ord = m.order[c];
+    for (int j = 0; j < m.K; ++j) {
+        const int k = (ord >> (2 * j)) & 3;
+        const int f = m.slot_face[k * C + c];
+        if (f < 0) continue;
+        const int meta = m.slot_meta[k * C + c];
+        if (m.slot_nbr[k * C + c] < 0 && meta_bc(meta) < 0) continue;
+        if (meta_isL(meta)) {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[(size_t)i * F + f];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)2 * NQ + i) * F + f];
+        } else {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)NQ + i) * F + f];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] += fb[((size_t)2 * NQ + i) * F + f];
+        }
+    }
+    stage_update<M>(m, o, c, I, acc, mode, x_in, x_out, base, dt_step, aux, params, xl_out);
+}
+
+// ------------------------------------------------------- fused face + gather
+// Device view of FaceTiles (prepared_mesh.h).
+struct TilesDev {
+    const int* cell_off;  // [n + 1]
+    const int* face_off;  // [n + 1]
+    const int* in_off;    // [n + 1]
+    const int* in_faces;
+    const int* ord_lf;    // [K][C]
+    int stride;           // shared-memory row length (>= the most faces of a tile)
+};
+
+// One block per tile: every face the tile's cells touch is evaluated once in
+// this block (face_contrib) into shared memory, rows [3 NQ][stride]; after a
+// barrier each cell sums its faces' rows in the reference's order -- for
+// each face in increasing original face id the fluctuation, then the flux
+// (TransportStep.hpp:464-466, 529-531) -- and applies the stage update.  The
+// sums are those of face_kernel + gather_kernel operation for operation,
+// without the face-indexed contribution array in HBM; a face between two
+// tiles is evaluated by both, each using its own side.
+// Dynamic shared memory: 3 NQ stride doubles.
+template <class M, class N, int MINB>
+__global__ void __launch_bounds__(128, MINB) flux_tile_kernel(MeshDev m, Opts o, TilesDev tl,
+                                                        const double* __restrict__ fs,
+                                                        const double* __restrict__ aux,
+                                                        const double* __restrict__ params, double t_host,
+                                                        const double* t_dev, double stage_frac,
+                                                        const double* __restrict__ dt_step,
+                                                        const int* __restrict__ active, int mode,
+                                                        const double* x_in, double* x_out, double* base,
+                                                        double* __restrict__ xl_out) {
+    constexpr int NQ = M::n_dof_q;
+    extern __shared__ double rows[];
+    const int b = blockIdx.x;
+    const int f0 = tl.face_off[b], nown = tl.face_off[b + 1] - f0;
+    const int i0 = tl.in_off[b], nf = nown + tl.in_off[b + 1] - i0;
+    const int st = tl.stride;
+    for (int lf = threadIdx.x; lf < nf; lf += blockDim.x) {
+        const int f = lf < nown ? f0 + lf : tl.in_faces[i0 + lf - nown];
+        face_contrib<M, N>(m, f, fs, aux, params, t_host, t_dev, stage_frac, dt_step, active, rows + lf,
+                           (size_t)st);
+    }
+    __syncthreads();
+    const int C = m.C, K = m.K;
+    const int c1 = tl.cell_off[b + 1];
+    for (int c = tl.cell_off[b] + threadIdx.x; c < c1; c += blockDim.x) {
+        const int I = cell_instance(m, c);
+        if (active && !active[I]) continue;
+        double acc[NQ];
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) acc[i] = 0.0;
+        for (int j = 0; j < K; ++j) {
+            const int e = tl.ord_lf[j * C + c];
+            if (e < 0) continue;
+            const double* rw = rows + (e >> 1);
+            if (e & 1) {   // the cell is the face's support[0]
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] -= rw[i * st];
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] -= rw[(2 * NQ + i) * st];
+            } else {
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] -= rw[(NQ + i) * st];
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) acc[i] += rw[(2 * NQ + i) * st];
+            }
+        }
+        stage_update<M>(m, o, c, I, acc, mode, x_in, x_out, base, dt_step, aux, params, xl_out);
     }
 }
 

@@ -243,6 +243,83 @@ int prepare_mesh(const zsme_mesh& m, PreparedMesh& out) {
     return ZSME_OK;
 }
 
+int build_tiles(const PreparedMesh& p, int max_faces, FaceTiles& t) {
+    const int C = p.C, F = p.F, K = p.K;
+    if (max_faces < 2 * K) return set_error(ZSME_ERR_ARG, "tile_faces must be at least twice the face slots");
+    t = FaceTiles();
+    // faces owned by each cell: those whose lowest cell it is (contiguous runs)
+    std::vector<int> own(C, 0);
+    for (int f = 0; f < F; ++f) {
+        const int L = p.face_L[f], R = p.face_R[f];
+        const int lo = R >= 0 ? std::min(L, R) : L;
+        if (f > 0) {
+            const int pL = p.face_L[f - 1], pR = p.face_R[f - 1];
+            if ((pR >= 0 ? std::min(pL, pR) : pL) > lo) return set_error(ZSME_ERR_MESH, "faces not sorted by lowest cell");
+        }
+        own[lo]++;
+    }
+    t.cell_off.push_back(0);
+    t.face_off.push_back(0);
+    t.in_off.push_back(0);
+    t.ord_lf.assign((size_t)K * C, -1);
+    std::vector<int> in_lf;  // local index of each incoming face of the current tile, per cell slot
+    int c0 = 0, f0 = 0;
+    while (c0 < C) {
+        // grow the tile while its faces fit
+        int c = c0, nown = 0, nin = 0;
+        while (c < C) {
+            int in_c = 0;
+            for (int k = 0; k < K; ++k) {
+                const int nb = p.slot_nbr[(size_t)k * C + c];
+                if (nb >= 0 && nb < c0) in_c++;
+            }
+            if (c > c0 && nown + nin + own[c] + in_c > max_faces) break;
+            nown += own[c];
+            nin += in_c;
+            ++c;
+        }
+        const int c1 = c;
+        // local face indices: owned faces first (face order), then incoming ones
+        int j = 0;
+        for (int cc = c0; cc < c1; ++cc) {
+            int lf_slot[4] = {-1, -1, -1, -1};
+            for (int k = 0; k < K; ++k) {
+                const size_t s = (size_t)k * C + cc;
+                const int f = p.slot_face[s];
+                if (f < 0) continue;
+                const int nb = p.slot_nbr[s];
+                if (nb >= 0 && nb < c0) {
+                    t.in_faces.push_back(f);
+                    lf_slot[k] = nown + j++;
+                } else {
+                    if (f < f0 || f >= f0 + nown) return set_error(ZSME_ERR_MESH, "tile face outside its range");
+                    lf_slot[k] = f - f0;
+                }
+            }
+            const int ord = p.order[cc];
+            for (int q = 0; q < K; ++q) {
+                const int k = (ord >> (2 * q)) & 3;
+                const size_t s = (size_t)k * C + cc;
+                if (lf_slot[k] < 0) continue;
+                const int meta = p.slot_meta[s];
+                const bool bc_none = p.slot_nbr[s] < 0 && ((meta >> 3) - 2) < 0;
+                if (bc_none) continue;   // exterior face without a condition: no flux
+                t.ord_lf[(size_t)q * C + cc] = (lf_slot[k] << 1) | ((meta >> 2) & 1);
+            }
+        }
+        if (j != nin) return set_error(ZSME_ERR_MESH, "incoming face count mismatch");
+        t.max_faces = std::max(t.max_faces, nown + nin);
+        f0 += nown;
+        c0 = c1;
+        t.cell_off.push_back(c0);
+        t.face_off.push_back(f0);
+        t.in_off.push_back((int)t.in_faces.size());
+        t.n++;
+    }
+    if (f0 != F) return set_error(ZSME_ERR_MESH, "tiles do not cover the faces");
+    return ZSME_OK;
+}
+
 int concat_meshes(std::vector<PreparedMesh>& parts, PreparedMesh& out) {
     if (parts.empty()) return set_error(ZSME_ERR_ARG, "no instances");
     const int K = parts[0].K, D = parts[0].dim;

@@ -34,7 +34,27 @@ struct LaunchConfig {
     int prep, face, gather, finalize;  // threads per block
     int prep_occ = 1, face_occ = 1;    // register cap, blocks per SM: prep 1, 2, 3, 4, 6, 8; face 1-4
     int finalize_occ = 1;              // register cap of finalize, blocks of 128 per SM: 1-4
+    int tile_faces = 0;                // > 0: fused face + gather kernel over tiles of at most this many
+                                       // faces (64..1024); 0: separate face and gather kernels
 };
+
+// Tiles of the fused face + gather kernel.  A tile is a run of consecutive
+// cells; it evaluates the faces whose lowest cell lies in the tile (a
+// contiguous range, faces being sorted by their lowest cell) and the
+// "incoming" faces whose other cell lies in an earlier tile, keeps their
+// contributions in shared memory and sums them per cell.  An incoming face is
+// evaluated by both tiles it touches, each keeping its own side.
+struct FaceTiles {
+    int n = 0;          // tiles
+    int max_faces = 0;  // most faces evaluated by one tile (shared memory rows)
+    std::vector<int> cell_off, face_off, in_off;  // [n + 1]
+    std::vector<int> in_faces;                    // [in_off[n]] incoming faces, tile by tile
+    // [K][C]: the cell's j-th face in accumulation order (increasing original
+    // face id) as (local face index << 1) | (cell is support[0]); -1: no face
+    // or an exterior face without a condition (no flux)
+    std::vector<int> ord_lf;
+};
+int build_tiles(const PreparedMesh& p, int max_faces, FaceTiles& out);
 
 // Builds the layout (validates the connectivity; computes the least-squares
 // weights as LeastSquaresGradient::Setup does, Gradient.hpp:222-298).

@@ -79,6 +79,10 @@ class Solver final : public SolverBase {
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
     DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag, [5] deferred finalize cells, [6] MOOD cells
     DevBuf<int> fin_list_;        // [C] cells deferred to the generic Newton path
+    // tiles of the fused face + gather kernel (LaunchConfig::tile_faces > 0)
+    DevBuf<int> tile_cell_off_, tile_face_off_, tile_in_off_, tile_in_faces_, tile_ord_lf_;
+    int tile_n_ = 0, tile_stride_ = 0, tile_built_ = 0;  // tile_built_: the tile_faces they were built for
+    bool ready_ = false;          // init done: mesh on the device
     int sm_count_ = 148;
     DevBuf<unsigned long long> ratio_;
     // discrete adjoint (allocated by the first zsme_adjoint call)
@@ -175,11 +179,42 @@ class Solver final : public SolverBase {
             return set_error(ZSME_ERR_ARG, "prep occupancy cap must be 1, 2, 3, 4, 6 or 8 blocks per SM");
         if (lc.face_occ < 1 || lc.face_occ > 4 || lc.finalize_occ < 1 || lc.finalize_occ > 4)
             return set_error(ZSME_ERR_ARG, "face and finalize occupancy caps must be 1..4 blocks per SM");
+        if (lc.tile_faces != 0 && (lc.tile_faces < 64 || lc.tile_faces > 1024))
+            return set_error(ZSME_ERR_ARG, "tile_faces must be 0 (separate face and gather kernels) or 64..1024");
+        if ((size_t)lc.tile_faces * 3 * NQ * sizeof(double) > kMaxTileSmem)
+            return set_error(ZSME_ERR_ARG, "tile_faces too large for this model's shared-memory rows (at most " +
+                                               std::to_string(kMaxTileSmem / (3 * NQ * sizeof(double))) + ")");
         lc_ = lc;
         if (graph_) {
             cudaGraphExecDestroy(graph_);
             graph_ = nullptr;
         }
+        if (ready_) return ensure_tiles();
+        return ZSME_OK;
+    }
+    // Shared memory of one tile: 3 NQ rows of the tile's faces.
+    static constexpr size_t kMaxTileSmem = 200 * 1024;
+    // (Re)builds the tiles for lc_.tile_faces; outside any stream capture
+    // (set-up and zsme_set_launch only).
+    int ensure_tiles() {
+        if (lc_.tile_faces <= 0 || tile_built_ == lc_.tile_faces) return ZSME_OK;
+        FaceTiles t;
+        int rc = build_tiles(pm_, lc_.tile_faces, t);
+        if (rc) return rc;
+        ZSME_CUDA(tile_cell_off_.upload(t.cell_off, stream_));
+        ZSME_CUDA(tile_face_off_.upload(t.face_off, stream_));
+        ZSME_CUDA(tile_in_off_.upload(t.in_off, stream_));
+        if (t.in_faces.empty()) t.in_faces.push_back(0);
+        ZSME_CUDA(tile_in_faces_.upload(t.in_faces, stream_));
+        ZSME_CUDA(tile_ord_lf_.upload(t.ord_lf, stream_));
+        tile_n_ = t.n;
+        tile_stride_ = t.max_faces;
+        const int smem = (int)((size_t)tile_stride_ * 3 * NQ * sizeof(double));
+        ZSME_CUDA(cudaFuncSetAttribute(flux_tile_kernel<M, N, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ZSME_CUDA(cudaFuncSetAttribute(flux_tile_kernel<M, N, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ZSME_CUDA(cudaFuncSetAttribute(flux_tile_kernel<M, N, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        ZSME_CUDA(cudaFuncSetAttribute(flux_tile_kernel<M, N, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        tile_built_ = lc_.tile_faces;
         return ZSME_OK;
     }
     LaunchConfig launch() const override { return lc_; }
@@ -199,7 +234,13 @@ class Solver final : public SolverBase {
             st_.cfl = 1.0 / 6.0;
         ZSME_CUDA(cudaSetDevice(device_));
         ZSME_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        ZSME_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
         LaunchConfig lc{128, 128, 128, 128};
+        // fused face + gather tiles of up to 256 faces, smaller while the mesh
+        // would give fewer than three tiles per SM
+        int tf = std::min(256, (int)(kMaxTileSmem / (3 * NQ * sizeof(double))));
+        while (tf > 64 && pm_.F / tf < 3 * sm_count_) tf /= 2;
+        lc.tile_faces = tf;
         if (st_.block_size > 0) lc.prep = lc.face = lc.gather = st_.block_size;
         int rc = set_launch(lc);
         if (rc) return rc;
@@ -249,7 +290,6 @@ class Solver final : public SolverBase {
             ZSME_CUDA(cudaMemsetAsync(b->p, 0, n_inst_ * sizeof(double), stream_));
         }
         ZSME_CUDA(fin_list_.alloc((size_t)C));
-        ZSME_CUDA(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
         ZSME_CUDA(active_.alloc(n_inst_));
         ZSME_CUDA(cudaMemsetAsync(active_.p, 0, n_inst_ * sizeof(int), stream_));
         ZSME_CUDA(iscal_.alloc(8));
@@ -264,7 +304,8 @@ class Solver final : public SolverBase {
             for (int k = 0; k < NP; ++k) pv[(size_t)i * NP + k] = params ? params[(size_t)i * NP + k] : dp[k];
         ZSME_CUDA(params_.upload(pv, stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
-        return ZSME_OK;
+        ready_ = true;
+        return ensure_tiles();
     }
 
     StepDev step_dev(const double* dts) {
@@ -479,6 +520,26 @@ class Solver final : public SolverBase {
     }
     void launch_flux(int mode, double t_host, const double* t_dev, double frac, const double* x_in, double* x_out,
                      double* base, const double* dt, const int* active, double* xl_out = nullptr) {
+        if (lc_.tile_faces > 0) {   // fused face + gather over tiles
+            mark(ZSME_KERNEL_FLUX, true);
+            const TilesDev tl{tile_cell_off_.p, tile_face_off_.p, tile_in_off_.p, tile_in_faces_.p, tile_ord_lf_.p,
+                              tile_stride_};
+            const size_t smem = (size_t)tile_stride_ * 3 * NQ * sizeof(double);
+            switch (lc_.face_occ) {
+#define ZSME_TILE(OCC)                                                                                        \
+    case OCC:                                                                                                 \
+        flux_tile_kernel<M, N, OCC><<<tile_n_, lc_.face, smem, stream_>>>(md_, opts_, tl, fs_.p, aux_.p,        \
+                                                                       params_.p, t_host, t_dev, frac, dt,     \
+                                                                       active, mode, x_in, x_out, base,        \
+                                                                       xl_out);                                \
+        break;
+                ZSME_TILE(2) ZSME_TILE(3) ZSME_TILE(4)
+                default: ZSME_TILE(1)
+#undef ZSME_TILE
+            }
+            mark(ZSME_KERNEL_FLUX, false);
+            return;
+        }
         mark(ZSME_KERNEL_FLUX, true);
         const int gf = blocks_for(pm_.F, lc_.face);
         switch (lc_.face_occ) {
@@ -638,7 +699,8 @@ class Solver final : public SolverBase {
         mark(ZSME_KERNEL_END, false);
     }
     int launches_per_step() const override {
-        return 3 + (st_.reconstruction_order < 2 ? 3 : 3 * st_.ssp_stages) +
+        const int per_stage = lc_.tile_faces > 0 ? 2 : 3;
+        return 3 + (st_.reconstruction_order < 2 ? per_stage : per_stage * st_.ssp_stages) +
                (st_.positivity == ZSME_POSITIVITY_MOOD ? 2 : 0) + (st_.source ? 1 : 0);
     }
 

@@ -138,6 +138,26 @@ int zsme_create(const char* model, const zsme_mesh* mesh, const zsme_settings* s
     return ZSME_OK;
 }
 
+int zsme_mesh_tiles(const zsme_mesh* mesh, int32_t tile_faces, int32_t* stats) {
+    if (!mesh || !stats) return set_error(ZSME_ERR_ARG, "null argument");
+    zsme::PreparedMesh pm;
+    int rc = zsme::prepare_mesh(*mesh, pm);
+    if (rc) return rc;
+    zsme::FaceTiles t;
+    rc = zsme::build_tiles(pm, tile_faces, t);
+    if (rc) return rc;
+    int64_t covered = 0, slots = 0;
+    for (int c = 0; c < pm.C; ++c)
+        for (int j = 0; j < pm.K; ++j) slots += t.ord_lf[(size_t)j * pm.C + c] >= 0;
+    for (int b = 0; b < t.n; ++b) covered += t.face_off[b + 1] - t.face_off[b];
+    stats[0] = t.n;
+    stats[1] = t.max_faces;
+    stats[2] = (int32_t)t.in_faces.size();
+    stats[3] = (int32_t)covered;
+    stats[4] = (int32_t)slots;
+    return ZSME_OK;
+}
+
 int zsme_destroy(zsme_handle* h) {
     if (!h) return ZSME_OK;
     if (h->s) {
@@ -335,7 +355,7 @@ int zsme_set_launch(zsme_handle* h, const int32_t* blocks) {
     CHECK_H(h);
     if (!blocks) return set_error(ZSME_ERR_ARG, "null block sizes");
     return h->s->set_launch(
-        zsme::LaunchConfig{blocks[0], blocks[1], blocks[2], blocks[3], blocks[4], blocks[5], blocks[6]});
+        zsme::LaunchConfig{blocks[0], blocks[1], blocks[2], blocks[3], blocks[4], blocks[5], blocks[6], blocks[7]});
 }
 int zsme_adjoint(zsme_handle* h, int32_t nsteps, int32_t checkpoint_every, int32_t n_obs, const int32_t* obs_step,
                  const int32_t* obs_cell, const int32_t* obs_comp, const double* obs_target,
@@ -368,6 +388,7 @@ int zsme_get_launch(zsme_handle* h, int32_t* blocks) {
     blocks[4] = lc.prep_occ;
     blocks[5] = lc.face_occ;
     blocks[6] = lc.finalize_occ;
+    blocks[7] = lc.tile_faces;
     return ZSME_OK;
 }
 

@@ -87,6 +87,7 @@ def load():
     lib.zsme_model_info.argtypes = [ct.c_char_p] + [ct.POINTER(ct.c_int32)] * 4
     lib.zsme_create.argtypes = [ct.c_char_p, vp, vp, P, ct.c_int, ct.POINTER(vp)]
     lib.zsme_destroy.argtypes = [vp]
+    lib.zsme_mesh_tiles.argtypes = [vp, ct.c_int32, ct.POINTER(ct.c_int32)]
     lib.zsme_set_state.argtypes = [vp, P, ct.c_double]
     lib.zsme_get_state.argtypes = [vp, P]
     lib.zsme_get_aux.argtypes = [vp, P]
@@ -132,6 +133,16 @@ def load():
 def check(rc):
     if rc != 0:
         raise ZsmeError(rc, load().zsme_last_error().decode())
+
+
+def mesh_tiles(mesh, tile_faces: int) -> dict:
+    """The fused face + gather kernel's tiling of `mesh` (a mesh.Mesh) at
+    tile_faces, computed on the host (zsme_mesh_tiles)."""
+    lib = load()
+    m, keep = make_mesh_struct(mesh.as_abi_arrays())
+    st = (ct.c_int32 * 5)()
+    check(lib.zsme_mesh_tiles(ct.byref(m), int(tile_faces), st))
+    return dict(tiles=st[0], max_faces=st[1], incoming=st[2], covered=st[3], flux_slots=st[4])
 
 
 def model_names():
