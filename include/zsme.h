@@ -235,14 +235,21 @@ int zsme_batch_set_state(zsme_handle* h, int32_t i, const double* q_aos, double 
 int zsme_batch_get_state(zsme_handle* h, int32_t i, double* q_aos);
 int zsme_batch_get_time(zsme_handle* h, int32_t i, double* t, double* dt);
 
-/* Launch configuration, 8 ints: threads per block {prep, face, gather,
+/* Launch configuration, 10 ints: threads per block {prep, face, gather,
  * finalize} (multiples of 32, <= 128), the register caps {prep, face,
  * finalize} as resident blocks of 128 threads per SM (1 = uncapped; prep 2,
  * 3, 4, 6 or 8, face and finalize 2..4), tile_faces: 0 runs the face
  * fluxes and the per-cell gather as two kernels with the face contributions
  * in device memory; 64..1024 runs them as one kernel over tiles of
  * consecutive cells evaluating at most that many faces each, the
- * contributions kept in shared memory (the face block size and cap apply).
+ * contributions kept in shared memory (the face block size and cap apply);
+ * fuse_final: 1 lets the finalize kernel form the last SSP stage's result
+ * itself from the face contributions (separate face and gather kernels,
+ * order 2, positivity other than "mood"), so that result never round-trips
+ * through device memory; prep_lean: 1 (default) forms the order-2 face
+ * states with the lean kernel (32-bit offsets, branch-free neighbour
+ * bounds), 0 with the plain one.  Every configuration gives the same results
+ * bit for bit.
  * The knobs of the autotuner (zoomy-dmplex_b200/autotune.py).  Setting them
  * outside stream capture only: a new tile_faces rebuilds the tiles. */
 int zsme_set_launch(zsme_handle* h, const int32_t* blocks);

@@ -25,8 +25,8 @@ from . import native
 from .solver import LAUNCH_KEYS, get_launch, set_launch
 
 KNOBS = (("tile_faces", (0, 64, 128, 256, 512)), ("face", (64, 128)), ("face_occ", (1, 2, 3, 4)),
-         ("prep", (64, 128)), ("prep_occ", (1, 2, 3, 4, 6, 8)), ("gather", (64, 128)),
-         ("finalize", (64, 128)), ("finalize_occ", (1, 2, 3, 4)))
+         ("prep_lean", (0, 1)), ("prep", (64, 128)), ("prep_occ", (1, 2, 3, 4, 6, 8)), ("gather", (64, 128)),
+         ("finalize", (64, 128)), ("finalize_occ", (1, 2, 3, 4)), ("fuse_final", (0, 1)))
 # searched together first: which face path, its block size and its register cap
 # decide each other's worth (the fused kernel's shared memory per block is fixed
 # by its tile size, so its occupancy depends on all three)

@@ -165,6 +165,61 @@ __device__ __forceinline__ void stage_update(const MeshDev& m, const Opts& o, in
     }
 }
 
+// The last SSP stage's gather, for finalize_kernel to fuse: the face
+// contributions, the stage state W_{s-1} and the step's per-instance dt.
+struct FinalGather {
+    const double* fb;
+    const double* w;
+    const double* dt_step;
+    int stages;
+};
+
+// Cell c's state after the last SSP stage (gather_kernel's MODE_FINAL
+// value, the same operations in the same order) into q, from the step's
+// start state x; nothing is written.
+template <class M>
+__device__ __forceinline__ void gather_final_state(const MeshDev& m, int c, int I, const FinalGather& fg,
+                                                   const double* __restrict__ x, double* q) {
+    constexpr int NQ = M::n_dof_q;
+    const int C = m.C, F = m.F;
+    const double* __restrict__ fb = fg.fb;
+    double acc[NQ];
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) acc[i] = 0.0;
+    const int ord = m.order[c];
+    for (int j = 0; j < m.K; ++j) {
+        const int k = (ord >> (2 * j)) & 3;
+        const int f = m.slot_face[k * C + c];
+        if (f < 0) continue;
+        const int meta = m.slot_meta[k * C + c];
+        if (m.slot_nbr[k * C + c] < 0 && meta_bc(meta) < 0) continue;
+        if (meta_isL(meta)) {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[(size_t)i * F + f];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)2 * NQ + i) * F + f];
+        } else {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] -= fb[((size_t)NQ + i) * F + f];
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) acc[i] += fb[((size_t)2 * NQ + i) * F + f];
+        }
+    }
+    const double v = m.vol[c];
+    if (v > 1e-15) {
+#pragma unroll
+        for (int i = 0; i < NQ; ++i) acc[i] /= v;
+    }
+    const int s = fg.stages;
+    const double h = fg.dt_step[I];
+    const double al = (s - 1.) / s, be = h / s, ga = 1. / s;
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        const size_t id = (size_t)i * C + c;
+        q[i] = al * fg.w[id] + be * acc[i] + ga * x[id];
+    }
+}
+
 // cells [c0, c0 + cn)
 template <class M>
 __global__ void __launch_bounds__(128) gather_kernel(MeshDev m, Opts o, int c0, int cn,

@@ -36,6 +36,9 @@ struct LaunchConfig {
     int finalize_occ = 1;              // register cap of finalize, blocks of 128 per SM: 1-4
     int tile_faces = 0;                // > 0: fused face + gather kernel over tiles of at most this many
                                        // faces (64..1024); 0: separate face and gather kernels
+    int fuse_final = 0;                // 1: with separate face and gather kernels, the last stage's
+                                       // gather runs inside the finalize kernel
+    int prep_lean = 1;                 // order-2 face states by prep_lean_kernel (1) or prep_kernel (0)
 };
 
 // Tiles of the fused face + gather kernel.  A tile is a run of consecutive

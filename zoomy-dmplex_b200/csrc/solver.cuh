@@ -83,6 +83,7 @@ class Solver final : public SolverBase {
     DevBuf<int> tile_cell_off_, tile_face_off_, tile_in_off_, tile_in_faces_, tile_ord_lf_;
     int tile_n_ = 0, tile_stride_ = 0, tile_built_ = 0;  // tile_built_: the tile_faces they were built for
     bool ready_ = false;          // init done: mesh on the device
+    bool lean_ok_ = false;        // 32-bit element offsets cover every array prep_lean_kernel indexes
     int sm_count_ = 148;
     DevBuf<unsigned long long> ratio_;
     // discrete adjoint (allocated by the first zsme_adjoint call)
@@ -179,6 +180,8 @@ class Solver final : public SolverBase {
             return set_error(ZSME_ERR_ARG, "prep occupancy cap must be 1, 2, 3, 4, 6 or 8 blocks per SM");
         if (lc.face_occ < 1 || lc.face_occ > 4 || lc.finalize_occ < 1 || lc.finalize_occ > 4)
             return set_error(ZSME_ERR_ARG, "face and finalize occupancy caps must be 1..4 blocks per SM");
+        if (lc.fuse_final < 0 || lc.fuse_final > 1) return set_error(ZSME_ERR_ARG, "fuse_final must be 0 or 1");
+        if (lc.prep_lean < 0 || lc.prep_lean > 1) return set_error(ZSME_ERR_ARG, "prep_lean must be 0 or 1");
         if (lc.tile_faces != 0 && (lc.tile_faces < 64 || lc.tile_faces > 1024))
             return set_error(ZSME_ERR_ARG, "tile_faces must be 0 (separate face and gather kernels) or 64..1024");
         if ((size_t)lc.tile_faces * 3 * NQ * sizeof(double) > kMaxTileSmem)
@@ -304,6 +307,8 @@ class Solver final : public SolverBase {
             for (int k = 0; k < NP; ++k) pv[(size_t)i * NP + k] = params ? params[(size_t)i * NP + k] : dp[k];
         ZSME_CUDA(params_.upload(pv, stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));
+        lean_ok_ = 2LL * NQ * F < 0x7fffffffLL && (long long)NQ * C < 0x7fffffffLL &&
+                   (long long)pm_.K * 2 * C < 0x7fffffffLL;
         ready_ = true;
         return ensure_tiles();
     }
@@ -502,6 +507,24 @@ class Solver final : public SolverBase {
             mark(ZSME_KERNEL_PREP, false);
             return;
         }
+        if (lc_.prep_lean && st_.reconstruction_order >= 2 && lean_ok_) {
+            switch (lc_.prep_occ) {
+#define ZSME_PREPL(OCC)                                                                                         \
+    case OCC:                                                                                                   \
+        if (pm_.K == 3)                                                                                         \
+            prep_lean_kernel<M, OCC, 3><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, params_.p,   \
+                                                                      fs_.p, active);                           \
+        else                                                                                                    \
+            prep_lean_kernel<M, OCC, 4><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, params_.p,   \
+                                                                      fs_.p, active);                           \
+        break;
+                ZSME_PREPL(2) ZSME_PREPL(3) ZSME_PREPL(4) ZSME_PREPL(6) ZSME_PREPL(8)
+                default: ZSME_PREPL(1)
+#undef ZSME_PREPL
+            }
+            mark(ZSME_KERNEL_PREP, false);
+            return;
+        }
         switch (lc_.prep_occ) {
 #define ZSME_PREP(OCC)                                                                                          \
     case OCC:                                                                                                   \
@@ -518,8 +541,11 @@ class Solver final : public SolverBase {
         }
         mark(ZSME_KERNEL_PREP, false);
     }
+    // face_only: the face kernel alone (split path), its gather left to the
+    // finalize kernel (fused_final_stage)
     void launch_flux(int mode, double t_host, const double* t_dev, double frac, const double* x_in, double* x_out,
-                     double* base, const double* dt, const int* active, double* xl_out = nullptr) {
+                     double* base, const double* dt, const int* active, double* xl_out = nullptr,
+                     bool face_only = false) {
         if (lc_.tile_faces > 0) {   // fused face + gather over tiles
             mark(ZSME_KERNEL_FLUX, true);
             const TilesDev tl{tile_cell_off_.p, tile_face_off_.p, tile_in_off_.p, tile_in_faces_.p, tile_ord_lf_.p,
@@ -553,25 +579,41 @@ class Solver final : public SolverBase {
 #undef ZSME_FACE
         }
         mark(ZSME_KERNEL_FLUX, false);
+        if (face_only) return;
         mark(ZSME_KERNEL_GATHER, true);
         gather_kernel<M><<<blocks_for(pm_.C, lc_.gather), lc_.gather, 0, stream_>>>(md_, opts_, 0, pm_.C, fb_.p,
                                                                                    mode, x_in, x_out, base, dt,
                                                                                    active, aux_.p, params_.p, xl_out);
         mark(ZSME_KERNEL_GATHER, false);
     }
-    void finalize_range(int c0, int cn, const StepDev& sd, const double* dt_src, int flags) {
+    // fg: the last SSP stage's gather, fused into the finalize kernel (or nullptr)
+    void finalize_range(int c0, int cn, const StepDev& sd, const double* dt_src, int flags,
+                        const FinalGather* fg = nullptr) {
         const int gb = blocks_for(cn, lc_.finalize);
         if (flags & FIN_SOURCE) cudaMemsetAsync(sd.n_fallback, 0, sizeof(int), stream_);
         mark(ZSME_KERNEL_FINALIZE, true);
-        switch (lc_.finalize_occ) {
+        if (fg) {
+            switch (lc_.finalize_occ) {
+#define ZSME_FING(OCC)                                                                                           \
+    case OCC:                                                                                                    \
+        finalize_kernel<M, N, OCC, true><<<gb, lc_.finalize, 0, stream_>>>(md_, c0, cn, x_.p, aux_.p, params_.p,  \
+                                                                           sd, dt_src, flags, *fg);              \
+        break;
+                ZSME_FING(2) ZSME_FING(3) ZSME_FING(4)
+                default: ZSME_FING(1)
+#undef ZSME_FING
+            }
+        } else {
+            switch (lc_.finalize_occ) {
 #define ZSME_FIN(OCC)                                                                                            \
     case OCC:                                                                                                    \
         finalize_kernel<M, N, OCC><<<gb, lc_.finalize, 0, stream_>>>(md_, c0, cn, x_.p, aux_.p, params_.p, sd,    \
                                                                      dt_src, flags);                             \
         break;
-            ZSME_FIN(2) ZSME_FIN(3) ZSME_FIN(4)
-            default: ZSME_FIN(1)
+                ZSME_FIN(2) ZSME_FIN(3) ZSME_FIN(4)
+                default: ZSME_FIN(1)
 #undef ZSME_FIN
+            }
         }
         mark(ZSME_KERNEL_FINALIZE, false);
         if (flags & FIN_SOURCE) {   // the cells whose Newton update needs the generic GEPP (usually none)
@@ -581,8 +623,8 @@ class Solver final : public SolverBase {
             mark(ZSME_KERNEL_FALLBACK, false);
         }
     }
-    void launch_finalize(const StepDev& sd, const double* dt_src, int flags) {
-        finalize_range(0, pm_.C, sd, dt_src, flags);
+    void launch_finalize(const StepDev& sd, const double* dt_src, int flags, const FinalGather* fg = nullptr) {
+        finalize_range(0, pm_.C, sd, dt_src, flags, fg);
     }
 
     int rhs(double t, const double* x_aos, double* f_aos) override {
@@ -655,6 +697,11 @@ class Solver final : public SolverBase {
         mark(ZSME_KERNEL_BEGIN, false);
         const bool mood = st_.positivity == ZSME_POSITIVITY_MOOD;
         if (mood) cudaMemcpyAsync(xs_.p, x_.p, xs_.n * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
+        // the last stage's gather inside finalize: separate face and gather
+        // kernels at order 2, and the stage result not needed on its own
+        // (MOOD inspects it, the adjoint's tape keeps it)
+        const bool fuse_final = lc_.fuse_final && lc_.tile_faces == 0 && st_.reconstruction_order >= 2 && !mood &&
+                                !tape;
         if (st_.reconstruction_order < 2) {
             launch_prep(x_.p, x_.p, act);
             tape_fs(0);
@@ -676,7 +723,7 @@ class Solver final : public SolverBase {
             }
             launch_prep(w_.p, wl_.p, act);
             tape_fs(s - 1);
-            launch_flux(MODE_FINAL, 0.0, t, 1.0, w_.p, nullptr, x_.p, dt, act);
+            launch_flux(MODE_FINAL, 0.0, t, 1.0, w_.p, nullptr, x_.p, dt, act, nullptr, fuse_final);
             if (tape)
                 cudaMemcpyAsync(tape + (size_t)s * tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice,
                                 stream_);
@@ -693,14 +740,17 @@ class Solver final : public SolverBase {
             mark(ZSME_KERNEL_MOOD, false);
         }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
-        launch_finalize(sd, sd.dt_step, flags);
+        const FinalGather fg{fb_.p, w_.p, sd.dt_step, st_.ssp_stages};
+        launch_finalize(sd, sd.dt_step, flags, fuse_final ? &fg : nullptr);
         mark(ZSME_KERNEL_END, true);
         end_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_, 1, 0.0, nullptr);
         mark(ZSME_KERNEL_END, false);
     }
     int launches_per_step() const override {
         const int per_stage = lc_.tile_faces > 0 ? 2 : 3;
-        return 3 + (st_.reconstruction_order < 2 ? per_stage : per_stage * st_.ssp_stages) +
+        const bool fuse_final = lc_.fuse_final && lc_.tile_faces == 0 && st_.reconstruction_order >= 2 &&
+                                st_.positivity != ZSME_POSITIVITY_MOOD;
+        return 3 - (fuse_final ? 1 : 0) + (st_.reconstruction_order < 2 ? per_stage : per_stage * st_.ssp_stages) +
                (st_.positivity == ZSME_POSITIVITY_MOOD ? 2 : 0) + (st_.source ? 1 : 0);
     }
 

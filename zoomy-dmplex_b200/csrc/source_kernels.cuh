@@ -278,14 +278,18 @@ enum FinalizeFlags {
 // One cell of the finalize step: constraints, source, constraints, store,
 // CFL ratio (into ratio).  GENERIC = false: returns -1 without storing
 // anything when the Newton iteration needs the generic full-size GEPP.
-template <class M, class N, bool GENERIC>
+// GATHER: the cell's state is the last SSP stage's result, formed here from
+// the face contributions (gather_final_state) instead of read from x.
+template <class M, class N, bool GENERIC, bool GATHER = false>
 __device__ __forceinline__ int finalize_cell(const MeshDev& m, int c, int I, double* __restrict__ x,
                                              double* __restrict__ aux, const double* p, const StepDev& sd,
-                                             const double* __restrict__ dt_src, int flags, double& ratio) {
+                                             const double* __restrict__ dt_src, int flags, double& ratio,
+                                             const FinalGather* fg = nullptr) {
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux, DIM = M::dimension;
     const int C = m.C;
     double q[NQ], a[NA];
-    load_q<NQ>(x, C, c, q);
+    if constexpr (GATHER) gather_final_state<M>(m, c, I, *fg, x, q);
+    else load_q<NQ>(x, C, c, q);
 #pragma unroll
     for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
     if (flags & FIN_PRE) constrain<M>(q, a, p);
@@ -338,18 +342,31 @@ __device__ __forceinline__ int finalize_cell(const MeshDev& m, int c, int I, dou
 // kernel lowers its stack and register pressure (1.29 -> 0.99 ms on the
 // 1400^2 level-4 workload).
 // MINB: resident blocks of 128 threads per SM the register allocation must allow (1 = no cap)
-template <class M, class N, int MINB>
+// GATHER: the kernel also performs the last SSP stage's gather (fg), so the
+// stage result never round-trips through x; a deferred cell gets that result
+// written to x for finalize_fallback_kernel.
+template <class M, class N, int MINB, bool GATHER = false>
 __global__ void __launch_bounds__(128, MINB) finalize_kernel(MeshDev m, int c0, int cn, double* __restrict__ x,
                                                        double* __restrict__ aux, const double* __restrict__ params,
-                                                       StepDev sd, const double* __restrict__ dt_src, int flags) {
+                                                       StepDev sd, const double* __restrict__ dt_src, int flags,
+                                                       FinalGather fg = FinalGather{}) {
+    constexpr int NQ = M::n_dof_q;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = c0 + r;
     const int I = r < cn ? cell_instance(m, c) : -1;
     double ratio = DBL_MAX;
     const bool act = I >= 0 && (sd.active ? (sd.active[I] != 0) : true);
     bool defer = false;
-    if (act) defer = finalize_cell<M, N, false>(m, c, I, x, aux, params + (size_t)I * m.np, sd, dt_src, flags,
-                                                 ratio) < 0;
+    if (act) defer = finalize_cell<M, N, false, GATHER>(m, c, I, x, aux, params + (size_t)I * m.np, sd, dt_src,
+                                                         flags, ratio, &fg) < 0;
+    if constexpr (GATHER) {
+        if (defer) {   // the generic path restarts from the stage result
+            double q[NQ];
+            gather_final_state<M>(m, c, I, fg, x, q);
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) x[(size_t)i * m.C + c] = q[i];
+        }
+    }
     if (flags & FIN_SOURCE) {
         const unsigned dm = __ballot_sync(0xffffffffu, defer);
         if (dm) {

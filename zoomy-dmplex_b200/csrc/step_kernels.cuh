@@ -345,6 +345,176 @@ __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int 
     }
 }
 
+// ---------------------------------------------------------- prep, lean form
+// prep_kernel's order-2 face states (positivity "none") with less integer and
+// branch work, bit for bit the same:
+//  * per-component base pointers and 32-bit element offsets (the host uses
+//    this kernel only when 2 NQ F and NQ C fit in an int);
+//  * a missing neighbour (boundary slot) is replaced by the cell itself in the
+//    limiter bounds and the vacuum minimum, where a comparison with the cell's
+//    own value never changes the running minimum or maximum (NaN included);
+//  * the Green-Gauss orientation is folded into a signed normal: g - fv N is
+//    g + fv (-N) exactly in IEEE arithmetic, and qc + qn equals qn + qc.
+// Sums run in the reference's order as in prep_kernel: least squares in cone
+// order, Green-Gauss in increasing original face order, bounds in cone order.
+template <class M, int MINB, int KM>
+__global__ void __launch_bounds__(128, MINB) prep_lean_kernel(MeshDev m, Opts o, int c0, int cn,
+                                                        const double* __restrict__ w,
+                                                        const double* __restrict__ wl,
+                                                        const double* __restrict__ params,
+                                                        double* __restrict__ fs, const int* __restrict__ active) {
+    constexpr int NQ = M::n_dof_q, DIM = M::dimension;
+    const int C = m.C, F = m.F;
+    const int K = KM == 3 ? 3 : m.K;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    const int I = cell_instance(m, c);
+    if (active && !active[I]) return;
+    const double* p = params + (size_t)I * m.np;
+    int nbc[KM], fso[KM];
+    bool hasn[KM];
+    double dx[KM][DIM];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) {
+        int n = -2, f = -1, side = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) dx[k][d] = 0.0;
+        if (k < K) {
+            n = m.slot_nbr[k * C + c];
+            f = m.slot_face[k * C + c];
+            side = meta_isL(m.slot_meta[k * C + c]) ? 0 : 1;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) dx[k][d] = m.slot_dx[(k * 2 + d) * C + c];
+        }
+        hasn[k] = n >= 0;
+        nbc[k] = n >= 0 ? n : c;
+        fso[k] = f >= 0 ? side * NQ * F + f : -1;
+    }
+    double g[NQ * DIM];
+#pragma unroll
+    for (int i = 0; i < NQ * DIM; ++i) g[i] = 0.0;
+    if (o.gradient == 1) {   // least squares, cone order (Gradient.hpp:330-346)
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (!hasn[k]) continue;
+            double wk[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) wk[d] = m.slot_w[(k * 2 + d) * C + c];
+            const double* wp = w;
+#pragma unroll
+            for (int i = 0; i < NQ; ++i, wp += C) {
+                const double du = wp[nbc[k]] - wp[c];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) g[i * DIM + d] += wk[d] * du;
+            }
+        }
+    } else {                 // Green-Gauss, increasing original face order (Gradient.hpp:91-176)
+        const int ord = m.order[c];
+#pragma unroll
+        for (int j = 0; j < KM; ++j) {
+            if (j >= K) continue;
+            const int k = (ord >> (2 * j)) & 3;
+            const int f = m.slot_face[k * C + c];
+            if (f < 0) continue;
+            const int meta = m.slot_meta[k * C + c];
+            const int n = m.slot_nbr[k * C + c];
+            const double Nf[2] = {m.fnr[f], m.fnr[F + f]};
+            if (n >= 0) {
+                double sN[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) sN[d] = meta_isL(meta) ? Nf[d] : -Nf[d];
+                const double* wp = w;
+#pragma unroll
+                for (int i = 0; i < NQ; ++i, wp += C) {
+                    const double fv = 0.5 * (wp[c] + wp[n]);
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) g[i * DIM + d] += fv * sN[d];
+                }
+            } else if (meta_bc(meta) >= 0) {
+                double qg[NQ];
+                load_q<NQ>(w, C, c, qg);
+                const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
+                const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
+                const auto qb = M::boundary_conditions(meta_bc(meta), qg, (const double*)nullptr, p, nh, xf, 0.0, 0.0);
+#pragma unroll
+                for (int i = 0; i < NQ; ++i)
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) g[i * DIM + d] += qb[i] * Nf[d];
+            }
+        }
+        const double v = m.vol[c];
+        if (v > 1e-15) {
+#pragma unroll
+            for (int i = 0; i < NQ * DIM; ++i) g[i] /= v;
+        }
+    }
+    // pass 1: each face's alpha = min over components of min(vacuum, tvd)
+    double al[KM];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) al[k] = 1.0;
+    if (o.limiter) {
+        bool vac = false;   // VacuumLimiter: minimum depth (component 1) over the cell and its neighbours
+        if constexpr (NQ > 1) {
+            double mnh = wl[C + c];
+#pragma unroll
+            for (int k = 0; k < KM; ++k) {
+                const double v = wl[C + nbc[k]];
+                if (v < mnh) mnh = v;
+            }
+            vac = mnh < 1e-2;
+        }
+        if (vac) {
+#pragma unroll
+            for (int k = 0; k < KM; ++k) al[k] = 0.0;
+        } else {
+            const double* wp = wl;
+#pragma unroll
+            for (int i = 0; i < NQ; ++i, wp += C) {
+                const double q = wp[c];
+                double mn = q, mx = q;
+#pragma unroll
+                for (int k = 0; k < KM; ++k) {
+                    const double v = wp[nbc[k]];
+                    if (v < mn) mn = v;
+                    if (v > mx) mx = v;
+                }
+#pragma unroll
+                for (int k = 0; k < KM; ++k) {
+                    if (fso[k] < 0) continue;
+                    double d = 0.0;
+#pragma unroll
+                    for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+                    const double qfu = q + d;
+                    const double dq = qfu - q;
+                    const bool pos = dq > 0;
+                    const double rr = (pos ? mx : mn) - q;
+                    const bool room = pos ? (mx > q) : (mn < q);
+                    const bool lim = !(pos ? (rr >= dq) : (rr <= dq));
+                    const bool small = fabs(dq) < 1e-12;
+                    double a = small ? 1.0 : (room ? 1.0 : 0.0);
+                    if (!small && room && lim) a = fmin(1.0, rr / dq);
+                    if (a < al[k]) al[k] = a;
+                }
+            }
+        }
+    }
+    // pass 2: face states q + alpha * delta
+    const double* wp = wl;
+#pragma unroll
+    for (int i = 0; i < NQ; ++i, wp += C) {
+        const double q = wp[c];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (fso[k] < 0) continue;
+            double d = 0.0;
+#pragma unroll
+            for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+            fs[fso[k] + i * F] = q + al[k] * d;
+        }
+    }
+}
+
 // Venkatakrishnan eps^2 = vol^(2/dim) (TransportStep.hpp:279), exact in 1-D and 2-D.
 template <int DIM>
 __host__ __device__ __forceinline__ double venkat_eps2(double v) {

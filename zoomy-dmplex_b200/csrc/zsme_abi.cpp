@@ -355,7 +355,8 @@ int zsme_set_launch(zsme_handle* h, const int32_t* blocks) {
     CHECK_H(h);
     if (!blocks) return set_error(ZSME_ERR_ARG, "null block sizes");
     return h->s->set_launch(
-        zsme::LaunchConfig{blocks[0], blocks[1], blocks[2], blocks[3], blocks[4], blocks[5], blocks[6], blocks[7]});
+        zsme::LaunchConfig{blocks[0], blocks[1], blocks[2], blocks[3], blocks[4], blocks[5], blocks[6], blocks[7],
+                           blocks[8], blocks[9]});
 }
 int zsme_adjoint(zsme_handle* h, int32_t nsteps, int32_t checkpoint_every, int32_t n_obs, const int32_t* obs_step,
                  const int32_t* obs_cell, const int32_t* obs_comp, const double* obs_target,
@@ -389,6 +390,8 @@ int zsme_get_launch(zsme_handle* h, int32_t* blocks) {
     blocks[5] = lc.face_occ;
     blocks[6] = lc.finalize_occ;
     blocks[7] = lc.tile_faces;
+    blocks[8] = lc.fuse_final;
+    blocks[9] = lc.prep_lean;
     return ZSME_OK;
 }
 

@@ -152,6 +152,13 @@ class Printer:
                 return "std::cbrt(" + bs + ")"
             if x == sp.Rational(-1, 3):
                 return "(1.0/std::cbrt(" + bs + "))"
+            if x.is_Rational and x.q == 3:
+                # b^(m + r/3) = b*...*b * cbrt(b)^r: one cube root, shared by every
+                # such power of b after the compiler's CSE, instead of a pow each
+                if x < 0:
+                    return "(1.0/" + self.p(sp.Pow(b, -x, evaluate=False)) + ")"
+                m, r = divmod(int(x.p), 3)
+                return "(" + "*".join([bs] * m + ["std::cbrt(" + bs + ")"] * r) + ")"
             return "std::pow(" + bs + ", " + _num(x) + ")"
         if isinstance(e, (sp.Max, sp.Min)):
             fn = "std::max" if isinstance(e, sp.Max) else "std::min"
@@ -252,6 +259,13 @@ def _vjp(e, a, acc):
         elif x == sp.Rational(-1, 3):                      # 1.0/std::cbrt(b)
             c = sp.cbrt(b)
             _vjp(b, -a * e ** 2 * SelNZ(c, 1 / (3 * c * c), 0), acc)
+        elif x.is_Rational and x.q == 3 and x > 0:         # b*...*b*cbrt(b)^r
+            m, r = divmod(int(x.p), 3)
+            c = sp.cbrt(b)
+            dc = SelNZ(c, 1 / (3 * c * c), 0)
+            _vjp(b, a * (m * b ** (m - 1) * c ** r + b ** m * r * c ** (r - 1) * dc), acc)
+        elif x.is_Rational and x.q == 3:                   # 1.0/(b*...*b*cbrt(b)^r)
+            _vjp(sp.Pow(b, -x, evaluate=False), -a * e ** 2, acc)
         else:                                              # std::pow(b, x)
             _vjp(b, a * SelNZ(b, x * b ** (x - 1), 0), acc)
     elif isinstance(e, (sp.Max, sp.Min)):

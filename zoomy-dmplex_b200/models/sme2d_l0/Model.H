@@ -148,7 +148,7 @@ struct Model {
     {
     T t0 = (Qaux[0]*p[1]/(p[2]));
     T t1 = (Qaux[0]*Qaux[0]);
-    T t2 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((1e-24 + t1*(Q[2]*Q[2]) + t1*(Q[3]*Q[3])));
+    T t2 = p[0]*(Qaux[0]*std::cbrt(Qaux[0]))*(p[3]*p[3])*std::sqrt((1e-24 + t1*(Q[2]*Q[2]) + t1*(Q[3]*Q[3])));
     SimpleArray<T, 4> res;
     res[0] = 0.0;
     res[1] = 0.0;
@@ -230,11 +230,11 @@ struct Model {
     T t5 = std::sqrt((1e-24 + t0*t3 + t0*t4));
     T t6 = p[0]*(p[3]*p[3]);
     T t7 = t5*t6;
-    T t8 = 1.3333333333333333*t7*std::pow(Qaux[0], (7.0/3.0));
+    T t8 = 1.3333333333333333*t7*(Qaux[0]*Qaux[0]*std::cbrt(Qaux[0]));
     T t9 = (t6/(t5));
-    T t10 = t9*std::pow(Qaux[0], (13.0/3.0))*(t3 + t4);
-    T t11 = t9*std::pow(Qaux[0], (10.0/3.0));
-    T t12 = (Qaux[0]*t1 + t7*std::pow(Qaux[0], (4.0/3.0)));
+    T t10 = t9*(Qaux[0]*Qaux[0]*Qaux[0]*Qaux[0]*std::cbrt(Qaux[0]))*(t3 + t4);
+    T t11 = t9*(Qaux[0]*Qaux[0]*Qaux[0]*std::cbrt(Qaux[0]));
+    T t12 = (Qaux[0]*t1 + t7*(Qaux[0]*std::cbrt(Qaux[0])));
     T t13 = (-Q[2]*Q[3]*t11);
     SimpleArray<T, 16> res;
     res[0] = 0.0;

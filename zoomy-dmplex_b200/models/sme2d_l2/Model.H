@@ -276,7 +276,7 @@ struct Model {
     T t1 = t0*(Q[2] + Q[3] + Q[4]);
     T t2 = Qaux[0]*p[1];
     T t3 = (Qaux[0]*Qaux[0]);
-    T t4 = p[0]*std::pow(Qaux[0], (4.0/3.0))*(p[3]*p[3])*std::sqrt((1e-24 + t3*(Q[2]*Q[2]) + t3*(Q[5]*Q[5])));
+    T t4 = p[0]*(Qaux[0]*std::cbrt(Qaux[0]))*(p[3]*p[3])*std::sqrt((1e-24 + t3*(Q[2]*Q[2]) + t3*(Q[5]*Q[5])));
     T t5 = 4.0*Qaux[0];
     T t6 = 3.0*t2;
     T t7 = 12.0*Qaux[0];
@@ -493,13 +493,13 @@ struct Model {
     T t6 = std::sqrt((1e-24 + t2*t4 + t2*t5));
     T t7 = p[0]*(p[3]*p[3]);
     T t8 = t6*t7;
-    T t9 = 1.3333333333333333*t8*std::pow(Qaux[0], (7.0/3.0));
+    T t9 = 1.3333333333333333*t8*(Qaux[0]*Qaux[0]*std::cbrt(Qaux[0]));
     T t10 = (t7/(t6));
-    T t11 = t10*std::pow(Qaux[0], (13.0/3.0))*(t4 + t5);
-    T t12 = t10*std::pow(Qaux[0], (10.0/3.0));
+    T t11 = t10*(Qaux[0]*Qaux[0]*Qaux[0]*Qaux[0]*std::cbrt(Qaux[0]))*(t4 + t5);
+    T t12 = t10*(Qaux[0]*Qaux[0]*Qaux[0]*std::cbrt(Qaux[0]));
     T t13 = Qaux[0]*p[1];
     T t14 = t0*t13;
-    T t15 = (t14 + t8*std::pow(Qaux[0], (4.0/3.0)));
+    T t15 = (t14 + t8*(Qaux[0]*std::cbrt(Qaux[0])));
     T t16 = (-t14);
     T t17 = (-Q[2]*Q[5]*t12);
     T t18 = 8.0*Qaux[0];

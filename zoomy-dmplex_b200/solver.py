@@ -330,16 +330,19 @@ class BatchSolver:
         return n.value
 
 
-LAUNCH_KEYS = ("prep", "face", "gather", "finalize", "prep_occ", "face_occ", "finalize_occ", "tile_faces")
+LAUNCH_KEYS = ("prep", "face", "gather", "finalize", "prep_occ", "face_occ", "finalize_occ", "tile_faces",
+               "fuse_final", "prep_lean")
 LAUNCH_DEFAULTS = {"prep": 128, "face": 128, "gather": 128, "finalize": 128, "prep_occ": 1, "face_occ": 1,
-                   "finalize_occ": 1, "tile_faces": 256}
+                   "finalize_occ": 1, "tile_faces": 256, "fuse_final": 0, "prep_lean": 1}
 
 
 def set_launch(h, cfg):
     """Launch configuration of a handle: dict with LAUNCH_KEYS (threads per
     block of each kernel, register caps as blocks per SM, tile_faces: 0 for
     the separate face and gather kernels, else the fused tile kernel's most
-    faces per tile); missing keys take LAUNCH_DEFAULTS."""
+    faces per tile, fuse_final: the last stage's gather inside the finalize
+    kernel, prep_lean: the lean face-state kernel); missing keys take
+    LAUNCH_DEFAULTS."""
     lib = native.load()
     b = (ct.c_int32 * len(LAUNCH_KEYS))(*[int(cfg.get(k, LAUNCH_DEFAULTS[k])) for k in LAUNCH_KEYS])
     native.check(lib.zsme_set_launch(h, b))
