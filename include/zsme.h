@@ -92,7 +92,10 @@ typedef struct zsme_settings {
     int32_t source;               /* 1: operator-split implicit source ("splitting") */
     int32_t block_size;           /* CUDA block size, 0 = library default */
     int32_t positivity;           /* ZSME_POSITIVITY_* */
-    int32_t reserved[5];
+    int32_t refresh_derivative_aux; /* solver.refresh_derivative_aux: before every state update, fill the
+                                     plugin's derivative aux slots (its field-level update_aux_variables;
+                                     Green-Gauss derivatives, TransportStep.hpp:161-192) */
+    int32_t reserved[4];
     double wet_dry_eps;           /* solver.wet_dry_eps (reference default 1e-2): dry threshold of the
                                      positivity variants, read only when positivity != NONE */
 } zsme_settings;

@@ -61,13 +61,10 @@ namespace sme2d_l4 {
 }
 #ifdef ORACLE_WITH_REFERENCE_MODEL
 // The reference's own generated 1-D level-0 headers (oracle/_ref build only).
-// Its field-level update_aux_variables needs a mesh handle and
-// compute_derivative (reference UserFunctions.H:46-112); the derivative aux is
-// never refreshed on this path, so inert stand-ins suffice.
+// Its field-level update_aux_variables calls compute_derivative on the mesh
+// handle of model_prelude.h, which the oracle serves with its restatement of
+// the reference's Green-Gauss derivative (Oracle::compute_derivative_gg).
 namespace ref1d {
-struct ZoomyMesh {};
-template <typename T>
-inline void compute_derivative(T*, const T*, int, int, int, const ZoomyMesh&) {}
 #include "Model.H"
 #include "Numerics.H"
 }
@@ -273,9 +270,69 @@ struct Oracle : OracleBase {
         auto ra = M::update_aux_variables(q, a, params.data(), 0.0, X0);
         for (int i = 0; i < NA; ++i) a[i] = ra[i];
     }
-    // TransportStep::UpdateState (TransportStep.hpp:196-230)
+    // TransportStep::UpdateState (TransportStep.hpp:196-230): the derivative
+    // aux first (when refreshed), then the pointwise clamp and aux per cell.
     void update_state_vec(std::vector<T>& x, std::vector<T>& a) const {
+        if (st.refresh_derivative_aux) refresh_derivative_aux(x, a);
         par_for(C, [&](int c, int) { constrain_cell(&x[(size_t)c * NQ], &a[(size_t)c * NA]); });
+    }
+    // TransportStep::RefreshDerivativeAux (TransportStep.hpp:161-192): the state
+    // and aux de-interleaved into per-variable fields, the plugin's field-level
+    // update_aux_variables called on them (it fills its derivative slots through
+    // compute_derivative), the aux interleaved back.  Plugins without that
+    // overload have nothing to refresh; so do the dual-number and counting
+    // instances, whose derivative slots feed no state update.
+    void refresh_derivative_aux(const std::vector<T>& x, std::vector<T>& a) const {
+        if constexpr (zsme::HasFieldAuxUpdate<M>::value && std::is_same<T, double>::value) {
+            std::vector<std::vector<double>> Qf(NQ, std::vector<double>(C)), Af(NA, std::vector<double>(C));
+            for (int c = 0; c < C; ++c) {
+                for (int i = 0; i < NQ; ++i) Qf[i][c] = x[(size_t)c * NQ + i];
+                for (int k = 0; k < NA; ++k) Af[k][c] = a[(size_t)c * NA + k];
+            }
+            std::vector<double*> Qp(NQ), Ap(NA);
+            for (int i = 0; i < NQ; ++i) Qp[i] = Qf[i].data();
+            for (int k = 0; k < NA; ++k) Ap[k] = Af[k].data();
+            const ZoomyMesh mesh{&Oracle::derivative_request, (void*)this};
+            M::update_aux_variables(Qp.data(), Ap.data(), 0.0, mesh);
+            for (int c = 0; c < C; ++c)
+                for (int k = 0; k < NA; ++k) a[(size_t)c * NA + k] = Af[k][c];
+        }
+    }
+    static void derivative_request(const ZoomyMesh& mesh, double* result, const double* source, int dx, int dy,
+                                   int dz) {
+        static_cast<const Oracle*>(mesh.ctx)->compute_derivative_gg(result, source, dx, dy, dz);
+    }
+    // compute_derivative (UserFunctions.H:60-112): the Green-Gauss cell gradient
+    // of one field -- every face in increasing face order adds 0.5 (s_L + s_R) N
+    // to its first cell and subtracts it from its second; a boundary face adds
+    // s_cell N (zero Neumann) -- then the requested axis / volume where the
+    // volume is positive (0 elsewhere); the identity for order 0.
+    void compute_derivative_gg(double* result, const double* src, int dx, int dy, int dz) const {
+        const int total = dx + dy + dz;
+        const int axis = dx == 1 ? 0 : (dy == 1 ? 1 : 2);
+        for (int c = 0; c < C; ++c) result[c] = 0.0;
+        if (total == 0) {
+            for (int c = 0; c < C; ++c) result[c] = src[c];
+            return;
+        }
+        std::vector<double> grad((size_t)C * DIM, 0.0);
+        for (int f = 0; f < F; ++f) {
+            const int a = fcell[2 * f], b = fcell[2 * f + 1];
+            if (b >= 0) {
+                const double fv = 0.5 * (src[a] + src[b]);
+                for (int d = 0; d < DIM; ++d) {
+                    const double v = fv * fn[2 * f + d];
+                    grad[(size_t)a * DIM + d] += v;
+                    grad[(size_t)b * DIM + d] -= v;
+                }
+            } else {
+                const double fv = src[a];
+                for (int d = 0; d < DIM; ++d) grad[(size_t)a * DIM + d] += fv * fn[2 * f + d];
+            }
+        }
+        if (axis >= DIM) return;
+        for (int c = 0; c < C; ++c)
+            if (vol[c] > 0) result[c] = grad[(size_t)c * DIM + axis] / vol[c];
     }
 
     // ------------------------------------------------------------ gradients

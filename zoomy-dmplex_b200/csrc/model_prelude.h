@@ -45,6 +45,24 @@ ZSME_HD inline T Heaviside(T x, double h0) {
     return x < T(0) ? T(0) : (x > T(0) ? T(1) : T(h0));
 }
 
+// Mesh handle of the plugins' field-level update_aux_variables(Q, Qaux, dt,
+// mesh) overload (reference UserFunctions.H:46-58), which fills derivative
+// aux slots through compute_derivative(result, source, dx, dy, dz, mesh) on
+// whole per-variable fields.  Here the handle carries the routine that
+// serves each such request: the oracle computes the Green-Gauss derivative
+// over its mesh (UserFunctions.H:60-112), the GPU library records which
+// slot takes the derivative of which variable along which axis and runs a
+// cell kernel for it.  Host only; instances on dual or counting scalars do
+// not refresh (the derivative slots feed no step update).
+struct ZoomyMesh {
+    void (*derivative)(const ZoomyMesh& mesh, double* result, const double* source, int dx, int dy, int dz);
+    void* ctx;
+};
+template <typename T>
+inline void compute_derivative(T* result, const T* source, int dx, int dy, int dz, const ZoomyMesh& mesh) {
+    if constexpr (std::is_same<T, double>::value) mesh.derivative(mesh, result, source, dx, dy, dz);
+}
+
 namespace zsme {
 
 // The scalar type T of a plugin instantiation Model<T> (double, or a dual
@@ -87,5 +105,15 @@ struct HasFluxVJP<N, std::void_t<decltype(N::numerical_flux_fluct_vjp(
     (const typename ScalarOf<N>::type*)nullptr, (const typename ScalarOf<N>::type*)nullptr,
     (const typename ScalarOf<N>::type*)nullptr, (const typename ScalarOf<N>::type*)nullptr,
     (const typename ScalarOf<N>::type*)nullptr, (typename ScalarOf<N>::type*)nullptr))>> : std::true_type {};
+
+// Field-level update_aux_variables(T* const* Q, T* const* Qaux, T dt, const
+// ZoomyMesh&) present?  (TransportStep.hpp:33-40: RefreshDerivativeAux runs
+// only for plugins that emit it.)
+template <class M, typename = void>
+struct HasFieldAuxUpdate : std::false_type {};
+template <class M>
+struct HasFieldAuxUpdate<M, std::void_t<decltype(M::update_aux_variables(
+    (typename ScalarOf<M>::type* const*)nullptr, (typename ScalarOf<M>::type* const*)nullptr,
+    (typename ScalarOf<M>::type)0, std::declval<const ZoomyMesh&>()))>> : std::true_type {};
 
 }  // namespace zsme

@@ -84,6 +84,7 @@ class Solver final : public SolverBase {
     int tile_n_ = 0, tile_stride_ = 0, tile_built_ = 0;  // tile_built_: the tile_faces they were built for
     bool ready_ = false;          // init done: mesh on the device
     bool lean_ok_ = false;        // 32-bit element offsets cover every array prep_lean_kernel indexes
+    DerivSpecs deriv_{};          // derivative aux slots refreshed at every state update (n = 0: none)
     int sm_count_ = 148;
     DevBuf<unsigned long long> ratio_;
     // discrete adjoint (allocated by the first zsme_adjoint call)
@@ -309,8 +310,61 @@ class Solver final : public SolverBase {
         ZSME_CUDA(cudaStreamSynchronize(stream_));
         lean_ok_ = 2LL * NQ * F < 0x7fffffffLL && (long long)NQ * C < 0x7fffffffLL &&
                    (long long)pm_.K * 2 * C < 0x7fffffffLL;
+        if (st_.refresh_derivative_aux) {
+            int rc2 = record_derivative_aux();
+            if (rc2) return rc2;
+        }
         ready_ = true;
         return ensure_tiles();
+    }
+
+    // The plugin's field-level update_aux_variables, called once on the host
+    // with one stand-in pointer per field: each compute_derivative request it
+    // makes is recorded as (aux slot, state variable, axis, order) for
+    // derivative_aux_kernel.  Plugins without the overload record nothing.
+    struct DerivRecorder {
+        const double* qf;
+        const double* af;
+        DerivSpecs* ds;
+        bool bad;
+    };
+    static void record_request(const ZoomyMesh& mesh, double* result, const double* source, int dx, int dy, int dz) {
+        auto* r = static_cast<DerivRecorder*>(mesh.ctx);
+        const long k = result - r->af, i = source - r->qf;
+        const int total = dx + dy + dz;
+        if (k < 0 || k >= NA || i < 0 || i >= NQ || total > 1 || r->ds->n >= 8) {
+            r->bad = true;
+            return;
+        }
+        const int e = r->ds->n++;
+        r->ds->aux[e] = (int)k;
+        r->ds->comp[e] = (int)i;
+        r->ds->axis[e] = dx == 1 ? 0 : (dy == 1 ? 1 : 2);
+        r->ds->order[e] = total;
+    }
+    int record_derivative_aux() {
+        deriv_ = DerivSpecs{};
+        if constexpr (HasFieldAuxUpdate<M>::value) {
+            double qf[NQ] = {}, af[NA] = {};
+            double* Qp[NQ];
+            double* Ap[NA];
+            for (int i = 0; i < NQ; ++i) Qp[i] = &qf[i];
+            for (int k = 0; k < NA; ++k) Ap[k] = &af[k];
+            DerivRecorder rec{qf, af, &deriv_, false};
+            const ZoomyMesh mesh{&Solver::record_request, &rec};
+            M::update_aux_variables(Qp, Ap, 0.0, mesh);
+            if (rec.bad)
+                return set_error(ZSME_ERR_MODEL, "the plugin's field-level update_aux_variables asks for a derivative "
+                                                 "this solver does not provide (state variable to aux slot, first "
+                                                 "order, at most 8)");
+        }
+        return ZSME_OK;
+    }
+    // RefreshDerivativeAux of state xs into aux_ (no-op without derivative slots)
+    void launch_derivative_aux(const double* xs, const int* active) {
+        if (!deriv_.n) return;
+        derivative_aux_kernel<M><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, deriv_, 0, pm_.C, xs, aux_.p,
+                                                                             active);
     }
 
     StepDev step_dev(const double* dts) {
@@ -357,6 +411,7 @@ class Solver final : public SolverBase {
         if (inst == 0) ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, 8 * sizeof(int), stream_));
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
+        launch_derivative_aux(x_.p, nullptr);      // PostStep's UpdateState: the derivative aux first
         finalize_range(c0, cn, sd, nullptr, FIN_POST | FIN_WRITE | FIN_DT);
         ZSME_CUDA(cudaGetLastError());
         end_step_kernel<<<1, 32, 0, stream_>>>(step_dev(nullptr), inst, 1, 0, st_.min_dt, nullptr);
@@ -642,6 +697,7 @@ class Solver final : public SolverBase {
     int update_state() override {
         StepDev sd = step_dev(nullptr);
         sd.active = nullptr;
+        launch_derivative_aux(x_.p, nullptr);
         launch_finalize(sd, nullptr, FIN_PRE | FIN_WRITE);
         ZSME_CUDA(cudaGetLastError());
         ZSME_CUDA(cudaStreamSynchronize(stream_));
@@ -701,8 +757,9 @@ class Solver final : public SolverBase {
         // kernels at order 2, and the stage result not needed on its own
         // (MOOD inspects it, the adjoint's tape keeps it)
         const bool fuse_final = lc_.fuse_final && lc_.tile_faces == 0 && st_.reconstruction_order >= 2 && !mood &&
-                                !tape;
+                                !tape && !deriv_.n;
         if (st_.reconstruction_order < 2) {
+            launch_derivative_aux(x_.p, act);       // FormRHS's UpdateState of the stage state
             launch_prep(x_.p, x_.p, act);
             tape_fs(0);
             launch_flux(MODE_EULER, 0.0, t, 0.0, nullptr, nullptr, x_.p, dt, act);
@@ -712,6 +769,7 @@ class Solver final : public SolverBase {
             const int s = st_.ssp_stages;
             for (int i = 0; i < s - 1; ++i) {
                 const double frac = i / (s - 1.);
+                launch_derivative_aux(i == 0 ? x_.p : w_.p, act);   // FormRHS's UpdateState of the stage state
                 // later stages get their clamped copy from gather
                 launch_prep(i == 0 ? x_.p : w_.p, i == 0 ? wl0 : wl_.p, act);
                 tape_fs(i);
@@ -721,6 +779,7 @@ class Solver final : public SolverBase {
                     cudaMemcpyAsync(tape + (size_t)(i + 1) * tape_n, w_.p, tape_n * sizeof(double),
                                     cudaMemcpyDeviceToDevice, stream_);
             }
+            launch_derivative_aux(w_.p, act);
             launch_prep(w_.p, wl_.p, act);
             tape_fs(s - 1);
             launch_flux(MODE_FINAL, 0.0, t, 1.0, w_.p, nullptr, x_.p, dt, act, nullptr, fuse_final);
@@ -741,7 +800,11 @@ class Solver final : public SolverBase {
         }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
         const FinalGather fg{fb_.p, w_.p, sd.dt_step, st_.ssp_stages};
+        // EnforcePhysicalConstraints' UpdateState: the derivative aux of the
+        // transport result before the constraints and the source
+        launch_derivative_aux(x_.p, act);
         launch_finalize(sd, sd.dt_step, flags, fuse_final ? &fg : nullptr);
+        launch_derivative_aux(x_.p, act);           // PostStep's UpdateState
         mark(ZSME_KERNEL_END, true);
         end_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_, 1, 0.0, nullptr);
         mark(ZSME_KERNEL_END, false);
@@ -749,8 +812,10 @@ class Solver final : public SolverBase {
     int launches_per_step() const override {
         const int per_stage = lc_.tile_faces > 0 ? 2 : 3;
         const bool fuse_final = lc_.fuse_final && lc_.tile_faces == 0 && st_.reconstruction_order >= 2 &&
-                                st_.positivity != ZSME_POSITIVITY_MOOD;
-        return 3 - (fuse_final ? 1 : 0) + (st_.reconstruction_order < 2 ? per_stage : per_stage * st_.ssp_stages) +
+                                st_.positivity != ZSME_POSITIVITY_MOOD && !deriv_.n;
+        const int derivs = deriv_.n ? (st_.reconstruction_order < 2 ? 1 : st_.ssp_stages) + 2 : 0;
+        return 3 + derivs - (fuse_final ? 1 : 0) +
+               (st_.reconstruction_order < 2 ? per_stage : per_stage * st_.ssp_stages) +
                (st_.positivity == ZSME_POSITIVITY_MOOD ? 2 : 0) + (st_.source ? 1 : 0);
     }
 

@@ -660,6 +660,73 @@ __global__ void __launch_bounds__(128, MINB) prep_wb_kernel(MeshDev m, Opts o, i
     }
 }
 
+// ------------------------------------------------------- derivative aux
+// The derivative aux slots a plugin fills through its field-level
+// update_aux_variables (one entry per compute_derivative call it makes).
+struct DerivSpecs {
+    int n;
+    int aux[8], comp[8], axis[8], order[8];   // slot, state variable, axis, total derivative order
+};
+
+// TransportStep::RefreshDerivativeAux with compute_derivative
+// (TransportStep.hpp:161-192, UserFunctions.H:60-112) for cells [c0, c0 + cn):
+// per requested slot, the Green-Gauss gradient of state variable comp of x --
+// the cell's faces in increasing original face id (the reference's face loop
+// order), 0.5 (s_support0 + s_support1) N added when the cell is support[0]
+// and subtracted otherwise, s_cell N on every exterior face (zero Neumann) --
+// along `axis`, / volume where positive (else 0); order 0 copies the variable.
+template <class M>
+__global__ void __launch_bounds__(128) derivative_aux_kernel(MeshDev m, DerivSpecs ds, int c0, int cn,
+                                                             const double* __restrict__ x,
+                                                             double* __restrict__ aux,
+                                                             const int* __restrict__ active) {
+    constexpr int DIM = M::dimension;
+    const int C = m.C, F = m.F;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    if (active && !active[cell_instance(m, c)]) return;
+    const int ord = m.order[c];
+    for (int e = 0; e < ds.n; ++e) {
+        const double* s = x + (size_t)ds.comp[e] * C;
+        double result = 0.0;
+        if (ds.order[e] == 0) {
+            result = s[c];
+        } else {
+            double g[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) g[d] = 0.0;
+            for (int j = 0; j < m.K; ++j) {
+                const int k = (ord >> (2 * j)) & 3;
+                const int f = m.slot_face[k * C + c];
+                if (f < 0) continue;
+                const int n = m.slot_nbr[k * C + c];
+                const double Nf[2] = {m.fnr[f], m.fnr[F + f]};
+                if (n >= 0) {
+                    const bool isL = meta_isL(m.slot_meta[k * C + c]);
+                    const double fv = 0.5 * (isL ? (s[c] + s[n]) : (s[n] + s[c]));
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        const double v = fv * Nf[d];
+                        if (isL) g[d] += v;
+                        else g[d] -= v;
+                    }
+                } else {
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) g[d] += s[c] * Nf[d];
+                }
+            }
+            const double v = m.vol[c];
+            if (ds.axis[e] < DIM && v > 0) {
+#pragma unroll
+                for (int d = 0; d < DIM; ++d)
+                    if (d == ds.axis[e]) result = g[d] / v;
+            }
+        }
+        aux[(size_t)ds.aux[e] * C + c] = result;
+    }
+}
+
 // ------------------------------------------------------------------ MOOD
 // Local MOOD (MUSCLSolver.hpp:150-170, 197-229; TransportStep.hpp:363-381,
 // 412-418): a cell whose depth after the transport step is below -1e-10 is

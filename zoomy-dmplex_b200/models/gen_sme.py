@@ -504,6 +504,31 @@ def gen_model(S):
     fn("update_aux_variables", qa3 + ["const T time", "const T* X"], ua)
     Jua = [sp.diff(ua[k], Q[j]) if k == S.ihinv else sp.Integer(0) for k in range(na) for j in range(nq)]
     fn("update_aux_variables_jacobian_wrt_variables", qa3 + ["const T time", "const T* X"], Jua)
+    # field-level overload filling the derivative aux slots ("d<var>d<axis>")
+    # from whole fields through the solver's compute_derivative (the interface
+    # of the reference's generated header, Model.H:250-262)
+    deriv = []
+    for k, nm in enumerate(S.aux_names):
+        if nm.startswith("d") and len(nm) > 3 and nm[-2] == "d" and nm[-1] in "xyz":
+            var, axis = nm[1:-2], nm[-1]
+            qi = {"b": 0, "h": 1}.get(var)
+            if qi is None and var.startswith("q"):
+                qi = S.im(0, int(var[1:]))
+            deriv.append((k, nm, qi, "xyz".index(axis)))
+    if deriv:
+        w("    static inline void update_aux_variables(")
+        w("        T* const* Q,")
+        w("        T* const* Qaux,")
+        w("        const T dt,")
+        w("        const ZoomyMesh& mesh)")
+        w("    {")
+        for k, nm, qi, ax in deriv:
+            order = [0, 0, 0]
+            order[ax] = 1
+            w("    // Qaux[%d] (%s) = D^(%s) Q[%d]" % (k, nm, ",".join(str(o) for o in order[:S.dim]) + ("," if S.dim == 1 else ""), qi))
+            w("    compute_derivative(Qaux[%d], Q[%d], %d, %d, %d, mesh);" % (k, qi, order[0], order[1], order[2]))
+        w("    }")
+        w("")
     ic = [sp.Integer(0)] * nq
     ic[0] = sp.Integer(1)
     fn("initial_condition", ["const T* X", "const T* p"], ic)

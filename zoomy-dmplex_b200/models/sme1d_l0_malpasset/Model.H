@@ -230,6 +230,20 @@ struct Model {
     return res;
     }
 
+    static inline void update_aux_variables(
+        T* const* Q,
+        T* const* Qaux,
+        const T dt,
+        const ZoomyMesh& mesh)
+    {
+    // Qaux[0] (dq0dx) = D^(1,) Q[2]
+    compute_derivative(Qaux[0], Q[2], 1, 0, 0, mesh);
+    // Qaux[1] (dhdx) = D^(1,) Q[1]
+    compute_derivative(Qaux[1], Q[1], 1, 0, 0, mesh);
+    // Qaux[2] (dbdx) = D^(1,) Q[0]
+    compute_derivative(Qaux[2], Q[0], 1, 0, 0, mesh);
+    }
+
     PORTABLE_FN static inline SimpleArray<T, 3> initial_condition(
         const T* X,
         const T* p)

@@ -34,7 +34,8 @@ class ZsmeSettings(ct.Structure):
         ("cfl", ct.c_double), ("t_end", ct.c_double), ("min_dt", ct.c_double),
         ("reconstruction_order", ct.c_int32), ("limiter", ct.c_int32), ("gradient", ct.c_int32),
         ("ssp_stages", ct.c_int32), ("source", ct.c_int32), ("block_size", ct.c_int32),
-        ("positivity", ct.c_int32), ("reserved", ct.c_int32 * 5), ("wet_dry_eps", ct.c_double),
+        ("positivity", ct.c_int32), ("refresh_derivative_aux", ct.c_int32), ("reserved", ct.c_int32 * 4),
+        ("wet_dry_eps", ct.c_double),
     ]
 
 

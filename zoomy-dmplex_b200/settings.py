@@ -18,6 +18,10 @@ How the reference interprets the strings, and so how they map here:
   (``MUSCLSolver.hpp:43``, ``Reconstruction.hpp:170-175``);
 * ``time_integration``: ``"splitting"`` (explicit transport + implicit source)
   is the only strategy of this path; ``"imex"``/``"implicit"`` are rejected;
+* ``refresh_derivative_aux`` (reference default true): before each state
+  update the plugin's derivative aux slots are refilled with Green-Gauss
+  derivatives of the state (``TransportStep.hpp:161-202``); plugins without
+  the field-level ``update_aux_variables`` overload have nothing to refresh;
 * ``positivity``: ``"none"`` (limited linear reconstruction), ``"zhang_shu"``
   or ``"mood"`` (the eta-well-balanced reconstruction with the Zhang-Shu
   theta, or with the a-posteriori first-order override of cells that end
@@ -45,6 +49,7 @@ class SolverSettings:
     ssp_stages: int = 5
     gradient: str = "green_gauss"
     block_size: int = 0
+    refresh_derivative_aux: bool = True
 
     def to_struct(self) -> native.ZsmeSettings:
         if self.time_integration != "splitting":
@@ -67,6 +72,7 @@ class SolverSettings:
         s.block_size = int(self.block_size)
         s.positivity = native.POSITIVITY[self.positivity]
         s.wet_dry_eps = float(self.wet_dry_eps)
+        s.refresh_derivative_aux = 1 if self.refresh_derivative_aux else 0
         return s
 
 
