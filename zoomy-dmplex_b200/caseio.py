@@ -26,9 +26,10 @@ are "Q" (n_dof_q components) and "Aux" (n_dof_qaux), base64-encoded.
 
 Initial states (``load_state``, ``overlay_state``).  The reference loads the
 dataset "state" of an HDF5 file, whole or only the components listed in
-``initial_condition_mask`` (``IOManager.hpp:122-192``).  This image has no
-HDF5 library, so the same array is read from ``.npy`` / ``.npz`` (key
-"state"), in the mesh's cell order.
+``initial_condition_mask`` (``IOManager.hpp:122-192``), in the mesh's
+natural cell order as its ``generate_ic.py`` writes it.  HDF5 files are read
+by the library-free reader of ``hdf5.py`` (contiguous datasets, the layout
+that script writes); ``.npy`` / ``.npz`` (key "state") hold the same array.
 """
 from __future__ import annotations
 
@@ -335,17 +336,22 @@ def run_with_snapshots(solver, mesh: Mesh, writer: SnapshotWriter, t_end: float,
 
 
 # ------------------------------------------------------------ initial states
-def load_state(path: str) -> np.ndarray:
-    """The "state" array of an initial-condition file: .npy, or .npz with key
-    "state" ([C, n_dof_q] or flat, natural cell order).  HDF5 files need an
-    HDF5 library, which this image lacks."""
+def load_state(path: str, n_cells: Optional[int] = None, n_dof_q: Optional[int] = None) -> np.ndarray:
+    """The "state" array of an initial-condition file (natural cell order):
+    HDF5 (.h5 / .hdf5: dataset "state", flat cell-major float64 with the
+    num_components attribute, as the reference's generate_ic.py writes it;
+    returned as [C, n_components]), .npy, or .npz with key "state" ([C,
+    n_dof_q] or flat).  n_cells / n_dof_q check or supply the shape."""
+    if path.endswith((".h5", ".hdf5")):
+        from . import hdf5
+
+        return hdf5.read_state(path, n_cells=n_cells, n_dof_q=n_dof_q)
     if path.endswith(".npy"):
         return np.load(path)
     if path.endswith(".npz"):
         with np.load(path) as z:
             return z["state"]
-    raise ValueError("%s: initial states are read from .npy / .npz ('state'); HDF5 needs h5py, "
-                     "absent in this image" % path)
+    raise ValueError("%s: initial states are read from .h5 / .hdf5 ('state'), .npy or .npz ('state')" % path)
 
 
 def overlay_state(q: np.ndarray, loaded: np.ndarray, mask: Sequence[int] = ()) -> np.ndarray:
