@@ -196,6 +196,15 @@ int zsme_compute_dt(zsme_handle* h, double* dt);
 int zsme_step(zsme_handle* h, int32_t nsteps);
 /* Same, but with the dt of every step imposed by the caller (dts[nsteps]). */
 int zsme_step_dt(zsme_handle* h, int32_t nsteps, const double* dts);
+/* Same, with the dts in device memory (d_dts[nsteps]), read in stream order:
+ * a distributed caller can reduce the parts' CFL dts on the device (an
+ * all-reduce with MIN, the reference's MPI_Allreduce of VirtualSolver.hpp:349)
+ * and step without synchronising the host.  Single-instance handles. */
+int zsme_step_dt_device(zsme_handle* h, int32_t nsteps, const double* d_dts);
+/* The time and the CFL dt of the next step copied to device memory (d_t,
+ * d_dt; either may be NULL) in stream order, without synchronising the host.
+ * Single-instance handles. */
+int zsme_get_time_device(zsme_handle* h, double* d_t, double* d_dt);
 /* Wait for the handle's stream; returns ZSME_ERR_STATE if the last step left
  * non-finite values or negative depth (counts in zsme_diag). */
 int zsme_sync(zsme_handle* h);

@@ -140,3 +140,80 @@ def test_gloo_halo_exchange():
         p.join(timeout=60)
     assert [r[1] for r in res] == [True, True]
     assert [r[2] for r in res] == [0.1, 0.1]
+
+
+class OracleBackend:
+    """PartRunner's backend over an oracle part (CPU tensors): what
+    DevicePart does on the GPU -- the part's CFL dt, a step at an imposed dt,
+    owned cells packed for a neighbour, received values unpacked into the
+    halo -- on the CPU restatement."""
+
+    def __init__(self, part, oracle, nq):
+        self.part, self.o, self.nq = part, oracle, nq
+
+    def local_dt(self):
+        import torch
+
+        return torch.tensor([self.o.time()[1]], dtype=torch.float64)
+
+    def step(self, dt):
+        self.o.step(1, dts=[float(dt.item())])
+
+    def pack(self, dst):
+        import torch
+
+        return torch.from_numpy(np.ascontiguousarray(self.o.get_state()[self.part.send[dst]]))
+
+    def recv_buffer(self, src):
+        import torch
+
+        return torch.empty((len(self.part.recv[src]), self.nq), dtype=torch.float64)
+
+    def unpack(self, src, buf):
+        q = self.o.get_state()
+        q[self.part.recv[src]] = buf.numpy()
+        self.o.set_state(q, self.o.time()[0])
+
+
+def _runner_rank(rank, world, port, q, steps):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        c = cases.level2(24)
+        parts = P.build_parts(c.mesh, world, P.halo_layers(2, c.settings.ssp_stages))
+        pt = parts[rank]
+        o = O.Oracle(c.model, pt.mesh.as_abi_arrays(), c.settings.to_struct(), params(c))
+        o.set_state(c.q0[pt.cells])
+        P.PartRunner(pt, OracleBackend(pt, o, c.q0.shape[1]), P.TorchComm(dist)).step(steps)
+        q.put((rank, pt.cells[pt.owned], o.get_state()[pt.owned], o.time()[0]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_part_runner_equals_undivided():
+    """PartRunner over torch.distributed (two gloo ranks, one oracle part
+    each): the global dt by all-reduce MIN, the step, the halo exchange by
+    batched point-to-point messages; 12 steps end bit for bit on the
+    undivided oracle run."""
+    steps = 12
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_runner_rank, args=(r, 2, port, q, steps)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = [q.get(timeout=300) for _ in ps]
+    for p in ps:
+        p.join(timeout=60)
+    c = cases.level2(24)
+    o = O.Oracle(c.model, c.mesh.as_abi_arrays(), c.settings.to_struct(), params(c))
+    o.set_state(c.q0)
+    o.step(steps)
+    full = o.get_state()
+    got = np.full_like(full, np.nan)
+    for _, cells, vals, t in res:
+        got[cells] = vals
+        assert t == o.time()[0]
+    assert np.array_equal(got, full)

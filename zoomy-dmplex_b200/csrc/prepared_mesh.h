@@ -101,6 +101,10 @@ class SolverBase {
     virtual int source(double dt) = 0;
     virtual int compute_dt(int inst, double* dt) = 0;
     virtual int step(int nsteps, const double* dts) = 0;
+    // imposed dts read from device memory, in stream order (no host synchronisation)
+    virtual int step_device_dts(int nsteps, const double* d_dts) = 0;
+    // time and CFL dt of instance 0 copied to device memory, in stream order
+    virtual int get_time_device(double* d_t, double* d_dt) = 0;
     virtual int sync(int inst, zsme_diag* d) = 0;
     virtual void* stream() = 0;
     virtual int launches_per_step() const = 0;

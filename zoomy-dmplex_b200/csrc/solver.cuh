@@ -859,6 +859,27 @@ class Solver final : public SolverBase {
         return ZSME_OK;
     }
 
+    int step_device_dts(int nsteps, const double* d_dts) override {
+        if (nsteps <= 0) return ZSME_OK;
+        if (n_inst_ != 1) return set_error(ZSME_ERR_ARG, "imposed dts need a single-instance handle");
+        ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 4 * sizeof(int), stream_));
+        ZSME_CUDA(cudaMemsetAsync(iscal_.p + 7, 0, sizeof(int), stream_));
+        ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));   // index into d_dts
+        const bool unclamped = !x_clamped_ && st_.reconstruction_order >= 2;
+        x_clamped_ = true;
+        if (unclamped)
+            clamp_kernel<M><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, 0, pm_.C, x_.p, aux_.p, params_.p,
+                                                                        wl_.p);
+        for (int i = 0; i < nsteps; ++i) enqueue_step(d_dts, (unclamped && i == 0) ? wl_.p : x_.p);
+        ZSME_CUDA(cudaGetLastError());
+        return collect_profile();
+    }
+    int get_time_device(double* d_t, double* d_dt) override {
+        if (d_t) ZSME_CUDA(cudaMemcpyAsync(d_t, t_.p, sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        if (d_dt) ZSME_CUDA(cudaMemcpyAsync(d_dt, dt_cfl_.p, sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        return ZSME_OK;
+    }
+
     // ------------------------------------------------------ discrete adjoint
     // R'(W)^T (factor * dt * src) + c_src * src -> dst for the stage state W with
     // face states fs.  dt = *dtp and the stage time *tp + frac * dt are device

@@ -247,6 +247,15 @@ int zsme_step_dt(zsme_handle* h, int32_t n, const double* dts) {
         if (!(dts[i] >= 0)) return set_error(ZSME_ERR_ARG, "dts must be >= 0");
     return h->s->step(n, dts);
 }
+int zsme_step_dt_device(zsme_handle* h, int32_t n, const double* d_dts) {
+    CHECK_SINGLE(h);
+    if (n < 0 || (n > 0 && !d_dts)) return set_error(ZSME_ERR_ARG, "bad dts");
+    return h->s->step_device_dts(n, d_dts);
+}
+int zsme_get_time_device(zsme_handle* h, double* d_t, double* d_dt) {
+    CHECK_SINGLE(h);
+    return h->s->get_time_device(d_t, d_dt);
+}
 int zsme_get_diag(zsme_handle* h, zsme_diag* d) {
     CHECK_H(h);
     if (!d) return set_error(ZSME_ERR_ARG, "null output");

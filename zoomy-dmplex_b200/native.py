@@ -105,6 +105,8 @@ def load():
     lib.zsme_compute_dt.argtypes = [vp, P]
     lib.zsme_step.argtypes = [vp, ct.c_int32]
     lib.zsme_step_dt.argtypes = [vp, ct.c_int32, P]
+    lib.zsme_step_dt_device.argtypes = [vp, ct.c_int32, vp]
+    lib.zsme_get_time_device.argtypes = [vp, vp, vp]
     lib.zsme_sync.argtypes = [vp]
     lib.zsme_get_diag.argtypes = [vp, ct.POINTER(ZsmeDiag)]
     lib.zsme_get_time.argtypes = [vp, P, P]

@@ -28,6 +28,19 @@ by an unmodified solver handle:
 ``PartitionedSolver`` runs all parts in one process (one GPU, host-side
 exchange); ``exchange`` is the same schedule over ``torch.distributed``
 point-to-point messages for one part per rank.
+
+``PartRunner`` is the device-resident form: a part's step loop -- the
+global dt as an all-reduce with MIN of the parts' CFL dts (the reference's
+``MPI_Allreduce``, ``VirtualSolver.hpp:349``), the step at that dt, the halo
+refresh -- as tensor operations in stream order.  With ``DevicePart`` (a
+solver handle; halo cells packed and unpacked on the GPU by
+``zsme_get_cells`` / ``zsme_set_cells`` on device buffers, the dt read and
+imposed through ``zsme_get_time_device`` / ``zsme_step_dt_device``) and
+``TorchComm`` over NCCL, nothing in a step synchronises the host: the
+collectives are issued on the handle's stream, NCCL sends each packed halo
+straight into the receiver's own receive buffer, and the receiver unpacks
+it into its ghost cells.  ``LocalComm`` performs the same schedule for
+several parts held by one process.
 """
 from __future__ import annotations
 
@@ -233,3 +246,172 @@ def global_dt(local_dt: float, dist, device=None) -> float:
     t = torch.tensor([local_dt], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MIN)
     return float(t.item())
+
+
+# --------------------------------------------------------------- device form
+class TorchComm:
+    """The collectives of PartRunner over torch.distributed (NCCL for GPU
+    tensors, gloo for CPU tensors).  `stream`: the torch stream the tensors
+    are ordered on (the solver handle's), made current while the
+    collectives are issued, so NCCL's work is ordered against the handle's
+    kernels on the device."""
+
+    def __init__(self, dist, stream=None):
+        self.dist = dist
+        self.stream = stream
+
+    def _ctx(self):
+        import contextlib
+
+        import torch
+
+        return torch.cuda.stream(self.stream) if self.stream is not None else contextlib.nullcontext()
+
+    def min_(self, t):
+        with self._ctx():
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN)
+
+    def exchange(self, sends, recvs):
+        """Post every send and receive, then wait for all: no pair of ranks
+        depends on the other's order."""
+        with self._ctx():
+            ops = [self.dist.P2POp(self.dist.isend, buf, dst) for dst, buf in sorted(sends.items())]
+            ops += [self.dist.P2POp(self.dist.irecv, buf, src) for src, buf in sorted(recvs.items())]
+            if ops:
+                for r in self.dist.batch_isend_irecv(ops):
+                    r.wait()
+
+
+class PartRunner:
+    """One part's step loop with the halo refresh.  backend: local_dt()
+    -> 1-element tensor of the part's CFL dt; step(dt) at a 1-element tensor
+    dt; pack(dst) -> [n, nq] tensor of the owned cells `dst` needs;
+    unpack(src, values) into the halo cells `src` fills; recv_buffer(src)
+    -> the tensor a message from src lands in.  comm: min_(tensor) in place
+    over all parts, exchange(sends, recvs)."""
+
+    def __init__(self, part: Part, backend, comm):
+        self.part, self.backend, self.comm = part, backend, comm
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            dt = self.backend.local_dt()
+            self.comm.min_(dt)
+            self.backend.step(dt)
+            sends = {dst: self.backend.pack(dst) for dst in self.part.send}
+            recvs = {src: self.backend.recv_buffer(src) for src in self.part.recv}
+            self.comm.exchange(sends, recvs)
+            for src, buf in recvs.items():
+                self.backend.unpack(src, buf)
+
+
+class DevicePart:
+    """A part on a GPU: its solver handle and device-resident halo buffers.
+    Every call is ordered on the handle's stream (``stream``)."""
+
+    def __init__(self, part: Part, model, settings, params, device: int = 0, launch=None):
+        import torch
+
+        from .solver import Solver, set_launch
+
+        self.part = part
+        self.solver = Solver(model, part.mesh, settings, params, device=device)
+        if launch:
+            set_launch(self.solver.h, launch)
+        self.lib = self.solver.lib
+        self.nq = self.solver.nq
+        self.dev = torch.device("cuda", device)
+        self.stream = torch.cuda.ExternalStream(self.solver.stream, device=self.dev)
+        i32 = dict(dtype=torch.int32, device=self.dev)
+        f64 = dict(dtype=torch.float64, device=self.dev)
+        # caller (local mesh) ids of the cells each message carries
+        self.send_ids = {d: torch.as_tensor(c, **i32) for d, c in part.send.items()}
+        self.recv_ids = {s: torch.as_tensor(c, **i32) for s, c in part.recv.items()}
+        self.send_buf = {d: torch.empty((len(c), self.nq), **f64) for d, c in part.send.items()}
+        self.recv_buf = {s: torch.empty((len(c), self.nq), **f64) for s, c in part.recv.items()}
+        self.t_dev = torch.zeros(1, **f64)
+        self.dt_dev = torch.zeros(1, **f64)
+
+    def set_state(self, q_global: np.ndarray, t: float = 0.0):
+        self.solver.set_state(q_global[self.part.cells], t)
+
+    def local_dt(self):
+        from . import native
+
+        native.check(self.lib.zsme_get_time_device(self.solver.h, None, self.dt_dev.data_ptr()))
+        return self.dt_dev
+
+    def step(self, dt):
+        from . import native
+
+        native.check(self.lib.zsme_step_dt_device(self.solver.h, 1, dt.data_ptr()))
+
+    def pack(self, dst):
+        from . import native
+
+        ids, buf = self.send_ids[dst], self.send_buf[dst]
+        native.check(self.lib.zsme_get_cells(self.solver.h, len(ids), ids.data_ptr(), buf.data_ptr(), 1))
+        return buf
+
+    def recv_buffer(self, src):
+        return self.recv_buf[src]
+
+    def unpack(self, src, buf):
+        from . import native
+
+        ids = self.recv_ids[src]
+        native.check(self.lib.zsme_set_cells(self.solver.h, len(ids), ids.data_ptr(), buf.data_ptr(), 1))
+
+    def owned_state(self):
+        """(global ids, values) of the part's owned cells."""
+        q = self.solver.get_state()
+        return self.part.cells[self.part.owned], q[self.part.owned]
+
+
+class LocalComm:
+    """PartRunner's collectives for several parts held by one process: the
+    minimum over the parts' dt tensors, and each packed halo copied into the
+    receiving part's buffer.  Parts on one device with their own streams are
+    ordered by synchronising the device between the phases (a test and
+    single-process harness; across ranks TorchComm keeps everything on the
+    device)."""
+
+    def __init__(self):
+        self.runners: List[PartRunner] = []
+        self._dts = {}
+        self._sends = {}
+
+    @staticmethod
+    def _sync():
+        try:
+            import torch
+
+            if torch.cuda.is_available():
+                torch.cuda.synchronize()
+        except ImportError:
+            pass
+
+    def step(self, n: int = 1):
+        """Advance every registered part n steps (the per-part PartRunner
+        loop, phase by phase across the parts)."""
+        for _ in range(n):
+            dts = [r.backend.local_dt() for r in self.runners]
+            self._sync()
+            m = dts[0].clone()
+            for d in dts[1:]:
+                m = m.minimum(d.to(m.device))
+            for d in dts:
+                d.copy_(m.to(d.device))
+            self._sync()
+            for r in self.runners:
+                r.backend.step(dts[self.runners.index(r)])
+            packed = {(r.part.rank, dst): r.backend.pack(dst) for r in self.runners for dst in r.part.send}
+            self._sync()
+            by_rank = {r.part.rank: r for r in self.runners}
+            for (src, dst), buf in packed.items():
+                by_rank[dst].backend.recv_buffer(src).copy_(buf)
+            self._sync()
+            for r in self.runners:
+                for src in r.part.recv:
+                    r.backend.unpack(src, r.backend.recv_buffer(src))
+            self._sync()
