@@ -143,8 +143,14 @@ def test_initial_state_overlay(tmp_path):
         assert np.array_equal(caseio.overlay_state(q, loaded), f)
         o = caseio.overlay_state(q, loaded, [1, 3, 9])
         assert np.array_equal(o[:, [0, 2]], q[:, [0, 2]]) and np.array_equal(o[:, [1, 3]], f[:, [1, 3]])
-    with pytest.raises(ValueError, match="HDF5"):
-        caseio.load_state(str(tmp_path / "s.h5"))
+    # HDF5 in the reference's layout (hdf5.write_state, as its generate_ic.py writes it)
+    from zoomy_dmplex_b200 import hdf5
+
+    hdf5.write_state(str(tmp_path / "s.h5"), f)
+    loaded = caseio.load_state(str(tmp_path / "s.h5"))
+    assert np.array_equal(caseio.overlay_state(q, loaded, [1, 3])[:, [1, 3]], f[:, [1, 3]])
+    with pytest.raises(ValueError, match="h5"):
+        caseio.load_state(str(tmp_path / "s.txt"))
 
 
 @pytest.mark.skipif(not os.environ.get("ZSME_GMSH_DIR"), reason="ZSME_GMSH_DIR (a directory of gmsh cases) unset")
