@@ -35,6 +35,20 @@
 #pragma once
 #include "dual.h"
 
+// Register caps of the reverse kernels as resident 128-thread blocks per SM
+// (1 = uncapped): compile-time constants, chosen by measurement on the
+// adjoint workload (SME level 1, 79k cells: every reverse kernel is one or a
+// few waves, so resident blocks decide its time).
+#ifndef ZSME_ADJ_FACE_MINB
+#define ZSME_ADJ_FACE_MINB 1
+#endif
+#ifndef ZSME_ADJ_CELL_MINB
+#define ZSME_ADJ_CELL_MINB 1
+#endif
+#ifndef ZSME_ADJ_FIN_MINB
+#define ZSME_ADJ_FIN_MINB 1
+#endif
+
 namespace zsme {
 
 // li = J^T lo, J the Jacobian of update_variables at (q, a) (identity when the
@@ -250,7 +264,7 @@ __device__ __noinline__ void ghost_state(const double* qL, const double* aLc, co
 // nothing), the ghost state's dependence on the inner one pulled back by
 // ghost_state.
 template <template <typename> class MT, template <typename> class NT>
-__global__ void __launch_bounds__(128) adj_face_vjp_kernel(MeshDev m, const double* __restrict__ fs,
+__global__ void __launch_bounds__(128, ZSME_ADJ_FACE_MINB) adj_face_vjp_kernel(MeshDev m, const double* __restrict__ fs,
                                                            const double* __restrict__ aux,
                                                            const double* __restrict__ params, const double* tp,
                                                            double frac, const double* dtp, double factor,
@@ -323,7 +337,7 @@ __global__ void __launch_bounds__(128) adj_face_vjp_kernel(MeshDev m, const doub
 // from its own face states; out_w / out_wl [K][NQ][C]: what the cell owes
 // the neighbour of each slot (raw: gradient stencil; clamped: limiter bound).
 template <template <typename> class MT, int KM>
-__global__ void __launch_bounds__(128) adj_cell_kernel(MeshDev m, Opts o, const double* __restrict__ w,
+__global__ void __launch_bounds__(128, ZSME_ADJ_CELL_MINB) adj_cell_kernel(MeshDev m, Opts o, const double* __restrict__ w,
                                                        const double* __restrict__ wl,
                                                        const double* __restrict__ params,
                                                        const double* __restrict__ gfs, double* __restrict__ own_w,
@@ -748,7 +762,7 @@ __device__ __forceinline__ void adj_finalize_cell(const MeshDev& m, int c, const
 }
 
 template <template <typename> class MT>
-__global__ void __launch_bounds__(128) adj_finalize_kernel(MeshDev m, const double* __restrict__ xp,
+__global__ void __launch_bounds__(128, ZSME_ADJ_FIN_MINB) adj_finalize_kernel(MeshDev m, const double* __restrict__ xp,
                                                            const double* __restrict__ aux,
                                                            const double* __restrict__ params, const double* dtp,
                                                            int flags, const double* __restrict__ lam_out,

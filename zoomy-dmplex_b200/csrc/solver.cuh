@@ -73,6 +73,7 @@ class Solver final : public SolverBase {
     DevBuf<double> slot_dx_, slot_w_, vol_, rc_, fn_, farea_, fc_, fnr_;
     // state
     DevBuf<double> x_, w_, wl_, aux_, fs_, fb_, tmp_a_, tmp_b_, params_, dts_;
+    double* fs_cur_ = nullptr;  // face states the prep and face kernels use: fs_, or a tape slot in a replay
     DevBuf<double> xs_;  // MOOD: the state at the start of the step
     DevBuf<int> mood_list_;  // MOOD: the troubled cells of the step (count in iscal_[6])
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
@@ -283,6 +284,7 @@ class Solver final : public SolverBase {
             ZSME_CUDA(mood_list_.alloc((size_t)C));
         }
         ZSME_CUDA(fs_.alloc((size_t)2 * NQ * F));
+        fs_cur_ = fs_.p;
         ZSME_CUDA(fb_.alloc((size_t)3 * NQ * F));
         // staging for state (NQ per cell) and aux (NA per cell) conversions
         ZSME_CUDA(tmp_a_.alloc((size_t)std::max(NQ, NA) * C));
@@ -550,10 +552,10 @@ class Solver final : public SolverBase {
     case OCC:                                                                                                   \
         if (pm_.K == 3)                                                                                         \
             prep_wb_kernel<M, 3, OCC><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps, \
-                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active); \
+                                                                    0, pm_.C, w, wl, params_.p, fs_cur_, active); \
         else                                                                                                    \
             prep_wb_kernel<M, 4, OCC><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, st_.positivity, st_.wet_dry_eps, \
-                                                                    0, pm_.C, w, wl, params_.p, fs_.p, active); \
+                                                                    0, pm_.C, w, wl, params_.p, fs_cur_, active); \
         break;
                 ZSME_PREPWB(2) ZSME_PREPWB(3) ZSME_PREPWB(4) ZSME_PREPWB(6) ZSME_PREPWB(8)
                 default: ZSME_PREPWB(1)
@@ -568,10 +570,10 @@ class Solver final : public SolverBase {
     case OCC:                                                                                                   \
         if (pm_.K == 3)                                                                                         \
             prep_lean_kernel<M, OCC, 3><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, params_.p,   \
-                                                                      fs_.p, active);                           \
+                                                                      fs_cur_, active);                         \
         else                                                                                                    \
             prep_lean_kernel<M, OCC, 4><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, params_.p,   \
-                                                                      fs_.p, active);                           \
+                                                                      fs_cur_, active);                         \
         break;
                 ZSME_PREPL(2) ZSME_PREPL(3) ZSME_PREPL(4) ZSME_PREPL(6) ZSME_PREPL(8)
                 default: ZSME_PREPL(1)
@@ -585,10 +587,10 @@ class Solver final : public SolverBase {
     case OCC:                                                                                                   \
         if (pm_.K == 3)                                                                                         \
             prep_kernel<M, OCC, 3><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, aux_.p, params_.p,\
-                                                                 fs_.p, active);                                \
+                                                                 fs_cur_, active);                              \
         else                                                                                                    \
             prep_kernel<M, OCC, 4><<<gb, lc_.prep, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, aux_.p, params_.p,\
-                                                                 fs_.p, active);                                \
+                                                                 fs_cur_, active);                              \
         break;
             ZSME_PREP(2) ZSME_PREP(3) ZSME_PREP(4) ZSME_PREP(6) ZSME_PREP(8)
             default: ZSME_PREP(1)
@@ -609,7 +611,7 @@ class Solver final : public SolverBase {
             switch (lc_.face_occ) {
 #define ZSME_TILE(OCC)                                                                                        \
     case OCC:                                                                                                 \
-        flux_tile_kernel<M, N, OCC><<<tile_n_, lc_.face, smem, stream_>>>(md_, opts_, tl, fs_.p, aux_.p,        \
+        flux_tile_kernel<M, N, OCC><<<tile_n_, lc_.face, smem, stream_>>>(md_, opts_, tl, fs_cur_, aux_.p,      \
                                                                        params_.p, t_host, t_dev, frac, dt,     \
                                                                        active, mode, x_in, x_out, base,        \
                                                                        xl_out);                                \
@@ -626,7 +628,7 @@ class Solver final : public SolverBase {
         switch (lc_.face_occ) {
 #define ZSME_FACE(OCC)                                                                                          \
     case OCC:                                                                                                   \
-        face_kernel<M, N, OCC><<<gf, lc_.face, 0, stream_>>>(md_, 0, pm_.F, fs_.p, aux_.p, params_.p, t_host,    \
+        face_kernel<M, N, OCC><<<gf, lc_.face, 0, stream_>>>(md_, 0, pm_.F, fs_cur_, aux_.p, params_.p, t_host,  \
                                                              t_dev, frac, dt, fb_.p, active);                   \
         break;
             ZSME_FACE(2) ZSME_FACE(3) ZSME_FACE(4)
@@ -739,10 +741,11 @@ class Solver final : public SolverBase {
         const size_t tape_n = (size_t)NQ * pm_.C;
         const size_t fs_n = (size_t)2 * NQ * pm_.F;
         const int ns = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
-        auto tape_fs = [&](int i) {
-            if (tape)
-                cudaMemcpyAsync(tape + (size_t)(ns + 1) * tape_n + (size_t)i * fs_n, fs_.p, fs_n * sizeof(double),
-                                cudaMemcpyDeviceToDevice, stream_);
+        // with a tape (adjoint replay) each stage's face states and stage state are
+        // produced in their tape slots directly: slot k < s holds W_k, slot s the
+        // stage result X', then one slot of face states per stage
+        auto stage_fs = [&](int i) {
+            fs_cur_ = tape ? tape + (size_t)(ns + 1) * tape_n + (size_t)i * fs_n : fs_.p;
         };
         StepDev sd = step_dev(dts);
         const double* t = sd.t;
@@ -758,10 +761,11 @@ class Solver final : public SolverBase {
         // (MOOD inspects it, the adjoint's tape keeps it)
         const bool fuse_final = lc_.fuse_final && lc_.tile_faces == 0 && st_.reconstruction_order >= 2 && !mood &&
                                 !tape && !deriv_.n;
+        double* w_last = x_.p;   // the last stage's state
         if (st_.reconstruction_order < 2) {
             launch_derivative_aux(x_.p, act);       // FormRHS's UpdateState of the stage state
+            stage_fs(0);
             launch_prep(x_.p, x_.p, act);
-            tape_fs(0);
             launch_flux(MODE_EULER, 0.0, t, 0.0, nullptr, nullptr, x_.p, dt, act);
             if (tape)
                 cudaMemcpyAsync(tape + tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
@@ -769,24 +773,24 @@ class Solver final : public SolverBase {
             const int s = st_.ssp_stages;
             for (int i = 0; i < s - 1; ++i) {
                 const double frac = i / (s - 1.);
-                launch_derivative_aux(i == 0 ? x_.p : w_.p, act);   // FormRHS's UpdateState of the stage state
+                double* w_in = i == 0 ? x_.p : w_last;
+                double* w_out = tape ? tape + (size_t)(i + 1) * tape_n : w_.p;
+                launch_derivative_aux(w_in, act);   // FormRHS's UpdateState of the stage state
+                stage_fs(i);
                 // later stages get their clamped copy from gather
-                launch_prep(i == 0 ? x_.p : w_.p, i == 0 ? wl0 : wl_.p, act);
-                tape_fs(i);
-                launch_flux(i == 0 ? MODE_FIRST : MODE_MID, 0.0, t, frac, i == 0 ? x_.p : w_.p, w_.p, nullptr, dt,
-                            act, wl_.p);
-                if (tape)
-                    cudaMemcpyAsync(tape + (size_t)(i + 1) * tape_n, w_.p, tape_n * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, stream_);
+                launch_prep(w_in, i == 0 ? wl0 : wl_.p, act);
+                launch_flux(i == 0 ? MODE_FIRST : MODE_MID, 0.0, t, frac, w_in, w_out, nullptr, dt, act, wl_.p);
+                w_last = w_out;
             }
-            launch_derivative_aux(w_.p, act);
-            launch_prep(w_.p, wl_.p, act);
-            tape_fs(s - 1);
-            launch_flux(MODE_FINAL, 0.0, t, 1.0, w_.p, nullptr, x_.p, dt, act, nullptr, fuse_final);
+            launch_derivative_aux(w_last, act);
+            stage_fs(s - 1);
+            launch_prep(w_last, wl_.p, act);
+            launch_flux(MODE_FINAL, 0.0, t, 1.0, w_last, nullptr, x_.p, dt, act, nullptr, fuse_final);
             if (tape)
                 cudaMemcpyAsync(tape + (size_t)s * tape_n, x_.p, tape_n * sizeof(double), cudaMemcpyDeviceToDevice,
                                 stream_);
         }
+        fs_cur_ = fs_.p;
         if (mood) {   // a-posteriori first-order override of troubled cells
             cudaMemsetAsync(iscal_.p + 6, 0, sizeof(int), stream_);
             mark(ZSME_KERNEL_MOOD, true);
@@ -799,7 +803,7 @@ class Solver final : public SolverBase {
             mark(ZSME_KERNEL_MOOD, false);
         }
         const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
-        const FinalGather fg{fb_.p, w_.p, sd.dt_step, st_.ssp_stages};
+        const FinalGather fg{fb_.p, w_last, sd.dt_step, st_.ssp_stages};
         // EnforcePhysicalConstraints' UpdateState: the derivative aux of the
         // transport result before the constraints and the source
         launch_derivative_aux(x_.p, act);
