@@ -524,6 +524,12 @@ def run_adjoint(a, dev, torch, dist, rank, world):
     names, _ = models.parameter_table(c.model)
     C, F = c.mesh.n_cells, c.mesh.n_faces
     g = Solver(c.model, c.mesh, c.settings, p, device=dev)
+    tuned = None
+    if not a.no_tune:   # the forward's launch configuration (the replay runs the same kernels)
+        from zoomy_dmplex_b200 import autotune
+
+        g.set_state(c.q0)
+        tuned = autotune.tune(g, c.model, C, steps=2, use_cache=False, write_cache=False)
     cells = adj.gauges(C, ngauge, seed=0)
     steps = list(range(10, N + 1, 10))
     targets = adj.observe_run(g, tgt.q0, N, steps, cells)
@@ -608,7 +614,8 @@ def run_adjoint(a, dev, torch, dist, rank, world):
                        "l2_flush": "not needed for the ratio: both runs see the same cache state",
                        "timing": "forward: CUDA events around N graph-launched steps; adjoint: host wall clock "
                                  "around the (synchronising) zsme_adjoint call, forward pass with checkpoints, "
-                                 "segment replays and reverse sweep included"},
+                                 "segment replays and reverse sweep included",
+                       "launch": tuned or "default"},
             "adjoint": {"forward_ms_per_step": fwd_ms / N, "adjoint_call_ms_per_step": 1e3 * adj_s / N,
                         "adjoint_call_over_forward": 1e3 * adj_s / fwd_ms,
                         "phases_ms_per_step": {k: v / N for k, v in phases.items()},

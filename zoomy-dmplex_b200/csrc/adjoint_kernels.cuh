@@ -38,15 +38,17 @@
 // Register caps of the reverse kernels as resident 128-thread blocks per SM
 // (1 = uncapped): compile-time constants, chosen by measurement on the
 // adjoint workload (SME level 1, 79k cells: every reverse kernel is one or a
-// few waves, so resident blocks decide its time).
+// few waves, so resident blocks decide its time).  Uncapped the reverse sweep
+// took 0.255 ms per step; caps 3 / 3 / 2 give 0.229 ms with the same
+// gradients bit for bit (caps 2 / 2 / 2: 0.256 ms; 3 / 4 / 3: 0.230 ms).
 #ifndef ZSME_ADJ_FACE_MINB
-#define ZSME_ADJ_FACE_MINB 1
+#define ZSME_ADJ_FACE_MINB 3
 #endif
 #ifndef ZSME_ADJ_CELL_MINB
-#define ZSME_ADJ_CELL_MINB 1
+#define ZSME_ADJ_CELL_MINB 3
 #endif
 #ifndef ZSME_ADJ_FIN_MINB
-#define ZSME_ADJ_FIN_MINB 1
+#define ZSME_ADJ_FIN_MINB 2
 #endif
 
 namespace zsme {
