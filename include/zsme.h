@@ -79,6 +79,11 @@ typedef struct zsme_mesh {
                                        depth ends below -1e-10 redone by a first-order Euler step
                                        (MUSCLSolver.hpp:130-171, 197-229) */
 
+/* settings.solver.time_integration (Settings.hpp:34, MUSCLSolver.hpp:56-72) */
+#define ZSME_TIME_SPLITTING 0 /* "splitting": SSP-RK(s,2) transport, then the implicit source step */
+#define ZSME_TIME_IMEX 1      /* "imex": additive Runge-Kutta 2E (explicit transport, implicit source per
+                                 cell; SolverStrategies.hpp:62-128) at the step's CFL dt */
+
 /* The solver keys of the reference's Settings (Settings.hpp:13-40) that change
  * the step. */
 typedef struct zsme_settings {
@@ -95,7 +100,8 @@ typedef struct zsme_settings {
     int32_t refresh_derivative_aux; /* solver.refresh_derivative_aux: before every state update, fill the
                                      plugin's derivative aux slots (its field-level update_aux_variables;
                                      Green-Gauss derivatives, TransportStep.hpp:161-192) */
-    int32_t reserved[4];
+    int32_t time_integration;     /* ZSME_TIME_SPLITTING or ZSME_TIME_IMEX */
+    int32_t reserved[3];
     double wet_dry_eps;           /* solver.wet_dry_eps (reference default 1e-2): dry threshold of the
                                      positivity variants, read only when positivity != NONE */
 } zsme_settings;

@@ -37,6 +37,8 @@
 #include <memory>
 #include <string>
 #include <thread>
+
+#include "imex_tableau.h"
 #include <vector>
 
 namespace sme1d_l0_malpasset {
@@ -740,6 +742,128 @@ par_for(C, [&](int c, int) {
         }
         return iter >= 15 ? 1 : 0;
     }
+    // ---------------------------------------------------------------- IMEX
+    // The implicit source of the IMEX strategy at state y: the state clamped and
+    // its aux updated (UpdateState), the plugin's source there, zero in cells
+    // with depth below 1e-6 (ModularSolver::AddImplicitSourceToResidual,
+    // ModularSolver.hpp:82-124).
+    void imex_source_cell(const T* y, const T* aux_init, T* S) const {
+        const T X0[3] = {0, 0, 0};
+        T ys[NQ], a[NA];
+        for (int i = 0; i < NQ; ++i) ys[i] = y[i];
+        for (int i = 0; i < NA; ++i) a[i] = aux_init[i];
+        constrain_cell(ys, a);
+        if (NQ > 1 && ys[1] < zsme::ark2e::dry_residual) {
+            for (int i = 0; i < NQ; ++i) S[i] = 0.0;
+            return;
+        }
+        auto r = M::source(ys, a, params.data(), (T)0, (T)0, X0);
+        for (int i = 0; i < NQ; ++i) S[i] = r[i];
+    }
+    // One implicit stage of the IMEX step in one cell: y - z - hg S(y) = 0 by
+    // Newton from y = z, the Jacobian I - hg (dS/dQ + dS/dAux dAux/dQ) at the
+    // clamped state (the identity in cells drier than 1e-4,
+    // ModularSolver::FormSourceJacobian, ModularSolver.hpp:403-460), the
+    // elimination and the stopping rule of the source step (|residual| < 1e-8,
+    // at most 15 updates).  Returns 1 when the update limit was hit.
+    int imex_solve_cell(T hg, const T* z, T* y, const T* aux_init) const {
+        T S[NQ], res[NQ], delta[NQ], J[NQ * NQ];
+        for (int i = 0; i < NQ; ++i) y[i] = z[i];
+        const T* p = params.data();
+        int iter = 0;
+        for (; iter < 15; ++iter) {
+            imex_source_cell(y, aux_init, S);
+            T rn = 0.0;
+            for (int i = 0; i < NQ; ++i) {
+                res[i] = y[i] - z[i] - hg * S[i];
+                rn += res[i] * res[i];
+            }
+            if (std::sqrt(rn) < 1e-8) break;
+            T ys[NQ], a[NA];
+            for (int i = 0; i < NQ; ++i) ys[i] = y[i];
+            for (int i = 0; i < NA; ++i) a[i] = aux_init[i];
+            constrain_cell(ys, a);
+            for (int i = 0; i < NQ * NQ; ++i) J[i] = 0.0;
+            for (int i = 0; i < NQ; ++i) J[i * NQ + i] = 1.0;
+            if (!(NQ > 1 && ys[1] < zsme::ark2e::dry_jacobian)) {
+                auto dSdQ = M::source_jacobian_wrt_variables(ys, a, p);
+                auto dSdA = M::source_jacobian_wrt_aux_variables(ys, a, p);
+                T dAdQ[NA * NQ];
+                aux_jacobian<NQ, NA>(ys, a, p, dAdQ);
+                for (int i = 0; i < NQ; ++i)
+                    for (int j = 0; j < NQ; ++j) {
+                        T term = dSdQ[i * NQ + j];
+                        for (int k = 0; k < NA; ++k) term += dSdA[i * NA + k] * dAdQ[k * NQ + j];
+                        J[i * NQ + j] -= hg * term;
+                    }
+            }
+            for (int i = 0; i < NQ; ++i) res[i] = -res[i];
+            if (!gepp(J, res, delta)) break;
+            for (int i = 0; i < NQ; ++i) y[i] += delta[i];
+        }
+        return iter >= 15 ? 1 : 0;
+    }
+    // out = x + h (sum_j a_j G_j + sum_j at_j S_j), the terms added in order
+    static void imex_combine(const std::vector<T>& x, T h, int n, const std::vector<T>* const* G, const double* a,
+                             const std::vector<T>* const* S, const double* at, std::vector<T>& out) {
+        out.resize(x.size());
+        for (size_t k = 0; k < x.size(); ++k) {
+            T acc = 0.0;
+            for (int j = 0; j < n; ++j) acc += a[j] * (*G[j])[k];
+            for (int j = 0; j < n; ++j) acc += at[j] * (*S[j])[k];
+            out[k] = x[k] + h * acc;
+        }
+    }
+    // The IMEX strategy's step (SolverStrategies.hpp:62-128: TSARKIMEX "2e",
+    // transport explicit through FormRHS, source implicit) at the imposed dt h
+    // without PETSc's step-size control: stage 0 is X; stages 1 and 2 solve
+    // Y_i - h gamma S(Y_i) = Z_i per cell, their implicit derivative taken as
+    // (Y_i - Z_i) / (h gamma); X <- X + h sum_j b_j (G_j + S_j).
+    void imex_step(double t0, T h) {
+        namespace K = zsme::ark2e;
+        std::vector<T> G0, G1, G2, S0(X.size()), S1(X.size()), S2(X.size()), Z, Y1(X.size()), Y2(X.size());
+        int nu = 0;
+        form_rhs(t0, X, G0);
+        par_for(C, [&](int c, int) { imex_source_cell(&X[(size_t)c * NQ], &A[(size_t)c * NA], &S0[(size_t)c * NQ]); });
+        const T hg = h * K::gamma;
+        auto stage = [&](std::vector<T>& Y, std::vector<T>& Si) {
+            std::vector<int> part(par_width(C), 0);
+            par_for(C, [&](int c, int t) {
+                part[t] += imex_solve_cell(hg, &Z[(size_t)c * NQ], &Y[(size_t)c * NQ], &A[(size_t)c * NA]);
+                for (int i = 0; i < NQ; ++i) {
+                    const size_t id = (size_t)c * NQ + i;
+                    Si[id] = (Y[id] - Z[id]) / hg;
+                }
+            });
+            for (int v : part) nu += v;
+        };
+        {
+            const std::vector<T>* G[1] = {&G0};
+            const std::vector<T>* S[1] = {&S0};
+            const double a[1] = {K::a10}, at[1] = {K::t10};
+            imex_combine(X, h, 1, G, a, S, at, Z);
+        }
+        stage(Y1, S1);
+        form_rhs(t0 + K::c1 * zsme::value(h), Y1, G1);
+        {
+            const std::vector<T>* G[2] = {&G0, &G1};
+            const std::vector<T>* S[2] = {&S0, &S1};
+            const double a[2] = {K::a20, K::a21}, at[2] = {K::t20, K::t21};
+            imex_combine(X, h, 2, G, a, S, at, Z);
+        }
+        stage(Y2, S2);
+        form_rhs(t0 + K::c2 * zsme::value(h), Y2, G2);
+        {
+            const std::vector<T>* G[3] = {&G0, &G1, &G2};
+            const std::vector<T>* S[3] = {&S0, &S1, &S2};
+            const double b[3] = {K::b0, K::b1, K::b2};
+            std::vector<T> Xn;
+            imex_combine(X, h, 3, G, b, S, b, Xn);
+            X.swap(Xn);
+        }
+        n_unconv = nu;
+    }
+
     void source_solve(T dtl) {
         std::vector<int> part(par_width(C), 0);
         par_for(C, [&](int c, int t) { part[t] += solve_cell(dtl, &X[(size_t)c * NQ], &A[(size_t)c * NA]); });
@@ -949,12 +1073,14 @@ par_for(C, [&](int c, int) {
             const bool mood = st.positivity == ZSME_POSITIVITY_MOOD;
             std::vector<T> Xs;
             if (mood) Xs = X;
-            ts_step(t0, d0);
+            const bool imex = st.time_integration == ZSME_TIME_IMEX;
+            if (imex) imex_step(t0, d0);
+            else ts_step(t0, d0);
             ph(zsme_flops::FINAL);
             time = t0 + d0;
             update_state_vec(X, A);                            // EnforcePhysicalConstraints
             if (mood) mood_override(t0, d0, Xs);
-            if (st.source) {
+            if (st.source && !imex) {                          // IMEX carries the source in its stages
                 source_solve(d0);
                 update_state_vec(X, A);
             }

@@ -19,6 +19,7 @@
 #include "face_kernels.cuh"
 #include "source_kernels.cuh"
 #include "adjoint_kernels.cuh"
+#include "imex_kernels.cuh"
 #include "zsme.h"
 
 namespace zsme {
@@ -76,6 +77,7 @@ class Solver final : public SolverBase {
     double* fs_cur_ = nullptr;  // face states the prep and face kernels use: fs_, or a tape slot in a replay
     DevBuf<double> xs_;  // MOOD: the state at the start of the step
     DevBuf<int> mood_list_;  // MOOD: the troubled cells of the step (count in iscal_[6])
+    DevBuf<double> imex_g_[3], imex_s_[3], imex_y_[2];   // IMEX: stage right-hand sides, implicit derivatives, states
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
     DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag, [5] deferred finalize cells, [6] MOOD cells
@@ -232,6 +234,8 @@ class Solver final : public SolverBase {
         if (pm_.dim != DIM) return set_error(ZSME_ERR_ARG, "mesh dimension does not match the model");
         if (st_.reconstruction_order >= 2 && st_.ssp_stages < 2)
             return set_error(ZSME_ERR_ARG, "ssp_stages must be >= 2");
+        if (st_.time_integration != ZSME_TIME_SPLITTING && st_.time_integration != ZSME_TIME_IMEX)
+            return set_error(ZSME_ERR_ARG, "time_integration must be ZSME_TIME_SPLITTING or ZSME_TIME_IMEX");
         if (st_.positivity != ZSME_POSITIVITY_NONE && (NQ < 3 || !(st_.wet_dry_eps >= 0)))
             return set_error(ZSME_ERR_ARG, "positivity variants need a [b, h, momentum...] model and wet_dry_eps >= 0");
         // Zhang-Shu positivity holds for CFL <= 1/6 at order 2 (MUSCLSolver.hpp:33-38)
@@ -279,6 +283,13 @@ class Solver final : public SolverBase {
         ZSME_CUDA(w_.alloc((size_t)NQ * C));
         ZSME_CUDA(wl_.alloc((size_t)NQ * C));
         ZSME_CUDA(aux_.alloc((size_t)NA * C));
+        if (st_.time_integration == ZSME_TIME_IMEX) {
+            for (int j = 0; j < 3; ++j) {
+                ZSME_CUDA(imex_g_[j].alloc((size_t)NQ * C));
+                ZSME_CUDA(imex_s_[j].alloc((size_t)NQ * C));
+            }
+            for (int j = 0; j < 2; ++j) ZSME_CUDA(imex_y_[j].alloc((size_t)NQ * C));
+        }
         if (st_.positivity == ZSME_POSITIVITY_MOOD) {
             ZSME_CUDA(xs_.alloc((size_t)NQ * C));
             ZSME_CUDA(mood_list_.alloc((size_t)C));
@@ -760,9 +771,12 @@ class Solver final : public SolverBase {
         // kernels at order 2, and the stage result not needed on its own
         // (MOOD inspects it, the adjoint's tape keeps it)
         const bool fuse_final = lc_.fuse_final && lc_.tile_faces == 0 && st_.reconstruction_order >= 2 && !mood &&
-                                !tape && !deriv_.n;
+                                !tape && !deriv_.n && st_.time_integration == ZSME_TIME_SPLITTING;
         double* w_last = x_.p;   // the last stage's state
-        if (st_.reconstruction_order < 2) {
+        const bool imex = st_.time_integration == ZSME_TIME_IMEX;
+        if (imex) {
+            enqueue_imex_stages(t, dt, act, wl0);
+        } else if (st_.reconstruction_order < 2) {
             launch_derivative_aux(x_.p, act);       // FormRHS's UpdateState of the stage state
             stage_fs(0);
             launch_prep(x_.p, x_.p, act);
@@ -802,7 +816,8 @@ class Solver final : public SolverBase {
                 md_, x_.p, xs_.p, aux_.p, params_.p, sd, mood_list_.p, iscal_.p + 6);
             mark(ZSME_KERNEL_MOOD, false);
         }
-        const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source ? FIN_SOURCE : 0);
+        // IMEX carries the source in its stages (MUSCLSolver.hpp:173-182)
+        const int flags = FIN_PRE | FIN_POST | FIN_WRITE | FIN_DT | (st_.source && !imex ? FIN_SOURCE : 0);
         const FinalGather fg{fb_.p, w_last, sd.dt_step, st_.ssp_stages};
         // EnforcePhysicalConstraints' UpdateState: the derivative aux of the
         // transport result before the constraints and the source
@@ -813,7 +828,43 @@ class Solver final : public SolverBase {
         end_step_kernel<<<blocks_for(n_inst_, 128), 128, 0, stream_>>>(sd, 0, n_inst_, 1, 0.0, nullptr);
         mark(ZSME_KERNEL_END, false);
     }
+    // The IMEX strategy's transport + source update of one step (SolverStrategies.hpp:62-128,
+    // additive Runge-Kutta 2E at the step's dt): G_j = FormRHS(Y_j) by the
+    // prep / face / gather kernels in MODE_RHS, Y_0 = x_ with its implicit
+    // source, two implicit stages solved per cell, then x_ updated in place.
+    void enqueue_imex_stages(const double* t, const double* dt, const int* act, const double* wl0) {
+        namespace K = ark2e;
+        const int C = pm_.C, nb = blocks_for(C, 128);
+        auto rhs = [&](double* y, const double* wl, double frac, double* g) {
+            launch_derivative_aux(y, act);
+            launch_prep(y, wl, act);
+            launch_flux(MODE_RHS, 0.0, t, frac, nullptr, g, nullptr, dt, act);
+        };
+        rhs(x_.p, wl0, 0.0, imex_g_[0].p);
+        imex_source_kernel<M><<<nb, 128, 0, stream_>>>(md_, x_.p, aux_.p, params_.p, imex_s_[0].p, act);
+        const ImexTerms t1{{imex_g_[0].p}, {imex_s_[0].p}, {K::a10}, {K::t10}, 1};
+        imex_stage_kernel<M><<<blocks_for(C, 64), 64, 0, stream_>>>(md_, t1, x_.p, aux_.p, params_.p, dt, act,
+                                                                    imex_y_[0].p, imex_s_[1].p, iscal_.p + 1);
+        clamp_kernel<M><<<nb, 128, 0, stream_>>>(md_, 0, C, imex_y_[0].p, aux_.p, params_.p, wl_.p);
+        rhs(imex_y_[0].p, wl_.p, K::c1, imex_g_[1].p);
+        const ImexTerms t2{{imex_g_[0].p, imex_g_[1].p}, {imex_s_[0].p, imex_s_[1].p}, {K::a20, K::a21},
+                           {K::t20, K::t21}, 2};
+        imex_stage_kernel<M><<<blocks_for(C, 64), 64, 0, stream_>>>(md_, t2, x_.p, aux_.p, params_.p, dt, act,
+                                                                    imex_y_[1].p, imex_s_[2].p, iscal_.p + 1);
+        clamp_kernel<M><<<nb, 128, 0, stream_>>>(md_, 0, C, imex_y_[1].p, aux_.p, params_.p, wl_.p);
+        rhs(imex_y_[1].p, wl_.p, K::c2, imex_g_[2].p);
+        const ImexTerms tb{{imex_g_[0].p, imex_g_[1].p, imex_g_[2].p},
+                           {imex_s_[0].p, imex_s_[1].p, imex_s_[2].p},
+                           {K::b0, K::b1, K::b2},
+                           {K::b0, K::b1, K::b2},
+                           3};
+        imex_final_kernel<M><<<nb, 128, 0, stream_>>>(md_, tb, x_.p, dt, act);
+    }
     int launches_per_step() const override {
+        if (st_.time_integration == ZSME_TIME_IMEX) {
+            const int per_rhs = (lc_.tile_faces > 0 ? 2 : 3) + (deriv_.n ? 1 : 0);
+            return 3 + 3 * per_rhs + 6 + (deriv_.n ? 2 : 0) + (st_.positivity == ZSME_POSITIVITY_MOOD ? 2 : 0);
+        }
         const int per_stage = lc_.tile_faces > 0 ? 2 : 3;
         const bool fuse_final = lc_.fuse_final && lc_.tile_faces == 0 && st_.reconstruction_order >= 2 &&
                                 st_.positivity != ZSME_POSITIVITY_MOOD && !deriv_.n;
@@ -980,6 +1031,8 @@ class Solver final : public SolverBase {
             return set_error(ZSME_ERR_ARG, "adjoint: null observation array");
         if (!x_clamped_)
             return set_error(ZSME_ERR_STATE, "adjoint: the state is not constrained (call zsme_update_state)");
+        if (st_.time_integration != ZSME_TIME_SPLITTING)
+            return set_error(ZSME_ERR_ARG, "adjoint: only the splitting time integration is differentiated");
         if (st_.positivity != ZSME_POSITIVITY_NONE)
             return set_error(ZSME_ERR_ARG, "adjoint: the positivity variants are not differentiated (positivity none only)");
         const int C = pm_.C, F = pm_.F, K = pm_.K, NS = A.nsteps, E = A.every;

@@ -16,6 +16,8 @@ LIB_PATH = os.path.join(PKG, "libzsme.so")
 ZSME_LIMITER_NONE, ZSME_LIMITER_TVD = 0, 1
 ZSME_GRADIENT_GREEN_GAUSS, ZSME_GRADIENT_LSQ = 0, 1
 ZSME_POSITIVITY_NONE, ZSME_POSITIVITY_ZHANG_SHU, ZSME_POSITIVITY_MOOD = 0, 1, 2
+ZSME_TIME_SPLITTING, ZSME_TIME_IMEX = 0, 1
+TIME_INTEGRATION = {"splitting": ZSME_TIME_SPLITTING, "imex": ZSME_TIME_IMEX}
 POSITIVITY = {"none": ZSME_POSITIVITY_NONE, "zhang_shu": ZSME_POSITIVITY_ZHANG_SHU, "mood": ZSME_POSITIVITY_MOOD}
 KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step", "gather", "finalize_fallback", "mood")
 
@@ -34,7 +36,8 @@ class ZsmeSettings(ct.Structure):
         ("cfl", ct.c_double), ("t_end", ct.c_double), ("min_dt", ct.c_double),
         ("reconstruction_order", ct.c_int32), ("limiter", ct.c_int32), ("gradient", ct.c_int32),
         ("ssp_stages", ct.c_int32), ("source", ct.c_int32), ("block_size", ct.c_int32),
-        ("positivity", ct.c_int32), ("refresh_derivative_aux", ct.c_int32), ("reserved", ct.c_int32 * 4),
+        ("positivity", ct.c_int32), ("refresh_derivative_aux", ct.c_int32), ("time_integration", ct.c_int32),
+        ("reserved", ct.c_int32 * 3),
         ("wet_dry_eps", ct.c_double),
     ]
 

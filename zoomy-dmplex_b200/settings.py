@@ -16,8 +16,11 @@ How the reference interprets the strings, and so how they map here:
   the default ``"venkatakrishnan"``) installs Vacuum + TVD limiting through
   the backward-compatible ``LinearReconstructor`` constructor
   (``MUSCLSolver.hpp:43``, ``Reconstruction.hpp:170-175``);
-* ``time_integration``: ``"splitting"`` (explicit transport + implicit source)
-  is the only strategy of this path; ``"imex"``/``"implicit"`` are rejected;
+* ``time_integration``: ``"splitting"`` (explicit transport, then the implicit
+  source step) or ``"imex"`` (the additive Runge-Kutta scheme 2E of the
+  reference's IMEX strategy, explicit transport and implicit source in every
+  stage, at the step's CFL dt); ``"implicit"`` (BDF2 with matrix-free Newton)
+  is rejected;
 * ``refresh_derivative_aux`` (reference default true): before each state
   update the plugin's derivative aux slots are refilled with Green-Gauss
   derivatives of the state (``TransportStep.hpp:161-202``); plugins without
@@ -52,9 +55,9 @@ class SolverSettings:
     refresh_derivative_aux: bool = True
 
     def to_struct(self) -> native.ZsmeSettings:
-        if self.time_integration != "splitting":
-            raise ValueError("time_integration %r is not on this path (only 'splitting')"
-                             % self.time_integration)
+        if self.time_integration not in native.TIME_INTEGRATION:
+            raise ValueError("time_integration %r is not on this path ('splitting' or 'imex'; the fully implicit "
+                             "BDF2 + matrix-free Newton strategy is not built)" % self.time_integration)
         if self.positivity not in native.POSITIVITY:
             raise ValueError("positivity must be one of %s" % sorted(native.POSITIVITY))
         if self.gradient not in ("least_squares", "green_gauss"):
@@ -73,6 +76,7 @@ class SolverSettings:
         s.positivity = native.POSITIVITY[self.positivity]
         s.wet_dry_eps = float(self.wet_dry_eps)
         s.refresh_derivative_aux = 1 if self.refresh_derivative_aux else 0
+        s.time_integration = native.TIME_INTEGRATION[self.time_integration]
         return s
 
 
