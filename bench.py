@@ -948,7 +948,8 @@ def main():
                     "outputs_match_blocking": same},
             "gpu_launches": a.steps * g.launches_per_step(),
             "diag": {"nonfinite": diag.n_nonfinite, "negative_depth": diag.n_negative_depth,
-                     "newton_unconverged": diag.n_newton_unconverged, "mood_cells": diag.n_mood_cells},
+                     "newton_unconverged": diag.n_newton_unconverged, "mood_cells": diag.n_mood_cells,
+                     "newton_deferred_cells": diag.n_newton_deferred},
             "clocks": clocks}
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         v, nt, Cs, dts, ns = cpu_sample(side, seconds=a.cpu_seconds, positivity=a.positivity, built=case)

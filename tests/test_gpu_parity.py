@@ -345,3 +345,20 @@ def test_fp64_fma_peak_is_measured():
     v = ct.c_double()
     native.check(native.load().zsme_fp64_fma_peak(0, ct.byref(v)))
     assert 5.0 < v.value < 200.0, v.value
+
+
+def test_newton_fast_path_coverage():
+    """Which cells leave the Newton register fast path for the generic
+    elimination (zsme_diag.n_newton_deferred): none for the generated 2-D
+    plugins, whose source does not depend on the aux variables (Manning
+    friction on level 0 and Navier slip on level 2 included), and the cells
+    that take a Newton update for the 1-D model, whose slip term multiplies
+    hinv (dS/dAux != 0)."""
+    for c, want_all in ((cases.plain_l0(30), False), (cases.level2(30), False), (case_1d(), True)):
+        g, _ = pair(c)
+        g.step(3)
+        d = g.sync()
+        if want_all:
+            assert d.n_newton_deferred > 0, (c.name, d.n_newton_deferred)
+        else:
+            assert d.n_newton_deferred == 0, (c.name, d.n_newton_deferred)
