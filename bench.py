@@ -572,6 +572,7 @@ def run_adjoint(a, dev, torch, dist, rank, world):
     loss, gq, gp, dts = g.adjoint(N, *obs, checkpoint_every=every)
     adj_s = time.perf_counter() - w0
     phases = g.adjoint_phases()
+    overlapped = g.adjoint_overlapped()
     # end to end: initial state from the host, adjoint, gradients back
     w0 = time.perf_counter()
     g.set_state(c.q0)
@@ -634,6 +635,11 @@ def run_adjoint(a, dev, torch, dist, rank, world):
                         "phases_ms_per_step": {k: v / N for k, v in phases.items()},
                         "reverse_step_over_forward_step": phases["reverse"] / fwd_ms,
                         "replay_plus_reverse_over_forward": (phases["replay"] + phases["reverse"]) / fwd_ms,
+                        "replays_overlap_reverse": overlapped,
+                        "phases_note": ("replays on a side stream into a second tape buffer, overlapping the "
+                                        "reverse sweep: 'replay' is the first (exposed) replay, 'reverse' the rest "
+                                        "of the reverse phase" if overlapped else
+                                        "replay and reverse sweep in sequence per segment"),
                         "loss": loss, "grad_n_manning": float(gp[ni]), "grad_b_norm": float(np.linalg.norm(gq[:, 0])),
                         "fd": {"directions": len(errs), "eps": eps, "kind": "smooth random b directions",
                                "max_rel_err": float(max(errs)) if errs else None,

@@ -266,8 +266,11 @@ int zsme_batch_get_time(zsme_handle* h, int32_t i, double* t, double* dt);
  * order 2, positivity other than "mood"), so that result never round-trips
  * through device memory; prep_lean: 1 (default) forms the order-2 face
  * states with the lean kernel (32-bit offsets, branch-free neighbour
- * bounds), 0 with the plain one.  Every configuration gives the same results
- * bit for bit.
+ * bounds), 0 with the plain one, 2..4 with the lean kernel split over that
+ * many threads per cell, each owning a slice of the components (blocks of
+ * 64 or 96..128 threads of its own; the prep block size does not apply and
+ * its register cap takes 4, 6, 8 or none).  Every configuration gives the
+ * same results bit for bit.
  * The knobs of the autotuner (zoomy-dmplex_b200/autotune.py).  Setting them
  * outside stream capture only: a new tile_faces rebuilds the tiles. */
 int zsme_set_launch(zsme_handle* h, const int32_t* blocks);
@@ -295,8 +298,18 @@ int zsme_adjoint(zsme_handle* h, int32_t nsteps, int32_t checkpoint_every, int32
                  double* grad_params, double* dts);
 /* Device time (ms) of the last zsme_adjoint call's three phases: the
  * forward run with checkpoints, the segment replays into the tape, and the
- * reverse sweep.  No counterpart in the reference. */
+ * reverse sweep.  When the call overlapped its replays with the reverse
+ * sweep (zsme_adjoint_overlapped), the second figure is the first replay
+ * alone (the one nothing overlaps) and the third the rest of the reverse
+ * phase, replays included; the sum of the two is the reverse phase's device
+ * time either way.  No counterpart in the reference. */
 int zsme_adjoint_phases(zsme_handle* h, double* ms3);
+/* 1 when the last zsme_adjoint call replayed each checkpoint segment on a
+ * side stream into a second tape buffer while the reverse sweep of the
+ * segment after it ran (every segment full, at least two, and device memory
+ * for both tapes), else 0.  The gradients are the same bit for bit either
+ * way.  No counterpart in the reference. */
+int zsme_adjoint_overlapped(zsme_handle* h, int32_t* overlapped);
 
 /* CFL time step of a caller-owned state with no device allocation.
  * No counterpart in the reference, which has no GPU path.  It serves callers

@@ -349,16 +349,38 @@ def test_fp64_fma_peak_is_measured():
 
 def test_newton_fast_path_coverage():
     """Which cells leave the Newton register fast path for the generic
-    elimination (zsme_diag.n_newton_deferred): none for the generated 2-D
-    plugins, whose source does not depend on the aux variables (Manning
-    friction on level 0 and Navier slip on level 2 included), and the cells
-    that take a Newton update for the 1-D model, whose slip term multiplies
-    hinv (dS/dAux != 0)."""
-    for c, want_all in ((cases.plain_l0(30), False), (cases.level2(30), False), (case_1d(), True)):
+    elimination (zsme_diag.n_newton_deferred): none for the generated
+    plugins, whose sources do not depend on the aux variables (Manning
+    friction on level 0, Navier slip on level 2, the 1-D model's slip)."""
+    for c in (cases.plain_l0(30), cases.level2(30), case_1d()):
         g, _ = pair(c)
         g.step(3)
         d = g.sync()
-        if want_all:
-            assert d.n_newton_deferred > 0, (c.name, d.n_newton_deferred)
-        else:
-            assert d.n_newton_deferred == 0, (c.name, d.n_newton_deferred)
+        assert d.n_newton_deferred == 0, (c.name, d.n_newton_deferred)
+
+
+@pytest.mark.parametrize("prep_lean", [0, 2, 3, 4])
+@pytest.mark.parametrize("name", ["l2", "l4", "1d", "mixed"])
+@pytest.mark.parametrize("grad", ["green_gauss", "least_squares"])
+def test_face_state_kernels_bitwise(prep_lean, name, grad):
+    """The order-2 face-state kernels (prep_lean 0: plain, 1: lean, 2..4: lean
+    split over that many threads per cell) give the same RHS as the oracle bit
+    for bit, and the same steps as the default kernel bit for bit."""
+    from zoomy_dmplex_b200.solver import set_launch
+
+    c = CASES[name]
+    g, o = pair(c, gradient=grad)
+    ref, _ = pair(c, gradient=grad)
+    set_launch(g.h, {"prep_lean": prep_lean, "tile_faces": 0})
+    set_launch(ref.h, {"prep_lean": 1, "tile_faces": 0})
+    x = c.q0.copy()
+    x[:, 2] += 0.01
+    assert np.array_equal(g.rhs(x), o.rhs(x))
+    for k in range(8):
+        _, dt = o.time()
+        o.step(1)
+        g.step(1, dts=[dt])
+        ref.step(1, dts=[dt])
+        qg = g.get_state()
+        assert np.array_equal(qg, ref.get_state()), k
+        assert errs(qg, o.get_state()).max() <= TOL, k

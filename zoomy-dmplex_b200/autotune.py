@@ -25,12 +25,16 @@ from . import native
 from .solver import LAUNCH_KEYS, get_launch, set_launch
 
 KNOBS = (("tile_faces", (0, 64, 128, 256, 512)), ("face", (64, 128)), ("face_occ", (1, 2, 3, 4)),
-         ("prep_lean", (0, 1)), ("prep", (64, 128)), ("prep_occ", (1, 2, 3, 4, 6, 8)), ("gather", (64, 128)),
+         ("prep_lean", (0, 1, 2, 3, 4)), ("prep", (64, 128)), ("prep_occ", (1, 2, 3, 4, 6, 8)), ("gather", (64, 128)),
          ("finalize", (64, 128)), ("finalize_occ", (1, 2, 3, 4)), ("fuse_final", (0, 1)))
 # searched together first: which face path, its block size and its register cap
 # decide each other's worth (the fused kernel's shared memory per block is fixed
 # by its tile size, so its occupancy depends on all three)
 JOINT = ("tile_faces", "face", "face_occ")
+# then the face-state kernel's form with its register cap (a split form runs
+# more threads per cell with fewer registers each, so the cap worth having
+# depends on the form)
+JOINT_PREP = ("prep_lean", "prep_occ")
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_launch.json")
 
 
@@ -101,8 +105,17 @@ def tune(solver, model, n_cells, steps=2, cache=DEFAULT_CACHE, use_cache=True, w
                 if best_t is None or t < best_t:
                     best, best_t = (tf, fb, fo), t
     cfg.update(dict(zip(JOINT, best)))
+    best, best_t = None, None
+    for pl in values["prep_lean"]:
+        for po in values["prep_occ"]:
+            trial = dict(cfg, prep_lean=pl, prep_occ=po)
+            t = _measure(solver, trial, steps)
+            trace.append(("prep_lean/prep_occ", (pl, po), t))
+            if best_t is None or t < best_t:
+                best, best_t = (pl, po), t
+    cfg.update(dict(zip(JOINT_PREP, best)))
     for knob, values in KNOBS:
-        if knob in JOINT:
+        if knob in JOINT or knob in JOINT_PREP:
             continue
         best_v, best_t = cfg[knob], None
         for v in values:

@@ -38,7 +38,8 @@ struct LaunchConfig {
                                        // faces (64..1024); 0: separate face and gather kernels
     int fuse_final = 0;                // 1: with separate face and gather kernels, the last stage's
                                        // gather runs inside the finalize kernel
-    int prep_lean = 1;                 // order-2 face states by prep_lean_kernel (1) or prep_kernel (0)
+    int prep_lean = 1;                 // order-2 face states: prep_kernel (0), prep_lean_kernel (1),
+                                       // prep_split_kernel with 2..4 threads per cell
 };
 
 // Tiles of the fused face + gather kernel.  A tile is a run of consecutive
@@ -118,6 +119,7 @@ class SolverBase {
                         double* dts) = 0;
     // device times of the last adjoint call's forward pass, replays and reverse sweep (ms)
     virtual int adjoint_phases(double* ms) = 0;
+    virtual bool adjoint_overlapped() const = 0;
 };
 
 }  // namespace zsme

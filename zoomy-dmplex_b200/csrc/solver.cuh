@@ -96,6 +96,16 @@ class Solver final : public SolverBase {
     DevBuf<int> adj_ocell_, adj_ocomp_, adj_first_, adj_segn0_all_, adj_seg_n0_;
     DevBuf<double> adj_th_, adj_seg_dt_, adj_seg_t_;
     size_t adj_tstride_ = 0;
+    // two tape buffers when the replay of one checkpoint segment overlaps the
+    // reverse sweep of the next (side stream); adj_par_ selects the buffer the
+    // enqueued replay / reverse launches use, adj_aux_cur_ the aux array the
+    // reverse launches read (the live aux, or its snapshot at the end of the
+    // segment's replay)
+    DevBuf<double> adj_aux_snap_;
+    cudaStream_t adj_side_ = nullptr;
+    int adj_par_ = 0, adj_tape_steps_ = 0;
+    const double* adj_aux_cur_ = nullptr;
+    bool adj_overlapped_ = false;  // the last zsme_adjoint overlapped its replays with the reverse sweep
     double adj_phase_ms_[3] = {0, 0, 0};  // last zsme_adjoint: forward pass, replays, reverse sweep
     MeshDev md_{};
     Opts opts_{};
@@ -125,6 +135,7 @@ class Solver final : public SolverBase {
             cudaStreamDestroy(h2d_);
             cudaStreamDestroy(d2h_);
         }
+        if (adj_side_) cudaStreamDestroy(adj_side_);
         if (stream_) cudaStreamDestroy(stream_);
     }
 
@@ -185,7 +196,8 @@ class Solver final : public SolverBase {
         if (lc.face_occ < 1 || lc.face_occ > 4 || lc.finalize_occ < 1 || lc.finalize_occ > 4)
             return set_error(ZSME_ERR_ARG, "face and finalize occupancy caps must be 1..4 blocks per SM");
         if (lc.fuse_final < 0 || lc.fuse_final > 1) return set_error(ZSME_ERR_ARG, "fuse_final must be 0 or 1");
-        if (lc.prep_lean < 0 || lc.prep_lean > 1) return set_error(ZSME_ERR_ARG, "prep_lean must be 0 or 1");
+        if (lc.prep_lean < 0 || lc.prep_lean > 4)
+            return set_error(ZSME_ERR_ARG, "prep_lean must be 0 (plain), 1 (lean) or 2..4 (lean, threads per cell)");
         if (lc.tile_faces != 0 && (lc.tile_faces < 64 || lc.tile_faces > 1024))
             return set_error(ZSME_ERR_ARG, "tile_faces must be 0 (separate face and gather kernels) or 64..1024");
         if ((size_t)lc.tile_faces * 3 * NQ * sizeof(double) > kMaxTileSmem)
@@ -575,6 +587,15 @@ class Solver final : public SolverBase {
             mark(ZSME_KERNEL_PREP, false);
             return;
         }
+        if (lc_.prep_lean >= 2 && st_.reconstruction_order >= 2 && lean_ok_) {
+            switch (lc_.prep_lean) {
+                case 2: launch_prep_split<2>(w, wl, active); break;
+                case 3: launch_prep_split<3>(w, wl, active); break;
+                default: launch_prep_split<4>(w, wl, active); break;
+            }
+            mark(ZSME_KERNEL_PREP, false);
+            return;
+        }
         if (lc_.prep_lean && st_.reconstruction_order >= 2 && lean_ok_) {
             switch (lc_.prep_occ) {
 #define ZSME_PREPL(OCC)                                                                                         \
@@ -608,6 +629,26 @@ class Solver final : public SolverBase {
 #undef ZSME_PREP
         }
         mark(ZSME_KERNEL_PREP, false);
+    }
+    // prep_lean_kernel's face states, P threads per cell (prep_split_kernel)
+    template <int P>
+    void launch_prep_split(const double* w, const double* wl, const int* active) {
+        const int gb = blocks_for(pm_.C, SplitShape<P>::CB);
+        constexpr int T = SplitShape<P>::threads;
+        switch (lc_.prep_occ) {
+#define ZSME_PREPS(OCC)                                                                                         \
+    case OCC:                                                                                                   \
+        if (pm_.K == 3)                                                                                         \
+            prep_split_kernel<M, OCC, 3, P><<<gb, T, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, params_.p,      \
+                                                                   fs_cur_, active);                            \
+        else                                                                                                    \
+            prep_split_kernel<M, OCC, 4, P><<<gb, T, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl, params_.p,      \
+                                                                   fs_cur_, active);                            \
+        break;
+            ZSME_PREPS(4) ZSME_PREPS(6) ZSME_PREPS(8)
+            default: ZSME_PREPS(1)
+#undef ZSME_PREPS
+        }
     }
     // face_only: the face kernel alone (split path), its gather left to the
     // finalize kernel (fused_final_stage)
@@ -946,15 +987,15 @@ class Solver final : public SolverBase {
         const int C = pm_.C, F = pm_.F;
         const double* wl = W;
         if (!W0) {
-            clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, W, aux_.p, params_.p, adj_wl_.p);
+            clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, W, adj_aux_cur_, params_.p, adj_wl_.p);
             wl = adj_wl_.p;
         }
         if constexpr (HasFluxVJP<N>::value) {   // the plugin's generated reverse sweep
-            adj_face_vjp_kernel<MT, NT><<<blocks_for(F, 128), 128, 0, stream_>>>(md_, fs, aux_.p, params_.p, tp,
+            adj_face_vjp_kernel<MT, NT><<<blocks_for(F, 128), 128, 0, stream_>>>(md_, fs, adj_aux_cur_, params_.p, tp,
                                                                                 frac, dtp, factor, src, adj_gfs_.p);
         } else {
             adj_face_kernel<MT, NT><<<blocks_for((long long)F * 2, 128), 128, 0, stream_>>>(
-                md_, fs, aux_.p, params_.p, tp, frac, dtp, factor, src, adj_gfs_.p);
+                md_, fs, adj_aux_cur_, params_.p, tp, frac, dtp, factor, src, adj_gfs_.p);
         }
         if (pm_.K == 3)
             adj_cell_kernel<MT, 3><<<blocks_for(C, 128), 128, 0, stream_>>>(
@@ -962,7 +1003,7 @@ class Solver final : public SolverBase {
         else
             adj_cell_kernel<MT, 4><<<blocks_for(C, 128), 128, 0, stream_>>>(
                 md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);
-        adj_combine_kernel<MT><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, W, aux_.p, params_.p, adj_own_w_.p,
+        adj_combine_kernel<MT><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, W, adj_aux_cur_, params_.p, adj_own_w_.p,
                                                                         adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p,
                                                                         src, c_src, dst);
     }
@@ -973,15 +1014,16 @@ class Solver final : public SolverBase {
     void adj_step(int k) {
         const int C = pm_.C;
         const size_t nv = (size_t)NQ * C, fs_n = (size_t)2 * NQ * pm_.F;
-        const double* tape = adj_tape_.p + (size_t)k * adj_tstride_;
-        const double* dtp = adj_seg_dt_.p + k;
-        const double* tp = adj_seg_t_.p + k;
+        const size_t par = (size_t)adj_par_ * adj_tape_steps_;
+        const double* tape = adj_tape_.p + (par + k) * adj_tstride_;
+        const double* dtp = adj_seg_dt_.p + par + k;
+        const double* tp = adj_seg_t_.p + par + k;
         double *lam = adj_lam0_.p, *t1 = adj_lam1_.p, *t2 = adj_lam2_.p;
         const int flags = FIN_PRE | FIN_POST | (st_.source ? FIN_SOURCE : 0);
         const int s = st_.reconstruction_order < 2 ? 1 : st_.ssp_stages;
         const int nb = blocks_for(C, 128);
-        adj_finalize_kernel<MT><<<nb, 128, 0, stream_>>>(md_, tape + (size_t)s * nv, aux_.p, params_.p, dtp, flags,
-                                                         lam, t1, adj_lp_cell_.p);
+        adj_finalize_kernel<MT><<<nb, 128, 0, stream_>>>(md_, tape + (size_t)s * nv, adj_aux_cur_, params_.p, dtp,
+                                                         flags, lam, t1, adj_lp_cell_.p);
         adj_param_reduce_kernel<<<NP, 256, 0, stream_>>>(adj_lp_cell_.p, nb, adj_lp_.p);
         const double* fst = tape + (size_t)(s + 1) * nv;
         if (st_.reconstruction_order < 2) {  // X' = W0 + dt R(W0)
@@ -1000,24 +1042,27 @@ class Solver final : public SolverBase {
             axpby_kernel<<<blocks_for((long long)nv, 256), 256, 0, stream_>>>((long long)nv, 1.0 / s, t1, 1.0, cur);
             if (cur != lam) cudaMemcpyAsync(lam, cur, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
         }
-        adj_seed_seg_kernel<<<1, 1, 0, stream_>>>(adj_first_.p, adj_seg_n0_.p, k, adj_ocell_.p, adj_ocomp_.p,
-                                                  adj_oseed_.p, C, lam);
+        adj_seed_seg_kernel<<<1, 1, 0, stream_>>>(adj_first_.p, adj_seg_n0_.p + adj_par_, k, adj_ocell_.p,
+                                                  adj_ocomp_.p, adj_oseed_.p, C, lam);
     }
 
-    // Replay of steps n0 .. n0+cnt-1 with the segment's dts into the tape.
+    // Replay of steps n0 .. n0+cnt-1 with the segment's dts into the tape
+    // buffer adj_par_.
     void adj_replay(int cnt) {
         const size_t nv = (size_t)NQ * pm_.C;
+        const size_t par = (size_t)adj_par_ * adj_tape_steps_;
         cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_);
         for (int k = 0; k < cnt; ++k) {
-            double* tp = adj_tape_.p + (size_t)k * adj_tstride_;
+            double* tp = adj_tape_.p + (par + k) * adj_tstride_;
             cudaMemcpyAsync(tp, x_.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
-            enqueue_step(adj_seg_dt_.p, x_.p, tp);
+            enqueue_step(adj_seg_dt_.p + par, x_.p, tp);
         }
     }
     void adj_reverse(int cnt) {
         for (int k = cnt - 1; k >= 0; --k) adj_step(k);
     }
 
+    bool adjoint_overlapped() const override { return adj_overlapped_; }
     int adjoint_phases(double* ms) override {
         for (int i = 0; i < 3; ++i) ms[i] = adj_phase_ms_[i];
         return ZSME_OK;
@@ -1062,14 +1107,29 @@ class Solver final : public SolverBase {
         ZSME_CUDA(adj_ocomp_.upload(ocomp, stream_));
         ZSME_CUDA(adj_first_.upload(first, stream_));
         ZSME_CUDA(adj_segn0_all_.upload(seg_n0, stream_));
-        ZSME_CUDA(adj_seg_n0_.alloc(1));
+        ZSME_CUDA(adj_seg_n0_.alloc(2));
         ZSME_CUDA(adj_oval_.alloc(std::max(1, A.nobs)));
         ZSME_CUDA(adj_oseed_.alloc(std::max(1, A.nobs)));
         ZSME_CUDA(adj_ck_x_.alloc((size_t)(nseg + 1) * nv));
         ZSME_CUDA(adj_ck_a_.alloc((size_t)(nseg + 1) * na));
         adj_tstride_ = (size_t)(s + 1) * nv + (size_t)s * 2 * NQ * F;  // one step's tape
         const int tape_steps = std::min(E, std::max(NS, 1));
-        ZSME_CUDA(adj_tape_.alloc((size_t)tape_steps * adj_tstride_));
+        // the replay of segment g-1 runs on a side stream while the reverse sweep
+        // of segment g runs on the handle's stream: two tape buffers, CUDA graphs
+        // for every segment (all segments full), and room for both buffers
+        const size_t tape_bytes = (size_t)tape_steps * adj_tstride_ * sizeof(double);
+        bool overlap = !profiling_ && nseg >= 2 && NS % E == 0;
+        if (overlap) {
+            size_t fr = 0, tot = 0;
+            ZSME_CUDA(cudaMemGetInfo(&fr, &tot));
+            const size_t held = adj_tape_.n * sizeof(double);
+            overlap = fr + held >= 2 * tape_bytes + ((size_t)2 << 30);
+        }
+        if (overlap && !adj_side_) ZSME_CUDA(cudaStreamCreateWithFlags(&adj_side_, cudaStreamNonBlocking));
+        adj_tape_steps_ = tape_steps;
+        adj_overlapped_ = overlap;
+        ZSME_CUDA(adj_tape_.alloc((size_t)(overlap ? 2 : 1) * tape_steps * adj_tstride_));
+        ZSME_CUDA(adj_aux_snap_.alloc((size_t)2 * na));
         for (auto* b : {&adj_lam0_, &adj_lam1_, &adj_lam2_, &adj_own_w_, &adj_own_wl_, &adj_wl_})
             ZSME_CUDA(b->alloc(nv));
         ZSME_CUDA(adj_out_w_.alloc((size_t)K * nv));
@@ -1079,8 +1139,8 @@ class Solver final : public SolverBase {
         ZSME_CUDA(adj_lp_.alloc(NP));
         ZSME_CUDA(adj_dts_.alloc(std::max(1, NS)));
         ZSME_CUDA(adj_th_.alloc((size_t)NS + 1));
-        ZSME_CUDA(adj_seg_dt_.alloc(tape_steps));
-        ZSME_CUDA(adj_seg_t_.alloc(tape_steps));
+        ZSME_CUDA(adj_seg_dt_.alloc((size_t)2 * tape_steps));
+        ZSME_CUDA(adj_seg_t_.alloc((size_t)2 * tape_steps));
         auto obs_values = [&](int n) {
             const int cnt = first[n + 1] - first[n];
             if (cnt > 0)
@@ -1093,10 +1153,9 @@ class Solver final : public SolverBase {
             cudaMemcpyAsync(adj_ck_a_.p + (size_t)slot * na, aux_.p, na * sizeof(double), cudaMemcpyDeviceToDevice,
                             stream_);
         };
-        auto restore = [&](int slot) {
-            cudaMemcpyAsync(x_.p, adj_ck_x_.p + (size_t)slot * nv, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
-            cudaMemcpyAsync(aux_.p, adj_ck_a_.p + (size_t)slot * na, na * sizeof(double), cudaMemcpyDeviceToDevice,
-                            stream_);
+        auto restore = [&](int slot, cudaStream_t st) {
+            cudaMemcpyAsync(x_.p, adj_ck_x_.p + (size_t)slot * nv, nv * sizeof(double), cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(aux_.p, adj_ck_a_.p + (size_t)slot * na, na * sizeof(double), cudaMemcpyDeviceToDevice, st);
         };
         cudaEvent_t ev[4];
         for (auto& e : ev) ZSME_CUDA(cudaEventCreate(&e));
@@ -1163,15 +1222,14 @@ class Solver final : public SolverBase {
                                                       adj_oseed_.p + first[NS], C, adj_lam0_.p);
         }
         const bool graphs = !profiling_;
-        cudaGraphExec_t g_replay = nullptr, g_reverse = nullptr;
+        cudaGraphExec_t gx[4] = {nullptr, nullptr, nullptr, nullptr};   // replay, reverse per tape buffer
         struct GraphGuard {
-            cudaGraphExec_t* a;
-            cudaGraphExec_t* b;
+            cudaGraphExec_t* g;
             ~GraphGuard() {
-                if (*a) cudaGraphExecDestroy(*a);
-                if (*b) cudaGraphExecDestroy(*b);
+                for (int i = 0; i < 4; ++i)
+                    if (g[i]) cudaGraphExecDestroy(g[i]);
             }
-        } graph_guard{&g_replay, &g_reverse};
+        } graph_guard{gx};
         auto capture = [&](cudaGraphExec_t* out, bool replay) -> int {
             cudaGraph_t gr = nullptr;
             ZSME_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1183,46 +1241,99 @@ class Solver final : public SolverBase {
             ZSME_CUDA(e);
             return ZSME_OK;
         };
+        // the segment's start time, dts, step times and first step index into buffer par
+        auto seg_scalars = [&](int seg, int par, int cnt, cudaStream_t st) -> int {
+            const int n0 = seg * E;
+            const size_t o = (size_t)par * tape_steps;
+            ZSME_CUDA(cudaMemcpyAsync(t_.p, adj_th_.p + n0, sizeof(double), cudaMemcpyDeviceToDevice, st));
+            ZSME_CUDA(cudaMemcpyAsync(adj_seg_dt_.p + o, adj_dts_.p + n0, cnt * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, st));
+            ZSME_CUDA(cudaMemcpyAsync(adj_seg_t_.p + o, adj_th_.p + n0, cnt * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, st));
+            ZSME_CUDA(cudaMemcpyAsync(adj_seg_n0_.p + par, adj_segn0_all_.p + seg, sizeof(int),
+                                      cudaMemcpyDeviceToDevice, st));
+            return ZSME_OK;
+        };
         float replay_ms = 0.f, reverse_ms = 0.f;
-        for (int seg = nseg - 1; seg >= 0; --seg) {
-            const int n0 = seg * E, cnt = std::min(NS, n0 + E) - n0;
-            const bool full = cnt == E && graphs;
-            ZSME_CUDA(cudaEventRecord(ev[2], stream_));
-            restore(seg);
-            ZSME_CUDA(cudaMemcpyAsync(t_.p, adj_th_.p + n0, sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-            ZSME_CUDA(cudaMemcpyAsync(adj_seg_dt_.p, adj_dts_.p + n0, cnt * sizeof(double), cudaMemcpyDeviceToDevice,
-                                      stream_));
-            ZSME_CUDA(cudaMemcpyAsync(adj_seg_t_.p, adj_th_.p + n0, cnt * sizeof(double), cudaMemcpyDeviceToDevice,
-                                      stream_));
-            ZSME_CUDA(cudaMemcpyAsync(adj_seg_n0_.p, adj_segn0_all_.p + seg, sizeof(int), cudaMemcpyDeviceToDevice,
-                                      stream_));
-            if (full) {
-                if (!g_replay) {
-                    int rc = capture(&g_replay, true);
-                    if (rc) return rc;
+        if (!overlap) {
+            // one tape buffer: replay, then reverse, segment by segment; the
+            // reverse reads the aux array as the replay left it
+            adj_par_ = 0;
+            adj_aux_cur_ = aux_.p;
+            for (int seg = nseg - 1; seg >= 0; --seg) {
+                const int n0 = seg * E, cnt = std::min(NS, n0 + E) - n0;
+                const bool full = cnt == E && graphs;
+                ZSME_CUDA(cudaEventRecord(ev[2], stream_));
+                restore(seg, stream_);
+                int rc = seg_scalars(seg, 0, cnt, stream_);
+                if (rc) return rc;
+                if (full) {
+                    if (!gx[0] && (rc = capture(&gx[0], true))) return rc;
+                    ZSME_CUDA(cudaGraphLaunch(gx[0], stream_));
+                } else {
+                    adj_replay(cnt);
                 }
-                ZSME_CUDA(cudaGraphLaunch(g_replay, stream_));
-            } else {
-                adj_replay(cnt);
+                ZSME_CUDA(cudaEventRecord(ev[3], stream_));
+                if (full) {
+                    if (!gx[2] && (rc = capture(&gx[2], false))) return rc;
+                    ZSME_CUDA(cudaGraphLaunch(gx[2], stream_));
+                } else {
+                    adj_reverse(cnt);
+                }
+                ZSME_CUDA(cudaGetLastError());
+                ZSME_CUDA(cudaEventRecord(ev[1], stream_));
+                ZSME_CUDA(cudaEventSynchronize(ev[1]));
+                float a1 = 0.f, a2 = 0.f;
+                ZSME_CUDA(cudaEventElapsedTime(&a1, ev[2], ev[3]));
+                ZSME_CUDA(cudaEventElapsedTime(&a2, ev[3], ev[1]));
+                replay_ms += a1;
+                reverse_ms += a2;
             }
-            ZSME_CUDA(cudaEventRecord(ev[3], stream_));
-            if (full) {
-                if (!g_reverse) {
-                    int rc = capture(&g_reverse, false);
-                    if (rc) return rc;
-                }
-                ZSME_CUDA(cudaGraphLaunch(g_reverse, stream_));
-            } else {
-                adj_reverse(cnt);
+        } else {
+            // two tape buffers: segment g's replay (side stream) fills buffer g % 2
+            // while the handle's stream runs the reverse sweep of segment g + 1 out
+            // of the other one.  Every segment is full, so the four graphs are
+            // captured once, up front.  The reverse reads the aux snapshot taken
+            // at the end of its own segment's replay, the array the one-buffer
+            // form reads at that point.
+            int rc = 0;
+            for (int par = 0; par < 2; ++par) {
+                adj_par_ = par;
+                adj_aux_cur_ = adj_aux_snap_.p + (size_t)par * na;
+                if ((rc = capture(&gx[par], true)) || (rc = capture(&gx[2 + par], false))) return rc;
+            }
+            cudaEvent_t ov[5];   // replay done (2), reverse done (2), start
+            int made = 0;
+            struct OvGuard {
+                cudaEvent_t* e;
+                int* n;
+                ~OvGuard() { for (int i = 0; i < *n; ++i) cudaEventDestroy(e[i]); }
+            } ov_guard{ov, &made};
+            for (; made < 5; ++made) ZSME_CUDA(cudaEventCreateWithFlags(&ov[made], cudaEventDisableTiming));
+            ZSME_CUDA(cudaEventRecord(ev[2], stream_));
+            ZSME_CUDA(cudaEventRecord(ov[4], stream_));
+            ZSME_CUDA(cudaStreamWaitEvent(adj_side_, ov[4], 0));
+            bool rev_issued[2] = {false, false};
+            for (int seg = nseg - 1; seg >= 0; --seg) {
+                const int par = seg & 1;
+                if (rev_issued[par]) ZSME_CUDA(cudaStreamWaitEvent(adj_side_, ov[2 + par], 0));
+                restore(seg, adj_side_);
+                if ((rc = seg_scalars(seg, par, E, adj_side_))) return rc;
+                ZSME_CUDA(cudaGraphLaunch(gx[par], adj_side_));
+                ZSME_CUDA(cudaMemcpyAsync(adj_aux_snap_.p + (size_t)par * na, aux_.p, na * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, adj_side_));
+                ZSME_CUDA(cudaEventRecord(ov[par], adj_side_));
+                ZSME_CUDA(cudaStreamWaitEvent(stream_, ov[par], 0));
+                if (seg == nseg - 1) ZSME_CUDA(cudaEventRecord(ev[3], stream_));   // the first replay is exposed
+                ZSME_CUDA(cudaGraphLaunch(gx[2 + par], stream_));
+                ZSME_CUDA(cudaEventRecord(ov[2 + par], stream_));
+                rev_issued[par] = true;
             }
             ZSME_CUDA(cudaGetLastError());
             ZSME_CUDA(cudaEventRecord(ev[1], stream_));
             ZSME_CUDA(cudaEventSynchronize(ev[1]));
-            float a1 = 0.f, a2 = 0.f;
-            ZSME_CUDA(cudaEventElapsedTime(&a1, ev[2], ev[3]));
-            ZSME_CUDA(cudaEventElapsedTime(&a2, ev[3], ev[1]));
-            replay_ms += a1;
-            reverse_ms += a2;
+            ZSME_CUDA(cudaEventElapsedTime(&replay_ms, ev[2], ev[3]));
+            ZSME_CUDA(cudaEventElapsedTime(&reverse_ms, ev[3], ev[1]));
         }
         adj_phase_ms_[1] = replay_ms;
         adj_phase_ms_[2] = reverse_ms;
@@ -1232,7 +1343,7 @@ class Solver final : public SolverBase {
             if (rc) return rc;
         }
         if (grad_p) ZSME_CUDA(cudaMemcpyAsync(grad_p, adj_lp_.p, NP * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-        restore(nseg);
+        restore(nseg, stream_);
         ZSME_CUDA(cudaMemcpyAsync(t_.p, &t_fin, sizeof(double), cudaMemcpyHostToDevice, stream_));
         ZSME_CUDA(cudaMemcpyAsync(dt_cfl_.p, &dtc_fin, sizeof(double), cudaMemcpyHostToDevice, stream_));
         ZSME_CUDA(cudaStreamSynchronize(stream_));

@@ -515,6 +515,232 @@ __global__ void __launch_bounds__(128, MINB) prep_lean_kernel(MeshDev m, Opts o,
     }
 }
 
+// ---------------------------------------------------- prep, split over threads
+// prep_lean_kernel's face states with P threads per cell: thread part p owns
+// components [p NC, p NC + NC), NC = ceil(NQ / P), and keeps only their
+// gradient rows in registers, so the kernel needs far fewer registers and runs
+// more warps per SM to hide its gathered neighbour loads.  A block holds CB
+// cells (a multiple of 32, so each warp serves one part) times P parts; the
+// warps of part p load the CB cells' geometry and their components coalesced.
+// The limiter's alpha = min over components meets in shared memory: each part
+// lowers its own copy of every face's alpha from 1.0 over its components,
+// then every part takes the minimum of the P copies.  With the comparisons of
+// the one-thread form ("<" skips NaN, and every candidate alpha is in [0, 1]
+// or NaN), the minimum of minima is the same value, so the face states are
+// bit for bit those of prep_lean_kernel.  The vacuum test reads only the depth
+// of the cell and its neighbours and is evaluated by every part alike.
+template <int P>
+struct SplitShape {
+    static constexpr int CB = P == 2 ? 64 : 32;   // cells per block
+    static constexpr int threads = CB * P;
+};
+
+template <class M, int MINB, int KM, int P>
+__global__ void __launch_bounds__(128, MINB) prep_split_kernel(MeshDev m, Opts o, int c0, int cn,
+                                                         const double* __restrict__ w,
+                                                         const double* __restrict__ wl,
+                                                         const double* __restrict__ params,
+                                                         double* __restrict__ fs, const int* __restrict__ active) {
+    constexpr int NQ = M::n_dof_q, DIM = M::dimension;
+    constexpr int CB = SplitShape<P>::CB, NC = (NQ + P - 1) / P;
+    __shared__ double al_sh[P][KM][CB];
+    __shared__ double qb_sh[KM][NQ][CB];   // Green-Gauss boundary values of the block's boundary slots
+    const int C = m.C, F = m.F;
+    const int K = KM == 3 ? 3 : m.K;
+    const int part = threadIdx.x / CB, lc = threadIdx.x - part * CB;
+    const int r = blockIdx.x * CB + lc;
+    const int i0 = part * NC;
+    const int c = c0 + r;
+    bool live = r < cn;
+    int I = 0;
+    if (live) {
+        I = cell_instance(m, c);
+        if (active && !active[I]) live = false;
+    }
+    if (o.gradient != 1) {
+        // the boundary condition of every boundary slot, evaluated once (by the
+        // part k mod P) before anything else is held in registers, so that its
+        // full-state temporaries do not set the kernel's register count
+        if (live) {
+            const double* p = params + (size_t)I * m.np;
+#pragma unroll
+            for (int k = part; k < KM; k += P) {
+                if (k >= K) continue;
+                const int f = m.slot_face[k * C + c];
+                const int meta = m.slot_meta[k * C + c];
+                if (f < 0 || m.slot_nbr[k * C + c] >= 0 || meta_bc(meta) < 0) continue;
+                double qg[NQ];
+                load_q<NQ>(w, C, c, qg);
+                const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
+                const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
+                const auto qb = M::boundary_conditions(meta_bc(meta), qg, (const double*)nullptr, p, nh, xf, 0.0, 0.0);
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) qb_sh[k][i][lc] = qb[i];
+            }
+        }
+        __syncthreads();
+    }
+    int nbc[KM], fso[KM];
+    bool hasn[KM];
+    double dx[KM][DIM], g[NC * DIM], al[KM];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) al[k] = 1.0;
+    if (live) {
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            int n = -2, f = -1, side = 0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) dx[k][d] = 0.0;
+            if (k < K) {
+                n = m.slot_nbr[k * C + c];
+                f = m.slot_face[k * C + c];
+                side = meta_isL(m.slot_meta[k * C + c]) ? 0 : 1;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) dx[k][d] = m.slot_dx[(k * 2 + d) * C + c];
+            }
+            hasn[k] = n >= 0;
+            nbc[k] = n >= 0 ? n : c;
+            fso[k] = f >= 0 ? side * NQ * F + f : -1;
+        }
+#pragma unroll
+        for (int i = 0; i < NC * DIM; ++i) g[i] = 0.0;
+        if (o.gradient == 1) {   // least squares, cone order (Gradient.hpp:330-346)
+#pragma unroll
+            for (int k = 0; k < KM; ++k) {
+                if (!hasn[k]) continue;
+                double wk[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) wk[d] = m.slot_w[(k * 2 + d) * C + c];
+                const double* wp = w + i0 * C;
+#pragma unroll
+                for (int i = 0; i < NC; ++i, wp += C) {
+                    if (i0 + i >= NQ) break;
+                    const double du = wp[nbc[k]] - wp[c];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) g[i * DIM + d] += wk[d] * du;
+                }
+            }
+        } else {                 // Green-Gauss, increasing original face order (Gradient.hpp:91-176)
+            const int ord = m.order[c];
+#pragma unroll
+            for (int j = 0; j < KM; ++j) {
+                if (j >= K) continue;
+                const int k = (ord >> (2 * j)) & 3;
+                const int f = m.slot_face[k * C + c];
+                if (f < 0) continue;
+                const int meta = m.slot_meta[k * C + c];
+                const int n = m.slot_nbr[k * C + c];
+                const double Nf[2] = {m.fnr[f], m.fnr[F + f]};
+                if (n >= 0) {
+                    double sN[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) sN[d] = meta_isL(meta) ? Nf[d] : -Nf[d];
+                    const double* wp = w + i0 * C;
+#pragma unroll
+                    for (int i = 0; i < NC; ++i, wp += C) {
+                        if (i0 + i >= NQ) break;
+                        const double fv = 0.5 * (wp[c] + wp[n]);
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) g[i * DIM + d] += fv * sN[d];
+                    }
+                } else if (meta_bc(meta) >= 0) {
+#pragma unroll
+                    for (int i = 0; i < NC; ++i) {
+                        if (i0 + i >= NQ) break;
+                        const double qb = qb_sh[k][i0 + i][lc];
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) g[i * DIM + d] += qb * Nf[d];
+                    }
+                }
+            }
+            const double v = m.vol[c];
+            if (v > 1e-15) {
+#pragma unroll
+                for (int i = 0; i < NC * DIM; ++i) g[i] /= v;
+            }
+        }
+        // pass 1: this part's alpha per face = min over its components
+        if (o.limiter) {
+            bool vac = false;   // VacuumLimiter: minimum depth (component 1) over the cell and its neighbours
+            if constexpr (NQ > 1) {
+                double mnh = wl[C + c];
+#pragma unroll
+                for (int k = 0; k < KM; ++k) {
+                    const double v = wl[C + nbc[k]];
+                    if (v < mnh) mnh = v;
+                }
+                vac = mnh < 1e-2;
+            }
+            if (vac) {
+#pragma unroll
+                for (int k = 0; k < KM; ++k) al[k] = 0.0;
+            } else {
+                const double* wp = wl + i0 * C;
+#pragma unroll
+                for (int i = 0; i < NC; ++i, wp += C) {
+                    if (i0 + i >= NQ) break;
+                    const double q = wp[c];
+                    double mn = q, mx = q;
+#pragma unroll
+                    for (int k = 0; k < KM; ++k) {
+                        const double v = wp[nbc[k]];
+                        if (v < mn) mn = v;
+                        if (v > mx) mx = v;
+                    }
+#pragma unroll
+                    for (int k = 0; k < KM; ++k) {
+                        if (fso[k] < 0) continue;
+                        double d = 0.0;
+#pragma unroll
+                        for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+                        const double qfu = q + d;
+                        const double dq = qfu - q;
+                        const bool pos = dq > 0;
+                        const double rr = (pos ? mx : mn) - q;
+                        const bool room = pos ? (mx > q) : (mn < q);
+                        const bool lim = !(pos ? (rr >= dq) : (rr <= dq));
+                        const bool small = fabs(dq) < 1e-12;
+                        double a = small ? 1.0 : (room ? 1.0 : 0.0);
+                        if (!small && room && lim) a = fmin(1.0, rr / dq);
+                        if (a < al[k]) al[k] = a;
+                    }
+                }
+            }
+        }
+    }
+    if (o.limiter) {   // the parts' minima meet (every thread of the block reaches this barrier)
+#pragma unroll
+        for (int k = 0; k < KM; ++k) al_sh[part][k][lc] = al[k];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            double a = 1.0;
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                const double v = al_sh[q][k][lc];
+                if (v < a) a = v;
+            }
+            al[k] = a;
+        }
+    }
+    if (!live) return;
+    // pass 2: this part's face states q + alpha * delta
+    const double* wp = wl + i0 * C;
+#pragma unroll
+    for (int i = 0; i < NC; ++i, wp += C) {
+        if (i0 + i >= NQ) break;
+        const double q = wp[c];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (fso[k] < 0) continue;
+            double d = 0.0;
+#pragma unroll
+            for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+            fs[fso[k] + (i0 + i) * F] = q + al[k] * d;
+        }
+    }
+}
+
 // Venkatakrishnan eps^2 = vol^(2/dim) (TransportStep.hpp:279), exact in 1-D and 2-D.
 template <int DIM>
 __host__ __device__ __forceinline__ double venkat_eps2(double v) {

@@ -387,6 +387,12 @@ int zsme_adjoint_phases(zsme_handle* h, double* ms3) {
     if (!ms3) return set_error(ZSME_ERR_ARG, "null output");
     return h->s->adjoint_phases(ms3);
 }
+int zsme_adjoint_overlapped(zsme_handle* h, int32_t* overlapped) {
+    CHECK_SINGLE(h);
+    if (!overlapped) return set_error(ZSME_ERR_ARG, "null output");
+    *overlapped = h->s->adjoint_overlapped() ? 1 : 0;
+    return ZSME_OK;
+}
 int zsme_get_launch(zsme_handle* h, int32_t* blocks) {
     CHECK_H(h);
     if (!blocks) return set_error(ZSME_ERR_ARG, "null output");

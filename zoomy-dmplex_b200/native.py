@@ -132,6 +132,7 @@ def load():
     I32 = ct.POINTER(ct.c_int32)
     lib.zsme_adjoint.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, I32, I32, I32, P, P, P, P, P, P]
     lib.zsme_adjoint_phases.argtypes = [vp, P]
+    lib.zsme_adjoint_overlapped.argtypes = [vp, I32]
     _lib = lib
     return lib
 

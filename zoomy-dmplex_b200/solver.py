@@ -201,6 +201,14 @@ class Solver:
         native.check(self.lib.zsme_adjoint_phases(self.h, _p(ms)))
         return {"forward": float(ms[0]), "replay": float(ms[1]), "reverse": float(ms[2])}
 
+    def adjoint_overlapped(self):
+        """Whether the last adjoint call overlapped its segment replays with
+        the reverse sweep; then "replay" in adjoint_phases() is the first
+        replay alone and "reverse" the rest of the reverse phase."""
+        v = ct.c_int32()
+        native.check(self.lib.zsme_adjoint_overlapped(self.h, ct.byref(v)))
+        return bool(v.value)
+
     def time(self):
         t, d = ct.c_double(), ct.c_double()
         native.check(self.lib.zsme_get_time(self.h, ct.byref(t), ct.byref(d)))
