@@ -124,16 +124,16 @@ def step_bytes_survey(nq):
 # DRAM bytes (read + write) per cell of one launch, from the ncu captures of
 # profiles/sme2d_l4_kernels_900.md (900x900 grid, 1,616,402 cells; mean of
 # two launches) in the launch configuration the autotuner picks at level 4:
-# separate face and gather kernels, the lean face-state kernel, the last
-# stage's gather inside finalize.  The streams scale with the cell count, so
+# separate face and gather kernels, the face-state kernel split over four
+# threads per cell, the last stage's gather inside finalize.  The streams scale with the cell count, so
 # a 1400x1400 launch moves these figures times its cells.
 NCU_DRAM_BYTES_PER_CELL = {
-    "sme2d_l4/prep": (453.5 + 431.4) * 1e6 / 1616402,
-    "sme2d_l4/flux": (544.7 + 652.5) * 1e6 / 1616402,
-    "sme2d_l4/gather": (1126.5 + 283.8) * 1e6 / 1616402,
-    "sme2d_l4/finalize+gather": (1123.3 + 296.2) * 1e6 / 1616402,
+    "sme2d_l4/prep": (436.6 + 425.4) * 1e6 / 1616402,
+    "sme2d_l4/flux": (544.7 + 652.4) * 1e6 / 1616402,
+    "sme2d_l4/gather": (1143.8 + 282.5) * 1e6 / 1616402,
+    "sme2d_l4/finalize+gather": (1123.1 + 297.0) * 1e6 / 1616402,
 }
-NCU_LAUNCH = {"tile_faces": 0, "fuse_final": 1, "prep_lean": 1}
+NCU_LAUNCH = {"tile_faces": 0, "fuse_final": 1, "prep_lean": 4}
 
 
 def traffic_per_cell_step(model, launch, stages):
