@@ -38,6 +38,8 @@ extern "C" {
 #define ZSME_ERR_STATE 4    /* non-finite state or negative depth detected */
 #define ZSME_ERR_MESH 5     /* inconsistent mesh connectivity */
 #define ZSME_ERR_LIMIT 6    /* a compiled size limit was exceeded */
+#define ZSME_ERR_SOLVE 7    /* an implicit step's Newton iteration did not converge; the state, time and
+                               step history are those before the step */
 
 /* Face boundary markers in zsme_mesh.face_bc */
 #define ZSME_FACE_INTERIOR (-1)
@@ -83,6 +85,11 @@ typedef struct zsme_mesh {
 #define ZSME_TIME_SPLITTING 0 /* "splitting": SSP-RK(s,2) transport, then the implicit source step */
 #define ZSME_TIME_IMEX 1      /* "imex": additive Runge-Kutta 2E (explicit transport, implicit source per
                                  cell; SolverStrategies.hpp:62-128) at the step's CFL dt */
+#define ZSME_TIME_IMPLICIT 2  /* "implicit": BDF (order 1 on the first step after a state is set, 2
+                                 after) of F = Xdot - S(X) - R(X), Newton with a matrix-free Jacobian
+                                 and GMRES preconditioned by the diagonal blocks of the reference's
+                                 assembled Jacobian (SolverStrategies.hpp:133-195) at the step's CFL
+                                 dt; single-instance handles, positivity "none" or "zhang_shu" */
 
 /* The solver keys of the reference's Settings (Settings.hpp:13-40) that change
  * the step. */
@@ -100,7 +107,7 @@ typedef struct zsme_settings {
     int32_t refresh_derivative_aux; /* solver.refresh_derivative_aux: before every state update, fill the
                                      plugin's derivative aux slots (its field-level update_aux_variables;
                                      Green-Gauss derivatives, TransportStep.hpp:161-192) */
-    int32_t time_integration;     /* ZSME_TIME_SPLITTING or ZSME_TIME_IMEX */
+    int32_t time_integration;     /* ZSME_TIME_SPLITTING, ZSME_TIME_IMEX or ZSME_TIME_IMPLICIT */
     int32_t reserved[3];
     double wet_dry_eps;           /* solver.wet_dry_eps (reference default 1e-2): dry threshold of the
                                      positivity variants, read only when positivity != NONE */
@@ -186,6 +193,28 @@ int zsme_stream_wait_copies(zsme_handle* h);
 /* F = dQ/dt of the transport for state X (TransportStep::FormRHS,
  * TransportStep.hpp:325-357).  Host AoS buffers, caller order. */
 int zsme_rhs(zsme_handle* h, double t, const double* x_aos, double* f_aos);
+/* The fully implicit strategy's residual F(t, X, Xdot) = Xdot - S(X) - R(X)
+ * (SolverStrategies.hpp:163-174 IFunctionWrapper: S the source at the
+ * clamped state, zero where the depth is below 1e-6, R = FormRHS).  Host AoS
+ * buffers [C][n_dof_q], caller order.  Needs time_integration
+ * ZSME_TIME_IMPLICIT and a single-instance handle. */
+int zsme_implicit_function(zsme_handle* h, double t, const double* x_aos, const double* xdot_aos, double* f_aos);
+/* The preconditioning matrix of the implicit strategy at (t, X, shift a)
+ * (ModularSolver::FormImplicitJacobian, ModularSolver.hpp:238-371): per cell
+ * a I - dS/dQ - dS/dAux dAux/dQ (a I where the clamped depth is below 1e-4)
+ * plus each face's forward-difference flux and fluctuation Jacobians at the
+ * cell states scaled by area / volume.  diag_blocks [C][n_dof_q][n_dof_q] in
+ * caller cell order (row-major blocks); face_blocks [F][2][n_dof_q][n_dof_q]
+ * per caller face: the block at (row cell face_cells[0], column
+ * face_cells[1]) and the one at (row face_cells[1], column face_cells[0]),
+ * zero for boundary faces.  Either pointer may be NULL. */
+int zsme_implicit_jacobian(zsme_handle* h, double t, const double* x_aos, double shift, double* diag_blocks,
+                           double* face_blocks);
+/* Counters of the last implicit step: Newton iterations, GMRES iterations
+ * (all Newton iterations), line-search halvings, and how Newton stopped (1:
+ * residual norm within tolerance, 2: update below 1e-8 of the state, 0:
+ * neither within 50 iterations). */
+int zsme_implicit_stats(zsme_handle* h, int32_t* stats4);
 /* Physical constraints on the resident state (MUSCLSolver.hpp:234-254):
  * update_variables clamp + update_aux_variables (TransportStep.hpp:196-230). */
 int zsme_update_state(zsme_handle* h);

@@ -121,6 +121,10 @@ struct OracleBase {
     // tangent-linear (dual-number) instances only: seed / read directions
     virtual void set_tangent(const double*, const double*) {}
     virtual void get_tangent(double*) const {}
+    // the fully implicit strategy (double instances only)
+    virtual void implicit_function(double, const double*, const double*, double*) {}
+    virtual void implicit_jacobian(double, const double*, double, double*, double*) {}
+    virtual int implicit_stats(int*) const { return 0; }
 };
 
 // S: the scalar of state and parameters -- double, Dual<1> for the
@@ -911,8 +915,422 @@ par_for(C, [&](int c, int) {
         return st.cfl * best;
     }
 
+    // ------------------------------------------------- fully implicit strategy
+    // SolverStrategies.hpp:133-195 (TSBDF order 2, IFunctionWrapper,
+    // IJacobianWrapper with a matrix-free Jacobian and the assembled matrix as
+    // the preconditioner's source) restated without PETSc: the residual and
+    // the matrix blocks follow ModularSolver.hpp:82-124 and 238-371 operation
+    // for operation; the Newton-Krylov iteration (Newton with backtracking,
+    // left-preconditioned restarted GMRES with classical Gram-Schmidt, the
+    // matrix's diagonal blocks as block-Jacobi preconditioner, Walker-Pernice
+    // differencing) and BDF with variable-step coefficients are the same
+    // algorithm as the GPU's, since PETSc's own SNES/KSP/TSAdapt histories
+    // cannot be reproduced without PETSc.  Double precision only.
+    bool imp_have_prev = false;
+    double imp_h_prev = 0.0;
+    int imp_stats_v[4] = {0, 0, 0, 0};
+    std::vector<double> imp_xn, imp_xnm1;
+
+    // f = (Xdot - S(x)) - R(x); xdot given, or (c0 x + c1 xn + c2 xnm1) / h
+    void imp_residual(double t, const std::vector<double>& x, const double* xdot, const double* bdf,
+                      const std::vector<double>* xn, const std::vector<double>* xnm1, std::vector<double>& f) {
+        if constexpr (std::is_same<T, double>::value) {
+            std::vector<double> R;
+            form_rhs(t, x, R);
+            f.resize(x.size());
+            par_for(C, [&](int c, int) {
+                double S[NQ];
+                imex_source_cell(&x[(size_t)c * NQ], &A[(size_t)c * NA], S);
+                for (int i = 0; i < NQ; ++i) {
+                    const size_t id = (size_t)c * NQ + i;
+                    const double xd = xdot ? xdot[id]
+                                           : (bdf[0] * x[id] + bdf[1] * (*xn)[id] + bdf[2] * (*xnm1)[id]) / bdf[3];
+                    f[id] = (xd - S[i]) - R[id];
+                }
+            });
+        }
+    }
+    // ComputeFaceJacobian_FD / ComputeBoundaryJacobian_FD (ModularSolver.hpp:130-236)
+    void imp_face_fd(const double* qL, const double* qR, const double* aL, const double* aR, const double* nh,
+                     double* JLL, double* JLR, double* JRL, double* JRR) const {
+        if constexpr (std::is_same<T, double>::value) {
+            const double eps = 1e-7;
+            const double X0[3] = {0, 0, 0};
+            const double* p = params.data();
+            auto Fb = N::numerical_flux(qL, qR, aL, aR, p, nh);
+            auto NCb = N::numerical_fluctuations(qL, qR, aL, aR, p, nh);
+            for (int j = 0; j < NQ; ++j) {
+                double qp[NQ], ap[NA + 1];
+                for (int k = 0; k < NQ; ++k) qp[k] = qL[k];
+                for (int k = 0; k < NA; ++k) ap[k] = aL[k];
+                qp[j] += eps;
+                if (NA > 0) {
+                    auto ra = M::update_aux_variables(qp, ap, p, 0.0, X0);
+                    for (int k = 0; k < NA; ++k) ap[k] = ra[k];
+                }
+                auto Fp = N::numerical_flux(qp, qR, ap, aR, p, nh);
+                auto NCp = N::numerical_fluctuations(qp, qR, ap, aR, p, nh);
+                for (int i = 0; i < NQ; ++i) {
+                    double dFlux = (Fp[i] - Fb[i]) / eps;
+                    JLL[i * NQ + j] += dFlux;
+                    JRL[i * NQ + j] -= dFlux;
+                    JLL[i * NQ + j] += (NCp[NQ + i] - NCb[NQ + i]) / eps;
+                    JRL[i * NQ + j] += (NCp[i] - NCb[i]) / eps;
+                }
+            }
+            for (int j = 0; j < NQ; ++j) {
+                double qp[NQ], ap[NA + 1];
+                for (int k = 0; k < NQ; ++k) qp[k] = qR[k];
+                for (int k = 0; k < NA; ++k) ap[k] = aR[k];
+                qp[j] += eps;
+                if (NA > 0) {
+                    auto ra = M::update_aux_variables(qp, ap, p, 0.0, X0);
+                    for (int k = 0; k < NA; ++k) ap[k] = ra[k];
+                }
+                auto Fp = N::numerical_flux(qL, qp, aL, ap, p, nh);
+                auto NCp = N::numerical_fluctuations(qL, qp, aL, ap, p, nh);
+                for (int i = 0; i < NQ; ++i) {
+                    double dFlux = (Fp[i] - Fb[i]) / eps;
+                    JLR[i * NQ + j] += dFlux;
+                    JRR[i * NQ + j] -= dFlux;
+                    JLR[i * NQ + j] += (NCp[NQ + i] - NCb[NQ + i]) / eps;
+                    JRR[i * NQ + j] += (NCp[i] - NCb[i]) / eps;
+                }
+            }
+        }
+    }
+    void imp_boundary_fd(const double* qL, const double* aL, const double* nh, const double* xf, double t, int bc,
+                         double* JLL) const {
+        if constexpr (std::is_same<T, double>::value) {
+            const double eps = 1e-7;
+            const double* p = params.data();
+            auto qRb = M::boundary_conditions(bc, qL, aL, p, nh, xf, t, 0.0);
+            double aRb[NA + 1];
+            if (NA > 0) {
+                auto ra = M::update_aux_variables(qRb.data, aL, p, t, xf);
+                for (int k = 0; k < NA; ++k) aRb[k] = ra[k];
+            }
+            auto Fb = N::numerical_flux(qL, qRb.data, aL, aRb, p, nh);
+            auto NCb = N::numerical_fluctuations(qL, qRb.data, aL, aRb, p, nh);
+            for (int j = 0; j < NQ; ++j) {
+                double qp[NQ], ap[NA + 1], ar[NA + 1];
+                for (int k = 0; k < NQ; ++k) qp[k] = qL[k];
+                for (int k = 0; k < NA; ++k) ap[k] = aL[k];
+                qp[j] += eps;
+                if (NA > 0) {
+                    auto ra = M::update_aux_variables(qp, ap, p, t, xf);
+                    for (int k = 0; k < NA; ++k) ap[k] = ra[k];
+                }
+                auto qr = M::boundary_conditions(bc, qp, ap, p, nh, xf, t, 0.0);
+                if (NA > 0) {
+                    auto ra = M::update_aux_variables(qr.data, ap, p, t, xf);
+                    for (int k = 0; k < NA; ++k) ar[k] = ra[k];
+                }
+                auto Fp = N::numerical_flux(qp, qr.data, ap, ar, p, nh);
+                auto NCp = N::numerical_fluctuations(qp, qr.data, ap, ar, p, nh);
+                for (int i = 0; i < NQ; ++i) {
+                    double dFlux = (Fp[i] - Fb[i]) / eps;
+                    JLL[i * NQ + j] += dFlux;
+                    JLL[i * NQ + j] += (NCp[NQ + i] - NCb[NQ + i]) / eps;
+                }
+            }
+        }
+    }
+    // FormImplicitJacobian (ModularSolver.hpp:238-371) at (t, x, a): Pd [C][NQ NQ]
+    // diagonal blocks, Po [F][2][NQ NQ] the (L, R) and (R, L) blocks; entries
+    // start at zero and take the source blocks, then the faces in order
+    void imp_assemble(double t, const std::vector<double>& xg, double a, std::vector<double>& Pd,
+                      std::vector<double>& Po) {
+        if constexpr (std::is_same<T, double>::value) {
+            constexpr int Q2 = NQ * NQ;
+            std::vector<double> xl = xg, al = A;
+            update_state_vec(xl, al);
+            Pd.assign((size_t)C * Q2, 0.0);
+            Po.assign((size_t)F * 2 * Q2, 0.0);
+            const double* p = params.data();
+            par_for(C, [&](int c, int) {
+                const double* qc = &xl[(size_t)c * NQ];
+                const double* ac = &al[(size_t)c * NA];
+                double J[Q2];
+                if (NQ > 1 && qc[1] < 1e-4) {
+                    for (int e = 0; e < Q2; ++e) J[e] = 0.0;
+                    for (int i = 0; i < NQ; ++i) J[i * NQ + i] = a;
+                } else {
+                    auto dSdQ = M::source_jacobian_wrt_variables(qc, ac, p);
+                    auto dSdA = M::source_jacobian_wrt_aux_variables(qc, ac, p);
+                    double dAdQ[NA * NQ + 1];
+                    aux_jacobian<NQ, NA>(qc, ac, p, dAdQ);
+                    for (int i = 0; i < NQ; ++i)
+                        for (int j = 0; j < NQ; ++j) {
+                            double val = i == j ? a : 0.0;
+                            double dSource = dSdQ[i * NQ + j];
+                            for (int k = 0; k < NA; ++k) dSource += dSdA[i * NA + k] * dAdQ[k * NQ + j];
+                            J[i * NQ + j] = val - dSource;
+                        }
+                }
+                for (int e = 0; e < Q2; ++e) Pd[(size_t)c * Q2 + e] += J[e];
+            });
+            for (int f = 0; f < F; ++f) {
+                double area = 0;
+                for (int d = 0; d < DIM; ++d) area += fn[2 * f + d] * fn[2 * f + d];
+                area = std::sqrt(area);
+                if (area <= 1e-15) continue;
+                double nh[3] = {0, 0, 0};
+                for (int d = 0; d < DIM; ++d) nh[d] = fn[2 * f + d] / area;
+                const int L = fcell[2 * f], R = fcell[2 * f + 1];
+                const double* qL = &xl[(size_t)L * NQ];
+                const double* aL = &al[(size_t)L * NA];
+                if (R >= 0) {
+                    double JLL[Q2] = {0}, JLR[Q2] = {0}, JRL[Q2] = {0}, JRR[Q2] = {0};
+                    imp_face_fd(qL, &xl[(size_t)R * NQ], aL, &al[(size_t)R * NA], nh, JLL, JLR, JRL, JRR);
+                    const double fL = area / vol[L], fR = area / vol[R];
+                    for (int e = 0; e < Q2; ++e) {
+                        JLL[e] *= fL; JLR[e] *= fL;
+                        JRL[e] *= fR; JRR[e] *= fR;
+                    }
+                    for (int e = 0; e < Q2; ++e) Pd[(size_t)L * Q2 + e] += JLL[e];
+                    for (int e = 0; e < Q2; ++e) Po[((size_t)f * 2 + 0) * Q2 + e] += JLR[e];
+                    for (int e = 0; e < Q2; ++e) Po[((size_t)f * 2 + 1) * Q2 + e] += JRL[e];
+                    for (int e = 0; e < Q2; ++e) Pd[(size_t)R * Q2 + e] += JRR[e];
+                } else if (fbc[f] >= 0) {
+                    double JLL[Q2] = {0};
+                    const double xf[3] = {fc[2 * f], fc[2 * f + 1], 0.0};
+                    imp_boundary_fd(qL, aL, nh, xf, t, fbc[f], JLL);
+                    const double fL = area / vol[L];
+                    for (int e = 0; e < Q2; ++e) JLL[e] *= fL;
+                    for (int e = 0; e < Q2; ++e) Pd[(size_t)L * Q2 + e] += JLL[e];
+                }
+            }
+        }
+    }
+    // LU with partial pivoting of every diagonal block (identity where a pivot
+    // vanishes), and the block solve z = D^-1 r
+    static void imp_block_lu(std::vector<double>& lu, std::vector<int>& piv, int C) {
+        constexpr int Q2 = NQ * NQ;
+        piv.assign((size_t)C * NQ, 0);
+        par_for(C, [&](int c, int) {
+            double* A_ = &lu[(size_t)c * Q2];
+            int* pv = &piv[(size_t)c * NQ];
+            bool ok = true;
+            for (int k = 0; k < NQ; ++k) {
+                int mr = k;
+                double mv = std::fabs(A_[k * NQ + k]);
+                for (int i = k + 1; i < NQ; ++i) {
+                    const double v = std::fabs(A_[i * NQ + k]);
+                    if (v > mv) { mv = v; mr = i; }
+                }
+                pv[k] = mr;
+                if (mr != k)
+                    for (int j = 0; j < NQ; ++j) std::swap(A_[k * NQ + j], A_[mr * NQ + j]);
+                const double pkk = A_[k * NQ + k];
+                if (!(mv > 0.0) || !std::isfinite(pkk)) { ok = false; break; }
+                for (int i = k + 1; i < NQ; ++i) {
+                    const double l = A_[i * NQ + k] / pkk;
+                    A_[i * NQ + k] = l;
+                    for (int j = k + 1; j < NQ; ++j) A_[i * NQ + j] -= l * A_[k * NQ + j];
+                }
+            }
+            if (!ok) {
+                for (int e = 0; e < Q2; ++e) A_[e] = 0.0;
+                for (int i = 0; i < NQ; ++i) { A_[i * NQ + i] = 1.0; pv[i] = i; }
+            }
+        });
+    }
+    static void imp_block_solve(const std::vector<double>& lu, const std::vector<int>& piv, int C,
+                                std::vector<double>& z) {
+        constexpr int Q2 = NQ * NQ;
+        par_for(C, [&](int c, int) {
+            const double* A_ = &lu[(size_t)c * Q2];
+            const int* pv = &piv[(size_t)c * NQ];
+            double* b = &z[(size_t)c * NQ];
+            for (int k = 0; k < NQ; ++k) {
+                const int mr = pv[k];
+                if (mr != k) std::swap(b[k], b[mr]);
+                for (int i = k + 1; i < NQ; ++i) b[i] -= A_[i * NQ + k] * b[k];
+            }
+            for (int i = NQ - 1; i >= 0; --i) {
+                double s = b[i];
+                for (int j = i + 1; j < NQ; ++j) s -= A_[i * NQ + j] * b[j];
+                b[i] = s / A_[i * NQ + i];
+            }
+        });
+    }
+    static double imp_dot(const std::vector<double>& a, const std::vector<double>& b) {
+        double s = 0.0;
+        for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+        return s;
+    }
+    // One BDF step of size h (the GPU's algorithm; see the header comment);
+    // false when Newton did not converge (the state is then the step's start)
+    bool imp_step(double t0, double h) {
+        if constexpr (std::is_same<T, double>::value) {
+            const size_t n = X.size();
+            if (imp_have_prev) std::swap(imp_xn, imp_xnm1);
+            imp_xn = X;
+            double bdf[4] = {1.0, -1.0, 0.0, h};
+            const std::vector<double>* xnm1 = &imp_xn;
+            if (imp_have_prev) {
+                const double w = h / imp_h_prev;
+                bdf[0] = (1.0 + 2.0 * w) / (1.0 + w);
+                bdf[1] = -(1.0 + w);
+                bdf[2] = w * w / (1.0 + w);
+                xnm1 = &imp_xnm1;
+            }
+            const double shift = bdf[0] / h, t1 = t0 + h;
+            auto resid = [&](const std::vector<double>& x, std::vector<double>& f) {
+                imp_residual(t1, x, nullptr, bdf, &imp_xn, xnm1, f);
+            };
+            std::vector<double> Fv, Ft, Pd, Po, lu, xt(n), d(n), w(n), r0(n), r(n);
+            std::vector<int> piv;
+            resid(X, Fv);
+            double fnorm = std::sqrt(imp_dot(Fv, Fv));
+            const double fnorm0 = fnorm;
+            int it = 0, gm_total = 0, halvings = 0, conv = 0;
+            constexpr int m = 30;
+            for (; it < 50; ++it) {
+                if (fnorm <= 1e-4 || (it > 0 && fnorm <= 1e-3 * fnorm0)) { conv = 1; break; }
+                if (!std::isfinite(fnorm)) break;
+                const double xnorm = std::sqrt(imp_dot(X, X));
+                imp_assemble(t1, X, shift, Pd, Po);
+                lu = Pd;
+                imp_block_lu(lu, piv, C);
+                // M^-1 J v by differencing
+                auto apply = [&](const std::vector<double>& v, std::vector<double>& out) {
+                    const double vnorm = std::sqrt(imp_dot(v, v));
+                    out.assign(n, 0.0);
+                    if (!(vnorm > 0.0)) return;
+                    const double hv = 1.4901161193847656e-08 * std::sqrt(1.0 + xnorm) / vnorm;
+                    for (size_t i = 0; i < n; ++i) xt[i] = 1.0 * X[i] + hv * v[i];
+                    resid(xt, Ft);
+                    for (size_t i = 0; i < n; ++i) out[i] = (Ft[i] - Fv[i]) / hv;
+                    imp_block_solve(lu, piv, C, out);
+                };
+                // GMRES
+                int gm = 0;
+                std::fill(d.begin(), d.end(), 0.0);
+                for (size_t i = 0; i < n; ++i) r0[i] = -1.0 * Fv[i];
+                imp_block_solve(lu, piv, C, r0);
+                double beta = std::sqrt(imp_dot(r0, r0));
+                if (beta > 0.0) {
+                    const double tol = std::max(1e-5 * beta, 1e-50);
+                    std::vector<std::vector<double>> V(m + 1, std::vector<double>(n));
+                    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+                    const std::vector<double>* rp = &r0;
+                    while (true) {
+                        for (size_t i = 0; i < n; ++i) V[0][i] = (1.0 / beta) * (*rp)[i];
+                        std::fill(g.begin(), g.end(), 0.0);
+                        g[0] = beta;
+                        int j = 0;
+                        bool done = false;
+                        for (; j < m;) {
+                            apply(V[j], w);
+                            double hcol[m + 1];
+                            for (int i = 0; i <= j; ++i) hcol[i] = imp_dot(V[i], w);
+                            for (size_t e = 0; e < n; ++e) {
+                                double s = w[e];
+                                for (int i = 0; i <= j; ++i) s -= hcol[i] * V[i][e];
+                                w[e] = s;
+                            }
+                            const double hn = std::sqrt(imp_dot(w, w));
+                            if (hn > 0.0)
+                                for (size_t e = 0; e < n; ++e) V[j + 1][e] = (1.0 / hn) * w[e];
+                            for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
+                            H[(size_t)(j + 1) * m + j] = hn;
+                            for (int i = 0; i < j; ++i) {
+                                const double a0 = H[(size_t)i * m + j], a1 = H[(size_t)(i + 1) * m + j];
+                                H[(size_t)i * m + j] = cs[i] * a0 + sn[i] * a1;
+                                H[(size_t)(i + 1) * m + j] = -sn[i] * a0 + cs[i] * a1;
+                            }
+                            const double hjj = H[(size_t)j * m + j], hj1 = H[(size_t)(j + 1) * m + j];
+                            const double den = std::sqrt(hjj * hjj + hj1 * hj1);
+                            cs[j] = den > 0.0 ? hjj / den : 1.0;
+                            sn[j] = den > 0.0 ? hj1 / den : 0.0;
+                            H[(size_t)j * m + j] = den;
+                            H[(size_t)(j + 1) * m + j] = 0.0;
+                            g[j + 1] = -sn[j] * g[j];
+                            g[j] = cs[j] * g[j];
+                            ++gm;
+                            ++j;
+                            const double res = std::fabs(g[j]);
+                            if (res <= tol || !(hn > 0.0) || gm >= 10000 || !std::isfinite(res)) {
+                                done = true;
+                                break;
+                            }
+                        }
+                        for (int i = j - 1; i >= 0; --i) {
+                            double s = g[i];
+                            for (int k = i + 1; k < j; ++k) s -= H[(size_t)i * m + k] * y[k];
+                            y[i] = H[(size_t)i * m + i] != 0.0 ? s / H[(size_t)i * m + i] : 0.0;
+                        }
+                        for (size_t e = 0; e < n; ++e) {
+                            double s = d[e];
+                            for (int k = 0; k < j; ++k) s += y[k] * V[k][e];
+                            d[e] = s;
+                        }
+                        if (done) break;
+                        apply(d, w);
+                        for (size_t e = 0; e < n; ++e) r[e] = 1.0 * r0[e] + -1.0 * w[e];
+                        rp = &r;
+                        beta = std::sqrt(imp_dot(r, r));
+                        if (!(beta > tol)) break;
+                    }
+                }
+                gm_total += gm;
+                // backtracking
+                double lambda = 1.0, ft = 0.0;
+                bool descent = false;
+                for (int ls = 0; ls < 10; ++ls) {
+                    for (size_t i = 0; i < n; ++i) xt[i] = 1.0 * X[i] + lambda * d[i];
+                    resid(xt, Ft);
+                    ft = std::sqrt(imp_dot(Ft, Ft));
+                    if (ft <= (1.0 - 1e-4 * lambda) * fnorm) { descent = true; break; }
+                    lambda *= 0.5;
+                    ++halvings;
+                }
+                if (!descent) break;
+                X = xt;
+                Fv = Ft;
+                fnorm = ft;
+                const double dnorm = std::sqrt(imp_dot(d, d)), xn2 = std::sqrt(imp_dot(X, X));
+                if (lambda * dnorm <= 1e-8 * xn2) { conv = fnorm <= 1e-4 || fnorm <= 1e-3 * fnorm0 ? 1 : 2; ++it; break; }
+            }
+            imp_stats_v[0] = it;
+            imp_stats_v[1] = gm_total;
+            imp_stats_v[2] = halvings;
+            imp_stats_v[3] = conv;
+            if (!conv) {   // nothing of the step is kept; the driver stops
+                X = imp_xn;
+                if (imp_have_prev) std::swap(imp_xn, imp_xnm1);
+                return false;
+            }
+            imp_h_prev = h;
+            imp_have_prev = true;
+        }
+        return true;
+    }
+    int implicit_stats(int* out) const override {
+        for (int i = 0; i < 4; ++i) out[i] = imp_stats_v[i];
+        return 0;
+    }
+    void implicit_function(double t, const double* x, const double* xdot, double* f) override {
+        if constexpr (std::is_same<T, double>::value) {
+            std::vector<double> xv(x, x + (size_t)C * NQ), fv;
+            imp_residual(t, xv, xdot, nullptr, nullptr, nullptr, fv);
+            for (size_t i = 0; i < fv.size(); ++i) f[i] = fv[i];
+        }
+    }
+    void implicit_jacobian(double t, const double* x, double a, double* diag, double* faces) override {
+        if constexpr (std::is_same<T, double>::value) {
+            std::vector<double> xv(x, x + (size_t)C * NQ), Pd, Po;
+            imp_assemble(t, xv, a, Pd, Po);
+            if (diag) std::copy(Pd.begin(), Pd.end(), diag);
+            if (faces) std::copy(Po.begin(), Po.end(), faces);
+        }
+    }
+
     // ------------------------------------------------------------ driver
     void set_state(const double* q, double t) override {
+        imp_have_prev = false;
         X.assign(q, q + (size_t)C * NQ);
         std::fill(A.begin(), A.end(), 0.0);
         time = t;
@@ -1074,13 +1492,18 @@ par_for(C, [&](int c, int) {
             std::vector<T> Xs;
             if (mood) Xs = X;
             const bool imex = st.time_integration == ZSME_TIME_IMEX;
+            const bool implicit = st.time_integration == ZSME_TIME_IMPLICIT;
             if (imex) imex_step(t0, d0);
-            else ts_step(t0, d0);
+            else if (implicit) {
+                if (!imp_step(t0, d0)) break;   // Newton failed: the step is not taken
+            } else {
+                ts_step(t0, d0);
+            }
             ph(zsme_flops::FINAL);
             time = t0 + d0;
             update_state_vec(X, A);                            // EnforcePhysicalConstraints
             if (mood) mood_override(t0, d0, Xs);
-            if (st.source && !imex) {                          // IMEX carries the source in its stages
+            if (st.source && !imex && !implicit) {             // IMEX and implicit carry the source
                 source_solve(d0);
                 update_state_vec(X, A);
             }
@@ -1295,6 +1718,15 @@ int oracle_step_dt(void* h, int n, const double* dts) { ((OracleBase*)h)->step(n
 int oracle_get_time(void* h, double* t, double* dt) { ((OracleBase*)h)->get_time(t, dt); return 0; }
 int oracle_set_params(void* h, const double* p) { ((OracleBase*)h)->set_params(p); return 0; }
 int oracle_newton_unconverged(void* h) { return ((OracleBase*)h)->newton_unconverged(); }
+int oracle_implicit_function(void* h, double t, const double* x, const double* xdot, double* f) {
+    ((OracleBase*)h)->implicit_function(t, x, xdot, f);
+    return 0;
+}
+int oracle_implicit_jacobian(void* h, double t, const double* x, double a, double* diag, double* faces) {
+    ((OracleBase*)h)->implicit_jacobian(t, x, a, diag, faces);
+    return 0;
+}
+int oracle_implicit_stats(void* h, int* out) { return ((OracleBase*)h)->implicit_stats(out); }
 long long oracle_mood_cells(void* h) { return ((OracleBase*)h)->mood_cells(); }
 
 }  // extern "C"

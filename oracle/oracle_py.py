@@ -64,6 +64,9 @@ def load(ref: bool = False):
     lib.oracle_flux_vjp.argtypes = [ct.c_char_p, P, P, P, P, P, P, P, P]
     lib.oracle_create_counting.argtypes = [ct.c_char_p, vp, vp, P, ct.POINTER(vp)]
     lib.oracle_flop_counts.argtypes = [ct.POINTER(ct.c_longlong)]
+    lib.oracle_implicit_function.argtypes = [vp, ct.c_double, P, P, P]
+    lib.oracle_implicit_jacobian.argtypes = [vp, ct.c_double, P, ct.c_double, P, P]
+    lib.oracle_implicit_stats.argtypes = [vp, ct.POINTER(ct.c_int)]
     _libs[path] = lib
     return lib
 
@@ -136,6 +139,7 @@ class Oracle:
         self.nq = self.info["n_dof_q"]
         self.na = self.info["n_dof_qaux"]
         self.C = mesh_abi["n_cells"]
+        self.F = mesh_abi["n_faces"]
         self._mesh_keep = native.make_mesh_struct(mesh_abi)
         self._settings = settings_struct
         h = ct.c_void_p()
@@ -183,6 +187,29 @@ class Oracle:
 
     def update_state(self):
         self.lib.oracle_update_state(self.h)
+
+    def implicit_function(self, x, xdot, t=0.0):
+        """F(t, X, Xdot) = Xdot - S(X) - R(X) of the fully implicit strategy."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.C, self.nq)
+        xd = np.ascontiguousarray(xdot, dtype=np.float64).reshape(self.C, self.nq)
+        f = np.zeros_like(x)
+        self.lib.oracle_implicit_function(self.h, float(t), _p(x), _p(xd), _p(f))
+        return f
+
+    def implicit_jacobian(self, x, shift, t=0.0):
+        """The implicit strategy's assembled matrix at (t, X, shift): diagonal
+        blocks [C, nq, nq] and per face the (L, R) and (R, L) blocks [F, 2, nq, nq]."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.C, self.nq)
+        d = np.zeros((self.C, self.nq, self.nq))
+        o = np.zeros((self.F, 2, self.nq, self.nq))
+        self.lib.oracle_implicit_jacobian(self.h, float(t), _p(x), float(shift), _p(d), _p(o))
+        return d, o
+
+    def implicit_stats(self):
+        """Last implicit step: Newton iterations, GMRES iterations, halvings, stop reason."""
+        v = (ct.c_int * 4)()
+        self.lib.oracle_implicit_stats(self.h, v)
+        return [int(x) for x in v]
 
     def source(self, dt):
         self.lib.oracle_source(self.h, float(dt))
@@ -265,6 +292,7 @@ class TangentOracle(Oracle):
         self.nq = self.info["n_dof_q"]
         self.na = self.info["n_dof_qaux"]
         self.C = mesh_abi["n_cells"]
+        self.F = mesh_abi["n_faces"]
         self._mesh_keep = native.make_mesh_struct(mesh_abi)
         self._settings = settings_struct
         h = ct.c_void_p()

@@ -1,0 +1,135 @@
+"""The fully implicit strategy on the GPU against the oracle (the CPU
+restatement of SolverStrategies.hpp:133-195 and ModularSolver.hpp:82-124,
+238-371 without PETSc):
+
+* the residual F(t, X, Xdot) = Xdot - S(X) - R(X) and the assembled
+  matrix's diagonal and face blocks equal the oracle's bit for bit, on
+  triangles, a mixed mesh and the 1-D model, at orders 1 and 2;
+* steps at the oracle's dts follow the oracle's Newton-Krylov iteration:
+  the same Newton iteration counts, GMRES counts within one, and states
+  within 1e-7 relative (the two differ only in the order of the GMRES inner
+  products, whose rounding the loose Newton tolerance the reference sets
+  lets through: about 1e-9 after six steps);
+* free-running steps take the same CFL dts;
+* where Newton fails (the limited second-order residual at a flat field) the
+  call returns ZSME_ERR_SOLVE and leaves state and time as they were;
+* ensembles and MOOD are rejected with the implicit strategy.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import oracle_py as O
+from zoomy_dmplex_b200 import cases, mesh as meshmod, models, native
+from zoomy_dmplex_b200.solver import BatchSolver, Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(c):
+    names, vals = models.parameter_table(c.model)
+    for k, v in c.params.items():
+        vals[names.index(k)] = v
+    return np.array(vals)
+
+
+def _case_1d():
+    x = np.linspace(-1.5, 1.5, 121)
+    m = meshmod.interval(x)
+    xc = m.cell_centroid[:, 0]
+    b = 0.2 * np.exp(-xc ** 2 / 0.05)
+    h = 1.0 - b + 0.1 * np.exp(-(xc + 0.5) ** 2 / 0.01)
+    q = np.stack([b, h, 0.3 * h], axis=1)
+    return cases.Case("1d", "sme1d_l0_malpasset", m, q, cases.default_settings(),
+                      dict(g=9.81, rho=1.0, nu=1.0, lambda_s=0.2, e_x=0.01), 20)
+
+
+CASES = {"l0": lambda: cases.plain_l0(16), "l2": lambda: cases.level2(16), "l4": lambda: cases.roofline_l4(12),
+         "1d": _case_1d, "mixed": lambda: cases.mixed_level2(10)}
+
+
+def _pair(c, **kw):
+    st = dataclasses.replace(c.settings, time_integration="implicit", **kw)
+    p = _params(c)
+    g = Solver(c.model, c.mesh, st, p)
+    o = O.Oracle(c.model, c.mesh.as_abi_arrays(), st.to_struct(), p)
+    g.set_state(c.q0)
+    o.set_state(c.q0)
+    return g, o
+
+
+def _perturbed(c, seed=3):
+    rng = np.random.default_rng(seed)
+    x = c.q0.copy()
+    x[:, 2:] += 0.05 * rng.standard_normal(x[:, 2:].shape) * x[:, 1:2]
+    return x
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("order", [1, 2])
+def test_residual_and_matrix_bitwise(name, order):
+    c = CASES[name]()
+    g, o = _pair(c, reconstruction_order=order)
+    x = _perturbed(c)
+    xdot = np.random.default_rng(1).standard_normal(x.shape)
+    assert np.array_equal(g.implicit_function(x, xdot, t=0.25), o.implicit_function(x, xdot, t=0.25))
+    dg, fg = g.implicit_jacobian(x, 312.5, t=0.25)
+    do, fo = o.implicit_jacobian(x, 312.5, t=0.25)
+    assert np.array_equal(dg, do)
+    assert np.array_equal(fg, fo)
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("name,kw", [("l2", {"reconstruction_order": 1}), ("l2", {"limiter": "none"}),
+                                     ("l0", {"reconstruction_order": 1}), ("1d", {"reconstruction_order": 1}),
+                                     ("mixed", {"limiter": "none"}), ("l4", {"reconstruction_order": 1})])
+def test_steps_follow_the_oracle(name, kw):
+    c = CASES[name]()
+    g, o = _pair(c, **kw)
+    for k in range(8):
+        _, dt = o.time()
+        o.step(1)
+        g.step(1, dts=[dt])
+        so, sg = o.implicit_stats(), g.implicit_stats()
+        assert so[3] > 0 and sg[3] > 0, (k, so, sg)
+        assert sg[0] == so[0], (k, so, sg)
+        assert abs(sg[1] - so[1]) <= 1, (k, so, sg)
+        assert _rel(g.get_state(), o.get_state()) <= 1e-7, k
+    tg, dg = g.time()
+    to, do = o.time()
+    assert abs(tg - to) <= 1e-13 * to and abs(dg - do) <= 1e-8 * do
+
+
+def test_free_running_cfl_steps():
+    c = CASES["l2"]()
+    g, o = _pair(c, reconstruction_order=1, cfl=2.0)
+    g.step(6)
+    o.step(6)
+    assert abs(g.time()[0] - o.time()[0]) <= 1e-9 * o.time()[0]
+    assert _rel(g.get_state(), o.get_state()) <= 1e-8
+
+
+def test_failed_newton_returns_an_error_and_keeps_the_state():
+    c = cases.level2(6)
+    g, o = _pair(c)
+    q0, t0 = g.get_state(), g.time()
+    with pytest.raises(native.ZsmeError) as e:
+        g.step(1)
+    assert e.value.code == 7
+    assert g.implicit_stats()[3] == 0
+    assert np.array_equal(g.get_state(), q0) and g.time() == t0
+    o.step(1)
+    assert o.implicit_stats()[3] == 0
+
+
+def test_rejected_combinations():
+    c = cases.level2(6)
+    st = dataclasses.replace(c.settings, time_integration="implicit")
+    with pytest.raises(native.ZsmeError):
+        BatchSolver(c.model, [c.mesh, c.mesh], st, [_params(c)] * 2)
+    with pytest.raises(native.ZsmeError):
+        Solver(c.model, c.mesh, dataclasses.replace(st, positivity="mood"), _params(c))

@@ -116,7 +116,7 @@ def test_stiff_source_stays_bounded():
     assert np.abs(q[:, 2:]).max() < np.abs(c.q0[:, 2:]).max()
 
 
-def test_implicit_strategy_is_rejected():
+def test_unknown_strategy_is_rejected():
     c = cases.level2(8)
     with pytest.raises(ValueError, match="implicit"):
-        dataclasses.replace(c.settings, time_integration="implicit").to_struct()
+        dataclasses.replace(c.settings, time_integration="rosenbrock").to_struct()

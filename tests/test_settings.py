@@ -26,8 +26,9 @@ def test_from_json_defaults_and_mapping(tmp_path):
 
 def test_rejects_out_of_path_strategies():
     with pytest.raises(ValueError):
-        SolverSettings(time_integration="implicit").to_struct()
+        SolverSettings(time_integration="explicit_only").to_struct()
     assert SolverSettings(time_integration="imex").to_struct().time_integration == native.ZSME_TIME_IMEX
+    assert SolverSettings(time_integration="implicit").to_struct().time_integration == native.ZSME_TIME_IMPLICIT
     assert SolverSettings().to_struct().refresh_derivative_aux == 1     # the reference's default
     with pytest.raises(ValueError):
         SolverSettings(positivity="bogus").to_struct()

@@ -120,6 +120,9 @@ class SolverBase {
     // device times of the last adjoint call's forward pass, replays and reverse sweep (ms)
     virtual int adjoint_phases(double* ms) = 0;
     virtual bool adjoint_overlapped() const = 0;
+    virtual int implicit_function(double t, const double* x_aos, const double* xdot_aos, double* f_aos) = 0;
+    virtual int implicit_jacobian(double t, const double* x_aos, double a, double* diag, double* offdiag) = 0;
+    virtual int implicit_stats(int* out) const = 0;
 };
 
 }  // namespace zsme

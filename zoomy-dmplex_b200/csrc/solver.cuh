@@ -20,6 +20,7 @@
 #include "source_kernels.cuh"
 #include "adjoint_kernels.cuh"
 #include "imex_kernels.cuh"
+#include "implicit_kernels.cuh"
 #include "zsme.h"
 
 namespace zsme {
@@ -78,6 +79,18 @@ class Solver final : public SolverBase {
     DevBuf<double> xs_;  // MOOD: the state at the start of the step
     DevBuf<int> mood_list_;  // MOOD: the troubled cells of the step (count in iscal_[6])
     DevBuf<double> imex_g_[3], imex_s_[3], imex_y_[2];   // IMEX: stage right-hand sides, implicit derivatives, states
+    // fully implicit strategy (allocated with the handle when selected):
+    // history X_n, X_{n-1}; residual F, trial residual, trial state, transport
+    // RHS, Krylov basis [31][NQ C], work, Newton update, preconditioned
+    // residual at zero, restart residual; clamped state and its aux; the
+    // assembled diagonal blocks, their LU factors and pivots; the face blocks
+    DevBuf<double> imp_xn_, imp_xnm1_, imp_F_, imp_Ft_, imp_xt_, imp_R_, imp_V_, imp_w_, imp_d_, imp_r0_, imp_r_;
+    DevBuf<double> imp_xl_, imp_al_, imp_pd_, imp_lu_, imp_fj_, imp_part_, imp_red_;
+    DevBuf<int> imp_piv_;
+    bool imp_have_prev_ = false;   // a previous implicit step exists: BDF2
+    double imp_h_prev_ = 0.0;
+    int imp_stats_[4] = {0, 0, 0, 0};   // last step: Newton iterations, GMRES iterations, halvings, converged
+    static constexpr int kImpRestart = 30;
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
     DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag, [5] deferred finalize cells, [6] MOOD cells
@@ -246,8 +259,14 @@ class Solver final : public SolverBase {
         if (pm_.dim != DIM) return set_error(ZSME_ERR_ARG, "mesh dimension does not match the model");
         if (st_.reconstruction_order >= 2 && st_.ssp_stages < 2)
             return set_error(ZSME_ERR_ARG, "ssp_stages must be >= 2");
-        if (st_.time_integration != ZSME_TIME_SPLITTING && st_.time_integration != ZSME_TIME_IMEX)
-            return set_error(ZSME_ERR_ARG, "time_integration must be ZSME_TIME_SPLITTING or ZSME_TIME_IMEX");
+        if (st_.time_integration != ZSME_TIME_SPLITTING && st_.time_integration != ZSME_TIME_IMEX &&
+            st_.time_integration != ZSME_TIME_IMPLICIT)
+            return set_error(ZSME_ERR_ARG,
+                             "time_integration must be ZSME_TIME_SPLITTING, ZSME_TIME_IMEX or ZSME_TIME_IMPLICIT");
+        if (st_.time_integration == ZSME_TIME_IMPLICIT &&
+            (n_inst_ != 1 || st_.positivity == ZSME_POSITIVITY_MOOD))
+            return set_error(ZSME_ERR_ARG, "the implicit strategy needs a single-instance handle and positivity "
+                                           "other than \"mood\"");
         if (st_.positivity != ZSME_POSITIVITY_NONE && (NQ < 3 || !(st_.wet_dry_eps >= 0)))
             return set_error(ZSME_ERR_ARG, "positivity variants need a [b, h, momentum...] model and wet_dry_eps >= 0");
         // Zhang-Shu positivity holds for CFL <= 1/6 at order 2 (MUSCLSolver.hpp:33-38)
@@ -301,6 +320,20 @@ class Solver final : public SolverBase {
                 ZSME_CUDA(imex_s_[j].alloc((size_t)NQ * C));
             }
             for (int j = 0; j < 2; ++j) ZSME_CUDA(imex_y_[j].alloc((size_t)NQ * C));
+        }
+        if (st_.time_integration == ZSME_TIME_IMPLICIT) {
+            const size_t n = (size_t)NQ * C;
+            for (auto* b : {&imp_xn_, &imp_xnm1_, &imp_F_, &imp_Ft_, &imp_xt_, &imp_R_, &imp_w_, &imp_d_, &imp_r0_,
+                            &imp_r_, &imp_xl_})
+                ZSME_CUDA(b->alloc(n));
+            ZSME_CUDA(imp_V_.alloc((size_t)(kImpRestart + 1) * n));
+            ZSME_CUDA(imp_al_.alloc((size_t)NA * C + 1));
+            ZSME_CUDA(imp_pd_.alloc((size_t)NQ * NQ * C));
+            ZSME_CUDA(imp_lu_.alloc((size_t)NQ * NQ * C));
+            ZSME_CUDA(imp_piv_.alloc((size_t)NQ * C));
+            ZSME_CUDA(imp_fj_.alloc((size_t)4 * NQ * NQ * F));
+            ZSME_CUDA(imp_part_.alloc((size_t)(kImpRestart + 1) * imp_dot_blocks()));
+            ZSME_CUDA(imp_red_.alloc((size_t)kImpRestart + 2));
         }
         if (st_.positivity == ZSME_POSITIVITY_MOOD) {
             ZSME_CUDA(xs_.alloc((size_t)NQ * C));
@@ -430,6 +463,7 @@ class Solver final : public SolverBase {
     // After a state (and its time) is in place: aux reset, constraints, then
     // dt_start = max(ComputeTimeStep, min_dt) (MUSCLSolver.hpp:51-54, 103).
     int enqueue_loaded(int inst, int c0, int cn) {
+        imp_have_prev_ = false;   // the implicit strategy restarts at BDF order 1
         for (int k = 0; k < NA; ++k)
             ZSME_CUDA(cudaMemsetAsync(aux_.p + (size_t)k * pm_.C + c0, 0, cn * sizeof(double), stream_));
         ZSME_CUDA(cudaMemsetAsync(active_.p + inst, 0, sizeof(int), stream_));
@@ -901,6 +935,296 @@ class Solver final : public SolverBase {
                            3};
         imex_final_kernel<M><<<nb, 128, 0, stream_>>>(md_, tb, x_.p, dt, act);
     }
+    // ------------------------------------------------ fully implicit strategy
+    // The Newton-Krylov iteration of one BDF step runs on the host around the
+    // kernels of implicit_kernels.cuh; every reduction it reads is a
+    // deterministic two-pass sum on the device.
+    int imp_dot_blocks() const { return std::max(1, std::min(2 * sm_count_, blocks_for((long long)NQ * pm_.C, 256))); }
+    long long imp_n() const { return (long long)NQ * pm_.C; }
+    // V_k . w for k < nk into imp_red_ (device) and out (host, when given)
+    int imp_dots(const double* V, long long ld, int nk, const double* w, double* out) {
+        const int nb = imp_dot_blocks();
+        imp_multi_dot_kernel<<<nb, 256, 0, stream_>>>(imp_n(), nk, V, ld, w, imp_part_.p);
+        imp_reduce_kernel<<<1, 64, 0, stream_>>>(nk, nb, imp_part_.p, imp_red_.p);
+        ZSME_CUDA(cudaGetLastError());
+        if (out) {
+            ZSME_CUDA(cudaMemcpyAsync(out, imp_red_.p, nk * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+            ZSME_CUDA(cudaStreamSynchronize(stream_));
+        }
+        return ZSME_OK;
+    }
+    int imp_norm(const double* w, double& out) {
+        double d = 0.0;
+        int rc = imp_dots(w, 0, 1, w, &d);
+        out = std::sqrt(d);
+        return rc;
+    }
+    void imp_lincomb(double a, const double* x, double b, const double* y, double* out) {
+        imp_lincomb_kernel<<<blocks_for(imp_n(), 256), 256, 0, stream_>>>(imp_n(), a, x, b, y, out);
+    }
+    // F(t, y, Xdot) = (Xdot - S(y)) - R(y) (IFunctionWrapper) into f
+    void imp_residual(double t, const double* y, const BdfTerms& b, double* f) {
+        const int C = pm_.C;
+        clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, y, aux_.p, params_.p, wl_.p);
+        launch_prep(y, wl_.p, nullptr);
+        launch_flux(MODE_RHS, t, nullptr, 0.0, nullptr, imp_R_.p, nullptr, nullptr, nullptr);
+        imp_residual_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, y, aux_.p, params_.p, imp_R_.p, b, f);
+    }
+    // P(t, y, a) (FormImplicitJacobian): the state clamped with its aux
+    // (UpdateState), the face blocks, the diagonal blocks in assembly order
+    void imp_assemble(double t, const double* y, double a) {
+        const int C = pm_.C, F = pm_.F;
+        imp_update_state_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, y, aux_.p, params_.p, imp_xl_.p,
+                                                                          imp_al_.p);
+        imp_face_jac_kernel<M, N><<<blocks_for(F, 128), 128, 0, stream_>>>(md_, imp_xl_.p, imp_al_.p, params_.p, t,
+                                                                          imp_fj_.p);
+        imp_cell_jac_kernel<M><<<blocks_for(C, 64), 64, 0, stream_>>>(md_, imp_xl_.p, imp_al_.p, params_.p, a,
+                                                                      imp_fj_.p, imp_pd_.p);
+    }
+    // out = D^-1 (F(X + hv v) - F(X)) / hv, hv = sqrt(eps) sqrt(1 + |X|) / |v| (the
+    // Walker-Pernice differencing parameter of PETSc's matrix-free Jacobian)
+    int imp_apply(double t, const BdfTerms& b, double xnorm, const double* v, double* out) {
+        double vnorm = 0.0;
+        int rc = imp_norm(v, vnorm);
+        if (rc) return rc;
+        if (!(vnorm > 0.0)) {
+            ZSME_CUDA(cudaMemsetAsync(out, 0, imp_n() * sizeof(double), stream_));
+            return ZSME_OK;
+        }
+        const double hv = 1.4901161193847656e-08 * std::sqrt(1.0 + xnorm) / vnorm;
+        imp_lincomb(1.0, x_.p, hv, v, imp_xt_.p);
+        imp_residual(t, imp_xt_.p, b, imp_Ft_.p);
+        imp_diffquot_kernel<<<blocks_for(imp_n(), 256), 256, 0, stream_>>>(imp_n(), imp_Ft_.p, imp_F_.p, hv, out);
+        imp_block_solve_kernel<NQ><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(pm_.C, imp_lu_.p, imp_piv_.p, out, out);
+        ZSME_CUDA(cudaGetLastError());
+        return ZSME_OK;
+    }
+    // Left-preconditioned restarted GMRES (restart 30, classical Gram-Schmidt,
+    // Givens rotations, zero initial guess) for (D^-1 J) d = D^-1 (-F) into
+    // imp_d_; stops when the preconditioned residual is below 1e-5 of its
+    // initial norm (PETSc's KSP defaults) or after 10000 iterations.
+    int imp_gmres(double t, const BdfTerms& b, double xnorm, int& its) {
+        constexpr int m = kImpRestart;
+        const long long n = imp_n();
+        const int C = pm_.C;
+        its = 0;
+        ZSME_CUDA(cudaMemsetAsync(imp_d_.p, 0, n * sizeof(double), stream_));
+        imp_lincomb(-1.0, imp_F_.p, 0.0, nullptr, imp_r0_.p);
+        imp_block_solve_kernel<NQ><<<blocks_for(C, 128), 128, 0, stream_>>>(C, imp_lu_.p, imp_piv_.p, imp_r0_.p,
+                                                                            imp_r0_.p);
+        double beta = 0.0;
+        int rc = imp_norm(imp_r0_.p, beta);
+        if (rc) return rc;
+        if (!(beta > 0.0)) return ZSME_OK;
+        const double tol = std::max(1e-5 * beta, 1e-50);
+        const double* r = imp_r0_.p;
+        std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 1);
+        while (true) {
+            imp_lincomb(1.0 / beta, r, 0.0, nullptr, imp_V_.p);
+            std::fill(g.begin(), g.end(), 0.0);
+            g[0] = beta;
+            int j = 0;
+            bool done = false;
+            for (; j < m;) {
+                double* vj = imp_V_.p + (size_t)j * n;
+                double* w = imp_w_.p;
+                if ((rc = imp_apply(t, b, xnorm, vj, w))) return rc;
+                if ((rc = imp_dots(imp_V_.p, n, j + 1, w, hcol.data()))) return rc;
+                imp_multi_axpy_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, j + 1, imp_V_.p, n, imp_red_.p, w);
+                double hn = 0.0;
+                if ((rc = imp_norm(w, hn))) return rc;
+                if (hn > 0.0) imp_lincomb(1.0 / hn, w, 0.0, nullptr, imp_V_.p + (size_t)(j + 1) * n);
+                for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
+                H[(size_t)(j + 1) * m + j] = hn;
+                for (int i = 0; i < j; ++i) {   // earlier rotations on the new column
+                    const double a0 = H[(size_t)i * m + j], a1 = H[(size_t)(i + 1) * m + j];
+                    H[(size_t)i * m + j] = cs[i] * a0 + sn[i] * a1;
+                    H[(size_t)(i + 1) * m + j] = -sn[i] * a0 + cs[i] * a1;
+                }
+                const double hjj = H[(size_t)j * m + j], hj1 = H[(size_t)(j + 1) * m + j];
+                const double den = std::sqrt(hjj * hjj + hj1 * hj1);
+                cs[j] = den > 0.0 ? hjj / den : 1.0;
+                sn[j] = den > 0.0 ? hj1 / den : 0.0;
+                H[(size_t)j * m + j] = den;
+                H[(size_t)(j + 1) * m + j] = 0.0;
+                g[j + 1] = -sn[j] * g[j];
+                g[j] = cs[j] * g[j];
+                ++its;
+                ++j;
+                const double res = std::fabs(g[j]);
+                if (res <= tol || !(hn > 0.0) || its >= 10000 || !std::isfinite(res)) {
+                    done = true;
+                    break;
+                }
+            }
+            // y = H^-1 g over the j columns taken; d += V y
+            for (int i = j - 1; i >= 0; --i) {
+                double s = g[i];
+                for (int k = i + 1; k < j; ++k) s -= H[(size_t)i * m + k] * y[k];
+                y[i] = H[(size_t)i * m + i] != 0.0 ? s / H[(size_t)i * m + i] : 0.0;
+            }
+            ZSME_CUDA(cudaMemcpyAsync(imp_red_.p, y.data(), j * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            imp_multi_add_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, j, imp_V_.p, n, imp_red_.p, imp_d_.p);
+            ZSME_CUDA(cudaGetLastError());
+            if (done) break;
+            // restart: r = D^-1 (-F) - D^-1 J d
+            if ((rc = imp_apply(t, b, xnorm, imp_d_.p, imp_w_.p))) return rc;
+            imp_lincomb(1.0, imp_r0_.p, -1.0, imp_w_.p, imp_r_.p);
+            r = imp_r_.p;
+            if ((rc = imp_norm(r, beta))) return rc;
+            if (!(beta > tol)) break;
+        }
+        return ZSME_OK;
+    }
+    // One BDF step of size h from the state in x_ at time t0 (TSBDF order 2,
+    // order 1 on the first step after a state is set; variable-step
+    // coefficients with w = h / h_prev): Newton on F(t0 + h, X, Xdot(X)) = 0 from
+    // X = X_n, stopping when |F| <= 1e-4 or |F| <= 1e-3 |F_0| (the SNES
+    // tolerances MUSCLSolver.hpp:107-110 sets) or the update is below 1e-8 |X|,
+    // at most 50 iterations; each iteration assembles the diagonal blocks at X,
+    // solves by GMRES and backtracks (halving, at most 10 times) until
+    // |F| <= (1 - 1e-4 lambda) |F_prev|; no such lambda ends Newton unconverged.
+    int imp_step(double t0, double h) {
+        const long long n = imp_n();
+        if (imp_have_prev_) std::swap(imp_xn_.p, imp_xnm1_.p);
+        ZSME_CUDA(cudaMemcpyAsync(imp_xn_.p, x_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        BdfTerms b{nullptr, imp_xn_.p, imp_xn_.p, 1.0, -1.0, 0.0, h};
+        if (imp_have_prev_) {
+            const double w = h / imp_h_prev_;
+            b = BdfTerms{nullptr, imp_xn_.p, imp_xnm1_.p, (1.0 + 2.0 * w) / (1.0 + w), -(1.0 + w),
+                         w * w / (1.0 + w), h};
+        }
+        const double shift = b.c0 / h;
+        const double t1 = t0 + h;
+        imp_residual(t1, x_.p, b, imp_F_.p);
+        double fnorm = 0.0;
+        int rc = imp_norm(imp_F_.p, fnorm);
+        if (rc) return rc;
+        const double fnorm0 = fnorm;
+        int it = 0, gm_total = 0, halvings = 0, conv = 0;
+        for (; it < 50; ++it) {
+            if (fnorm <= 1e-4 || (it > 0 && fnorm <= 1e-3 * fnorm0)) { conv = 1; break; }
+            if (!std::isfinite(fnorm)) break;
+            double xnorm = 0.0;
+            if ((rc = imp_norm(x_.p, xnorm))) return rc;
+            imp_assemble(t1, x_.p, shift);
+            imp_block_lu_kernel<NQ><<<blocks_for(pm_.C, 64), 64, 0, stream_>>>(pm_.C, imp_pd_.p, imp_lu_.p,
+                                                                              imp_piv_.p);
+            int gm = 0;
+            if ((rc = imp_gmres(t1, b, xnorm, gm))) return rc;
+            gm_total += gm;
+            double lambda = 1.0, ft = 0.0;
+            bool descent = false;
+            for (int ls = 0; ls < 10; ++ls) {
+                imp_lincomb(1.0, x_.p, lambda, imp_d_.p, imp_xt_.p);
+                imp_residual(t1, imp_xt_.p, b, imp_Ft_.p);
+                if ((rc = imp_norm(imp_Ft_.p, ft))) return rc;
+                if (ft <= (1.0 - 1e-4 * lambda) * fnorm) { descent = true; break; }
+                lambda *= 0.5;
+                ++halvings;
+            }
+            if (!descent) break;   // the line search failed: Newton diverged
+            ZSME_CUDA(cudaMemcpyAsync(x_.p, imp_xt_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(imp_F_.p, imp_Ft_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            fnorm = ft;
+            double dnorm = 0.0, xn2 = 0.0;
+            if ((rc = imp_norm(imp_d_.p, dnorm)) || (rc = imp_norm(x_.p, xn2))) return rc;
+            if (lambda * dnorm <= 1e-8 * xn2) { conv = fnorm <= 1e-4 || fnorm <= 1e-3 * fnorm0 ? 1 : 2; ++it; break; }
+        }
+        imp_stats_[0] = it;
+        imp_stats_[1] = gm_total;
+        imp_stats_[2] = halvings;
+        imp_stats_[3] = conv;
+        if (!conv) {   // as PETSc's TSStep after a diverged SNES: nothing of the step is kept
+            ZSME_CUDA(cudaMemcpyAsync(x_.p, imp_xn_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            if (imp_have_prev_) std::swap(imp_xn_.p, imp_xnm1_.p);
+            ZSME_CUDA(cudaStreamSynchronize(stream_));
+            return set_error(ZSME_ERR_SOLVE, "implicit step: Newton did not converge in 50 iterations");
+        }
+        imp_h_prev_ = h;
+        imp_have_prev_ = true;
+        return ZSME_OK;
+    }
+    // MUSCLSolver::Run with the implicit strategy: dt clamped to t_end, the BDF
+    // step, the constraints (EnforcePhysicalConstraints), PostStep's
+    // constraints and the next CFL dt.  Host-driven: no CUDA graph.
+    int implicit_steps(int nsteps, const double* dts_host) {
+        if (dts_host) {
+            ZSME_CUDA(dts_.alloc((size_t)nsteps));
+            ZSME_CUDA(cudaMemcpyAsync(dts_.p, dts_host, nsteps * sizeof(double), cudaMemcpyHostToDevice, stream_));
+            ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));
+        }
+        for (int i = 0; i < nsteps; ++i) {
+            StepDev sd = step_dev(dts_host ? dts_.p : nullptr);
+            begin_step_kernel<<<1, 32, 0, stream_>>>(sd, 0, 1);
+            double t0 = 0.0, h = 0.0;
+            int act = 0;
+            ZSME_CUDA(cudaMemcpyAsync(&t0, t_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(&h, dt_step_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(&act, active_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+            ZSME_CUDA(cudaStreamSynchronize(stream_));
+            if (!act) break;
+            int rc = imp_step(t0, h);
+            if (rc) return rc;
+            launch_finalize(sd, nullptr, FIN_PRE | FIN_POST | FIN_DT | FIN_WRITE);
+            end_step_kernel<<<1, 32, 0, stream_>>>(sd, 0, 1, 1, 0.0, nullptr);
+            ZSME_CUDA(cudaGetLastError());
+        }
+        x_clamped_ = true;
+        return collect_profile();
+    }
+    int implicit_stats(int* out) const override {
+        for (int i = 0; i < 4; ++i) out[i] = imp_stats_[i];
+        return ZSME_OK;
+    }
+    // F(t, X, Xdot) of caller states (AoS, caller order) into f_aos
+    int implicit_function(double t, const double* x_aos, const double* xdot_aos, double* f_aos) override {
+        if (st_.time_integration != ZSME_TIME_IMPLICIT)
+            return set_error(ZSME_ERR_ARG, "the handle's time_integration is not ZSME_TIME_IMPLICIT");
+        const int C = pm_.C;
+        const size_t bytes = (size_t)NQ * C * sizeof(double);
+        ZSME_CUDA(cudaMemcpyAsync(tmp_b_.p, x_aos, bytes, cudaMemcpyHostToDevice, stream_));
+        aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(tmp_b_.p, imp_xt_.p, old_of_new_.p, 0, C, C, NQ);
+        ZSME_CUDA(cudaMemcpyAsync(tmp_b_.p, xdot_aos, bytes, cudaMemcpyHostToDevice, stream_));
+        aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(tmp_b_.p, imp_w_.p, old_of_new_.p, 0, C, C, NQ);
+        const BdfTerms b{imp_w_.p, nullptr, nullptr, 0.0, 0.0, 0.0, 1.0};
+        imp_residual(t, imp_xt_.p, b, imp_Ft_.p);
+        ZSME_CUDA(cudaGetLastError());
+        return get_soa(0, imp_Ft_.p, NQ, f_aos, false);
+    }
+    // P(t, X, a) of a caller state: diagonal blocks [C][NQ][NQ] in caller
+    // cell order, and per original face its blocks (row cell L, column R) and
+    // (row R, column L), [F][2][NQ][NQ] (zero for boundary faces)
+    int implicit_jacobian(double t, const double* x_aos, double a, double* diag, double* offdiag) override {
+        if (st_.time_integration != ZSME_TIME_IMPLICIT)
+            return set_error(ZSME_ERR_ARG, "the handle's time_integration is not ZSME_TIME_IMPLICIT");
+        const int C = pm_.C, F = pm_.F;
+        constexpr int Q2 = NQ * NQ;
+        ZSME_CUDA(cudaMemcpyAsync(tmp_b_.p, x_aos, (size_t)NQ * C * sizeof(double), cudaMemcpyHostToDevice, stream_));
+        aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(tmp_b_.p, imp_xt_.p, old_of_new_.p, 0, C, C, NQ);
+        imp_assemble(t, imp_xt_.p, a);
+        ZSME_CUDA(cudaGetLastError());
+        std::vector<double> pd((size_t)Q2 * C), fj((size_t)4 * Q2 * F);
+        ZSME_CUDA(cudaMemcpyAsync(pd.data(), imp_pd_.p, pd.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ZSME_CUDA(cudaMemcpyAsync(fj.data(), imp_fj_.p, fj.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        ZSME_CUDA(cudaStreamSynchronize(stream_));
+        if (diag)
+            for (int c = 0; c < C; ++c) {
+                const int o = pm_.old_of_new[c];
+                for (int e = 0; e < Q2; ++e) diag[(size_t)o * Q2 + e] = pd[(size_t)e * C + c];
+            }
+        if (offdiag)
+            for (int f = 0; f < F; ++f) {
+                const int o = pm_.face_old_of_new[f];
+                const bool interior = pm_.face_R[f] >= 0 && pm_.farea[f] > 1e-15;
+                for (int e = 0; e < Q2; ++e) {
+                    // the matrix entry: zero plus the one block added there
+                    offdiag[((size_t)o * 2 + 0) * Q2 + e] = interior ? 0.0 + fj[((size_t)f * 4 + 1) * Q2 + e] : 0.0;
+                    offdiag[((size_t)o * 2 + 1) * Q2 + e] = interior ? 0.0 + fj[((size_t)f * 4 + 2) * Q2 + e] : 0.0;
+                }
+            }
+        return ZSME_OK;
+    }
     int launches_per_step() const override {
         if (st_.time_integration == ZSME_TIME_IMEX) {
             const int per_rhs = (lc_.tile_faces > 0 ? 2 : 3) + (deriv_.n ? 1 : 0);
@@ -918,6 +1242,11 @@ class Solver final : public SolverBase {
     int step(int nsteps, const double* dts_host) override {
         if (nsteps <= 0) return ZSME_OK;
         if (dts_host && n_inst_ != 1) return set_error(ZSME_ERR_ARG, "imposed dts need a single-instance handle");
+        if (st_.time_integration == ZSME_TIME_IMPLICIT) {
+            ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 4 * sizeof(int), stream_));
+            ZSME_CUDA(cudaMemsetAsync(iscal_.p + 7, 0, sizeof(int), stream_));
+            return implicit_steps(nsteps, dts_host);
+        }
         ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 4 * sizeof(int), stream_));
         ZSME_CUDA(cudaMemsetAsync(iscal_.p + 7, 0, sizeof(int), stream_));
         // x_ is constrained after set_state, update_state and every step (update_variables is a
@@ -958,6 +1287,8 @@ class Solver final : public SolverBase {
     int step_device_dts(int nsteps, const double* d_dts) override {
         if (nsteps <= 0) return ZSME_OK;
         if (n_inst_ != 1) return set_error(ZSME_ERR_ARG, "imposed dts need a single-instance handle");
+        if (st_.time_integration == ZSME_TIME_IMPLICIT)
+            return set_error(ZSME_ERR_ARG, "device-resident dts need an explicit or IMEX time integration");
         ZSME_CUDA(cudaMemsetAsync(iscal_.p + 1, 0, 4 * sizeof(int), stream_));
         ZSME_CUDA(cudaMemsetAsync(iscal_.p + 7, 0, sizeof(int), stream_));
         ZSME_CUDA(cudaMemsetAsync(iscal_.p, 0, sizeof(int), stream_));   // index into d_dts

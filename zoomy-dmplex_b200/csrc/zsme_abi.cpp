@@ -222,6 +222,24 @@ int zsme_rhs(zsme_handle* h, double t, const double* x, double* f) {
     if (!x || !f) return set_error(ZSME_ERR_ARG, "null buffer");
     return h->s->rhs(t, x, f);
 }
+int zsme_implicit_function(zsme_handle* h, double t, const double* x, const double* xdot, double* f) {
+    CHECK_SINGLE(h);
+    if (!x || !xdot || !f) return set_error(ZSME_ERR_ARG, "null buffer");
+    return h->s->implicit_function(t, x, xdot, f);
+}
+int zsme_implicit_jacobian(zsme_handle* h, double t, const double* x, double shift, double* diag, double* faces) {
+    CHECK_SINGLE(h);
+    if (!x) return set_error(ZSME_ERR_ARG, "null buffer");
+    return h->s->implicit_jacobian(t, x, shift, diag, faces);
+}
+int zsme_implicit_stats(zsme_handle* h, int32_t* stats) {
+    CHECK_SINGLE(h);
+    if (!stats) return set_error(ZSME_ERR_ARG, "null output");
+    int v[4];
+    int rc = h->s->implicit_stats(v);
+    for (int i = 0; i < 4; ++i) stats[i] = v[i];
+    return rc;
+}
 int zsme_update_state(zsme_handle* h) {
     CHECK_H(h);
     return h->s->update_state();

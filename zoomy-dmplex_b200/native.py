@@ -16,8 +16,8 @@ LIB_PATH = os.path.join(PKG, "libzsme.so")
 ZSME_LIMITER_NONE, ZSME_LIMITER_TVD = 0, 1
 ZSME_GRADIENT_GREEN_GAUSS, ZSME_GRADIENT_LSQ = 0, 1
 ZSME_POSITIVITY_NONE, ZSME_POSITIVITY_ZHANG_SHU, ZSME_POSITIVITY_MOOD = 0, 1, 2
-ZSME_TIME_SPLITTING, ZSME_TIME_IMEX = 0, 1
-TIME_INTEGRATION = {"splitting": ZSME_TIME_SPLITTING, "imex": ZSME_TIME_IMEX}
+ZSME_TIME_SPLITTING, ZSME_TIME_IMEX, ZSME_TIME_IMPLICIT = 0, 1, 2
+TIME_INTEGRATION = {"splitting": ZSME_TIME_SPLITTING, "imex": ZSME_TIME_IMEX, "implicit": ZSME_TIME_IMPLICIT}
 POSITIVITY = {"none": ZSME_POSITIVITY_NONE, "zhang_shu": ZSME_POSITIVITY_ZHANG_SHU, "mood": ZSME_POSITIVITY_MOOD}
 KERNEL_KINDS = ("begin_step", "prep", "flux", "finalize", "end_step", "gather", "finalize_fallback", "mood")
 
@@ -103,6 +103,9 @@ def load():
     lib.zsme_get_state_async.argtypes = [vp, vp]
     lib.zsme_stream_wait_copies.argtypes = [vp]
     lib.zsme_rhs.argtypes = [vp, ct.c_double, P, P]
+    lib.zsme_implicit_function.argtypes = [vp, ct.c_double, P, P, P]
+    lib.zsme_implicit_jacobian.argtypes = [vp, ct.c_double, P, ct.c_double, P, P]
+    lib.zsme_implicit_stats.argtypes = [vp, ct.POINTER(ct.c_int32)]
     lib.zsme_update_state.argtypes = [vp]
     lib.zsme_source.argtypes = [vp, ct.c_double]
     lib.zsme_compute_dt.argtypes = [vp, P]

@@ -19,8 +19,11 @@ How the reference interprets the strings, and so how they map here:
 * ``time_integration``: ``"splitting"`` (explicit transport, then the implicit
   source step) or ``"imex"`` (the additive Runge-Kutta scheme 2E of the
   reference's IMEX strategy, explicit transport and implicit source in every
-  stage, at the step's CFL dt); ``"implicit"`` (BDF2 with matrix-free Newton)
-  is rejected;
+  stage, at the step's CFL dt) or ``"implicit"`` (the fully implicit strategy:
+  BDF2 of the transport and the source together, Newton with a matrix-free
+  Jacobian and GMRES preconditioned by the diagonal blocks of the reference's
+  assembled Jacobian, at the step's CFL dt; single meshes, positivity other
+  than ``"mood"``);
 * ``refresh_derivative_aux`` (reference default true): before each state
   update the plugin's derivative aux slots are refilled with Green-Gauss
   derivatives of the state (``TransportStep.hpp:161-202``); plugins without
@@ -56,8 +59,8 @@ class SolverSettings:
 
     def to_struct(self) -> native.ZsmeSettings:
         if self.time_integration not in native.TIME_INTEGRATION:
-            raise ValueError("time_integration %r is not on this path ('splitting' or 'imex'; the fully implicit "
-                             "BDF2 + matrix-free Newton strategy is not built)" % self.time_integration)
+            raise ValueError("time_integration must be 'splitting', 'imex' or 'implicit', not %r"
+                             % self.time_integration)
         if self.positivity not in native.POSITIVITY:
             raise ValueError("positivity must be one of %s" % sorted(native.POSITIVITY))
         if self.gradient not in ("least_squares", "green_gauss"):

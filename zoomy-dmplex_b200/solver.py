@@ -139,6 +139,32 @@ class Solver:
         native.check(self.lib.zsme_rhs(self.h, float(t), _p(x), _p(f)))
         return f
 
+    def implicit_function(self, x: np.ndarray, xdot: np.ndarray, t: float = 0.0) -> np.ndarray:
+        """F(t, X, Xdot) = Xdot - S(X) - R(X) of the fully implicit strategy
+        (IFunctionWrapper, SolverStrategies.hpp:163-174)."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.C, self.nq)
+        xd = np.ascontiguousarray(xdot, dtype=np.float64).reshape(self.C, self.nq)
+        f = np.empty_like(x)
+        native.check(self.lib.zsme_implicit_function(self.h, float(t), _p(x), _p(xd), _p(f)))
+        return f
+
+    def implicit_jacobian(self, x: np.ndarray, shift: float, t: float = 0.0):
+        """The implicit strategy's assembled matrix at (t, X, shift)
+        (FormImplicitJacobian, ModularSolver.hpp:238-371): diagonal blocks
+        [C, nq, nq] and per face the (L, R) and (R, L) blocks [F, 2, nq, nq]."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(self.C, self.nq)
+        d = np.empty((self.C, self.nq, self.nq))
+        o = np.empty((self.mesh.n_faces, 2, self.nq, self.nq))
+        native.check(self.lib.zsme_implicit_jacobian(self.h, float(t), _p(x), float(shift), _p(d), _p(o)))
+        return d, o
+
+    def implicit_stats(self):
+        """Last implicit step: Newton iterations, GMRES iterations, line-search
+        halvings, stop reason (1 residual, 2 update size, 0 neither)."""
+        v = (ct.c_int32 * 4)()
+        native.check(self.lib.zsme_implicit_stats(self.h, v))
+        return [int(x) for x in v]
+
     def update_state(self):
         native.check(self.lib.zsme_update_state(self.h))
 
