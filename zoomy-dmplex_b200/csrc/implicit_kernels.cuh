@@ -344,6 +344,36 @@ __global__ void __launch_bounds__(128) imp_update_state_kernel(MeshDev m, const 
 }
 
 // ------------------------------------------------------------ vector kernels
+// The matrix-free Jacobian's differencing parameter from the device dot v.v:
+// hv = sqrt(eps) sqrt(1 + |X|) / |v| (0 for a zero vector)
+static __global__ void imp_hv_kernel(const double* __restrict__ vv, double xnorm, double* __restrict__ hv) {
+    const double vn = sqrt(*vv);
+    *hv = vn > 0.0 ? 1.4901161193847656e-08 * sqrt(1.0 + xnorm) / vn : 0.0;
+}
+// out = 1.0 x + hv v, hv a device scalar
+static __global__ void imp_perturb_kernel(long long n, const double* __restrict__ x, const double* __restrict__ v,
+                                          const double* __restrict__ hv, double* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = 1.0 * x[i] + *hv * v[i];
+}
+// out = (ft - f0) / hv, zero when hv is zero
+static __global__ void imp_diffquot_dev_kernel(long long n, const double* __restrict__ ft,
+                                               const double* __restrict__ f0, const double* __restrict__ hv,
+                                               double* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double h = *hv;
+    out[i] = h != 0.0 ? (ft[i] - f0[i]) / h : 0.0;
+}
+// out = (1.0 / sqrt(ww)) w where ww = w.w > 0 (the next Arnoldi vector)
+static __global__ void imp_normalize_kernel(long long n, const double* __restrict__ ww, const double* __restrict__ w,
+                                            double* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double hn = sqrt(*ww);
+    if (hn > 0.0) out[i] = (1.0 / hn) * w[i];
+}
 // out = (ft - f0) / h (the matrix-free Jacobian's difference quotient)
 static __global__ void imp_diffquot_kernel(long long n, const double* __restrict__ ft, const double* __restrict__ f0,
                                            double h, double* __restrict__ out) {

@@ -333,7 +333,7 @@ class Solver final : public SolverBase {
             ZSME_CUDA(imp_piv_.alloc((size_t)NQ * C));
             ZSME_CUDA(imp_fj_.alloc((size_t)4 * NQ * NQ * F));
             ZSME_CUDA(imp_part_.alloc((size_t)(kImpRestart + 1) * imp_dot_blocks()));
-            ZSME_CUDA(imp_red_.alloc((size_t)kImpRestart + 2));
+            ZSME_CUDA(imp_red_.alloc((size_t)kImpRestart + 8));
         }
         if (st_.positivity == ZSME_POSITIVITY_MOOD) {
             ZSME_CUDA(xs_.alloc((size_t)NQ * C));
@@ -941,14 +941,16 @@ class Solver final : public SolverBase {
     // deterministic two-pass sum on the device.
     int imp_dot_blocks() const { return std::max(1, std::min(2 * sm_count_, blocks_for((long long)NQ * pm_.C, 256))); }
     long long imp_n() const { return (long long)NQ * pm_.C; }
-    // V_k . w for k < nk into imp_red_ (device) and out (host, when given)
-    int imp_dots(const double* V, long long ld, int nk, const double* w, double* out) {
+    // V_k . w for k < nk into dev (device; imp_red_ by default) and out (host,
+    // when given: a synchronisation)
+    int imp_dots(const double* V, long long ld, int nk, const double* w, double* out, double* dev = nullptr) {
         const int nb = imp_dot_blocks();
+        if (!dev) dev = imp_red_.p;
         imp_multi_dot_kernel<<<nb, 256, 0, stream_>>>(imp_n(), nk, V, ld, w, imp_part_.p);
-        imp_reduce_kernel<<<1, 64, 0, stream_>>>(nk, nb, imp_part_.p, imp_red_.p);
+        imp_reduce_kernel<<<1, 64, 0, stream_>>>(nk, nb, imp_part_.p, dev);
         ZSME_CUDA(cudaGetLastError());
         if (out) {
-            ZSME_CUDA(cudaMemcpyAsync(out, imp_red_.p, nk * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(out, dev, nk * sizeof(double), cudaMemcpyDeviceToHost, stream_));
             ZSME_CUDA(cudaStreamSynchronize(stream_));
         }
         return ZSME_OK;
@@ -983,18 +985,17 @@ class Solver final : public SolverBase {
     }
     // out = D^-1 (F(X + hv v) - F(X)) / hv, hv = sqrt(eps) sqrt(1 + |X|) / |v| (the
     // Walker-Pernice differencing parameter of PETSc's matrix-free Jacobian)
+    // (no host synchronisation: |v| and hv stay on the device)
     int imp_apply(double t, const BdfTerms& b, double xnorm, const double* v, double* out) {
-        double vnorm = 0.0;
-        int rc = imp_norm(v, vnorm);
+        const long long n = imp_n();
+        double* vv = imp_red_.p + kImpRestart + 2;
+        double* hv = imp_red_.p + kImpRestart + 3;
+        int rc = imp_dots(v, 0, 1, v, nullptr, vv);
         if (rc) return rc;
-        if (!(vnorm > 0.0)) {
-            ZSME_CUDA(cudaMemsetAsync(out, 0, imp_n() * sizeof(double), stream_));
-            return ZSME_OK;
-        }
-        const double hv = 1.4901161193847656e-08 * std::sqrt(1.0 + xnorm) / vnorm;
-        imp_lincomb(1.0, x_.p, hv, v, imp_xt_.p);
+        imp_hv_kernel<<<1, 1, 0, stream_>>>(vv, xnorm, hv);
+        imp_perturb_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, x_.p, v, hv, imp_xt_.p);
         imp_residual(t, imp_xt_.p, b, imp_Ft_.p);
-        imp_diffquot_kernel<<<blocks_for(imp_n(), 256), 256, 0, stream_>>>(imp_n(), imp_Ft_.p, imp_F_.p, hv, out);
+        imp_diffquot_dev_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, imp_Ft_.p, imp_F_.p, hv, out);
         imp_block_solve_kernel<NQ><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(pm_.C, imp_lu_.p, imp_piv_.p, out, out);
         ZSME_CUDA(cudaGetLastError());
         return ZSME_OK;
@@ -1028,12 +1029,19 @@ class Solver final : public SolverBase {
             for (; j < m;) {
                 double* vj = imp_V_.p + (size_t)j * n;
                 double* w = imp_w_.p;
+                double* ww = imp_red_.p + kImpRestart + 4;
+                // one synchronisation per Arnoldi step: the projections and |w|^2 come back together
                 if ((rc = imp_apply(t, b, xnorm, vj, w))) return rc;
-                if ((rc = imp_dots(imp_V_.p, n, j + 1, w, hcol.data()))) return rc;
+                if ((rc = imp_dots(imp_V_.p, n, j + 1, w, nullptr))) return rc;
                 imp_multi_axpy_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, j + 1, imp_V_.p, n, imp_red_.p, w);
-                double hn = 0.0;
-                if ((rc = imp_norm(w, hn))) return rc;
-                if (hn > 0.0) imp_lincomb(1.0 / hn, w, 0.0, nullptr, imp_V_.p + (size_t)(j + 1) * n);
+                if ((rc = imp_dots(w, 0, 1, w, nullptr, ww))) return rc;
+                imp_normalize_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, ww, w, imp_V_.p + (size_t)(j + 1) * n);
+                double hn2 = 0.0;
+                ZSME_CUDA(cudaMemcpyAsync(hcol.data(), imp_red_.p, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                                          stream_));
+                ZSME_CUDA(cudaMemcpyAsync(&hn2, ww, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+                ZSME_CUDA(cudaStreamSynchronize(stream_));
+                const double hn = std::sqrt(hn2);
                 for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
                 H[(size_t)(j + 1) * m + j] = hn;
                 for (int i = 0; i < j; ++i) {   // earlier rotations on the new column
