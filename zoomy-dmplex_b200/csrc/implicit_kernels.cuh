@@ -22,12 +22,14 @@ constexpr double dry_jacobian = 1e-4;
 }  // namespace implicit_fd
 
 // f = (Xdot - S(y)) - R, Xdot = xdot[id] when given, else
-// (c0 y + c1 xn + c2 xnm1) / h (the BDF derivative of the step)
+// (c0 y + c1 xn + c2 xnm1) / h (the BDF derivative of the step), the
+// coefficients c0, c1, c2, h from device memory (coef) when given
 struct BdfTerms {
     const double* xdot;
     const double* xn;
     const double* xnm1;
     double c0, c1, c2, h;
+    const double* coef;
 };
 
 template <class M>
@@ -47,10 +49,12 @@ __global__ void __launch_bounds__(128) imp_residual_kernel(MeshDev m, const doub
 #pragma unroll
     for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
     imex_source_cell<M>(q, a, p, S);
+    const double c0 = b.coef ? b.coef[0] : b.c0, c1 = b.coef ? b.coef[1] : b.c1;
+    const double c2 = b.coef ? b.coef[2] : b.c2, h = b.coef ? b.coef[3] : b.h;
 #pragma unroll
     for (int i = 0; i < NQ; ++i) {
         const size_t id = (size_t)i * C + c;
-        const double xd = b.xdot ? b.xdot[id] : (b.c0 * q[i] + b.c1 * b.xn[id] + b.c2 * b.xnm1[id]) / b.h;
+        const double xd = b.xdot ? b.xdot[id] : (c0 * q[i] + c1 * b.xn[id] + c2 * b.xnm1[id]) / h;
         f[id] = (xd - S[i]) - R[id];
     }
 }
@@ -346,10 +350,12 @@ __global__ void __launch_bounds__(128) imp_update_state_kernel(MeshDev m, const 
 // ------------------------------------------------------------ vector kernels
 // The matrix-free Jacobian's differencing parameter from the device dot v.v:
 // hv = sqrt(eps) sqrt(1 + |X|) / |v| (0 for a zero vector)
-static __global__ void imp_hv_kernel(const double* __restrict__ vv, double xnorm, double* __restrict__ hv) {
+static __global__ void imp_hv_kernel(const double* __restrict__ vv, const double* __restrict__ xnorm,
+                                     double* __restrict__ hv) {
     const double vn = sqrt(*vv);
-    *hv = vn > 0.0 ? 1.4901161193847656e-08 * sqrt(1.0 + xnorm) / vn : 0.0;
+    *hv = vn > 0.0 ? 1.4901161193847656e-08 * sqrt(1.0 + *xnorm) / vn : 0.0;
 }
+static __global__ void imp_sqrt_kernel(const double* __restrict__ in, double* __restrict__ out) { *out = sqrt(*in); }
 // out = 1.0 x + hv v, hv a device scalar
 static __global__ void imp_perturb_kernel(long long n, const double* __restrict__ x, const double* __restrict__ v,
                                           const double* __restrict__ hv, double* __restrict__ out) {
@@ -394,30 +400,38 @@ static __global__ void imp_lincomb_kernel(long long n, double a, const double* x
 static __global__ void __launch_bounds__(256) imp_multi_dot_kernel(long long n, int nk, const double* __restrict__ V,
                                                                    long long ld, const double* __restrict__ w,
                                                                    double* __restrict__ partial) {
+    // grid (nb, nk): block (b, k) takes vector k's chunk b
     __shared__ double sh[256];
-    const int nb = gridDim.x;
-    for (int k = 0; k < nk; ++k) {
-        const double* v = V + (size_t)k * ld;
-        double s = 0.0;
-        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)nb * blockDim.x)
-            s += v[i] * w[i];
-        sh[threadIdx.x] = s;
-        __syncthreads();
-        for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-            if (threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) partial[(size_t)k * nb + blockIdx.x] = sh[0];
+    const int nb = gridDim.x, k = blockIdx.y;
+    if (k >= nk) return;
+    const double* v = V + (size_t)k * ld;
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)nb * blockDim.x)
+        s += v[i] * w[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
         __syncthreads();
     }
+    if (threadIdx.x == 0) partial[(size_t)k * nb + blockIdx.x] = sh[0];
 }
-// out[k] = sum of partial[k][0 .. nb) in block order
-static __global__ void imp_reduce_kernel(int nk, int nb, const double* __restrict__ partial, double* __restrict__ out) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+// out[k] = sum of partial[k][0 .. nb): one block of 256 threads per k, each
+// thread a fixed stride of the partials, then a fixed tree (deterministic)
+static __global__ void __launch_bounds__(256) imp_reduce_kernel(int nk, int nb, const double* __restrict__ partial,
+                                                                double* __restrict__ out) {
+    __shared__ double sh[256];
+    const int k = blockIdx.x;
     if (k >= nk) return;
     double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += partial[(size_t)k * nb + b];
-    out[k] = s;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[(size_t)k * nb + b];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) sh[threadIdx.x] += sh[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = sh[0];
 }
 // w -= sum_k h_k V_k (classical Gram-Schmidt projection, h on the device)
 static __global__ void imp_multi_axpy_kernel(long long n, int nk, const double* __restrict__ V, long long ld,

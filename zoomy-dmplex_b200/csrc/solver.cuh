@@ -79,6 +79,7 @@ class Solver final : public SolverBase {
     DevBuf<double> xs_;  // MOOD: the state at the start of the step
     DevBuf<int> mood_list_;  // MOOD: the troubled cells of the step (count in iscal_[6])
     DevBuf<double> imex_g_[3], imex_s_[3], imex_y_[2];   // IMEX: stage right-hand sides, implicit derivatives, states
+    static constexpr int kImpRestart = 30;   // GMRES restart length
     // fully implicit strategy (allocated with the handle when selected):
     // history X_n, X_{n-1}; residual F, trial residual, trial state, transport
     // RHS, Krylov basis [31][NQ C], work, Newton update, preconditioned
@@ -86,11 +87,15 @@ class Solver final : public SolverBase {
     // assembled diagonal blocks, their LU factors and pivots; the face blocks
     DevBuf<double> imp_xn_, imp_xnm1_, imp_F_, imp_Ft_, imp_xt_, imp_R_, imp_V_, imp_w_, imp_d_, imp_r0_, imp_r_;
     DevBuf<double> imp_xl_, imp_al_, imp_pd_, imp_lu_, imp_fj_, imp_part_, imp_red_;
+    // device scalars of the step: [0] t_{n+1}, [1] |X|, [2..5] BDF c0, c1, c2, h,
+    // [6] v.v, [7] differencing parameter, [8] w.w, [9] X.X
+    DevBuf<double> imp_scal_;
     DevBuf<int> imp_piv_;
+    cudaGraphExec_t imp_graph_[kImpRestart] = {};   // Arnoldi step j, captured on first use
     bool imp_have_prev_ = false;   // a previous implicit step exists: BDF2
     double imp_h_prev_ = 0.0;
     int imp_stats_[4] = {0, 0, 0, 0};   // last step: Newton iterations, GMRES iterations, halvings, converged
-    static constexpr int kImpRestart = 30;
+
     // per instance: t, dt_cfl, dt_step, dt_aux ; active ; ratio
     DevBuf<double> t_, dt_cfl_, dt_step_, dt_aux_;
     DevBuf<int> active_, iscal_;  // iscal_: [0] step_idx, [1..4] diag, [5] deferred finalize cells, [6] MOOD cells
@@ -139,6 +144,7 @@ class Solver final : public SolverBase {
   public:
     ~Solver() override {
         if (graph_) cudaGraphExecDestroy(graph_);
+        imp_drop_graphs();
         for (auto e : ev_pool_) cudaEventDestroy(e);
         if (h2d_) {
             cudaStreamSynchronize(h2d_);
@@ -221,6 +227,7 @@ class Solver final : public SolverBase {
             cudaGraphExecDestroy(graph_);
             graph_ = nullptr;
         }
+        imp_drop_graphs();
         if (ready_) return ensure_tiles();
         return ZSME_OK;
     }
@@ -334,6 +341,7 @@ class Solver final : public SolverBase {
             ZSME_CUDA(imp_fj_.alloc((size_t)4 * NQ * NQ * F));
             ZSME_CUDA(imp_part_.alloc((size_t)(kImpRestart + 1) * imp_dot_blocks()));
             ZSME_CUDA(imp_red_.alloc((size_t)kImpRestart + 8));
+            ZSME_CUDA(imp_scal_.alloc(16));
         }
         if (st_.positivity == ZSME_POSITIVITY_MOOD) {
             ZSME_CUDA(xs_.alloc((size_t)NQ * C));
@@ -946,8 +954,8 @@ class Solver final : public SolverBase {
     int imp_dots(const double* V, long long ld, int nk, const double* w, double* out, double* dev = nullptr) {
         const int nb = imp_dot_blocks();
         if (!dev) dev = imp_red_.p;
-        imp_multi_dot_kernel<<<nb, 256, 0, stream_>>>(imp_n(), nk, V, ld, w, imp_part_.p);
-        imp_reduce_kernel<<<1, 64, 0, stream_>>>(nk, nb, imp_part_.p, dev);
+        imp_multi_dot_kernel<<<dim3(nb, nk), 256, 0, stream_>>>(imp_n(), nk, V, ld, w, imp_part_.p);
+        imp_reduce_kernel<<<nk, 256, 0, stream_>>>(nk, nb, imp_part_.p, dev);
         ZSME_CUDA(cudaGetLastError());
         if (out) {
             ZSME_CUDA(cudaMemcpyAsync(out, dev, nk * sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -964,13 +972,26 @@ class Solver final : public SolverBase {
     void imp_lincomb(double a, const double* x, double b, const double* y, double* out) {
         imp_lincomb_kernel<<<blocks_for(imp_n(), 256), 256, 0, stream_>>>(imp_n(), a, x, b, y, out);
     }
-    // F(t, y, Xdot) = (Xdot - S(y)) - R(y) (IFunctionWrapper) into f
-    void imp_residual(double t, const double* y, const BdfTerms& b, double* f) {
+    // F(t, y, Xdot) = (Xdot - S(y)) - R(y) (IFunctionWrapper) into f; t_dev:
+    // the time in device memory (the step's), else t
+    void imp_residual(double t, const double* y, const BdfTerms& b, double* f, const double* t_dev = nullptr) {
         const int C = pm_.C;
         clamp_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, 0, C, y, aux_.p, params_.p, wl_.p);
         launch_prep(y, wl_.p, nullptr);
-        launch_flux(MODE_RHS, t, nullptr, 0.0, nullptr, imp_R_.p, nullptr, nullptr, nullptr);
+        launch_flux(MODE_RHS, t, t_dev, 0.0, nullptr, imp_R_.p, nullptr, nullptr, nullptr);
         imp_residual_kernel<M><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, y, aux_.p, params_.p, imp_R_.p, b, f);
+    }
+    // the step's residual: time and BDF coefficients from imp_scal_
+    BdfTerms imp_bdf() const {
+        return BdfTerms{nullptr, imp_xn_.p, imp_xnm1_.p, 0.0, 0.0, 0.0, 1.0, imp_scal_.p + 2};
+    }
+    void imp_residual_step(const double* y, double* f) { imp_residual(0.0, y, imp_bdf(), f, imp_scal_.p); }
+    void imp_drop_graphs() {
+        for (auto& g : imp_graph_)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
     }
     // P(t, y, a) (FormImplicitJacobian): the state clamped with its aux
     // (UpdateState), the face blocks, the diagonal blocks in assembly order
@@ -984,27 +1005,54 @@ class Solver final : public SolverBase {
                                                                       imp_fj_.p, imp_pd_.p);
     }
     // out = D^-1 (F(X + hv v) - F(X)) / hv, hv = sqrt(eps) sqrt(1 + |X|) / |v| (the
-    // Walker-Pernice differencing parameter of PETSc's matrix-free Jacobian)
-    // (no host synchronisation: |v| and hv stay on the device)
-    int imp_apply(double t, const BdfTerms& b, double xnorm, const double* v, double* out) {
+    // Walker-Pernice differencing parameter of PETSc's matrix-free Jacobian);
+    // |X|, |v| and hv stay on the device
+    void imp_apply(const double* v, double* out) {
         const long long n = imp_n();
-        double* vv = imp_red_.p + kImpRestart + 2;
-        double* hv = imp_red_.p + kImpRestart + 3;
-        int rc = imp_dots(v, 0, 1, v, nullptr, vv);
-        if (rc) return rc;
-        imp_hv_kernel<<<1, 1, 0, stream_>>>(vv, xnorm, hv);
-        imp_perturb_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, x_.p, v, hv, imp_xt_.p);
-        imp_residual(t, imp_xt_.p, b, imp_Ft_.p);
-        imp_diffquot_dev_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, imp_Ft_.p, imp_F_.p, hv, out);
+        double* sc = imp_scal_.p;
+        imp_dots(v, 0, 1, v, nullptr, sc + 6);
+        imp_hv_kernel<<<1, 1, 0, stream_>>>(sc + 6, sc + 1, sc + 7);
+        imp_perturb_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, x_.p, v, sc + 7, imp_xt_.p);
+        imp_residual_step(imp_xt_.p, imp_Ft_.p);
+        imp_diffquot_dev_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, imp_Ft_.p, imp_F_.p, sc + 7, out);
         imp_block_solve_kernel<NQ><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(pm_.C, imp_lu_.p, imp_piv_.p, out, out);
-        ZSME_CUDA(cudaGetLastError());
+    }
+    // Arnoldi step j: w = D^-1 J V_j, h = V_0..j . w (into imp_red_), w -= V h,
+    // w.w (imp_scal_[8]), V_{j+1} = w / |w|.  Fixed pointers and device
+    // scalars only, so it is captured once per handle as a CUDA graph.
+    void imp_enqueue_arnoldi(int j) {
+        const long long n = imp_n();
+        double* w = imp_w_.p;
+        imp_apply(imp_V_.p + (size_t)j * n, w);
+        imp_dots(imp_V_.p, n, j + 1, w, nullptr);
+        imp_multi_axpy_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, j + 1, imp_V_.p, n, imp_red_.p, w);
+        imp_dots(w, 0, 1, w, nullptr, imp_scal_.p + 8);
+        imp_normalize_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, imp_scal_.p + 8, w,
+                                                                      imp_V_.p + (size_t)(j + 1) * n);
+    }
+    int imp_arnoldi(int j) {
+        if (profiling_) {   // per-kernel timing records events: plain launches
+            imp_enqueue_arnoldi(j);
+            ZSME_CUDA(cudaGetLastError());
+            return ZSME_OK;
+        }
+        if (!imp_graph_[j]) {
+            cudaGraph_t g = nullptr;
+            ZSME_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            imp_enqueue_arnoldi(j);
+            ZSME_CUDA(cudaStreamEndCapture(stream_, &g));
+            cudaError_t e = cudaGraphInstantiate(&imp_graph_[j], g, 0);
+            cudaGraphDestroy(g);
+            ZSME_CUDA(e);
+        }
+        ZSME_CUDA(cudaGraphLaunch(imp_graph_[j], stream_));
         return ZSME_OK;
     }
     // Left-preconditioned restarted GMRES (restart 30, classical Gram-Schmidt,
     // Givens rotations, zero initial guess) for (D^-1 J) d = D^-1 (-F) into
     // imp_d_; stops when the preconditioned residual is below 1e-5 of its
     // initial norm (PETSc's KSP defaults) or after 10000 iterations.
-    int imp_gmres(double t, const BdfTerms& b, double xnorm, int& its) {
+    int imp_gmres(int& its) {
         constexpr int m = kImpRestart;
         const long long n = imp_n();
         const int C = pm_.C;
@@ -1027,19 +1075,12 @@ class Solver final : public SolverBase {
             int j = 0;
             bool done = false;
             for (; j < m;) {
-                double* vj = imp_V_.p + (size_t)j * n;
-                double* w = imp_w_.p;
-                double* ww = imp_red_.p + kImpRestart + 4;
                 // one synchronisation per Arnoldi step: the projections and |w|^2 come back together
-                if ((rc = imp_apply(t, b, xnorm, vj, w))) return rc;
-                if ((rc = imp_dots(imp_V_.p, n, j + 1, w, nullptr))) return rc;
-                imp_multi_axpy_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, j + 1, imp_V_.p, n, imp_red_.p, w);
-                if ((rc = imp_dots(w, 0, 1, w, nullptr, ww))) return rc;
-                imp_normalize_kernel<<<blocks_for(n, 256), 256, 0, stream_>>>(n, ww, w, imp_V_.p + (size_t)(j + 1) * n);
+                if ((rc = imp_arnoldi(j))) return rc;
                 double hn2 = 0.0;
                 ZSME_CUDA(cudaMemcpyAsync(hcol.data(), imp_red_.p, (j + 1) * sizeof(double), cudaMemcpyDeviceToHost,
                                           stream_));
-                ZSME_CUDA(cudaMemcpyAsync(&hn2, ww, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+                ZSME_CUDA(cudaMemcpyAsync(&hn2, imp_scal_.p + 8, sizeof(double), cudaMemcpyDeviceToHost, stream_));
                 ZSME_CUDA(cudaStreamSynchronize(stream_));
                 const double hn = std::sqrt(hn2);
                 for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = hcol[i];
@@ -1076,7 +1117,7 @@ class Solver final : public SolverBase {
             ZSME_CUDA(cudaGetLastError());
             if (done) break;
             // restart: r = D^-1 (-F) - D^-1 J d
-            if ((rc = imp_apply(t, b, xnorm, imp_d_.p, imp_w_.p))) return rc;
+            imp_apply(imp_d_.p, imp_w_.p);
             imp_lincomb(1.0, imp_r0_.p, -1.0, imp_w_.p, imp_r_.p);
             r = imp_r_.p;
             if ((rc = imp_norm(r, beta))) return rc;
@@ -1094,17 +1135,27 @@ class Solver final : public SolverBase {
     // |F| <= (1 - 1e-4 lambda) |F_prev|; no such lambda ends Newton unconverged.
     int imp_step(double t0, double h) {
         const long long n = imp_n();
-        if (imp_have_prev_) std::swap(imp_xn_.p, imp_xnm1_.p);
-        ZSME_CUDA(cudaMemcpyAsync(imp_xn_.p, x_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-        BdfTerms b{nullptr, imp_xn_.p, imp_xn_.p, 1.0, -1.0, 0.0, h};
+        const size_t bytes = n * sizeof(double);
+        // history: X_{n-1} (the start of the previous step; X_n itself on the
+        // first step, where its coefficient is zero) and X_n
+        ZSME_CUDA(cudaMemcpyAsync(imp_xnm1_.p, imp_have_prev_ ? imp_xn_.p : x_.p, bytes, cudaMemcpyDeviceToDevice,
+                                  stream_));
+        ZSME_CUDA(cudaMemcpyAsync(imp_xn_.p, x_.p, bytes, cudaMemcpyDeviceToDevice, stream_));
+        double c0 = 1.0, c1 = -1.0, c2 = 0.0;
         if (imp_have_prev_) {
             const double w = h / imp_h_prev_;
-            b = BdfTerms{nullptr, imp_xn_.p, imp_xnm1_.p, (1.0 + 2.0 * w) / (1.0 + w), -(1.0 + w),
-                         w * w / (1.0 + w), h};
+            c0 = (1.0 + 2.0 * w) / (1.0 + w);
+            c1 = -(1.0 + w);
+            c2 = w * w / (1.0 + w);
         }
-        const double shift = b.c0 / h;
+        const double shift = c0 / h;
         const double t1 = t0 + h;
-        imp_residual(t1, x_.p, b, imp_F_.p);
+        {
+            const double sc[6] = {t1, 0.0, c0, c1, c2, h};
+            ZSME_CUDA(cudaMemcpyAsync(imp_scal_.p, sc, sizeof(sc), cudaMemcpyHostToDevice, stream_));
+            ZSME_CUDA(cudaStreamSynchronize(stream_));
+        }
+        imp_residual_step(x_.p, imp_F_.p);
         double fnorm = 0.0;
         int rc = imp_norm(imp_F_.p, fnorm);
         if (rc) return rc;
@@ -1113,27 +1164,27 @@ class Solver final : public SolverBase {
         for (; it < 50; ++it) {
             if (fnorm <= 1e-4 || (it > 0 && fnorm <= 1e-3 * fnorm0)) { conv = 1; break; }
             if (!std::isfinite(fnorm)) break;
-            double xnorm = 0.0;
-            if ((rc = imp_norm(x_.p, xnorm))) return rc;
+            if ((rc = imp_dots(x_.p, 0, 1, x_.p, nullptr, imp_scal_.p + 9))) return rc;
+            imp_sqrt_kernel<<<1, 1, 0, stream_>>>(imp_scal_.p + 9, imp_scal_.p + 1);   // |X| for the differencing
             imp_assemble(t1, x_.p, shift);
             imp_block_lu_kernel<NQ><<<blocks_for(pm_.C, 64), 64, 0, stream_>>>(pm_.C, imp_pd_.p, imp_lu_.p,
                                                                               imp_piv_.p);
             int gm = 0;
-            if ((rc = imp_gmres(t1, b, xnorm, gm))) return rc;
+            if ((rc = imp_gmres(gm))) return rc;
             gm_total += gm;
             double lambda = 1.0, ft = 0.0;
             bool descent = false;
             for (int ls = 0; ls < 10; ++ls) {
                 imp_lincomb(1.0, x_.p, lambda, imp_d_.p, imp_xt_.p);
-                imp_residual(t1, imp_xt_.p, b, imp_Ft_.p);
+                imp_residual_step(imp_xt_.p, imp_Ft_.p);
                 if ((rc = imp_norm(imp_Ft_.p, ft))) return rc;
                 if (ft <= (1.0 - 1e-4 * lambda) * fnorm) { descent = true; break; }
                 lambda *= 0.5;
                 ++halvings;
             }
             if (!descent) break;   // the line search failed: Newton diverged
-            ZSME_CUDA(cudaMemcpyAsync(x_.p, imp_xt_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-            ZSME_CUDA(cudaMemcpyAsync(imp_F_.p, imp_Ft_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(x_.p, imp_xt_.p, bytes, cudaMemcpyDeviceToDevice, stream_));
+            ZSME_CUDA(cudaMemcpyAsync(imp_F_.p, imp_Ft_.p, bytes, cudaMemcpyDeviceToDevice, stream_));
             fnorm = ft;
             double dnorm = 0.0, xn2 = 0.0;
             if ((rc = imp_norm(imp_d_.p, dnorm)) || (rc = imp_norm(x_.p, xn2))) return rc;
@@ -1144,8 +1195,9 @@ class Solver final : public SolverBase {
         imp_stats_[2] = halvings;
         imp_stats_[3] = conv;
         if (!conv) {   // as PETSc's TSStep after a diverged SNES: nothing of the step is kept
-            ZSME_CUDA(cudaMemcpyAsync(x_.p, imp_xn_.p, n * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-            if (imp_have_prev_) std::swap(imp_xn_.p, imp_xnm1_.p);
+            ZSME_CUDA(cudaMemcpyAsync(x_.p, imp_xn_.p, bytes, cudaMemcpyDeviceToDevice, stream_));
+            if (imp_have_prev_)   // the history as before the step
+                ZSME_CUDA(cudaMemcpyAsync(imp_xn_.p, imp_xnm1_.p, bytes, cudaMemcpyDeviceToDevice, stream_));
             ZSME_CUDA(cudaStreamSynchronize(stream_));
             return set_error(ZSME_ERR_SOLVE, "implicit step: Newton did not converge in 50 iterations");
         }
@@ -1195,7 +1247,7 @@ class Solver final : public SolverBase {
         aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(tmp_b_.p, imp_xt_.p, old_of_new_.p, 0, C, C, NQ);
         ZSME_CUDA(cudaMemcpyAsync(tmp_b_.p, xdot_aos, bytes, cudaMemcpyHostToDevice, stream_));
         aos_to_soa_kernel<<<blocks_for(C, 128), 128, 0, stream_>>>(tmp_b_.p, imp_w_.p, old_of_new_.p, 0, C, C, NQ);
-        const BdfTerms b{imp_w_.p, nullptr, nullptr, 0.0, 0.0, 0.0, 1.0};
+        const BdfTerms b{imp_w_.p, nullptr, nullptr, 0.0, 0.0, 0.0, 1.0, nullptr};
         imp_residual(t, imp_xt_.p, b, imp_Ft_.p);
         ZSME_CUDA(cudaGetLastError());
         return get_soa(0, imp_Ft_.p, NQ, f_aos, false);
