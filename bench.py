@@ -702,7 +702,9 @@ def run_adjoint(a, dev, torch, dist, rank, world):
     fwd_ms, adj_s, e2e_s = (float(x) for x in t.tolist())
     s = c.settings.ssp_stages
     lps = g.launches_per_step()
-    rev_launches = 3 + s * 4 + (s - 1) + 1     # finalize, reduce, seeds; per stage prep/face/cell/combine; clamps; axpby
+    # per reverse step: finalize; per stage face VJP, cell, combine; the clamps of
+    # the stages after the first (odd s adds axpby, copy and seed kernels)
+    rev_launches = 1 + 3 * s + (s - 1) + (3 if s % 2 else 0)
     nv = C * g.nq * 8
     line = {"metric": METRIC, "value": C * N * world / adj_s, "unit": UNIT, "n_gpus": world, "steps": N,
             "warmup": a.warmup, "ms_per_step": 1e3 * adj_s / N, "higher_is_better": True, "scaling": "weak",

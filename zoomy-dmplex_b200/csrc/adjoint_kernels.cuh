@@ -35,17 +35,20 @@
 #pragma once
 #include "dual.h"
 
-// Register caps of the reverse kernels as resident 128-thread blocks per SM
-// (1 = uncapped): compile-time constants, chosen by measurement on the
-// adjoint workload (SME level 1, 79k cells: every reverse kernel is one or a
-// few waves, so resident blocks decide its time).  Uncapped the reverse sweep
-// took 0.255 ms per step; caps 3 / 3 / 2 give 0.229 ms with the same
-// gradients bit for bit (caps 2 / 2 / 2: 0.256 ms; 3 / 4 / 3: 0.230 ms).
+// Register caps of the reverse kernels (face VJP / cell / finalize) as
+// resident 128-thread blocks per SM (1 = uncapped): compile-time constants,
+// chosen by measurement on the adjoint workload (SME level 1, 79k cells, 400
+// steps, checkpoints every 20: every reverse kernel is one or a few waves, and
+// the segment replays run beside the reverse sweep on a second stream, so
+// resident blocks decide the time).  Replays plus reverse sweep per step:
+// caps 4 / 4 / 2 0.285 ms; 4 / 5 / 2 0.283; 4 / 4 / 3 0.287; 3 / 3 / 2 0.308;
+// 5 / 5 / 2 0.303; 6 / 6 / 2 0.327; 2 / 2 / 2 0.330.  The gradients are the
+// same bit for bit under every cap.
 #ifndef ZSME_ADJ_FACE_MINB
-#define ZSME_ADJ_FACE_MINB 3
+#define ZSME_ADJ_FACE_MINB 4
 #endif
 #ifndef ZSME_ADJ_CELL_MINB
-#define ZSME_ADJ_CELL_MINB 3
+#define ZSME_ADJ_CELL_MINB 4
 #endif
 #ifndef ZSME_ADJ_FIN_MINB
 #define ZSME_ADJ_FIN_MINB 2
@@ -630,6 +633,21 @@ __global__ void __launch_bounds__(128, ZSME_ADJ_CELL_MINB) adj_cell_kernel(MeshD
 
 // dst = c_src * src + (own + gathered neighbour terms), the clamped part
 // through the clamp's transposed Jacobian at w.
+// What the last combine of a reverse step also does, where its output is the
+// step's adjoint: ax_x != null makes it ax_a ax_x + 1 v (the W_0 share of X'),
+// then first != null adds the seeds of the observations of step *n0 + k, one
+// by one in list order (as adj_seed_seg_kernel does).
+struct AdjEpilogue {
+    const double* ax_x = nullptr;
+    double ax_a = 0.0;
+    const int* first = nullptr;
+    const int* n0 = nullptr;
+    int k = 0;
+    const int* cell = nullptr;
+    const int* comp = nullptr;
+    const double* seed = nullptr;
+};
+
 template <template <typename> class MT>
 __global__ void __launch_bounds__(128) adj_combine_kernel(MeshDev m, const double* __restrict__ w,
                                                           const double* __restrict__ aux,
@@ -638,7 +656,8 @@ __global__ void __launch_bounds__(128) adj_combine_kernel(MeshDev m, const doubl
                                                           const double* __restrict__ own_wl,
                                                           const double* __restrict__ out_w,
                                                           const double* __restrict__ out_wl, const double* src,
-                                                          double c_src, double* dst) {
+                                                          double c_src, double* dst,
+                                                          AdjEpilogue ep = AdjEpilogue{}) {
     using M = MT<double>;
     constexpr int NQ = M::n_dof_q, NA = M::n_dof_qaux;
     const int C = m.C;
@@ -665,14 +684,27 @@ __global__ void __launch_bounds__(128) adj_combine_kernel(MeshDev m, const doubl
 #pragma unroll
     for (int i = 0; i < NA; ++i) a[i] = aux[(size_t)i * C + c];
     clamp_adjoint<MT>(q, a, params + (size_t)cell_instance(m, c) * m.np, lwl, tl);
+    int j0 = 0, j1 = 0;
+    if (ep.first) {
+        const int n = *ep.n0 + ep.k;
+        j0 = ep.first[n];
+        j1 = ep.first[n + 1];
+    }
 #pragma unroll
-    for (int i = 0; i < NQ; ++i) dst[(size_t)i * C + c] = c_src * src[(size_t)i * C + c] + lw[i] + tl[i];
+    for (int i = 0; i < NQ; ++i) {
+        double v = c_src * src[(size_t)i * C + c] + lw[i] + tl[i];
+        if (ep.ax_x) v = ep.ax_a * ep.ax_x[(size_t)i * C + c] + 1.0 * v;
+        for (int j = j0; j < j1; ++j)
+            if (ep.cell[j] == c && ep.comp[j] == i) v += ep.seed[j];
+        dst[(size_t)i * C + c] = v;
+    }
 }
 
 // --------------------------------------------------------------- finalize
 // lam_in = adjoint of the stage output X' given lam_out, the adjoint of the
-// step's result; lp_part[NP][gridDim.x] = this step's parameter adjoint summed
-// over each block's cells (blockDim.x = 128, fixed-order tree).
+// step's result; lp_part[NP][gridDim.x] += this step's parameter adjoint summed
+// over each block's cells (blockDim.x = 128, fixed-order tree); the partials
+// are reduced over the blocks once, after the last step.
 // One cell of adj_finalize_kernel; lp[k * lp_stride] receives the cell's
 // parameter adjoint k.
 template <template <typename> class MT>
@@ -793,9 +825,9 @@ __global__ void __launch_bounds__(128, ZSME_ADJ_FIN_MINB) adj_finalize_kernel(Me
             for (int k = 0; k < NP; ++k) lp_sh[k][threadIdx.x] += lp_sh[k][threadIdx.x + h];
         __syncthreads();
     }
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0)   // each block accumulates its cells' sum over the steps
 #pragma unroll
-        for (int k = 0; k < NP; ++k) lp_part[(size_t)k * gridDim.x + blockIdx.x] = lp_sh[k][0];
+        for (int k = 0; k < NP; ++k) lp_part[(size_t)k * gridDim.x + blockIdx.x] += lp_sh[k][0];
 }
 
 // ------------------------------------------------------------- small ones

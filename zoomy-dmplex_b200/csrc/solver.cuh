@@ -1374,7 +1374,8 @@ class Solver final : public SolverBase {
     // same for every segment and replay as one CUDA graph.  W0: W is the step's
     // start state (its own clamped copy, as in the forward stage).
     void adj_apply_rt(const double* W, const double* fs, bool W0, const double* tp, double frac, const double* dtp,
-                      double factor, const double* src, double c_src, double* dst) {
+                      double factor, const double* src, double c_src, double* dst,
+                      const AdjEpilogue& ep = AdjEpilogue{}) {
         const int C = pm_.C, F = pm_.F;
         const double* wl = W;
         if (!W0) {
@@ -1396,7 +1397,7 @@ class Solver final : public SolverBase {
                 md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);
         adj_combine_kernel<MT><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, W, adj_aux_cur_, params_.p, adj_own_w_.p,
                                                                         adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p,
-                                                                        src, c_src, dst);
+                                                                        src, c_src, dst, ep);
     }
 
     // Reverse of step k of the current segment (tape slot k: W_0 .. W_{s-1}, X',
@@ -1415,26 +1416,42 @@ class Solver final : public SolverBase {
         const int nb = blocks_for(C, 128);
         adj_finalize_kernel<MT><<<nb, 128, 0, stream_>>>(md_, tape + (size_t)s * nv, adj_aux_cur_, params_.p, dtp,
                                                          flags, lam, t1, adj_lp_cell_.p);
-        adj_param_reduce_kernel<<<NP, 256, 0, stream_>>>(adj_lp_cell_.p, nb, adj_lp_.p);
+        // the observations of this step's start state, seeded by the last
+        // combine where that one writes lam
+        AdjEpilogue seeds;
+        seeds.first = adj_first_.p;
+        seeds.n0 = adj_seg_n0_.p + adj_par_;
+        seeds.k = k;
+        seeds.cell = adj_ocell_.p;
+        seeds.comp = adj_ocomp_.p;
+        seeds.seed = adj_oseed_.p;
         const double* fst = tape + (size_t)(s + 1) * nv;
         if (st_.reconstruction_order < 2) {  // X' = W0 + dt R(W0)
-            adj_apply_rt(tape, fst, true, tp, 0.0, dtp, 1.0, t1, 1.0, lam);
-        } else {
-            // X' = (s-1)/s W_{s-1} + dt/s R(W_{s-1}) + 1/s W_0
-            adj_apply_rt(tape + (size_t)(s - 1) * nv, fst + (size_t)(s - 1) * fs_n, s - 1 == 0, tp, 1.0, dtp,
-                         1.0 / s, t1, (s - 1.) / s, t2);
-            double* cur = t2;
-            double* oth = lam;
-            for (int i = s - 2; i >= 0; --i) {  // W_{i+1} = W_i + dt/(s-1) R(W_i)
-                adj_apply_rt(tape + (size_t)i * nv, fst + (size_t)i * fs_n, i == 0, tp, i / (s - 1.), dtp,
-                             1.0 / (s - 1.), cur, 1.0, oth);
-                std::swap(cur, oth);
-            }
-            axpby_kernel<<<blocks_for((long long)nv, 256), 256, 0, stream_>>>((long long)nv, 1.0 / s, t1, 1.0, cur);
-            if (cur != lam) cudaMemcpyAsync(lam, cur, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
+            adj_apply_rt(tape, fst, true, tp, 0.0, dtp, 1.0, t1, 1.0, lam, seeds);
+            return;
         }
-        adj_seed_seg_kernel<<<1, 1, 0, stream_>>>(adj_first_.p, adj_seg_n0_.p + adj_par_, k, adj_ocell_.p,
-                                                  adj_ocomp_.p, adj_oseed_.p, C, lam);
+        // X' = (s-1)/s W_{s-1} + dt/s R(W_{s-1}) + 1/s W_0
+        adj_apply_rt(tape + (size_t)(s - 1) * nv, fst + (size_t)(s - 1) * fs_n, s - 1 == 0, tp, 1.0, dtp, 1.0 / s, t1,
+                     (s - 1.) / s, t2);
+        double* cur = t2;
+        double* oth = lam;
+        for (int i = s - 2; i >= 0; --i) {  // W_{i+1} = W_i + dt/(s-1) R(W_i)
+            AdjEpilogue ep;
+            if (i == 0 && oth == lam) {     // the last combine writes lam: the W_0 share and the seeds with it
+                ep = seeds;
+                ep.ax_x = t1;
+                ep.ax_a = 1.0 / s;
+            }
+            adj_apply_rt(tape + (size_t)i * nv, fst + (size_t)i * fs_n, i == 0, tp, i / (s - 1.), dtp,
+                         1.0 / (s - 1.), cur, 1.0, oth, ep);
+            std::swap(cur, oth);
+        }
+        if (cur != lam) {   // odd s: the last combine wrote t2
+            axpby_kernel<<<blocks_for((long long)nv, 256), 256, 0, stream_>>>((long long)nv, 1.0 / s, t1, 1.0, cur);
+            cudaMemcpyAsync(lam, cur, nv * sizeof(double), cudaMemcpyDeviceToDevice, stream_);
+            adj_seed_seg_kernel<<<1, 1, 0, stream_>>>(adj_first_.p, adj_seg_n0_.p + adj_par_, k, adj_ocell_.p,
+                                                      adj_ocomp_.p, adj_oseed_.p, C, lam);
+        }
     }
 
     // Replay of steps n0 .. n0+cnt-1 with the segment's dts into the tape
@@ -1606,6 +1623,7 @@ class Solver final : public SolverBase {
         // ---- reverse, segment by segment; full segments replay captured graphs
         ZSME_CUDA(cudaMemsetAsync(adj_lam0_.p, 0, nv * sizeof(double), stream_));
         ZSME_CUDA(cudaMemsetAsync(adj_lp_.p, 0, NP * sizeof(double), stream_));
+        ZSME_CUDA(cudaMemsetAsync(adj_lp_cell_.p, 0, adj_lp_cell_.n * sizeof(double), stream_));
         {
             const int cnt = first[NS + 1] - first[NS];
             if (cnt > 0)
@@ -1728,6 +1746,9 @@ class Solver final : public SolverBase {
         }
         adj_phase_ms_[1] = replay_ms;
         adj_phase_ms_[2] = reverse_ms;
+        // the parameter adjoint: the per-block sums over all steps, over the blocks
+        adj_param_reduce_kernel<<<NP, 256, 0, stream_>>>(adj_lp_cell_.p, blocks_for(C, 128), adj_lp_.p);
+        ZSME_CUDA(cudaGetLastError());
         // ---- outputs; the handle keeps the final state of the forward run
         if (grad_q) {
             int rc = get_soa(0, adj_lam0_.p, NQ, grad_q, false);
