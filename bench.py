@@ -632,7 +632,9 @@ def run_adjoint(a, dev, torch, dist, rank, world):
         from zoomy_dmplex_b200 import autotune
 
         g.set_state(c.q0)
-        tuned = autotune.tune(g, c.model, C, steps=2, use_cache=False, write_cache=False)
+        # ten timed steps per trial: at 79k cells a step is about 0.1 ms, and two
+        # left the choice to timing noise
+        tuned = autotune.tune(g, c.model, C, steps=10, use_cache=False, write_cache=False)
     cells = adj.gauges(C, ngauge, seed=0)
     steps = list(range(10, N + 1, 10))
     targets = adj.observe_run(g, tgt.q0, N, steps, cells)
