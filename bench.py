@@ -116,7 +116,7 @@ def algorithmic_bytes(kind, C, F, nq, na, K, stages, fused=False):
     return 0.0
 
 
-def step_bytes_survey(nq):
+def step_bytes_fused(nq):
     """Per cell-step bytes of a fully fused SSP-RK2 step (5 m_e + 2 state
     arrays + 304 B of geometry, m_e = evolving variables)."""
     me = nq - 1
@@ -889,10 +889,10 @@ def main():
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell on the 900x900 grid, "
                                   "scaled to this launch's cells" if traffic else None,
                 "traffic_per_cell_step": tps,
-                "algorithmic_bytes_per_cell_step": step_bytes_survey(nq),
+                "algorithmic_bytes_per_cell_step": step_bytes_fused(nq),
                 "kernel_ms": dom_ms}
     step_ms = ms_max / a.steps
-    sb = step_bytes_survey(nq)
+    sb = step_bytes_fused(nq)
     roofline_step = {"bytes_per_cell_step": sb, "achieved": sb * C / (step_ms / 1e3) / 1e9, "peak": hbm,
                      "unit": "GB/s", "frac": sb * C / (step_ms / 1e3) / 1e9 / hbm}
     kernel_share = {k: {"ms_per_launch": v[0] / v[1], "launches": v[1], "share": v[0] / max(1e-30, sum(
