@@ -133,6 +133,9 @@ def test_rejected_combinations():
         BatchSolver(c.model, [c.mesh, c.mesh], st, [_params(c)] * 2)
     with pytest.raises(native.ZsmeError):
         Solver(c.model, c.mesh, dataclasses.replace(st, positivity="mood"), _params(c))
+    g = Solver(c.model, c.mesh, c.settings, _params(c))      # splitting: no implicit residual
+    with pytest.raises(native.ZsmeError):
+        g.implicit_function(c.q0, np.zeros_like(c.q0))
 
 
 def test_stiff_source_at_large_dt_follows_the_oracle():
