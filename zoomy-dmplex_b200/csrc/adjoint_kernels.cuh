@@ -347,7 +347,8 @@ __global__ void __launch_bounds__(128, ZSME_ADJ_CELL_MINB) adj_cell_kernel(MeshD
                                                        const double* __restrict__ params,
                                                        const double* __restrict__ gfs, double* __restrict__ own_w,
                                                        double* __restrict__ own_wl, double* __restrict__ out_w,
-                                                       double* __restrict__ out_wl) {
+                                                       double* __restrict__ out_wl,
+                                                       const double* __restrict__ dec = nullptr) {
     using M = MT<double>;
     constexpr int NQ = M::n_dof_q, DIM = M::dimension;
     const int C = m.C, F = m.F;
@@ -397,128 +398,149 @@ __global__ void __launch_bounds__(128, ZSME_ADJ_CELL_MINB) adj_cell_kernel(MeshD
         return;
     }
     // the forward gradient (prep_kernel, same operations)
+    // and its limiter, as the replay recorded them (prep_tape_kernel), or
+    // recomputed from the stage state
     double g[NQ * DIM];
+    double al[KM], dqs[KM];
+    int js[KM], ks[KM];
+    if (dec) {
 #pragma unroll
-    for (int i = 0; i < NQ * DIM; ++i) g[i] = 0.0;
-    if (o.gradient == 1) {
+        for (int i = 0; i < NQ * DIM; ++i) g[i] = dec[(size_t)i * C + c];
 #pragma unroll
         for (int k = 0; k < KM; ++k) {
-            if (nb[k] < 0) continue;
-            double wk[DIM];
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) wk[d] = m.slot_w[((size_t)k * 2 + d) * C + c];
-#pragma unroll
-            for (int i = 0; i < NQ; ++i) {
-                const double du = w[(size_t)i * C + nb[k]] - w[(size_t)i * C + c];
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) g[i * DIM + d] += wk[d] * du;
+            al[k] = 1.0;
+            dqs[k] = 1.0;
+            js[k] = -1;
+            ks[k] = -1;
+            if (k < K) {
+                al[k] = dec[((size_t)NQ * DIM + k) * C + c];
+                dqs[k] = dec[((size_t)NQ * DIM + K + k) * C + c];
+                const int jk = (int)dec[((size_t)NQ * DIM + 2 * K + k) * C + c];
+                js[k] = (jk & 255) - 1;
+                ks[k] = (jk >> 8) - 1;
             }
         }
     } else {
-        const int ord = m.order[c];
-        for (int j = 0; j < K; ++j) {
-            const int k = (ord >> (2 * j)) & 3;
-            const int f = m.slot_face[k * C + c];
-            if (f < 0) continue;
-            const int meta = m.slot_meta[k * C + c];
-            const int n = m.slot_nbr[k * C + c];
-            const double Nf[2] = {m.fnr[f], m.fnr[F + f]};
-            if (n >= 0) {
-                const bool isL = meta_isL(meta);
 #pragma unroll
-                for (int i = 0; i < NQ; ++i) {
-                    const double qc = w[(size_t)i * C + c], qn = w[(size_t)i * C + n];
-                    const double fv = 0.5 * (isL ? (qc + qn) : (qn + qc));
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) {
-                        const double vv = fv * Nf[d];
-                        if (isL) g[i * DIM + d] += vv;
-                        else g[i * DIM + d] -= vv;
-                    }
-                }
-            } else if (meta_bc(meta) >= 0) {
-                double qg[NQ];
-                load_q<NQ>(w, C, c, qg);
-                const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
-                const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
-                const auto qb = M::boundary_conditions(meta_bc(meta), qg, (const double*)nullptr, p, nh, xf, 0.0, 0.0);
-#pragma unroll
-                for (int i = 0; i < NQ; ++i)
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) g[i * DIM + d] += qb[i] * Nf[d];
-            }
-        }
-        const double vol = m.vol[c];
-        if (vol > 1e-15) {
-#pragma unroll
-            for (int i = 0; i < NQ * DIM; ++i) g[i] /= vol;
-        }
-    }
-    // the forward limiter, remembering which branch set each face's alpha
-    double al[KM], dqs[KM];
-    int js[KM], ks[KM];
-#pragma unroll
-    for (int k = 0; k < KM; ++k) { al[k] = 1.0; dqs[k] = 1.0; js[k] = -1; ks[k] = -1; }
-    if (o.limiter) {
-        bool vac = false;
-        if (NQ > 1) {
-            double mnh = wl[C + c];
+        for (int i = 0; i < NQ * DIM; ++i) g[i] = 0.0;
+        if (o.gradient == 1) {
 #pragma unroll
             for (int k = 0; k < KM; ++k) {
                 if (nb[k] < 0) continue;
-                const double vv = wl[(size_t)C + nb[k]];
-                if (vv < mnh) mnh = vv;
+                double wk[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) wk[d] = m.slot_w[((size_t)k * 2 + d) * C + c];
+#pragma unroll
+                for (int i = 0; i < NQ; ++i) {
+                    const double du = w[(size_t)i * C + nb[k]] - w[(size_t)i * C + c];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) g[i * DIM + d] += wk[d] * du;
+                }
             }
-            vac = mnh < 1e-2;
-        }
-        if (vac) {
-#pragma unroll
-            for (int k = 0; k < KM; ++k) al[k] = 0.0;
         } else {
+            const int ord = m.order[c];
+            for (int j = 0; j < K; ++j) {
+                const int k = (ord >> (2 * j)) & 3;
+                const int f = m.slot_face[k * C + c];
+                if (f < 0) continue;
+                const int meta = m.slot_meta[k * C + c];
+                const int n = m.slot_nbr[k * C + c];
+                const double Nf[2] = {m.fnr[f], m.fnr[F + f]};
+                if (n >= 0) {
+                    const bool isL = meta_isL(meta);
 #pragma unroll
-            for (int i = 0; i < NQ; ++i) {
-                const double q = wl[(size_t)i * C + c];
-                double mn = q, mx = q;
-                int kmn = -1, kmx = -1;
+                    for (int i = 0; i < NQ; ++i) {
+                        const double qc = w[(size_t)i * C + c], qn = w[(size_t)i * C + n];
+                        const double fv = 0.5 * (isL ? (qc + qn) : (qn + qc));
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) {
+                            const double vv = fv * Nf[d];
+                            if (isL) g[i * DIM + d] += vv;
+                            else g[i * DIM + d] -= vv;
+                        }
+                    }
+                } else if (meta_bc(meta) >= 0) {
+                    double qg[NQ];
+                    load_q<NQ>(w, C, c, qg);
+                    const double nh[3] = {m.fn[f], m.fn[F + f], 0.0};
+                    const double xf[3] = {m.fc[f], m.fc[F + f], 0.0};
+                    const auto qb = M::boundary_conditions(meta_bc(meta), qg, (const double*)nullptr, p, nh, xf, 0.0, 0.0);
+#pragma unroll
+                    for (int i = 0; i < NQ; ++i)
+#pragma unroll
+                        for (int d = 0; d < DIM; ++d) g[i * DIM + d] += qb[i] * Nf[d];
+                }
+            }
+            const double vol = m.vol[c];
+            if (vol > 1e-15) {
+#pragma unroll
+                for (int i = 0; i < NQ * DIM; ++i) g[i] /= vol;
+            }
+        }
+        // the forward limiter, remembering which branch set each face's alpha
+#pragma unroll
+        for (int k = 0; k < KM; ++k) { al[k] = 1.0; dqs[k] = 1.0; js[k] = -1; ks[k] = -1; }
+        if (o.limiter) {
+            bool vac = false;
+            if (NQ > 1) {
+                double mnh = wl[C + c];
 #pragma unroll
                 for (int k = 0; k < KM; ++k) {
                     if (nb[k] < 0) continue;
-                    const double vv = wl[(size_t)i * C + nb[k]];
-                    if (vv < mn) { mn = vv; kmn = k; }
-                    if (vv > mx) { mx = vv; kmx = k; }
+                    const double vv = wl[(size_t)C + nb[k]];
+                    if (vv < mnh) mnh = vv;
                 }
+                vac = mnh < 1e-2;
+            }
+            if (vac) {
 #pragma unroll
-                for (int k = 0; k < KM; ++k) {
-                    if (ff[k] < 0) continue;
-                    double d = 0.0;
+                for (int k = 0; k < KM; ++k) al[k] = 0.0;
+            } else {
 #pragma unroll
-                    for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
-                    const double qfu = q + d;
-                    const double dq = qfu - q;
-                    double a = 1.0;
-                    bool ratio = false;
-                    if (!(fabs(dq) < 1e-12)) {
-                        if (dq > 0) {
-                            const double rr = mx - q;
-                            if (mx > q) {
-                                if (!(rr >= dq)) { a = fmin(1.0, rr / dq); ratio = true; }
+                for (int i = 0; i < NQ; ++i) {
+                    const double q = wl[(size_t)i * C + c];
+                    double mn = q, mx = q;
+                    int kmn = -1, kmx = -1;
+#pragma unroll
+                    for (int k = 0; k < KM; ++k) {
+                        if (nb[k] < 0) continue;
+                        const double vv = wl[(size_t)i * C + nb[k]];
+                        if (vv < mn) { mn = vv; kmn = k; }
+                        if (vv > mx) { mx = vv; kmx = k; }
+                    }
+#pragma unroll
+                    for (int k = 0; k < KM; ++k) {
+                        if (ff[k] < 0) continue;
+                        double d = 0.0;
+#pragma unroll
+                        for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+                        const double qfu = q + d;
+                        const double dq = qfu - q;
+                        double a = 1.0;
+                        bool ratio = false;
+                        if (!(fabs(dq) < 1e-12)) {
+                            if (dq > 0) {
+                                const double rr = mx - q;
+                                if (mx > q) {
+                                    if (!(rr >= dq)) { a = fmin(1.0, rr / dq); ratio = true; }
+                                } else {
+                                    a = 0.0;
+                                }
                             } else {
-                                a = 0.0;
-                            }
-                        } else {
-                            const double rr = mn - q;
-                            if (mn < q) {
-                                if (!(rr <= dq)) { a = fmin(1.0, rr / dq); ratio = true; }
-                            } else {
-                                a = 0.0;
+                                const double rr = mn - q;
+                                if (mn < q) {
+                                    if (!(rr <= dq)) { a = fmin(1.0, rr / dq); ratio = true; }
+                                } else {
+                                    a = 0.0;
+                                }
                             }
                         }
-                    }
-                    if (a < al[k]) {
-                        al[k] = a;
-                        js[k] = ratio ? i : -1;
-                        ks[k] = dq > 0 ? kmx : kmn;
-                        dqs[k] = dq;
+                        if (a < al[k]) {
+                            al[k] = a;
+                            js[k] = ratio ? i : -1;
+                            ks[k] = dq > 0 ? kmx : kmn;
+                            dqs[k] = dq;
+                        }
                     }
                 }
             }

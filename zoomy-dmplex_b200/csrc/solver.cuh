@@ -76,6 +76,10 @@ class Solver final : public SolverBase {
     // state
     DevBuf<double> x_, w_, wl_, aux_, fs_, fb_, tmp_a_, tmp_b_, params_, dts_;
     double* fs_cur_ = nullptr;  // face states the prep and face kernels use: fs_, or a tape slot in a replay
+    double* dec_cur_ = nullptr; // in a replay at order 2: the tape slot for the stage's reconstruction record
+    // rows of one stage's reconstruction record (prep_tape_kernel): the gradient,
+    // then alpha, dq and branch per face slot
+    size_t dec_rows() const { return (size_t)NQ * DIM + 3 * (size_t)pm_.K; }
     DevBuf<double> xs_;  // MOOD: the state at the start of the step
     DevBuf<int> mood_list_;  // MOOD: the troubled cells of the step (count in iscal_[6])
     DevBuf<double> imex_g_[3], imex_s_[3], imex_y_[2];   // IMEX: stage right-hand sides, implicit derivatives, states
@@ -611,6 +615,18 @@ class Solver final : public SolverBase {
     void launch_prep(const double* w, const double* wl, const int* active) {
         mark(ZSME_KERNEL_PREP, true);
         const int gb = blocks_for(pm_.C, lc_.prep);
+        if (dec_cur_ && st_.positivity == ZSME_POSITIVITY_NONE) {   // adjoint replay: record the reconstruction
+            if (pm_.K == 3)
+                prep_tape_kernel<M, 3><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl,
+                                                                                   params_.p, fs_cur_, dec_cur_,
+                                                                                   active);
+            else
+                prep_tape_kernel<M, 4><<<blocks_for(pm_.C, 128), 128, 0, stream_>>>(md_, opts_, 0, pm_.C, w, wl,
+                                                                                   params_.p, fs_cur_, dec_cur_,
+                                                                                   active);
+            mark(ZSME_KERNEL_PREP, false);
+            return;
+        }
         if (st_.positivity != ZSME_POSITIVITY_NONE && st_.reconstruction_order >= 2) {
             switch (lc_.prep_occ) {
 #define ZSME_PREPWB(OCC)                                                                                        \
@@ -840,6 +856,9 @@ class Solver final : public SolverBase {
         // stage result X', then one slot of face states per stage
         auto stage_fs = [&](int i) {
             fs_cur_ = tape ? tape + (size_t)(ns + 1) * tape_n + (size_t)i * fs_n : fs_.p;
+            dec_cur_ = tape && st_.reconstruction_order >= 2
+                           ? tape + (size_t)(ns + 1) * tape_n + (size_t)ns * fs_n + (size_t)i * dec_rows() * pm_.C
+                           : nullptr;
         };
         StepDev sd = step_dev(dts);
         const double* t = sd.t;
@@ -888,6 +907,7 @@ class Solver final : public SolverBase {
                                 stream_);
         }
         fs_cur_ = fs_.p;
+        dec_cur_ = nullptr;
         if (mood) {   // a-posteriori first-order override of troubled cells
             cudaMemsetAsync(iscal_.p + 6, 0, sizeof(int), stream_);
             mark(ZSME_KERNEL_MOOD, true);
@@ -1375,7 +1395,7 @@ class Solver final : public SolverBase {
     // start state (its own clamped copy, as in the forward stage).
     void adj_apply_rt(const double* W, const double* fs, bool W0, const double* tp, double frac, const double* dtp,
                       double factor, const double* src, double c_src, double* dst,
-                      const AdjEpilogue& ep = AdjEpilogue{}) {
+                      const AdjEpilogue& ep = AdjEpilogue{}, const double* dec = nullptr) {
         const int C = pm_.C, F = pm_.F;
         const double* wl = W;
         if (!W0) {
@@ -1391,10 +1411,12 @@ class Solver final : public SolverBase {
         }
         if (pm_.K == 3)
             adj_cell_kernel<MT, 3><<<blocks_for(C, 128), 128, 0, stream_>>>(
-                md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);
+                md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p,
+                dec);
         else
             adj_cell_kernel<MT, 4><<<blocks_for(C, 128), 128, 0, stream_>>>(
-                md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p);
+                md_, opts_, W, wl, params_.p, adj_gfs_.p, adj_own_w_.p, adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p,
+                dec);
         adj_combine_kernel<MT><<<blocks_for(C, 128), 128, 0, stream_>>>(md_, W, adj_aux_cur_, params_.p, adj_own_w_.p,
                                                                         adj_own_wl_.p, adj_out_w_.p, adj_out_wl_.p,
                                                                         src, c_src, dst, ep);
@@ -1430,9 +1452,12 @@ class Solver final : public SolverBase {
             adj_apply_rt(tape, fst, true, tp, 0.0, dtp, 1.0, t1, 1.0, lam, seeds);
             return;
         }
+        // each stage's reconstruction record, after the face states
+        const size_t dec_n = dec_rows() * C;
+        const double* dect = fst + (size_t)s * fs_n;
         // X' = (s-1)/s W_{s-1} + dt/s R(W_{s-1}) + 1/s W_0
         adj_apply_rt(tape + (size_t)(s - 1) * nv, fst + (size_t)(s - 1) * fs_n, s - 1 == 0, tp, 1.0, dtp, 1.0 / s, t1,
-                     (s - 1.) / s, t2);
+                     (s - 1.) / s, t2, AdjEpilogue{}, dect + (size_t)(s - 1) * dec_n);
         double* cur = t2;
         double* oth = lam;
         for (int i = s - 2; i >= 0; --i) {  // W_{i+1} = W_i + dt/(s-1) R(W_i)
@@ -1443,7 +1468,7 @@ class Solver final : public SolverBase {
                 ep.ax_a = 1.0 / s;
             }
             adj_apply_rt(tape + (size_t)i * nv, fst + (size_t)i * fs_n, i == 0, tp, i / (s - 1.), dtp,
-                         1.0 / (s - 1.), cur, 1.0, oth, ep);
+                         1.0 / (s - 1.), cur, 1.0, oth, ep, dect + (size_t)i * dec_n);
             std::swap(cur, oth);
         }
         if (cur != lam) {   // odd s: the last combine wrote t2
@@ -1520,7 +1545,10 @@ class Solver final : public SolverBase {
         ZSME_CUDA(adj_oseed_.alloc(std::max(1, A.nobs)));
         ZSME_CUDA(adj_ck_x_.alloc((size_t)(nseg + 1) * nv));
         ZSME_CUDA(adj_ck_a_.alloc((size_t)(nseg + 1) * na));
-        adj_tstride_ = (size_t)(s + 1) * nv + (size_t)s * 2 * NQ * F;  // one step's tape
+        // one step's tape: the stage states and the stage output, each stage's
+        // face states, and at order 2 each stage's reconstruction record
+        adj_tstride_ = (size_t)(s + 1) * nv + (size_t)s * 2 * NQ * F +
+                       (st_.reconstruction_order >= 2 ? (size_t)s * dec_rows() * C : 0);
         const int tape_steps = std::min(E, std::max(NS, 1));
         // the replay of segment g-1 runs on a side stream while the reverse sweep
         // of segment g runs on the handle's stream: two tape buffers, CUDA graphs

@@ -345,6 +345,125 @@ __global__ void __launch_bounds__(128, MINB) prep_kernel(MeshDev m, Opts o, int 
     }
 }
 
+// ------------------------------------------------- prep, recording its decisions
+// prep_kernel's order-2 face states (positivity "none"), bit for bit, for the
+// adjoint's replay: besides the face states it records what the reverse
+// sweep needs of the reconstruction, so that adj_cell_kernel need not
+// recompute it.  dec [NQ DIM + 3 K][C]: the gradient rows, then per face slot
+// k the limiter's alpha, the dq of the branch that set it, and the branch
+// (js + 1) + 256 (ks + 1) (js: the component whose ratio set alpha, -1 for a
+// 0 / 1 branch; ks: the neighbour slot of that bound, -1 if none), all as
+// doubles.  The limiter runs as adj_cell_kernel's replay of it does (the same
+// branches, tie rules and first-minimum choice), with the values of
+// prep_kernel's selects.
+template <class M, int KM>
+__global__ void __launch_bounds__(128) prep_tape_kernel(MeshDev m, Opts o, int c0, int cn, const double* __restrict__ w,
+                                                        const double* __restrict__ wl,
+                                                        const double* __restrict__ params, double* __restrict__ fs,
+                                                        double* __restrict__ dec, const int* __restrict__ active) {
+    constexpr int NQ = M::n_dof_q, DIM = M::dimension;
+    const int C = m.C, F = m.F;
+    const int K = KM == 3 ? 3 : m.K;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= cn) return;
+    const int c = c0 + r;
+    const int I = cell_instance(m, c);
+    if (active && !active[I]) return;
+    const double* p = params + (size_t)I * m.np;
+    int nb[KM], ff[KM], sd[KM];
+    double dx[KM][DIM], g[NQ * DIM];
+    cell_slots_gradient<M, KM>(m, o, c, K, w, p, nb, ff, sd, dx, g);
+    double al[KM], dqs[KM];
+    int js[KM], ks[KM];
+#pragma unroll
+    for (int k = 0; k < KM; ++k) { al[k] = 1.0; dqs[k] = 1.0; js[k] = -1; ks[k] = -1; }
+    if (o.limiter) {
+        bool vac = false;
+        if (NQ > 1) {
+            double mnh = wl[C + c];
+#pragma unroll
+            for (int k = 0; k < KM; ++k) {
+                if (nb[k] < 0) continue;
+                const double v = wl[(size_t)C + nb[k]];
+                if (v < mnh) mnh = v;
+            }
+            vac = mnh < 1e-2;
+        }
+        if (vac) {
+#pragma unroll
+            for (int k = 0; k < KM; ++k) al[k] = 0.0;
+        } else {
+#pragma unroll
+            for (int i = 0; i < NQ; ++i) {
+                const double q = wl[(size_t)i * C + c];
+                double mn = q, mx = q;
+                int kmn = -1, kmx = -1;
+#pragma unroll
+                for (int k = 0; k < KM; ++k) {
+                    if (nb[k] < 0) continue;
+                    const double v = wl[(size_t)i * C + nb[k]];
+                    if (v < mn) { mn = v; kmn = k; }
+                    if (v > mx) { mx = v; kmx = k; }
+                }
+#pragma unroll
+                for (int k = 0; k < KM; ++k) {
+                    if (ff[k] < 0) continue;
+                    double d = 0.0;
+#pragma unroll
+                    for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+                    const double qfu = q + d;
+                    const double dq = qfu - q;
+                    double a = 1.0;
+                    bool ratio = false;
+                    if (!(fabs(dq) < 1e-12)) {
+                        if (dq > 0) {
+                            const double rr = mx - q;
+                            if (mx > q) {
+                                if (!(rr >= dq)) { a = fmin(1.0, rr / dq); ratio = true; }
+                            } else {
+                                a = 0.0;
+                            }
+                        } else {
+                            const double rr = mn - q;
+                            if (mn < q) {
+                                if (!(rr <= dq)) { a = fmin(1.0, rr / dq); ratio = true; }
+                            } else {
+                                a = 0.0;
+                            }
+                        }
+                    }
+                    if (a < al[k]) {
+                        al[k] = a;
+                        js[k] = ratio ? i : -1;
+                        ks[k] = dq > 0 ? kmx : kmn;
+                        dqs[k] = dq;
+                    }
+                }
+            }
+        }
+    }
+    // face states q + alpha * delta
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) {
+        const double q = wl[(size_t)i * C + c];
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+            if (ff[k] < 0) continue;
+            double d = 0.0;
+#pragma unroll
+            for (int e = 0; e < DIM; ++e) d += g[i * DIM + e] * dx[k][e];
+            fs[((size_t)sd[k] * NQ + i) * F + ff[k]] = q + al[k] * d;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NQ * DIM; ++i) dec[(size_t)i * C + c] = g[i];
+    for (int k = 0; k < K; ++k) {
+        dec[((size_t)NQ * DIM + k) * C + c] = al[k];
+        dec[((size_t)NQ * DIM + K + k) * C + c] = dqs[k];
+        dec[((size_t)NQ * DIM + 2 * K + k) * C + c] = (double)((js[k] + 1) + 256 * (ks[k] + 1));
+    }
+}
+
 // ---------------------------------------------------------- prep, lean form
 // prep_kernel's order-2 face states (positivity "none") with less integer and
 // branch work, bit for bit the same:
