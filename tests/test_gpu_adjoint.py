@@ -12,6 +12,8 @@
 The case is the level-1 adjoint case (Manning friction, order 2, Green-Gauss,
 Vacuum + TVD limiting) on small meshes; checkpoint intervals that do not
 divide the step count exercise partial segments."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -256,3 +258,31 @@ def test_dual_number_face_path_on_reference_style_header():
         assert abs(L - loss) <= 1e-12 * abs(L)
         ad = float(np.sum(gq * dq))
         assert abs(ad - dL) <= 1e-8 * max(abs(dL), 1e-30), (ad, dL)
+
+
+@pytest.mark.parametrize("kw", [{"reconstruction_order": 1}, {"ssp_stages": 3}, {"limiter": "none"}])
+@pytest.mark.parametrize("every", [4, 5])
+def test_adjoint_other_schemes(kw, every):
+    """First order (one stage, no reconstruction record), three SSP stages (the
+    reverse step's odd-stage path), no limiter; segments full (every 4: the
+    overlapped replays) and partial (every 5): the directional derivatives
+    agree with the tangent-linear oracle."""
+    c, p, names, obs = _setup(16, 12, 3, 20)
+    c.settings = dataclasses.replace(c.settings, **kw)
+    g = Solver(c.model, c.mesh, c.settings, p)
+    g.set_state(c.q0)
+    loss, gq, gp, dts = g.adjoint(12, *obs, checkpoint_every=every)
+    assert g.adjoint_overlapped() == (every == 4)
+    rng = np.random.default_rng(11)
+    ni = names.index("n_manning")
+    for what in ("b", "manning"):
+        dq = np.zeros_like(c.q0)
+        dp = np.zeros_like(p)
+        if what == "b":
+            dq[:, 0] = rng.standard_normal(c.mesh.n_cells)
+        else:
+            dp[ni] = 1.0
+        L, dL = _oracle_tlm(c, p, dts, obs, dq, dp)
+        assert abs(L - loss) <= 1e-12 * abs(L), (kw, L, loss)
+        ad = float(np.sum(gq * dq) + np.sum(gp * dp))
+        assert abs(ad - dL) <= 1e-8 * max(abs(dL), 1e-30), (kw, what, ad, dL)
