@@ -127,13 +127,14 @@ def step_bytes_fused(nq):
 # profiles/sme2d_l4_kernels_900.md (900x900 grid, 1,616,402 cells; mean of
 # two launches) in the launch configuration the autotuner picks at level 4:
 # separate face and gather kernels, the face-state kernel split over four
-# threads per cell, the last stage's gather inside finalize.  The streams scale with the cell count, so
-# a 1400x1400 launch moves these figures times its cells.
+# threads per cell, the last stage's gather inside finalize (register cap 4).
+# The streams scale with the cell count, so a 1400x1400 launch moves these
+# figures times its cells.
 NCU_DRAM_BYTES_PER_CELL = {
     "sme2d_l4/prep": (436.6 + 425.4) * 1e6 / 1616402,
     "sme2d_l4/flux": (544.7 + 652.4) * 1e6 / 1616402,
     "sme2d_l4/gather": (1143.8 + 282.5) * 1e6 / 1616402,
-    "sme2d_l4/finalize+gather": (1123.1 + 297.0) * 1e6 / 1616402,
+    "sme2d_l4/finalize+gather": (1125.9 + 422.2) * 1e6 / 1616402,
 }
 NCU_LAUNCH = {"tile_faces": 0, "fuse_final": 1, "prep_lean": 4}
 

@@ -22,6 +22,8 @@ CONFIGS = [
      "tile_faces": 128},
     {"prep": 128, "face": 128, "gather": 128, "finalize": 64, "prep_occ": 2, "face_occ": 3, "finalize_occ": 1,
      "tile_faces": 512},
+    {"prep": 128, "face": 128, "gather": 128, "finalize": 64, "prep_occ": 8, "face_occ": 3, "finalize_occ": 4,
+     "tile_faces": 0, "fuse_final": 1, "prep_lean": 4},
 ]
 
 

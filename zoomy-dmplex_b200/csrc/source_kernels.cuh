@@ -23,57 +23,9 @@
 // registers.  When any condition fails the generic full-size GEPP runs.
 #pragma once
 
-namespace zsme {
+#include "gepp_regs.h"
 
-// GEPP of SolveLinearSystem on an NB x NB block held in registers (all
-// indices compile-time; row swaps are predicated moves).  Returns false on a
-// pivot below 1e-14.
-template <int NB>
-__device__ __forceinline__ bool gepp_regs(double (&A)[NB][NB], double (&b)[NB], double (&x)[NB]) {
-    bool ok = true;
-#pragma unroll
-    for (int k = 0; k < NB; ++k) {
-        int mr = k;
-        double mv = fabs(A[k][k]);
-#pragma unroll
-        for (int i = k + 1; i < NB; ++i) {
-            const double v = fabs(A[i][k]);
-            if (v > mv) { mv = v; mr = i; }
-        }
-        if (mv < 1e-14) ok = false;
-#pragma unroll
-        for (int i = k + 1; i < NB; ++i) {
-            if (mr == i) {
-#pragma unroll
-                for (int j = k; j < NB; ++j) {
-                    const double tt = A[k][j];
-                    A[k][j] = A[i][j];
-                    A[i][j] = tt;
-                }
-                const double tt = b[k];
-                b[k] = b[i];
-                b[i] = tt;
-            }
-        }
-        const double pkk = A[k][k];
-        const double bk = b[k];
-#pragma unroll
-        for (int i = k + 1; i < NB; ++i) {
-            const double fct = A[i][k] / pkk;
-#pragma unroll
-            for (int j = k; j < NB; ++j) A[i][j] -= fct * A[k][j];
-            b[i] -= fct * bk;
-        }
-    }
-#pragma unroll
-    for (int i = NB - 1; i >= 0; --i) {
-        double sum = 0.0;
-#pragma unroll
-        for (int j = i + 1; j < NB; ++j) sum += A[i][j] * x[j];
-        x[i] = (b[i] - sum) / A[i][i];
-    }
-    return ok;
-}
+namespace zsme {
 
 template <class M>
 struct SmeLayout {
@@ -82,33 +34,6 @@ struct SmeLayout {
     static constexpr int NM = ok ? (NQ - 2) / DIM : 1;   // moments per direction
     static constexpr int NB = NQ - 2;                      // momentum block
 };
-
-// Generic GEPP over the full matrix (local memory).
-template <int NQ>
-__device__ bool gepp_full(double* J, double* bv, double* xv) {
-    for (int k = 0; k < NQ; ++k) {
-        int mr = k;
-        double mv = fabs(J[k * NQ + k]);
-        for (int i = k + 1; i < NQ; ++i)
-            if (fabs(J[i * NQ + k]) > mv) { mv = fabs(J[i * NQ + k]); mr = i; }
-        if (mv < 1e-14) return false;
-        if (mr != k) {
-            for (int j = k; j < NQ; ++j) { const double tt = J[k * NQ + j]; J[k * NQ + j] = J[mr * NQ + j]; J[mr * NQ + j] = tt; }
-            const double tt = bv[k]; bv[k] = bv[mr]; bv[mr] = tt;
-        }
-        for (int i = k + 1; i < NQ; ++i) {
-            const double fct = J[i * NQ + k] / J[k * NQ + k];
-            for (int j = k; j < NQ; ++j) J[i * NQ + j] -= fct * J[k * NQ + j];
-            bv[i] -= fct * bv[k];
-        }
-    }
-    for (int i = NQ - 1; i >= 0; --i) {
-        double sum = 0.0;
-        for (int j = i + 1; j < NQ; ++j) sum += J[i * NQ + j] * xv[j];
-        xv[i] = (bv[i] - sum) / J[i * NQ + i];
-    }
-    return true;
-}
 
 // One Newton update on the fast path; returns 1 if q was updated, 0 to fall
 // back to the generic path (structure not met, or a singular / non-finite
@@ -334,6 +259,59 @@ __device__ __forceinline__ int finalize_cell(const MeshDev& m, int c, int I, dou
     return 0;
 }
 
+// Appends the cells with defer set to sd.fallback (warp-aggregated, so runs
+// of consecutive cells stay together).  All lanes of the warp call it.
+__device__ __forceinline__ void defer_append(const StepDev& sd, bool defer, int c) {
+    const unsigned dm = __ballot_sync(0xffffffffu, defer);
+    if (dm) {
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == 0) base = atomicAdd(sd.n_fallback, __popc(dm));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (defer) sd.fallback[base + __popc(dm & ((1u << lane) - 1u))] = c;
+    }
+}
+
+// The block's CFL ratios into the per-instance minimum sd.ratio (I < 0: no
+// ratio).  Ratios are positive, so their bit patterns order like the values
+// and an integer atomicMin is exact (and order-free).  Warps whose lanes
+// share one instance reduce first; the block then issues one atomic per run
+// of warps with the same instance.  All threads of the block call it.
+__device__ __forceinline__ void block_ratio_min(const StepDev& sd, int I, double ratio) {
+    unsigned long long v = (unsigned long long)__double_as_longlong(ratio);
+    const int I0 = __shfl_sync(0xffffffffu, I, 0);
+    const bool uniform = __all_sync(0xffffffffu, I == I0);
+    __shared__ unsigned long long wv[32];
+    __shared__ int wi[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (uniform) {
+        for (int off = 16; off > 0; off >>= 1) {
+            const unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
+            if (o < v) v = o;
+        }
+        if (lane == 0) { wv[w] = v; wi[w] = I0; }
+    } else {
+        if (I >= 0 && v < ZSME_RATIO_NONE) atomicMin(&sd.ratio[I], v);
+        if (lane == 0) wi[w] = -1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x >> 5;
+        int cur = -1;
+        unsigned long long best = ZSME_RATIO_NONE;
+        for (int k = 0; k < nw; ++k) {
+            if (wi[k] < 0) continue;
+            if (wi[k] != cur) {
+                if (cur >= 0 && best < ZSME_RATIO_NONE) atomicMin(&sd.ratio[cur], best);
+                cur = wi[k];
+                best = ZSME_RATIO_NONE;
+            }
+            if (wv[k] < best) best = wv[k];
+        }
+        if (cur >= 0 && best < ZSME_RATIO_NONE) atomicMin(&sd.ratio[cur], best);
+    }
+}
+
 // cells [c0, c0 + cn); dt_src: per-instance dt of the source step.
 // The Newton iteration runs with the register fast path only; a cell whose
 // update needs the generic GEPP is left untouched and appended to
@@ -367,53 +345,8 @@ __global__ void __launch_bounds__(128, MINB) finalize_kernel(MeshDev m, int c0, 
             for (int i = 0; i < NQ; ++i) x[(size_t)i * m.C + c] = q[i];
         }
     }
-    if (flags & FIN_SOURCE) {
-        const unsigned dm = __ballot_sync(0xffffffffu, defer);
-        if (dm) {
-            const int lane = threadIdx.x & 31;
-            int base = 0;
-            if (lane == 0) base = atomicAdd(sd.n_fallback, __popc(dm));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (defer) sd.fallback[base + __popc(dm & ((1u << lane) - 1u))] = c;
-        }
-    }
-    if (!(flags & FIN_DT)) return;
-    // Minimum per instance.  Ratios are positive, so their bit patterns order
-    // like the values and an integer atomicMin is exact (and order-free).
-    // Warps whose lanes share one instance reduce first; the block then issues
-    // one atomic per run of warps with the same instance.
-    unsigned long long v = (unsigned long long)__double_as_longlong(ratio);
-    const int I0 = __shfl_sync(0xffffffffu, I, 0);
-    const bool uniform = __all_sync(0xffffffffu, I == I0);
-    __shared__ unsigned long long wv[32];
-    __shared__ int wi[32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (uniform) {
-        for (int off = 16; off > 0; off >>= 1) {
-            const unsigned long long o = __shfl_down_sync(0xffffffffu, v, off);
-            if (o < v) v = o;
-        }
-        if (lane == 0) { wv[w] = v; wi[w] = I0; }
-    } else {
-        if (I >= 0 && v < ZSME_RATIO_NONE) atomicMin(&sd.ratio[I], v);
-        if (lane == 0) wi[w] = -1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int nw = blockDim.x >> 5;
-        int cur = -1;
-        unsigned long long best = ZSME_RATIO_NONE;
-        for (int k = 0; k < nw; ++k) {
-            if (wi[k] < 0) continue;
-            if (wi[k] != cur) {
-                if (cur >= 0 && best < ZSME_RATIO_NONE) atomicMin(&sd.ratio[cur], best);
-                cur = wi[k];
-                best = ZSME_RATIO_NONE;
-            }
-            if (wv[k] < best) best = wv[k];
-        }
-        if (cur >= 0 && best < ZSME_RATIO_NONE) atomicMin(&sd.ratio[cur], best);
-    }
+    if (flags & FIN_SOURCE) defer_append(sd, defer, c);
+    if (flags & FIN_DT) block_ratio_min(sd, I, ratio);
 }
 
 // The deferred cells of finalize_kernel, with the generic Newton path
