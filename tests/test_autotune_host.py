@@ -106,3 +106,15 @@ def test_knobs_cover_the_launch_keys():
     assert set(dict(autotune.KNOBS)) == set(LAUNCH_KEYS)
     for k, vals in autotune.KNOBS:
         assert LAUNCH_DEFAULTS[k] in vals
+
+
+def test_unreadable_cache_is_retuned_and_rewritten(fake_launch, tmp_path):
+    cache = tmp_path / "tuned.json"
+    for junk in ("{not json", "[1, 2]"):
+        cache.write_text(junk)
+        assert autotune.load_cache(str(cache)) == {}
+        s = FakeSolver(cost)
+        fake_launch.solver = s
+        cfg = autotune.tune(s, "sme2d_l2", 114242, steps=1, cache=str(cache))
+        assert s.steps > 0
+        assert json.load(open(cache))[autotune.cache_key("sme2d_l2", 114242)]["config"] == cfg

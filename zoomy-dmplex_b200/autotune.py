@@ -52,10 +52,14 @@ def cache_key(model, n_cells):
 
 
 def load_cache(path=DEFAULT_CACHE):
-    if os.path.exists(path):
+    """The cached tunings ({} when the file is missing, unreadable or not a
+    JSON object: the tuner then measures afresh and rewrites it)."""
+    try:
         with open(path) as f:
-            return json.load(f)
-    return {}
+            db = json.load(f)
+    except (OSError, ValueError):
+        return {}
+    return db if isinstance(db, dict) else {}
 
 
 def _measure(solver, cfg, steps):
