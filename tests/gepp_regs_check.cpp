@@ -72,7 +72,30 @@ int check(int systems, long& swaps, long& singular) {
 
 }  // namespace
 
+// blend moves bits: NaN payloads, signed zeros and infinities come through
+int check_blend() {
+    const uint64_t pats[] = {0x7ff8000000000123ull, 0xfff0000000000001ull, 0x8000000000000000ull, 0ull,
+                             0x7ff0000000000000ull, 0xfff0000000000000ull, 0x0000000000000001ull,
+                             0x3ff0000000000000ull};
+    for (uint64_t a : pats)
+        for (uint64_t b : pats) {
+            double da, db;
+            std::memcpy(&da, &a, 8);
+            std::memcpy(&db, &b, 8);
+            const double r1 = zsme::blend(true, da, db), r0 = zsme::blend(false, da, db);
+            uint64_t u1, u0;
+            std::memcpy(&u1, &r1, 8);
+            std::memcpy(&u0, &r0, 8);
+            if (u1 != a || u0 != b) {
+                std::printf("blend %016llx %016llx\n", (unsigned long long)a, (unsigned long long)b);
+                return 1;
+            }
+        }
+    return 0;
+}
+
 int main() {
+    if (check_blend()) return 1;
     long swaps = 0, singular = 0;
     const int n = 20000;
     if (check<2>(n, swaps, singular) || check<3>(n, swaps, singular) || check<4>(n, swaps, singular) ||
